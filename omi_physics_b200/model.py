@@ -1,0 +1,163 @@
+"""OMI physics data model — the input schema of the step.
+
+Field names and defaults are those of the OMI glTF physics extensions, as the
+reference defines them in ``src/omi_physics/model.py:33-243``; keeping them
+identical is what lets a scene written against the reference load here
+unchanged. Only the parts the CUDA step consumes are listed (shapes, motion,
+collider, material, collision filter, global gravity) plus the joint/trigger
+records so documents round-trip; triggers, gravity volumes, capsules,
+cylinders and triangle meshes are rejected by the backend
+(:class:`omi_physics_b200.backend.UnsupportedFeature`).
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+STATIC = 'static'
+KINEMATIC = 'kinematic'
+DYNAMIC = 'dynamic'
+
+AVERAGE = 'average'
+MINIMUM = 'minimum'
+MAXIMUM = 'maximum'
+MULTIPLY = 'multiply'
+
+#: combine-mode codes the device tables use
+COMBINE_CODES = {AVERAGE: 0, MINIMUM: 1, MAXIMUM: 2, MULTIPLY: 3}
+
+
+@dataclass
+class Shape:
+    """``OMI_physics_shape``: one collision proxy, shared by index (model.py:33-82)."""
+    type: str = 'box'
+    size: tuple = (1.0, 1.0, 1.0)
+    radius: float = 0.5
+    height: float = 2.0
+    radiusBottom: float = 0.5
+    radiusTop: float = 0.5
+    points: Optional[np.ndarray] = None
+    indices: Optional[np.ndarray] = None
+    mesh: int = -1
+
+    @classmethod
+    def box(cls, size: Sequence[float] = (1.0, 1.0, 1.0)) -> 'Shape':
+        """Box with full extents ``size``."""
+        return cls(type='box', size=tuple(size))
+
+    @classmethod
+    def sphere(cls, radius: float = 0.5) -> 'Shape':
+        """Sphere of ``radius``."""
+        return cls(type='sphere', radius=float(radius))
+
+    @classmethod
+    def convex(cls, points) -> 'Shape':
+        """Convex hull of an ``(M, 3)`` local point cloud (its own hull)."""
+        return cls(type='convex', points=np.asarray(points, dtype='d'))
+
+    @classmethod
+    def capsule(cls, height: float = 1.0, radius: float = 0.5) -> 'Shape':
+        """Capsule (accepted by the schema, rejected by the CUDA backend)."""
+        return cls(type='capsule', height=float(height), radiusBottom=float(radius),
+                   radiusTop=float(radius))
+
+
+@dataclass
+class Motion:
+    """``OMI_physics_body.motion`` (model.py:86-102)."""
+    type: str = DYNAMIC
+    mass: float = 1.0
+    centerOfMass: tuple = (0.0, 0.0, 0.0)
+    inertiaDiagonal: tuple = (0.0, 0.0, 0.0)
+    inertiaOrientation: tuple = (0.0, 0.0, 0.0, 1.0)
+    linearVelocity: tuple = (0.0, 0.0, 0.0)
+    angularVelocity: tuple = (0.0, 0.0, 0.0)
+    gravityFactor: float = 1.0
+    linearDamping: float = 0.0
+    angularDamping: float = 0.0
+    quadraticDrag: float = 0.0
+
+
+@dataclass
+class Collider:
+    """``OMI_physics_body.collider`` (model.py:106-110)."""
+    shape: int = -1
+    physicsMaterial: int = -1
+    collisionFilter: int = -1
+
+
+@dataclass
+class Trigger:
+    """``OMI_physics_body.trigger`` (model.py:113-117); rejected by the backend."""
+    shape: int = -1
+    collisionFilter: int = -1
+
+
+@dataclass
+class Material:
+    """A physics material (model.py:121-127)."""
+    staticFriction: float = 0.6
+    dynamicFriction: float = 0.6
+    restitution: float = 0.0
+    frictionCombine: str = AVERAGE
+    restitutionCombine: str = AVERAGE
+
+
+@dataclass
+class CollisionFilter:
+    """Layer/mask filter (model.py:131-155); symmetric ``collides_with``."""
+    collisionSystems: tuple = ()
+    collideWithSystems: Optional[tuple] = None
+    notCollideWithSystems: tuple = ()
+
+    def collides_with(self, other: 'CollisionFilter') -> bool:
+        """Both filters must admit each other."""
+        return _admits(self, other) and _admits(other, self)
+
+
+def _admits(a, b) -> bool:
+    """``a``'s policy admits a body in ``b``'s systems."""
+    theirs = set(b.collisionSystems)
+    if theirs & set(a.notCollideWithSystems):
+        return False
+    if a.collideWithSystems is None:
+        return True
+    return bool(theirs & set(a.collideWithSystems))
+
+
+DIRECTIONAL = 'directional'
+POINT = 'point'
+
+
+@dataclass
+class Gravity:
+    """Global uniform gravity (model.py:163-178)."""
+    type: str = DIRECTIONAL
+    gravity: float = 9.81
+    direction: tuple = (0.0, -1.0, 0.0)
+    priority: int = 0
+    replace: bool = False
+    stop: bool = False
+    center: tuple = (0.0, 0.0, 0.0)
+
+
+@dataclass
+class Joint:
+    """A ``physicsJoints[]`` entry (model.py:205-209); kept for documents only."""
+    limits: List = field(default_factory=list)
+    drives: List = field(default_factory=list)
+
+
+DEFAULT_MATERIAL = Material()
+DEFAULT_FILTER = CollisionFilter()
+
+
+def combine(a: float, b: float, mode: str) -> float:
+    """Combine two material coefficients (model.py:231-243)."""
+    if mode == MINIMUM:
+        return min(a, b)
+    if mode == MAXIMUM:
+        return max(a, b)
+    if mode == MULTIPLY:
+        return a * b
+    return 0.5 * (a + b)

@@ -1,0 +1,243 @@
+"""Seeded synthetic scenes for the five benchmark workloads.
+
+Every builder takes an ``api`` namespace that provides ``PhysicsWorld``,
+``model`` and ``joints`` with the reference's signatures, so the same call
+builds an identical scene in this package or in the reference package (the
+golden-fixture generator uses the latter). Draw order from
+``np.random.default_rng(seed)`` is fixed per builder; a scene is fully
+determined by its arguments.
+
+Workloads (sizes and distributions as the benchmark describes them):
+  * ``pyramid``      10-level pyramid of 55 unit boxes on a 20x1x20 ground box
+  * ``debris``       N bodies, 70% boxes / 30% spheres, density 1000, 40x30x40 m
+  * ``convex_pile``  50/25/25 box/sphere/convex in a walled 100x100 m arena
+  * ``serving_mix``  request stream of debris worlds, N log-uniform in [16, 2048]
+  * ``joint_chain``  pinned chain of 0.2x0.2x1 m links plus loose boxes
+"""
+import math
+from types import SimpleNamespace
+from typing import List, Tuple
+
+import numpy as np
+
+
+def default_api():
+    """This package as a scene-building namespace."""
+    from . import joints, model
+    from .world import PhysicsWorld
+    return SimpleNamespace(PhysicsWorld=PhysicsWorld, model=model, joints=joints)
+
+
+def _quat_axis_angle(axis: np.ndarray, angle: float) -> Tuple[float, float, float, float]:
+    a = axis / np.linalg.norm(axis)
+    s = math.sin(0.5 * angle)
+    return (float(a[0] * s), float(a[1] * s), float(a[2] * s), float(math.cos(0.5 * angle)))
+
+
+def _set_iterations(world, iters: int) -> None:
+    """Solver iteration count, set where the reference keeps it (world.py:645-654)."""
+    world._collision.solver.velocity_iterations = iters
+
+
+def _new_world(api, backend=None, **kw):
+    if backend is not None:
+        kw['backend'] = backend
+    return api.PhysicsWorld(**kw)
+
+
+def pyramid(api=None, backend=None, levels: int = 10):
+    """Box pyramid: row l has ``levels - l`` unit boxes at y = 0.5 + l."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 60.0)
+    mat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5, restitution=0.0))
+    ground = w.add_shape(m.Shape.box((20.0, 1.0, 20.0)))
+    unit = w.add_shape(m.Shape.box((1.0, 1.0, 1.0)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=mat),
+               position=(0.0, -0.5, 0.0))
+    for lvl in range(levels):
+        for k in range(levels - lvl):
+            x = k - (levels - 1 - lvl) / 2.0
+            w.add_body(m.Motion(type=m.DYNAMIC, mass=1.0),
+                       m.Collider(shape=unit, physicsMaterial=mat),
+                       position=(x, 0.5 + lvl, 0.0))
+    _set_iterations(w, 10)
+    return w, dict(dt=1.0 / 60.0, steps=120, name='pyramid')
+
+
+def _debris_into(w, m, n: int, rng, lo=(-20.0, 1.0, -20.0), hi=(20.0, 31.0, 20.0),
+                 box_frac: float = 0.7):
+    kinds = rng.random(n) < box_frac
+    sizes = rng.uniform(0.5, 1.5, size=(n, 3))
+    radii = rng.uniform(0.25, 0.75, size=n)
+    pos = rng.uniform(lo, hi, size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    mus = rng.uniform(0.3, 0.8, size=n)
+    for i in range(n):
+        mat = w.add_material(m.Material(staticFriction=float(mus[i]),
+                                         dynamicFriction=float(mus[i])))
+        if kinds[i]:
+            sz = tuple(float(x) for x in sizes[i])
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        else:
+            r = float(radii[i])
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass),
+                   m.Collider(shape=shape, physicsMaterial=mat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+
+
+def debris(api=None, backend=None, n: int = 4096, seed: int = 0, iterations: int = 8,
+           extent: float = 20.0, height: float = 30.0, ground: float = 60.0):
+    """Random debris field above a static ground box (density 1000 kg/m^3)."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    gshape = w.add_shape(m.Shape.box((ground, 1.0, ground)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=gshape, physicsMaterial=gmat),
+               position=(0.0, -0.5, 0.0))
+    _debris_into(w, m, n, rng, lo=(-extent, 1.0, -extent), hi=(extent, 1.0 + height, extent))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=600, name='debris%d' % n)
+
+
+def _ellipsoid_points(rng, count: int, semi: np.ndarray) -> np.ndarray:
+    d = rng.normal(size=(count, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return d * semi
+
+
+def convex_pile(api=None, backend=None, n: int = 32768, seed: int = 0, iterations: int = 8,
+                arena: float = 100.0, height: float = 30.0):
+    """Box/sphere/convex pile (50/25/25) in a walled arena; convex via GJK/EPA."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    floor = w.add_shape(m.Shape.box((arena, 1.0, arena)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=floor, physicsMaterial=gmat),
+               position=(0.0, -0.5, 0.0))
+    half = arena / 2.0
+    wall_x = w.add_shape(m.Shape.box((1.0, 10.0, arena)))
+    wall_z = w.add_shape(m.Shape.box((arena, 10.0, 1.0)))
+    for sx in (-1.0, 1.0):
+        w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=wall_x, physicsMaterial=gmat),
+                   position=(sx * (half + 0.5), 5.0, 0.0))
+    for sz in (-1.0, 1.0):
+        w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=wall_z, physicsMaterial=gmat),
+                   position=(0.0, 5.0, sz * (half + 0.5)))
+    u = rng.random(n)
+    sizes = rng.uniform(0.5, 1.5, size=(n, 3))
+    radii = rng.uniform(0.25, 0.75, size=n)
+    semis = rng.uniform(0.3, 1.0, size=(n, 3))
+    counts = rng.integers(12, 33, size=n)
+    lim = half - 2.0
+    pos = rng.uniform((-lim, 1.0, -lim), (lim, 1.0 + height, lim), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    mus = rng.uniform(0.3, 0.8, size=n)
+    for i in range(n):
+        mat = w.add_material(m.Material(staticFriction=float(mus[i]),
+                                         dynamicFriction=float(mus[i])))
+        if u[i] < 0.5:
+            sz = tuple(float(x) for x in sizes[i])
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        elif u[i] < 0.75:
+            r = float(radii[i])
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        else:
+            pts = _ellipsoid_points(rng, int(counts[i]), semis[i])
+            shape = w.add_shape(m.Shape.convex(pts))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * float(np.prod(semis[i]))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass),
+                   m.Collider(shape=shape, physicsMaterial=mat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='convex%d' % n)
+
+
+def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
+                motor_frac: float = 0.1, iterations: int = 12):
+    """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
+
+    Links share the collision system ``'link'`` and ignore each other, so the
+    only link-link coupling is the point joints; loose boxes and the ground
+    use the default filter and collide with everything.
+    """
+    api = api or default_api()
+    m, J = api.model, api.joints
+    w = _new_world(api, backend, fixed_dt=1.0 / 240.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    link_filter = w.add_filter(m.CollisionFilter(collisionSystems=('link',),
+                                                 notCollideWithSystems=('link',)))
+    ground = w.add_shape(m.Shape.box((4.0 * links, 1.0, 40.0)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=gmat),
+               position=(0.0, -0.5, 0.0))
+    link_shape = w.add_shape(m.Shape.box((1.0, 0.2, 0.2)))
+    y = 3.0
+    x0 = -links / 2.0
+    first = w.body_count
+    for i in range(links):
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=2.0),
+                   m.Collider(shape=link_shape, physicsMaterial=gmat, collisionFilter=link_filter),
+                   position=(x0 + i + 0.5, y, 0.0))
+    motor_axes = rng.normal(size=(links + 1, 3))
+    motor_on = rng.random(links + 1) < motor_frac
+    for i in range(links + 1):
+        a = first + i - 1 if i > 0 else -1
+        b = first + i if i < links else -1
+        w.add_joint_constraint(J.PointConstraint(a, b, (x0 + i, y, 0.0)))
+        if motor_on[i]:
+            body = b if b >= 0 else a
+            w.add_joint_constraint(J.AngularMotor(body, motor_axes[i], 1.0, max_force=50.0))
+    sizes = rng.uniform(0.3, 0.6, size=(loose, 3))
+    pos = rng.uniform((x0, 4.0, -1.0), (-x0, 12.0, 1.0), size=(loose, 3))
+    axes = rng.normal(size=(loose, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=loose)
+    bshape_cache = {}
+    for i in range(loose):
+        sz = tuple(float(x) for x in sizes[i])
+        shape = w.add_shape(m.Shape.box(sz))
+        bshape_cache[i] = shape
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=1000.0 * sz[0] * sz[1] * sz[2]),
+                   m.Collider(shape=shape, physicsMaterial=gmat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    w.joint_iterations = iterations
+    return w, dict(dt=1.0 / 240.0, steps=480, name='chain%d' % links)
+
+
+def serving_requests(n_worlds: int = 1024, seed: int = 0, rate: float = 200.0,
+                     n_min: int = 16, n_max: int = 2048) -> List[dict]:
+    """The serving request stream: Poisson arrivals, log-uniform world sizes.
+
+    Each request is ``dict(arrival=s, bodies=N, steps=S, seed=k)``; the world
+    itself is ``debris(n=N, seed=k)`` scaled to the body count.
+    """
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=n_worlds)
+    arrivals = np.cumsum(gaps)
+    sizes = np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=n_worlds)).astype(int)
+    steps = rng.integers(60, 601, size=n_worlds)
+    return [dict(arrival=float(arrivals[i]), bodies=int(sizes[i]), steps=int(steps[i]),
+                 seed=int(seed * 100003 + i)) for i in range(n_worlds)]
+
+
+def serving_world(req: dict, api=None, backend=None):
+    """Debris-style world for one serving request, volume scaled to its size."""
+    n = req['bodies']
+    ext = max(2.0, 20.0 * (n / 4096.0) ** (1.0 / 3.0))
+    return debris(api, backend, n=n, seed=req['seed'], extent=ext, height=1.5 * ext,
+                  ground=3.0 * ext)
