@@ -1,0 +1,449 @@
+"""Benchmark: body-steps/s of the omi_physics step on B200.
+
+Default workload (N=1): the batched serving mix — 1024 independent debris
+worlds, body counts log-uniform in [16, 2048], all resident in HBM and
+advanced together by one CUDA graph per step (one "step" = every world
+advances one dt). Reported beside it:
+  * e2e: the same steps through the C ABI with the whole arena's mutable
+    state uploaded from pinned host memory and downloaded back every step;
+  * plain: the drop-in per-world path (one context per world, one graph
+    launch + sync per world per step) on a sample of the mix;
+  * roofline of the dominant stage from per-stage CUDA events;
+  * cpu_baseline: the reference's own CPU step (oracle/_ref, NumPy + its
+    Cython accelerators) on a bounded sample, all host cores.
+
+``--impl reference`` times the reference CPU implementation on the same
+workload and prints its JSON line (rank 0 only under torchrun).
+Multi-GPU (torchrun): each rank steps its own seeded copy of the mix — worlds
+are independent, so there is no collective on the data path (weak scaling);
+the barrier and the max-over-ranks time use torch.distributed.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=30)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--worlds', type=int, default=1024)
+    ap.add_argument('--plain-sample', type=int, default=48)
+    ap.add_argument('--cpu-sample-s', type=float, default=15.0)
+    ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--preroll', type=int, default=240,
+                    help='steps every world is advanced before timing (settled piles)')
+    ap.add_argument('--no-extras', action='store_true')
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(n):
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device('cuda', local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
+                 '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_mix(n_worlds, seed):
+    from omi_physics_b200 import scenes
+    reqs = scenes.serving_requests(n_worlds, seed=seed)
+    worlds = [scenes.serving_world(r)[0] for r in reqs]
+    return reqs, worlds
+
+
+def dynamic_bodies(worlds):
+    return int(sum(int(np.count_nonzero(w.motion_type == 2)) for w in worlds))
+
+
+def algorithmic_bytes(stage, N, P, K):
+    """Compulsory fp64 bytes per step of each stage (roofline)."""
+    return {
+        'refit+integrate_forces': 269 * N,
+        'broadphase': 48 * N + 256 * N + 8 * P,
+        'narrowphase': 160 * P + 64 * K,
+        'solve': 160 * K + 168 * N,
+        'integrate_positions_sleep': 170 * N,
+    }[stage]
+
+
+STAGE_GROUPS = {
+    'refit+integrate_forces': ('refit', 'integrate_forces'),
+    'broadphase': ('sort', 'pair_count', 'pair_scan', 'pair_emit'),
+    'narrowphase': ('narrow', 'gjk_epa', 'contact_scan', 'contact_compact'),
+    'solve': ('solve', 'cache_store'),
+    'integrate_positions_sleep': ('integrate_positions_sleep',),
+}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from omi_physics_b200 import WorldBatch
+    from omi_physics_b200._lib import D, U8, ptr
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
+    batch = WorldBatch(worlds, device=local)
+    batch.step(args.preroll)
+    setup_s = time.time() - t0
+    N = dynamic_bodies(worlds)
+    NB = batch.packed.n_bodies
+    # a dedicated stream shared with the library: the CUDA events below are
+    # recorded on the very stream the step kernels are launched on
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
+    batch.ctx.call('set_stream', stream.cuda_stream)
+
+    # ---- device-resident batched steps (the headline) ----
+    batch.step(args.warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    from omi_physics_b200._lib import OmiError
+    for attempt in range(4):
+        launches0 = batch.ctx.launches()
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            barrier(world)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            batch.step_async(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            barrier(world)
+        try:
+            batch.sync()          # raises if a step overflowed its buffers (then it did nothing)
+            ok = 1.0
+        except OmiError:
+            ok = 0.0
+        if max_over_ranks(1.0 - ok, world) == 0.0:
+            break
+        batch.step(1)             # synchronous step regrows the buffers; time again
+    ms = ev0.elapsed_time(ev1)
+    launches = batch.ctx.launches() - launches0
+    ms_max = max_over_ranks(ms, world)
+    total_N = sum_over_ranks(N, world)
+    value = total_N * args.steps / (ms_max / 1e3)
+    pairs, contacts = batch.counts()
+    P, K = int(pairs.sum()), int(contacts.sum())
+
+    # per-step tick latency distribution (graph replay, synchronised per tick)
+    ticks = []
+    for _ in range(max(10, min(args.steps, 50))):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.step_async(1)
+        b.record(stream)
+        b.synchronize()
+        ticks.append(a.elapsed_time(b))
+    batch.sync()
+
+    # ---- roofline: per-stage device time of eagerly launched steps ----
+    prof = {}
+    n_prof = 5
+    for _ in range(n_prof):
+        for k, v in batch.profile().items():
+            prof[k] = prof.get(k, 0.0) + v / n_prof
+    groups = {g: sum(prof.get(k, 0.0) for k in ks) for g, ks in STAGE_GROUPS.items()}
+    dominant = max(groups, key=groups.get)
+    dom_ms = groups[dominant]
+    alg = algorithmic_bytes(dominant, NB, P, K)
+    peaks = {}
+    if os.path.exists(MEASURED):
+        peaks = json.load(open(MEASURED))
+    peak = float(peaks.get('hbm_gbs', FALLBACK_HBM))
+    achieved = alg / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath)).get(dominant)
+        if tr is not None:
+            traffic = tr.get('bytes_per_body', 0.0) * NB + tr.get('bytes_per_contact', 0.0) * K
+    roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': round(achieved, 3), 'peak': peak,
+                'unit': 'GB/s', 'frac': achieved / peak, 'traffic': traffic,
+                'algorithmic_bytes': alg, 'kernel_ms': dom_ms,
+                'peak_source': 'measured' if 'hbm_gbs' in peaks else 'fallback',
+                'stage_ms': {k: round(v, 4) for k, v in groups.items()}}
+
+    # ---- e2e: whole-arena state through pinned host buffers every step ----
+    pin = {name: torch.empty(shape, dtype=dt, pin_memory=True).numpy() for name, shape, dt in (
+        ('pos', (NB, 3), torch.float64), ('q', (NB, 4), torch.float64),
+        ('v', (NB, 3), torch.float64), ('w', (NB, 3), torch.float64),
+        ('awake', (NB,), torch.uint8), ('timer', (NB,), torch.float64))}
+    c = batch.ctx
+    c.call('download_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
+           ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D), None, None)
+    h2d = sum(a.nbytes for a in pin.values())
+    e2e_steps = max(3, min(args.steps, 20))
+
+    def e2e_step():
+        c.call('upload_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
+               ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D))
+        c.call('step', 1)
+        c.call('download_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
+               ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D), None, None)
+
+    e2e_step()
+    barrier(world)
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t, world)
+    e2e = {'value': total_N * e2e_steps / e2e_s, 'unit': 'body-steps/s', 'h2d_bytes_per_step': h2d,
+           'd2h_bytes_per_step': h2d, 'path': 'omi_upload_state + omi_step + omi_download_state, pinned'}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras['plain'] = plain_per_world(worlds, reqs, args.plain_sample, local, args.preroll)
+    return dict(value=value, ms=ms_max, N=total_N, P=P, K=K, launches=launches, setup_s=setup_s,
+                ticks=ticks, roofline=roofline, e2e=e2e, clocks=clk.summary(), extras=extras,
+                NB=NB)
+
+
+def plain_per_world(worlds, reqs, sample, device, preroll):
+    """The drop-in path: one context per world, one step launch + sync each."""
+    from omi_physics_b200 import WorldBatch, scenes
+    rng = np.random.default_rng(7)
+    idx = sorted(rng.choice(len(reqs), size=min(sample, len(reqs)), replace=False))
+    sub = [scenes.serving_world(reqs[i])[0] for i in idx]
+    batches = [WorldBatch([w], device=device) for w in sub]
+    for b in batches:
+        b.step(preroll)
+    steps = 5
+    t = time.perf_counter()
+    for _ in range(steps):
+        for b in batches:
+            b.ctx.call('step', 1)
+    dt = time.perf_counter() - t
+    n = sum(int(np.count_nonzero(w.motion_type == 2)) for w in sub)
+    rate = n * steps / dt
+    for b in batches:
+        b.ctx.close()
+    return {'value': rate, 'unit': 'body-steps/s', 'worlds_sampled': len(sub),
+            'method': 'sequential per-world omi_step (graph launch + sync) over a sample of the mix'}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the reference built from its own sources)
+# ---------------------------------------------------------------------------
+def _ref_worker(payload):
+    idx, seed, n_worlds, budget_s, preroll = payload
+    sys.path.insert(0, os.path.join(ROOT, 'oracle', '_ref'))
+    from types import SimpleNamespace
+    import omi_physics as ref
+    from omi_physics import joints as rj, model as rm
+    from omi_physics_b200 import scenes
+    api = SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=rm, joints=rj)
+    reqs = scenes.serving_requests(n_worlds, seed=seed)
+    done = 0
+    t_total = 0.0
+    start = time.perf_counter()
+    for i in idx:
+        w, meta = scenes.serving_world(reqs[i], api=api)
+        n = int(np.count_nonzero(w.motion_type == 2))
+        for _ in range(preroll):                 # same settled state as the GPU arm
+            w.step(meta['dt'])
+        t = time.perf_counter()
+        for _ in range(2):
+            w.step(meta['dt'])
+        t_total += time.perf_counter() - t
+        done += 2 * n
+        if time.perf_counter() - start > budget_s:
+            break
+    return done, t_total
+
+
+def cpu_reference(n_worlds, seed, budget_s, preroll, cores=None):
+    import multiprocessing as mp
+    cores = cores or os.cpu_count() or 1
+    ref_dir = os.path.join(ROOT, 'oracle', '_ref', 'omi_physics')
+    if not os.path.isdir(ref_dir):
+        return None
+    rng = np.random.default_rng(11)
+    order = list(rng.permutation(n_worlds))
+    chunks = [order[i::cores] for i in range(cores)]
+    ctx = mp.get_context('spawn')
+    t = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(c, seed, n_worlds, budget_s, preroll) for c in chunks])
+    wall = time.perf_counter() - t
+    body_steps = sum(r[0] for r in res)
+    step_time = sum(r[1] for r in res)
+    # each process advanced its worlds one step each; throughput with all cores
+    per_core = body_steps / step_time if step_time > 0 else 0.0
+    return {'value': per_core * cores, 'unit': 'body-steps/s', 'cores': cores, 'kind': 'reference',
+            'sample': '%d body-steps: worlds of the serving mix pre-rolled %d steps, then 2 timed '
+                      'steps each; %d processes, %.1f s wall' % (body_steps, preroll, cores, wall),
+            'per_core': per_core}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    metric = 'body-steps/s (batched serving mix, 1 B200 per rank)'
+    config = {'workload': 'serving-mix', 'worlds_per_gpu': args.worlds,
+              'bodies': 'log-uniform [16,2048] per world, debris contents', 'dt': '1/120 s',
+              'iterations': 8, 'l2': 'inputs larger than L2 (arena state > 126 MB)',
+              'parallelism': 'world-sharded x%d (no data-path collective)' % world}
+    if args.impl == 'reference':
+        if rank == 0:
+            budget = max(5.0, args.cpu_sample_s)
+            r = cpu_reference(args.worlds, args.seed, budget, args.preroll)
+            if r is None:
+                print(json.dumps({'impl': 'reference', 'unavailable':
+                                  'oracle/_ref (the reference built from its sources) is missing'}))
+            else:
+                line = {'impl': 'reference', 'metric': metric, 'value': r['value'],
+                        'unit': 'body-steps/s', 'n_gpus': args.gpus, 'steps': args.steps,
+                        'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+                        'dtype': 'f64', 'data': 'synthetic', 'config': config,
+                        'cpu_baseline': {k: r[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')},
+                        'e2e': {'value': r['value'], 'unit': 'body-steps/s',
+                                'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+                print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    res = run_ours(args, rank, world, local)
+    if rank == 0:
+        ticks = sorted(res['ticks'])
+        line = {
+            'metric': metric, 'value': res['value'], 'unit': 'body-steps/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms'] / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic (seeded serving-mix scenes)', 'config': config,
+            'e2e': res['e2e'], 'roofline': res['roofline'], 'clocks': res['clocks'],
+            'gpu_launches': res['launches'],
+            'tick_latency_ms': {'p50': float(np.percentile(ticks, 50)),
+                                'p99': float(np.percentile(ticks, 99))},
+            'dynamic_bodies': res['N'], 'rows': res['NB'], 'pairs': res['P'], 'contacts': res['K'],
+        }
+        ex = res['extras']
+        if 'plain' in ex:
+            line['plain_per_world'] = ex['plain']
+            line['batched_over_plain'] = res['value'] / world / ex['plain']['value']
+        if not args.no_extras:
+            cb = cpu_reference(args.worlds, args.seed, args.cpu_sample_s, args.preroll)
+            if cb is not None:
+                line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,216 @@
+/*
+ * omi_b200 — C ABI of the B200 (sm_100a) rigid-body step.
+ *
+ * One context owns one CUDA stream and one device-resident "arena": any
+ * number of independent worlds, each a contiguous range of body rows in a
+ * structure-of-arrays layout identical to the reference's numpy columns
+ * (position (n,3), orientation (n,4) xyzw, ...; src/omi_physics/world.py:75-122).
+ * A plain PhysicsWorld is an arena of one world; the batched/serving forms
+ * step many worlds with the same launches.
+ *
+ * Conventions: every call returns 0 on success or a negative OMI_E_* code;
+ * omi_last_error() gives the message. Host buffers are caller-owned and are
+ * never retained past the call. A context is used from one host thread at a
+ * time. No call falls back to the CPU: without a usable device they fail.
+ */
+#ifndef OMI_B200_H
+#define OMI_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OMI_OK 0
+#define OMI_E_CUDA (-1)         /* CUDA runtime error (message has details) */
+#define OMI_E_ARG (-2)          /* bad argument / size */
+#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triggers, capsules ...) */
+#define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
+#define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
+#define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
+
+/* Shape types, combine modes, joint types: same meaning as the reference's
+ * model.Shape.type, model.combine modes (model.py:231-243) and joints.py. */
+enum { OMI_SHAPE_SPHERE = 1, OMI_SHAPE_BOX = 2, OMI_SHAPE_CONVEX = 3 };
+enum { OMI_AVERAGE = 0, OMI_MINIMUM = 1, OMI_MAXIMUM = 2, OMI_MULTIPLY = 3 };
+enum { OMI_JOINT_POINT = 0, OMI_JOINT_DISTANCE = 1, OMI_JOINT_MOTOR = 2 };
+/* per-world flag bits */
+enum { OMI_WF_SLEEP = 1, OMI_WF_WARM = 2, OMI_WF_COLLISION = 4, OMI_WF_ACTIVE = 8 };
+
+/*
+ * Scene tables for a whole arena (all worlds concatenated). Body, shape,
+ * material and joint indices are global (world-local index + the world's
+ * offset); -1 keeps the reference's meaning (no shape / default material /
+ * the world as a joint end). Filter rows are world-local: row 0 is the
+ * default filter, row f+1 is the world's filters[f]; each world's
+ * (rows x rows) collides_with matrix starts at w_filter_off[w].
+ * Pair-friction entries are per world, keyed like the reference's
+ * PhysicsWorld.pair_friction dict: by the bodies' raw (world-local)
+ * collider_material values with a <= b, sorted by (a, b) within each world's
+ * range (world.py:207-228); `material_key` carries those raw values per body.
+ */
+typedef struct OmiScene {
+    int32_t n_worlds;
+    const int32_t *w_body_off;      /* n_worlds+1 */
+    const double *w_gravity;        /* n_worlds*3, resolved (world.py:386-396) */
+    const double *w_dt;             /* n_worlds */
+    const int32_t *w_iters;         /* velocity iterations */
+    const int32_t *w_joint_iters;
+    const int32_t *w_flags;         /* OMI_WF_* */
+    const double *w_default_damp;   /* n_worlds*2: linear, angular */
+    const double *w_solver;         /* n_worlds*2: restitution threshold, slop */
+    const int32_t *w_filter_off, *w_filter_rows;
+    const int32_t *w_pf_off, *w_pf_n;
+    const int32_t *w_joint_off;     /* n_worlds+1 */
+
+    int32_t n_bodies;
+    const double *pos, *q, *v, *w;  /* n*3, n*4, n*3, n*3 */
+    const double *inv_mass, *inv_inertia;           /* n, n*3 */
+    const double *gravity_factor, *lin_damp, *ang_damp, *quad_drag, *sleep_timer;
+    const int32_t *motion_type;     /* 0 static, 1 kinematic, 2 dynamic */
+    const int32_t *shape;           /* global shape index or -1 */
+    const int32_t *material;        /* global material index or -1 (default material) */
+    const int32_t *material_key;    /* raw collider_material value (pair-friction key) */
+    const int32_t *filter_row;      /* world-local filter row */
+    const uint8_t *awake;
+
+    int32_t n_shapes;
+    const int32_t *shape_type;
+    const double *shape_radius, *shape_size;        /* n_shapes, n_shapes*3 */
+    const int32_t *shape_pt_off, *shape_pt_cnt;
+    int32_t n_points;
+    const double *points;                            /* local convex points */
+
+    int32_t n_materials;
+    const double *mat_dynf, *mat_rest;
+    const int32_t *mat_fcomb, *mat_rcomb;
+    int32_t n_pair_friction;
+    const int32_t *pf_a, *pf_b;
+    const double *pf_mu;
+    int32_t n_filter_bytes;
+    const uint8_t *filter_matrix;
+
+    int32_t n_joints;
+    const int32_t *j_type, *j_a, *j_b;              /* motor: j_a = body */
+    const double *j_anchor, *j_anchor_b, *j_local_a, *j_local_b;   /* *3 */
+    const uint8_t *j_has_local_a, *j_has_local_b;
+    const double *j_length;
+    const uint8_t *j_has_length;
+    const double *j_axis, *j_target, *j_max_force, *j_accum;
+} OmiScene;
+
+typedef struct OmiCtx OmiCtx;
+
+/* ---- context ---------------------------------------------------------- */
+int omi_create(int device, OmiCtx **out);
+int omi_destroy(OmiCtx *ctx);
+const char *omi_last_error(OmiCtx *ctx);
+/* Launch on this cudaStream_t (NULL = the context's own stream). */
+int omi_set_stream(OmiCtx *ctx, void *stream);
+/* Refuse arenas whose device footprint exceeds this many bytes (0 = none). */
+int omi_set_budget(OmiCtx *ctx, int64_t bytes);
+int64_t omi_device_bytes(OmiCtx *ctx);
+
+/* ---- scene ------------------------------------------------------------ */
+/* Upload a whole arena (replaces any previous one). Builds what the reference
+ * builds lazily on the first step: _build_refit_cache (world.py:443-469). */
+int omi_load(OmiCtx *ctx, const OmiScene *scene);
+/* Which worlds take part in the next steps (n_worlds bytes, 0/1). */
+int omi_set_active(OmiCtx *ctx, const uint8_t *active);
+/* Per-world step parameters (any pointer may be NULL to keep the current
+ * values): dt, velocity iterations, joint iterations, OMI_WF_* flags. */
+int omi_set_world_params(OmiCtx *ctx, const double *dt, const int32_t *iters,
+                         const int32_t *joint_iters, const int32_t *flags);
+
+/* ---- serving slots ------------------------------------------------------ */
+/* Capacities of one slot: an arena of n_slots empty, inactive worlds, each
+ * able to hold one world within these limits. */
+typedef struct OmiSlotCaps {
+    int32_t bodies, shapes, materials, points, joints, filter_rows, pair_friction;
+} OmiSlotCaps;
+int omi_reserve_slots(OmiCtx *ctx, int32_t n_slots, const OmiSlotCaps *caps);
+/* Admit one world (an OmiScene with n_worlds == 1, local indices) into a
+ * slot: its tables and state are copied in, its warm-start cache cleared and
+ * the slot activated when OMI_WF_ACTIVE is set. No reallocation, no graph
+ * rebuild: other slots keep stepping in the same launches. */
+int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *one);
+/* First arena row of a world and its live body count. */
+int omi_world_rows(OmiCtx *ctx, int32_t world, int32_t *first_row, int32_t *n_bodies);
+
+/* ---- state transfer (host columns <-> device arena) ------------------- */
+/* Rows [begin, begin+count) of the arena; any pointer may be NULL to skip. */
+int omi_upload_state(OmiCtx *ctx, int32_t begin, int32_t count, const double *pos,
+                     const double *q, const double *v, const double *w,
+                     const uint8_t *awake, const double *sleep_timer);
+int omi_download_state(OmiCtx *ctx, int32_t begin, int32_t count, double *pos, double *q,
+                       double *v, double *w, uint8_t *awake, double *sleep_timer,
+                       double *aabb_min, double *aabb_max);
+/* Joint state the reference keeps on the constraint objects
+ * (joints.py:88-91 local anchors, 151-152 rest length, 201 motor accum). */
+int omi_download_joints(OmiCtx *ctx, double *local_a, double *local_b, uint8_t *has_local_a,
+                        uint8_t *has_local_b, double *length, uint8_t *has_length,
+                        double *accum);
+
+/* Warm-start cache of one world, the reference's SequentialImpulseSolver._cache
+ * (solver.py:91, 272-278) flattened in insertion order: entry i is the pair
+ * (a[i], b[i]) (global body indices), its contact point (3) and accumulated
+ * impulses (normal, tangent0, tangent1). set replaces it; get returns the
+ * entry count (or a negative status), writing at most cap entries. */
+int omi_set_cache(OmiCtx *ctx, int32_t world, int32_t n, const int32_t *a, const int32_t *b,
+                  const double *point, const double *impulse);
+int omi_get_cache(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double *point,
+                  double *impulse, int32_t cap);
+
+/* ---- the step --------------------------------------------------------- */
+/* n_steps x PhysicsWorld.step(dt) (world.py:410-430) for every active world,
+ * each world with its own dt: integrate forces, refit, broadphase,
+ * narrowphase, contact solve, joints, integrate positions, sleep. Captured as
+ * a CUDA graph after the first step; capacity overflow is detected before any
+ * state changes, regrown and the step re-run, so results do not depend on it. */
+int omi_step(OmiCtx *ctx, int32_t n_steps);
+/* Same, enqueued without the final host synchronisation (use omi_sync). */
+int omi_step_async(OmiCtx *ctx, int32_t n_steps);
+int omi_sync(OmiCtx *ctx);
+
+/* ---- stage entry points (the backend seam and the collision stages) ---- */
+/* NumpyBackend.integrate_forces (backend.py:26-40) */
+int omi_integrate_forces(OmiCtx *ctx);
+/* NumpyBackend.refit_aabbs -> PhysicsWorld.refit_aabbs (backend.py:51-53, world.py:471-508) */
+int omi_refit_aabbs(OmiCtx *ctx);
+/* BroadPhase.pairs (broadphase.py:243-294): pair lists per world, in the
+ * reference's order; returns OMI_E_ARG-free status, counts via omi_counts */
+int omi_broadphase(OmiCtx *ctx);
+/* solid-pair filter + NarrowPhase.generate (world.py:661-671, narrowphase.py:51-100,
+ * _collide_native.box_box/sphere_sphere/sphere_box, gjk.collide_convex) */
+int omi_narrowphase(OmiCtx *ctx);
+/* SequentialImpulseSolver.solve (solver.py:192-278 -> _solver_native.prepare_and_solve,
+ * _solver_native.pyx:179-312), warm-start cache kept on the device */
+int omi_solve_contacts(OmiCtx *ctx);
+/* PhysicsWorld._solve_joints (world.py:599-611, joints.py:60-212) */
+int omi_solve_joints(OmiCtx *ctx);
+/* NumpyBackend.integrate_positions (backend.py:42-49) */
+int omi_integrate_positions(OmiCtx *ctx);
+/* PhysicsWorld._update_sleep (world.py:510-567) */
+int omi_update_sleep(OmiCtx *ctx);
+
+/* ---- results of the last step ----------------------------------------- */
+/* per-world pair and contact counts (n_worlds each) */
+int omi_counts(OmiCtx *ctx, int32_t *pairs, int32_t *contacts);
+/* broadphase pairs of one world as global body indices (2*cap int32) */
+int omi_get_pairs(OmiCtx *ctx, int32_t world, int32_t *out, int32_t cap);
+/* contacts of one world (Contact records, collide.py:37-53) with the solver's
+ * accumulated impulses (normal, tangent0, tangent1) */
+int omi_get_contacts(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double *point,
+                     double *normal, double *depth, double *impulse, int32_t cap);
+/* sleep-island label per body of one world (-1 = not in contact) */
+int omi_get_islands(OmiCtx *ctx, int32_t world, int32_t *labels);
+/* per-kernel device time (ms) of the last profiled step, see omi_profile_step */
+int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out);
+const char *omi_kernel_name(int32_t i);
+/* launches of the library's own kernels since load */
+int64_t omi_launch_count(OmiCtx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

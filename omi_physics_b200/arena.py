@@ -1,0 +1,305 @@
+"""Pack world objects into the library's arena tables (``OmiScene``).
+
+Accepts any world with the reference's ``PhysicsWorld`` layout — the
+reference's own class (``src/omi_physics/world.py``) or
+:class:`omi_physics_b200.PhysicsWorld` — and concatenates one or more of
+them. Indices become global (world offset added); ``-1`` keeps its meaning.
+What the device path does not implement is refused here with
+:class:`UnsupportedFeature`, never approximated.
+"""
+import ctypes as C
+from typing import List, Sequence
+
+import numpy as np
+
+from ._lib import D, I, U8, OmiScene, UnsupportedFeature, WF_ACTIVE, WF_COLLISION, WF_SLEEP, \
+    WF_WARM, ptr
+from .joints import joint_kind
+from .model import COMBINE_CODES
+
+SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3}
+JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
+
+
+def resolved_gravity(world) -> np.ndarray:
+    """The uniform gravity vector exactly as ``resolve_gravity`` forms it (world.py:386-392)."""
+    base = np.asarray(world.gravity.direction, dtype='d')
+    norm = np.linalg.norm(base)
+    base = base / norm if norm else base
+    return base * world.gravity.gravity
+
+
+def world_solver(world):
+    col = getattr(world, '_collision', None)
+    return getattr(col, 'solver', None) if col is not None else None
+
+
+def world_flags(world, active: bool = True) -> int:
+    solver = world_solver(world)
+    f = 0
+    if world.sleep_enabled:
+        f |= WF_SLEEP
+    if getattr(solver, 'warm_start', True):
+        f |= WF_WARM
+    if getattr(world, '_collision', None) is not None:
+        f |= WF_COLLISION
+    if active:
+        f |= WF_ACTIVE
+    return f
+
+
+def world_iterations(world) -> int:
+    solver = world_solver(world)
+    return int(getattr(solver, 'velocity_iterations', 10)) if solver is not None else 10
+
+
+def check_supported(world) -> None:
+    """Raise :class:`UnsupportedFeature` for anything outside the device step."""
+    n = world.body_count
+    if getattr(world, 'gravity_volumes', None):
+        raise UnsupportedFeature(-3, 'gravity volumes are not supported on the CUDA path')
+    if n and np.any(np.asarray(world._trigger_shape[:n]) >= 0):
+        raise UnsupportedFeature(-3, 'trigger shapes are not supported on the CUDA path')
+    cs = np.asarray(world._collider_shape[:n])
+    used = set(int(s) for s in cs[(cs >= 0) & (cs < len(world.shapes))])
+    for s in used:
+        t = world.shapes[s].type
+        if t not in SHAPE_CODES:
+            raise UnsupportedFeature(-3, 'shape type %r is not supported on the CUDA path' % t)
+
+
+class PackedScene:
+    """Numpy arrays behind one ``OmiScene`` (kept alive with it)."""
+
+    def __init__(self):
+        self.arrays = {}
+        self.scene = OmiScene()
+
+    def set(self, name, arr, t):
+        arr = np.ascontiguousarray(arr)
+        self.arrays[name] = arr
+        setattr(self.scene, name, ptr(arr, t))
+
+
+def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> PackedScene:
+    """Concatenate ``worlds`` into one arena description."""
+    W = len(worlds)
+    if W == 0:
+        raise ValueError('no worlds')
+    dts = list(dts) if dts is not None else [w.fixed_dt for w in worlds]
+    act = [active] * W if isinstance(active, bool) else list(active)
+    cols_f3 = ('position', 'linear_velocity', 'angular_velocity', 'inv_inertia')
+    parts = {k: [] for k in ('pos', 'q', 'v', 'w', 'inv_mass', 'inv_inertia', 'gravity_factor',
+                             'lin_damp', 'ang_damp', 'quad_drag', 'sleep_timer', 'motion_type',
+                             'shape', 'material', 'material_key', 'filter_row', 'awake',
+                             'shape_type', 'shape_radius', 'shape_size', 'shape_pt_off',
+                             'shape_pt_cnt', 'points', 'mat_dynf', 'mat_rest', 'mat_fcomb',
+                             'mat_rcomb', 'pf_a', 'pf_b', 'pf_mu', 'filter_matrix', 'j_type',
+                             'j_a', 'j_b', 'j_anchor', 'j_anchor_b', 'j_local_a', 'j_local_b',
+                             'j_has_local_a', 'j_has_local_b', 'j_length', 'j_has_length',
+                             'j_axis', 'j_target', 'j_max_force', 'j_accum')}
+    body_off, joint_off = [0], [0]
+    w_g, w_dt, w_iters, w_jiters, w_flags, w_damp, w_solver = [], [], [], [], [], [], []
+    w_foff, w_frows, w_pfoff, w_pfn = [], [], [], []
+    nb = ns = nm = npts = nf = npf = nj = 0
+    for wi, world in enumerate(worlds):
+        check_supported(world)
+        n = world.body_count
+        parts['pos'].append(np.asarray(world._position[:n], 'd'))
+        parts['q'].append(np.asarray(world._orientation[:n], 'd'))
+        parts['v'].append(np.asarray(world._linear_velocity[:n], 'd'))
+        parts['w'].append(np.asarray(world._angular_velocity[:n], 'd'))
+        parts['inv_mass'].append(np.asarray(world._inv_mass[:n], 'd'))
+        parts['inv_inertia'].append(np.asarray(world._inv_inertia[:n], 'd'))
+        parts['gravity_factor'].append(np.asarray(world._gravity_factor[:n], 'd'))
+        parts['lin_damp'].append(np.asarray(world._linear_damping[:n], 'd'))
+        parts['ang_damp'].append(np.asarray(world._angular_damping[:n], 'd'))
+        parts['quad_drag'].append(np.asarray(world._quadratic_drag[:n], 'd'))
+        parts['sleep_timer'].append(np.asarray(world._sleep_timer[:n], 'd'))
+        parts['motion_type'].append(np.asarray(world._motion_type[:n], np.int32))
+        parts['awake'].append(np.asarray(world._awake[:n], np.uint8))
+        cs = np.asarray(world._collider_shape[:n], np.int64)
+        valid = (cs >= 0) & (cs < len(world.shapes))
+        parts['shape'].append(np.where(valid, cs + ns, -1).astype(np.int32))
+        cm = np.asarray(world._collider_material[:n], np.int64)
+        mvalid = (cm >= 0) & (cm < len(world.materials))
+        parts['material'].append(np.where(mvalid, cm + nm, -1).astype(np.int32))
+        parts['material_key'].append(cm.astype(np.int32))
+        cf = np.asarray(world._collider_filter[:n], np.int64)
+        F = len(world.filters)
+        parts['filter_row'].append(np.where((cf >= 0) & (cf < F), cf + 1, 0).astype(np.int32))
+        # shapes
+        for sh in world.shapes:
+            code = SHAPE_CODES.get(sh.type, 0)
+            parts['shape_type'].append([code])
+            parts['shape_radius'].append([float(sh.radius)])
+            size = np.asarray(sh.size, 'd') if np.size(sh.size) == 3 else np.zeros(3)
+            parts['shape_size'].append(size.reshape(1, 3))
+            if sh.type == 'convex':
+                pts = np.asarray(sh.points, 'd').reshape(-1, 3)
+                parts['shape_pt_off'].append([npts])
+                parts['shape_pt_cnt'].append([len(pts)])
+                parts['points'].append(pts)
+                npts += len(pts)
+            else:
+                parts['shape_pt_off'].append([0])
+                parts['shape_pt_cnt'].append([0])
+        # materials
+        for m in world.materials:
+            parts['mat_dynf'].append([m.dynamicFriction])
+            parts['mat_rest'].append([m.restitution])
+            parts['mat_fcomb'].append([COMBINE_CODES.get(m.frictionCombine, 0)])
+            parts['mat_rcomb'].append([COMBINE_CODES.get(m.restitutionCombine, 0)])
+        pf = sorted(world.pair_friction.items())
+        w_pfoff.append(npf)
+        w_pfn.append(len(pf))
+        for (ka, kb), (_, mu) in pf:
+            parts['pf_a'].append([ka]); parts['pf_b'].append([kb]); parts['pf_mu'].append([mu])
+        npf += len(pf)
+        # filter matrix, row 0 = default filter
+        flist = [world.filter_for(-1)] + list(world.filters)
+        fm = np.array([[1 if a.collides_with(b) else 0 for b in flist] for a in flist], np.uint8)
+        w_foff.append(nf)
+        w_frows.append(F + 1)
+        parts['filter_matrix'].append(fm.reshape(-1))
+        nf += fm.size
+        # joints
+        js = list(world.joint_constraints)
+        for c in js:
+            k = joint_kind(c)
+            parts['j_type'].append([JOINT_CODES[k]])
+            z3 = np.zeros((1, 3))
+            if k == 'motor':
+                parts['j_a'].append([c.body + nb]); parts['j_b'].append([-1])
+                parts['j_anchor'].append(z3); parts['j_anchor_b'].append(z3)
+                parts['j_local_a'].append(z3); parts['j_local_b'].append(z3)
+                parts['j_has_local_a'].append([0]); parts['j_has_local_b'].append([0])
+                parts['j_length'].append([0.0]); parts['j_has_length'].append([0])
+                parts['j_axis'].append(np.asarray(c.axis, 'd').reshape(1, 3))
+                parts['j_target'].append([c.target]); parts['j_max_force'].append([c.max_force])
+                parts['j_accum'].append([c.accum])
+                continue
+            parts['j_a'].append([c.a + nb if c.a >= 0 else -1])
+            parts['j_b'].append([c.b + nb if c.b >= 0 else -1])
+            parts['j_axis'].append(z3); parts['j_target'].append([0.0])
+            parts['j_max_force'].append([0.0]); parts['j_accum'].append([0.0])
+            if k == 'point':
+                parts['j_anchor'].append(np.asarray(c.anchor, 'd').reshape(1, 3))
+                parts['j_anchor_b'].append(z3)
+                for side, loc in (('a', c.local_a), ('b', c.local_b)):
+                    has = loc is not None
+                    parts['j_local_' + side].append(np.asarray(loc, 'd').reshape(1, 3) if has else z3)
+                    parts['j_has_local_' + side].append([1 if has else 0])
+                parts['j_length'].append([0.0]); parts['j_has_length'].append([0])
+            else:
+                parts['j_anchor'].append(np.asarray(c.anchor_a, 'd').reshape(1, 3))
+                parts['j_anchor_b'].append(np.asarray(c.anchor_b, 'd').reshape(1, 3))
+                parts['j_local_a'].append(z3); parts['j_local_b'].append(z3)
+                parts['j_has_local_a'].append([0]); parts['j_has_local_b'].append([0])
+                has = c.length is not None
+                parts['j_length'].append([float(c.length) if has else 0.0])
+                parts['j_has_length'].append([1 if has else 0])
+        nj += len(js)
+        joint_off.append(nj)
+        # per-world parameters
+        w_g.append(resolved_gravity(world))
+        w_dt.append(float(dts[wi]))
+        w_iters.append(world_iterations(world))
+        w_jiters.append(int(world.joint_iterations))
+        w_flags.append(world_flags(world, act[wi]))
+        w_damp.append([world.default_linear_damping, world.default_angular_damping])
+        solver = world_solver(world)
+        w_solver.append([float(getattr(solver, 'restitution_threshold', 0.5)),
+                         float(getattr(solver, 'slop', 0.005))])
+        nb += n
+        ns += len(world.shapes)
+        nm += len(world.materials)
+        body_off.append(nb)
+
+    def cat(key, dtype, width=None):
+        xs = parts[key]
+        if not xs:
+            shape = (1,) if width is None else (1, width)
+            return np.zeros(shape, dtype)
+        arrs = [np.asarray(x, dtype) for x in xs]
+        if width is not None:
+            arrs = [a.reshape(-1, width) for a in arrs]
+            return np.concatenate(arrs, axis=0)
+        return np.concatenate([a.reshape(-1) for a in arrs])
+
+    P = PackedScene()
+    s = P.scene
+    s.n_worlds = W
+    P.set('w_body_off', np.array(body_off, np.int32), I)
+    P.set('w_gravity', np.array(w_g, 'd').reshape(W, 3), D)
+    P.set('w_dt', np.array(w_dt, 'd'), D)
+    P.set('w_iters', np.array(w_iters, np.int32), I)
+    P.set('w_joint_iters', np.array(w_jiters, np.int32), I)
+    P.set('w_flags', np.array(w_flags, np.int32), I)
+    P.set('w_default_damp', np.array(w_damp, 'd').reshape(W, 2), D)
+    P.set('w_solver', np.array(w_solver, 'd').reshape(W, 2), D)
+    P.set('w_filter_off', np.array(w_foff, np.int32), I)
+    P.set('w_filter_rows', np.array(w_frows, np.int32), I)
+    P.set('w_pf_off', np.array(w_pfoff, np.int32), I)
+    P.set('w_pf_n', np.array(w_pfn, np.int32), I)
+    P.set('w_joint_off', np.array(joint_off, np.int32), I)
+    s.n_bodies = nb
+    for key, t, dt, width in (('pos', D, 'd', 3), ('q', D, 'd', 4), ('v', D, 'd', 3),
+                              ('w', D, 'd', 3), ('inv_mass', D, 'd', None),
+                              ('inv_inertia', D, 'd', 3), ('gravity_factor', D, 'd', None),
+                              ('lin_damp', D, 'd', None), ('ang_damp', D, 'd', None),
+                              ('quad_drag', D, 'd', None), ('sleep_timer', D, 'd', None),
+                              ('motion_type', I, np.int32, None), ('shape', I, np.int32, None),
+                              ('material', I, np.int32, None), ('material_key', I, np.int32, None),
+                              ('filter_row', I, np.int32, None), ('awake', U8, np.uint8, None)):
+        P.set(key, cat(key, dt, width), t)
+    s.n_shapes = ns
+    P.set('shape_type', cat('shape_type', np.int32), I)
+    P.set('shape_radius', cat('shape_radius', 'd'), D)
+    P.set('shape_size', cat('shape_size', 'd', 3), D)
+    P.set('shape_pt_off', cat('shape_pt_off', np.int32), I)
+    P.set('shape_pt_cnt', cat('shape_pt_cnt', np.int32), I)
+    s.n_points = npts
+    P.set('points', cat('points', 'd', 3), D)
+    s.n_materials = nm
+    P.set('mat_dynf', cat('mat_dynf', 'd'), D)
+    P.set('mat_rest', cat('mat_rest', 'd'), D)
+    P.set('mat_fcomb', cat('mat_fcomb', np.int32), I)
+    P.set('mat_rcomb', cat('mat_rcomb', np.int32), I)
+    s.n_pair_friction = npf
+    P.set('pf_a', cat('pf_a', np.int32), I)
+    P.set('pf_b', cat('pf_b', np.int32), I)
+    P.set('pf_mu', cat('pf_mu', 'd'), D)
+    s.n_filter_bytes = nf
+    P.set('filter_matrix', cat('filter_matrix', np.uint8), U8)
+    s.n_joints = nj
+    for key, t, dt, width in (('j_type', I, np.int32, None), ('j_a', I, np.int32, None),
+                              ('j_b', I, np.int32, None), ('j_anchor', D, 'd', 3),
+                              ('j_anchor_b', D, 'd', 3), ('j_local_a', D, 'd', 3),
+                              ('j_local_b', D, 'd', 3), ('j_has_local_a', U8, np.uint8, None),
+                              ('j_has_local_b', U8, np.uint8, None), ('j_length', D, 'd', None),
+                              ('j_has_length', U8, np.uint8, None), ('j_axis', D, 'd', 3),
+                              ('j_target', D, 'd', None), ('j_max_force', D, 'd', None),
+                              ('j_accum', D, 'd', None)):
+        P.set(key, cat(key, dt, width), t)
+    P.body_off = body_off
+    P.joint_off = joint_off
+    P.n_bodies = nb
+    P.n_joints = nj
+    P.worlds = list(worlds)
+    return P
+
+
+def static_signature(world) -> tuple:
+    """What forces a re-pack when it changes: topology and the static columns."""
+    import zlib
+    n = world.body_count
+    crc = 0
+    for name in ('_inv_mass', '_inv_inertia', '_gravity_factor', '_linear_damping',
+                 '_angular_damping', '_quadratic_drag', '_motion_type', '_collider_shape',
+                 '_collider_material', '_collider_filter', '_trigger_shape'):
+        crc = zlib.crc32(np.ascontiguousarray(getattr(world, name)[:n]).view(np.uint8), crc)
+    return (n, len(world.shapes), len(world.materials), len(world.filters),
+            len(world.joint_constraints), tuple(sorted(world.pair_friction.items())),
+            tuple(id(c) for c in world.joint_constraints), world.gravity.gravity,
+            tuple(world.gravity.direction), crc)

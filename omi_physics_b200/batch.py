@@ -1,0 +1,184 @@
+"""Device-resident worlds: the batched form and the state shuttle the plain
+backend uses.
+
+:class:`WorldBatch` loads any number of independent worlds (reference
+``PhysicsWorld`` layout) into one device arena and steps them all with the
+same launches — one CUDA graph per step for every world, whatever their
+sizes. State stays in HBM between steps; :meth:`WorldBatch.sync_to_host`
+writes it back into each world's numpy columns.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Sequence
+
+import numpy as np
+
+from ._lib import D, I, U8, Context, ptr
+from .arena import pack_worlds, world_flags, world_iterations
+from .joints import joint_kind
+
+
+@dataclass
+class Contact:
+    """One contact record (collide.py:37-53): normal points from ``a`` to ``b``."""
+    a: int
+    b: int
+    point: np.ndarray
+    normal: np.ndarray
+    depth: float
+    normal_impulse: float = 0.0
+    tangent_impulse: np.ndarray = field(default_factory=lambda: np.zeros(2))
+
+
+class WorldBatch:
+    """Independent worlds stepped together on one GPU."""
+
+    def __init__(self, worlds: Sequence, device: int = 0, dts: Sequence[float] = None,
+                 ctx: Context = None):
+        self.worlds = list(worlds)
+        self.ctx = ctx or Context(device)
+        self.dts = list(dts) if dts is not None else [w.fixed_dt for w in self.worlds]
+        self.packed = pack_worlds(self.worlds, self.dts)
+        self.ctx.call('load', C.byref(self.packed.scene))
+        self.offsets = self.packed.body_off
+        self.joint_offsets = self.packed.joint_off
+
+    # -- stepping -----------------------------------------------------------
+    def step(self, n: int = 1) -> None:
+        """``n`` steps of every active world (capacity regrowth handled inside)."""
+        self.ctx.call('step', int(n))
+        for w, dt in zip(self.worlds, self.dts):
+            w.time += n * dt
+
+    def step_async(self, n: int = 1) -> None:
+        self.ctx.call('step_async', int(n))
+
+    def sync(self) -> None:
+        self.ctx.call('sync')
+
+    def set_active(self, mask: Sequence[bool]) -> None:
+        a = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        self.ctx.call('set_active', ptr(a, U8))
+
+    def refresh_params(self) -> None:
+        """Push dt, iteration counts and flags read from the world objects."""
+        dt = np.array(self.dts, 'd')
+        it = np.array([world_iterations(w) for w in self.worlds], np.int32)
+        jit = np.array([int(w.joint_iterations) for w in self.worlds], np.int32)
+        fl = np.array([world_flags(w) for w in self.worlds], np.int32)
+        self.ctx.call('set_world_params', ptr(dt, D), ptr(it, I), ptr(jit, I), ptr(fl, I))
+
+    # -- state ------------------------------------------------------------------
+    def upload_state(self, i: int) -> None:
+        """Host columns of world ``i`` -> device (pos, q, v, w, awake, sleep timer)."""
+        w = self.worlds[i]
+        n = w.body_count
+        b0 = self.offsets[i]
+        self.ctx.call('upload_state', b0, n, ptr(w._position, D), ptr(w._orientation, D),
+                      ptr(w._linear_velocity, D), ptr(w._angular_velocity, D),
+                      ptr(w._awake.view(np.uint8), U8), ptr(w._sleep_timer, D))
+
+    def download_state(self, i: int) -> None:
+        """Device -> host columns of world ``i`` (state and AABBs)."""
+        w = self.worlds[i]
+        n = w.body_count
+        b0 = self.offsets[i]
+        self.ctx.call('download_state', b0, n, ptr(w._position, D), ptr(w._orientation, D),
+                      ptr(w._linear_velocity, D), ptr(w._angular_velocity, D),
+                      ptr(w._awake.view(np.uint8), U8), ptr(w._sleep_timer, D),
+                      ptr(w._aabb_min, D), ptr(w._aabb_max, D))
+
+    def download_joints(self) -> None:
+        """Copy the lazily fixed joint state back onto the constraint objects."""
+        J = self.packed.n_joints
+        if J == 0:
+            return
+        la = np.zeros((J, 3)); lb = np.zeros((J, 3)); ln = np.zeros(J); acc = np.zeros(J)
+        hla = np.zeros(J, np.uint8); hlb = np.zeros(J, np.uint8); hln = np.zeros(J, np.uint8)
+        self.ctx.call('download_joints', ptr(la, D), ptr(lb, D), ptr(hla, U8), ptr(hlb, U8),
+                      ptr(ln, D), ptr(hln, U8), ptr(acc, D))
+        for wi, world in enumerate(self.worlds):
+            j0 = self.joint_offsets[wi]
+            for k, c in enumerate(world.joint_constraints):
+                j = j0 + k
+                kind = joint_kind(c)
+                if kind == 'motor':
+                    c.accum = float(acc[j])
+                elif kind == 'distance':
+                    if hln[j]:
+                        c.length = float(ln[j])
+                else:
+                    if hla[j]:
+                        c.local_a = la[j].copy()
+                    if hlb[j]:
+                        c.local_b = lb[j].copy()
+
+    def sync_to_host(self) -> None:
+        for i in range(len(self.worlds)):
+            self.download_state(i)
+        self.download_joints()
+
+    # -- results of the last step ------------------------------------------------
+    def counts(self):
+        W = len(self.worlds)
+        p = np.zeros(W, np.int32); c = np.zeros(W, np.int32)
+        self.ctx.call('counts', ptr(p, I), ptr(c, I))
+        return p, c
+
+    def pairs(self, i: int) -> np.ndarray:
+        """Broadphase pairs of world ``i`` (world-local indices), reference order."""
+        p, _ = self.counts()
+        out = np.zeros((max(int(p[i]), 1), 2), np.int32)
+        n = self.ctx.call('get_pairs', i, ptr(out, I), out.shape[0])
+        return out[:n] - self.offsets[i]
+
+    def contact_arrays(self, i: int) -> dict:
+        _, c = self.counts()
+        K = max(int(c[i]), 1)
+        a = np.zeros(K, np.int32); b = np.zeros(K, np.int32)
+        pt = np.zeros((K, 3)); nr = np.zeros((K, 3)); dp = np.zeros(K); imp = np.zeros((K, 3))
+        n = self.ctx.call('get_contacts', i, ptr(a, I), ptr(b, I), ptr(pt, D), ptr(nr, D),
+                          ptr(dp, D), ptr(imp, D), K)
+        off = self.offsets[i]
+        return dict(a=a[:n] - off, b=b[:n] - off, point=pt[:n], normal=nr[:n], depth=dp[:n],
+                    impulse=imp[:n])
+
+    def contacts(self, i: int) -> List[Contact]:
+        d = self.contact_arrays(i)
+        return [Contact(int(d['a'][k]), int(d['b'][k]), d['point'][k], d['normal'][k],
+                        float(d['depth'][k]), float(d['impulse'][k, 0]), d['impulse'][k, 1:].copy())
+                for k in range(len(d['a']))]
+
+    def islands(self, i: int) -> np.ndarray:
+        """Sleep-island label per body of world ``i`` (-1: not in contact)."""
+        n = self.worlds[i].body_count
+        lab = np.zeros(max(n, 1), np.int32)
+        self.ctx.call('get_islands', i, ptr(lab, I))
+        lab = lab[:n]
+        return np.where(lab >= 0, lab - self.offsets[i], -1)
+
+    def set_cache(self, i: int, a, b, point, impulse) -> None:
+        off = self.offsets[i]
+        a = np.ascontiguousarray(np.asarray(a, np.int32) + off)
+        b = np.ascontiguousarray(np.asarray(b, np.int32) + off)
+        point = np.ascontiguousarray(point, 'd').reshape(-1, 3)
+        impulse = np.ascontiguousarray(impulse, 'd').reshape(-1, 3)
+        self.ctx.call('set_cache', i, len(a), ptr(a, I), ptr(b, I), ptr(point, D), ptr(impulse, D))
+
+    def cache(self, i: int) -> dict:
+        cap = 1 << 16
+        while True:
+            a = np.zeros(cap, np.int32); b = np.zeros(cap, np.int32)
+            pt = np.zeros((cap, 3)); imp = np.zeros((cap, 3))
+            rc = self.ctx.lib.omi_get_cache(self.ctx.h, i, ptr(a, I), ptr(b, I), ptr(pt, D),
+                                            ptr(imp, D), cap)
+            if rc == -2 and cap < (1 << 26):
+                cap *= 8
+                continue
+            n = self.ctx.check(rc, 'omi_get_cache')
+            off = self.offsets[i]
+            return dict(a=a[:n] - off, b=b[:n] - off, point=pt[:n], impulse=imp[:n])
+
+    def profile(self) -> dict:
+        """Per-stage device milliseconds of one eagerly launched step."""
+        return self.ctx.profile_step()

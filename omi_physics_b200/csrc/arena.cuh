@@ -1,0 +1,118 @@
+// Device arena: every world of a context, concatenated body-row ranges in a
+// structure-of-arrays layout (the reference's numpy columns, world.py:75-122),
+// plus the per-step scratch of each stage. Passed to kernels by value.
+#pragma once
+#include <cstdint>
+
+namespace omi {
+
+// per-contact prepared solver row (AoS, CD doubles): rA, rB, n, t1, t2,
+// nMass, t1Mass, t2Mass, vBias, friction, inv mass a, inv mass b
+constexpr int CD = 24;
+// per-joint prepared row: invIa(9) invIb(9) rA(3) rB(3) K/LU(9) piv(3) bias(3)
+// n(3) mass bias_s
+constexpr int JD = 48;
+// narrowphase slot per pair: normal(3) + 4 x (point(3), depth)
+constexpr int SLOT = 3 + 16;
+
+// status words (device int array)
+enum {
+    ST_STEPS_DONE = 0,   // completed steps since the host last reset it
+    ST_OVERFLOW = 1,     // 1 when a step found more pairs than pair_cap
+    ST_PAIRS_NEEDED = 2, // pair count that overflowed
+    ST_EPA_LIMIT = 3,    // EPA polytope exceeded its bounded storage
+    ST_CASCADE = 4,      // wake cascades resolved sequentially (diagnostic)
+    ST_GJK_ITEMS = 5,    // convex pairs routed to GJK/EPA in the last step
+    ST_CONTACTS_NEEDED = 6,
+    ST_WORDS = 8
+};
+
+struct Arena {
+    int W, NB, NS, NM, NJ, NPTS;
+    int pair_cap, contact_cap, hash_mask;
+
+    // worlds
+    const int *w_body_off;          // row range of each world (its capacity)
+    const int *w_body_n;            // live rows of each world (<= capacity)
+    const int *w_joint_n;           // live joints of each world
+    const double *w_g, *w_dt;
+    const int *w_iters, *w_jiters;
+    const int *w_flags;
+    const uint8_t *w_active;
+    const double *w_def_damp, *w_solver;
+    const int *w_filter_off, *w_filter_rows, *w_pf_off, *w_pf_n, *w_joint_off;
+
+    // bodies
+    double *pos, *q, *v, *w, *prev_pos, *prev_q;
+    const double *inv_mass, *inv_inertia, *gf, *ld, *ad, *qd;
+    double *timer;
+    uint8_t *awake;
+    const int *mtype, *shape, *material, *material_key, *filter_row, *body_world;
+    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 other (convex)
+    const double *half;      // refit half extents (world.py:443-469)
+    double *aabb_min, *aabb_max, *invIw;
+
+    // shapes / materials / filters
+    const int *shape_type;
+    const double *shape_radius, *shape_size;
+    const int *pt_off, *pt_cnt;
+    const double *points;
+    const double *mat_dynf, *mat_rest;
+    const int *mat_fcomb, *mat_rcomb;
+    const int *pf_a, *pf_b;
+    const double *pf_mu;
+    const uint8_t *filter_matrix;
+
+    // joints
+    const int *j_type, *j_a, *j_b;
+    const double *j_anchor, *j_anchor_b, *j_axis, *j_target, *j_max_force;
+    double *j_local_a, *j_local_b, *j_length, *j_accum;
+    uint8_t *j_has_local_a, *j_has_local_b, *j_has_length;
+    double *j_data;
+    int *j_level, *j_order, *j_level_start;
+
+    // broadphase
+    int *order;              // sorted global body index per row (per world range)
+    double *sorted_x;
+    double *sort_k[2];
+    int *sort_v[2];
+    int *pair_cnt, *pair_scan;      // NB, NB+1
+    int *pair_a, *pair_b;           // pair_cap
+    uint8_t *pair_solid;
+
+    // narrowphase
+    int *slot_cnt;                  // pair_cap (+1 scratch)
+    double *slot;                   // pair_cap * SLOT
+    int *gjk_list, *gjk_n;
+    int *contact_scan;              // pair_cap + 1
+
+    // contacts
+    int *c_a, *c_b;
+    double *c_pt, *c_n, *c_depth, *c_imp, *c_data;
+    int *c_level, *c_order, *c_level_start;
+
+    // per-body scratch
+    int *b_last, *b_parent, *b_island;
+    int *b_flag;
+
+    // warm-start cache (ping-pong) and its hash tables
+    int *cache_a[2], *cache_b[2];
+    double *cache_pt[2], *cache_imp[2];
+    int *w_cache_off[2], *w_cache_n[2];
+    unsigned long long *hkey[2];
+    int *hval[2];                   // packed start, count (2 ints per slot)
+    int *hused[2], *hused_n;        // slots written by each table's last build; [2] = to clear
+    int *parity;                    // current cache buffer (device)
+    int *w_cache_new;               // W+1 scan scratch
+
+    // scan scratch
+    int *scan_blocks;
+
+    int *status;
+};
+
+__host__ __device__ inline bool world_active(const Arena &A, int w) {
+    return A.w_active[w] != 0;
+}
+
+}  // namespace omi

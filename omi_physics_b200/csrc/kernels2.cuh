@@ -1,0 +1,477 @@
+// Warm-start cache store, joints, and the integrate-positions + sleep pass.
+#pragma once
+#include "kernels.cuh"
+
+namespace omi {
+
+// ---------------------------------------------------------------------------
+// warm-start cache (solver.py:91, 271-278). A world that had contacts this
+// step (and warm starting on) replaces its cache with them; any other world
+// keeps its previous cache, as the reference does when solve() returns early.
+// The cache is double-buffered; a hash table per buffer maps a body pair to
+// its run of entries.
+// ---------------------------------------------------------------------------
+__global__ void k_cache_plan(Arena A) {   // one CTA
+    __shared__ int sh[32];
+    if (overflowed(A)) return;
+    const int cur = *A.parity, nxt = 1 - cur;
+    int carry = 0;
+    for (int base = 0; base < A.W; base += blockDim.x) {
+        const int w = base + threadIdx.x;
+        int n_new = 0;
+        if (w < A.W) {
+            int K = 0;
+            if (world_collides(A, w)) {
+                int c0, c1;
+                world_contacts(A, w, c0, c1);
+                K = c1 - c0;
+            }
+            const bool refresh = K > 0 && (A.w_flags[w] & WF_WARM) && world_collides(A, w);
+            n_new = refresh ? K : A.w_cache_n[cur][w];
+            A.w_cache_new[w] = refresh ? 1 : 0;
+        }
+        int total;
+        const int pre = block_exclusive_scan(n_new, sh, &total) + carry;
+        if (w < A.W) { A.w_cache_off[nxt][w] = pre; A.w_cache_n[nxt][w] = n_new; }
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        A.hused_n[2] = A.hused_n[nxt];   // slots of table nxt to clear
+        A.hused_n[nxt] = 0;
+    }
+}
+
+__global__ void k_hash_clear(Arena A) {
+    if (overflowed(A)) return;
+    const int nxt = 1 - *A.parity;
+    const int n = A.hused_n[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        A.hkey[nxt][A.hused[nxt][i]] = ~0ull;
+}
+
+__global__ void k_cache_copy(Arena A) {   // CTA per world
+    if (overflowed(A)) return;
+    const int cur = *A.parity, nxt = 1 - cur;
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
+        const int dst = A.w_cache_off[nxt][w], n = A.w_cache_n[nxt][w];
+        if (A.w_cache_new[w]) {
+            int c0, c1;
+            world_contacts(A, w, c0, c1);
+            for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                const int k = c0 + e, d = dst + e;
+                A.cache_a[nxt][d] = A.c_a[k];
+                A.cache_b[nxt][d] = A.c_b[k];
+                for (int c = 0; c < 3; c++) {
+                    A.cache_pt[nxt][d * 3 + c] = A.c_pt[k * 3 + c];
+                    A.cache_imp[nxt][d * 3 + c] = A.c_imp[k * 3 + c];
+                }
+            }
+        } else {
+            const int src = A.w_cache_off[cur][w];
+            for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                const int s = src + e, d = dst + e;
+                A.cache_a[nxt][d] = A.cache_a[cur][s];
+                A.cache_b[nxt][d] = A.cache_b[cur][s];
+                for (int c = 0; c < 3; c++) {
+                    A.cache_pt[nxt][d * 3 + c] = A.cache_pt[cur][s * 3 + c];
+                    A.cache_imp[nxt][d * 3 + c] = A.cache_imp[cur][s * 3 + c];
+                }
+            }
+        }
+    }
+}
+
+// insert one key per run of equal (a, b) entries into table t
+__device__ inline void hash_runs(const Arena &A, int t, int w) {
+    const int off = A.w_cache_off[t][w], n = A.w_cache_n[t][w];
+    const int *ca = A.cache_a[t], *cb = A.cache_b[t];
+    for (int e = off + threadIdx.x; e < off + n; e += blockDim.x) {
+        if (e > off && ca[e] == ca[e - 1] && cb[e] == cb[e - 1]) continue;
+        int len = 1;
+        while (e + len < off + n && ca[e + len] == ca[e] && cb[e + len] == cb[e]) len++;
+        const unsigned long long key = pair_key(ca[e], cb[e]);
+        int s = hash_slot(key, A.hash_mask);
+        for (int probe = 0; probe <= A.hash_mask; probe++) {
+            const unsigned long long prev = atomicCAS(&A.hkey[t][s], ~0ull, key);
+            if (prev == ~0ull || prev == key) {
+                A.hval[t][s * 2] = e;
+                A.hval[t][s * 2 + 1] = len;
+                if (prev == ~0ull) A.hused[t][atomicAdd(&A.hused_n[t], 1)] = s;
+                break;
+            }
+            s = (s + 1) & A.hash_mask;
+        }
+    }
+}
+
+__global__ void k_hash_build(Arena A) {   // CTA per world, table = next buffer
+    if (overflowed(A)) return;
+    const int nxt = 1 - *A.parity;
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) hash_runs(A, nxt, w);
+}
+
+__global__ void k_flip(Arena A) {
+    if (overflowed(A)) return;
+    *A.parity = 1 - *A.parity;
+}
+
+// rebuild table t from cache buffer t (after the host regrows the tables)
+__global__ void k_hash_rebuild(Arena A, int t) {
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) hash_runs(A, t, w);
+}
+
+// ---------------------------------------------------------------------------
+// joints (world.py:599-611, joints.py:60-212), one CTA per world; prepare in
+// parallel, then joint_iterations sweeps in registration order by levels
+// ---------------------------------------------------------------------------
+enum { J_IA = 0, J_IB = 9, J_RA = 18, J_RB = 21, J_LU = 24, J_PIV = 33, J_BIAS = 36, J_N = 39,
+       J_MASS = 42, J_BIASS = 43 };
+
+// joints.py:278-283: (R * invI) @ R.T through BLAS; zero for the world (-1)
+__device__ inline void joint_inv_inertia(const Arena &A, int i, double *W) {
+    if (i < 0) { for (int q = 0; q < 9; q++) W[q] = 0.0; return; }
+    double R[9], s[9];
+    quat_to_matrix(&A.q[i * 4], R);
+    const double *ii = &A.inv_inertia[i * 3];
+    for (int r = 0; r < 3; r++)
+        for (int j = 0; j < 3; j++) s[r * 3 + j] = R[r * 3 + j] * ii[j];
+    for (int r = 0; r < 3; r++)
+        for (int k = 0; k < 3; k++) W[r * 3 + k] = dot_blas(&s[r * 3], &R[k * 3]);
+}
+
+__device__ inline void mat3_mul(const double *X, const double *Y, double *Z) {
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) {
+            const double col[3] = {Y[k], Y[3 + k], Y[6 + k]};
+            Z[i * 3 + k] = dot_blas(&X[i * 3], col);
+        }
+}
+
+__device__ inline void skew(const double *r, double *S) {
+    S[0] = 0.0; S[1] = -r[2]; S[2] = r[1];
+    S[3] = r[2]; S[4] = 0.0; S[5] = -r[0];
+    S[6] = -r[1]; S[7] = r[0]; S[8] = 0.0;
+}
+
+__device__ inline void joint_prepare(const Arena &A, int j) {
+    double *D = &A.j_data[(size_t)j * JD];
+    const int t = A.j_type[j];
+    if (t == 2) {                                    // AngularMotor.prepare
+        const int body = A.j_a[j];
+        joint_inv_inertia(A, body, &D[J_IA]);
+        const double *ax = &A.j_axis[j * 3];
+        double u[3];
+        for (int k = 0; k < 3; k++) {
+            const double col[3] = {D[J_IA + k], D[J_IA + 3 + k], D[J_IA + 6 + k]};
+            u[k] = dot_blas(ax, col);
+        }
+        const double eff = dot_blas(u, ax);
+        D[J_MASS] = eff > 1e-12 ? 1.0 / eff : 0.0;
+        A.j_accum[j] = 0.0;
+        return;
+    }
+    const int a = A.j_a[j], b = A.j_b[j];
+    joint_inv_inertia(A, a, &D[J_IA]);
+    joint_inv_inertia(A, b, &D[J_IB]);
+    if (t == 0) {                                    // PointConstraint.prepare
+        const double *anchor = &A.j_anchor[j * 3];
+        const int ids[2] = {a, b};
+        double *locs[2] = {&A.j_local_a[j * 3], &A.j_local_b[j * 3]};
+        uint8_t *has[2] = {&A.j_has_local_a[j], &A.j_has_local_b[j]};
+        double posv[2][3];
+        for (int e = 0; e < 2; e++) {
+            const int i = ids[e];
+            double *r = &D[e == 0 ? J_RA : J_RB];
+            if (i < 0) {
+                for (int k = 0; k < 3; k++) { posv[e][k] = anchor[k]; r[k] = anchor[k] - anchor[k]; }
+                continue;
+            }
+            double R[9];
+            quat_to_matrix(&A.q[i * 4], R);
+            if (!*has[e]) {                          // _to_local: R.T @ (anchor - pos)
+                double dd[3];
+                sub3(anchor, &A.pos[i * 3], dd);
+                for (int k = 0; k < 3; k++) {
+                    const double col[3] = {R[k], R[3 + k], R[6 + k]};
+                    locs[e][k] = dot_blas(col, dd);
+                }
+                *has[e] = 1;
+            }
+            for (int k = 0; k < 3; k++) {
+                posv[e][k] = A.pos[i * 3 + k];
+                r[k] = (A.pos[i * 3 + k] + gemv_row(&R[k * 3], locs[e])) - posv[e][k];
+            }
+        }
+        const double im = (a < 0 ? 0.0 : A.inv_mass[a]) + (b < 0 ? 0.0 : A.inv_mass[b]);
+        double K[9], S[9], T[9], M[9];
+        for (int q = 0; q < 9; q++) K[q] = (q % 4 == 0) ? im * 1.0 : im * 0.0;
+        skew(&D[J_RA], S); mat3_mul(S, &D[J_IA], T); mat3_mul(T, S, M);
+        for (int q = 0; q < 9; q++) K[q] = K[q] - M[q];
+        skew(&D[J_RB], S); mat3_mul(S, &D[J_IB], T); mat3_mul(T, S, M);
+        for (int q = 0; q < 9; q++) K[q] = K[q] - M[q];
+        for (int k = 0; k < 3; k++) {
+            const double pa = posv[0][k] + D[J_RA + k], pb = posv[1][k] + D[J_RB + k];
+            D[J_BIAS + k] = 0.2 * (pb - pa);
+        }
+        // LU with partial pivoting of K, kept for every iteration's solve
+        for (int jj = 0; jj < 3; jj++) {
+            int p = jj;
+            double best = fabs(K[jj * 3 + jj]);
+            for (int i = jj + 1; i < 3; i++)
+                if (fabs(K[i * 3 + jj]) > best) { best = fabs(K[i * 3 + jj]); p = i; }
+            D[J_PIV + jj] = (double)p;
+            if (p != jj)
+                for (int k = 0; k < 3; k++) { const double tt = K[jj * 3 + k]; K[jj * 3 + k] = K[p * 3 + k]; K[p * 3 + k] = tt; }
+            for (int i = jj + 1; i < 3; i++) {
+                const double l = K[i * 3 + jj] / K[jj * 3 + jj];
+                K[i * 3 + jj] = l;
+                for (int k = jj + 1; k < 3; k++) K[i * 3 + k] = fma(-l, K[jj * 3 + k], K[i * 3 + k]);
+            }
+        }
+        for (int q = 0; q < 9; q++) D[J_LU + q] = K[q];
+        return;
+    }
+    // DistanceConstraint.prepare
+    const double *la = &A.j_anchor[j * 3], *lb = &A.j_anchor_b[j * 3];
+    double pa[3], pb[3], d[3];
+    for (int e = 0; e < 2; e++) {
+        const int i = e == 0 ? a : b;
+        const double *loc = e == 0 ? la : lb;
+        double *out = e == 0 ? pa : pb;
+        if (i < 0) { for (int k = 0; k < 3; k++) out[k] = loc[k]; }
+        else {
+            double R[9];
+            quat_to_matrix(&A.q[i * 4], R);
+            for (int k = 0; k < 3; k++) out[k] = A.pos[i * 3 + k] + gemv_row(&R[k * 3], loc);
+        }
+    }
+    sub3(pb, pa, d);
+    const double dist = sqrt(dot_blas(d, d));
+    double *n = &D[J_N];
+    if (dist > 1e-9) { for (int k = 0; k < 3; k++) n[k] = d[k] / dist; }
+    else { n[0] = 0.0; n[1] = 1.0; n[2] = 0.0; }
+    if (!A.j_has_length[j]) { A.j_length[j] = dist; A.j_has_length[j] = 1; }
+    for (int k = 0; k < 3; k++) {
+        D[J_RA + k] = pa[k] - (a < 0 ? la[k] : A.pos[a * 3 + k]);
+        D[J_RB + k] = pb[k] - (b < 0 ? la[k] : A.pos[b * 3 + k]);
+    }
+    double raxn[3], rbxn[3], u[3];
+    cross_np(&D[J_RA], n, raxn);
+    cross_np(&D[J_RB], n, rbxn);
+    double k = (a < 0 ? 0.0 : A.inv_mass[a]) + (b < 0 ? 0.0 : A.inv_mass[b]);
+    for (int q = 0; q < 3; q++) { const double col[3] = {D[J_IA + q], D[J_IA + 3 + q], D[J_IA + 6 + q]}; u[q] = dot_blas(raxn, col); }
+    k += dot_blas(u, raxn);
+    for (int q = 0; q < 3; q++) { const double col[3] = {D[J_IB + q], D[J_IB + 3 + q], D[J_IB + 6 + q]}; u[q] = dot_blas(rbxn, col); }
+    k += dot_blas(u, rbxn);
+    D[J_MASS] = k > 1e-12 ? 1.0 / k : 0.0;
+    D[J_BIASS] = 0.2 * (dist - A.j_length[j]);
+}
+
+__device__ inline void joint_apply(const Arena &A, int i, const double *invI, const double *r,
+                                   const double *P) {
+    if (i < 0 || A.mtype[i] != 2) return;
+    for (int q = 0; q < 3; q++) A.v[i * 3 + q] = A.v[i * 3 + q] + A.inv_mass[i] * P[q];
+    double c[3];
+    cross_np(r, P, c);
+    for (int q = 0; q < 3; q++) A.w[i * 3 + q] = A.w[i * 3 + q] + gemv_row(&invI[q * 3], c);
+}
+
+__device__ inline void joint_solve(const Arena &A, int j, double dt) {
+    const double *D = &A.j_data[(size_t)j * JD];
+    const int t = A.j_type[j];
+    if (t == 2) {                                    // AngularMotor.solve
+        const int body = A.j_a[j];
+        if (body < 0) return;
+        const double *ax = &A.j_axis[j * 3];
+        const double wv = dot_blas(&A.w[body * 3], ax);
+        double impulse = D[J_MASS] * (A.j_target[j] - wv);
+        const double limit = A.j_max_force[j] * dt;
+        double nw = A.j_accum[j] + impulse;
+        if (nw < -limit) nw = -limit;
+        if (nw > limit) nw = limit;
+        impulse = nw - A.j_accum[j];
+        A.j_accum[j] = nw;
+        if (A.mtype[body] != 2) return;
+        const double P[3] = {ax[0] * impulse, ax[1] * impulse, ax[2] * impulse};
+        for (int q = 0; q < 3; q++) A.w[body * 3 + q] = A.w[body * 3 + q] + gemv_row(&D[J_IA + q * 3], P);
+        return;
+    }
+    const int a = A.j_a[j], b = A.j_b[j];
+    double va[3] = {0.0, 0.0, 0.0}, vb[3] = {0.0, 0.0, 0.0}, P[3], nP[3], c[3];
+    if (b >= 0) { cross_np(&A.w[b * 3], &D[J_RB], c); for (int q = 0; q < 3; q++) vb[q] = A.v[b * 3 + q] + c[q]; }
+    if (a >= 0) { cross_np(&A.w[a * 3], &D[J_RA], c); for (int q = 0; q < 3; q++) va[q] = A.v[a * 3 + q] + c[q]; }
+    if (t == 0) {                                    // PointConstraint.solve
+        double x[3];
+        for (int q = 0; q < 3; q++) x[q] = -((vb[q] - va[q]) + D[J_BIAS + q] / dt);
+        for (int jj = 0; jj < 3; jj++) {
+            const int p = (int)D[J_PIV + jj];
+            if (p != jj) { const double tt = x[jj]; x[jj] = x[p]; x[p] = tt; }
+        }
+        const double *L = &D[J_LU];
+        for (int i = 0; i < 3; i++)
+            for (int k = 0; k < i; k++) x[i] = fma(-L[i * 3 + k], x[k], x[i]);
+        for (int i = 2; i >= 0; i--) {
+            for (int k = i + 1; k < 3; k++) x[i] = fma(-L[i * 3 + k], x[k], x[i]);
+            x[i] = x[i] / L[i * 3 + i];
+        }
+        P[0] = x[0]; P[1] = x[1]; P[2] = x[2];
+    } else {                                         // DistanceConstraint.solve
+        double dv[3];
+        sub3(vb, va, dv);
+        const double cdot = dot_blas(dv, &D[J_N]);
+        const double impulse = -D[J_MASS] * (cdot + D[J_BIASS] / dt);
+        for (int q = 0; q < 3; q++) P[q] = impulse * D[J_N + q];
+    }
+    neg3(P, nP);
+    joint_apply(A, a, &D[J_IA], &D[J_RA], nP);
+    joint_apply(A, b, &D[J_IB], &D[J_RB], P);
+}
+
+__global__ void k_joints(Arena A, int gated) {
+    __shared__ int s_D;
+    if (gated && overflowed(A)) return;
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
+        if (!A.w_active[w]) continue;
+        const int j0 = A.w_joint_off[w], J = A.w_joint_n[w], j1 = j0 + J;
+        if (J == 0) continue;
+        const double dt = A.w_dt[w];
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            if (A.j_type[j] == 2) { if (A.j_a[j] >= 0) wake_body(A, A.j_a[j]); }
+            else {
+                if (A.j_a[j] >= 0) wake_body(A, A.j_a[j]);
+                if (A.j_b[j] >= 0) wake_body(A, A.j_b[j]);
+            }
+            joint_prepare(A, j);
+        }
+        const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_last[i] = -1;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int D = warp_levels(J, A.j_a + j0, A.j_b + j0, A.mtype, A.b_last, A.j_level + j0);
+            if (threadIdx.x == 0) s_D = D;
+        }
+        __syncthreads();
+        const int D = s_D;
+        int *ls = A.j_level_start + j0 + w;
+        int *cursor = A.j_level_start + (A.NJ + A.W + 1) + j0 + w;
+        int *order = A.j_order + j0;
+        bucket_levels(J, D, A.j_level + j0, ls, cursor, order);
+        const int iters = A.w_jiters[w];
+        for (int it = 0; it < iters; it++) {
+            for (int l = 0; l < D; l++) {
+                for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) joint_solve(A, j0 + order[q], dt);
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// integrate positions (backend.py:42-49, mathutil.py:32-41,108-113) and
+// island sleeping (world.py:510-567), one CTA per world
+// ---------------------------------------------------------------------------
+enum { BF_SLOW = 1, BF_READY = 2, BF_CONTACTED = 4, BF_NOTREADY = 8 };
+enum { FIN_POSITIONS = 1, FIN_SLEEP = 2, FIN_COUNT = 4, FIN_GATED = 8 };
+
+__device__ inline int uf_find(int *parent, int x) {
+    volatile int *p = parent;
+    while (true) {
+        const int px = p[x];
+        if (px == x) return x;
+        const int gp = p[px];
+        if (gp != px) p[x] = gp;
+        x = px;
+    }
+}
+
+__device__ inline void uf_union(int *parent, int a, int b) {
+    while (true) {
+        a = uf_find(parent, a);
+        b = uf_find(parent, b);
+        if (a == b) return;
+        if (a > b) { const int t = a; a = b; b = t; }
+        if (atomicCAS(&parent[b], b, a) == b) return;
+    }
+}
+
+__global__ void k_finalize(Arena A, int mode) {
+    if ((mode & FIN_GATED) && overflowed(A)) return;
+    if ((mode & FIN_COUNT) && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.status[ST_STEPS_DONE], 1);
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
+        if (!A.w_active[w]) continue;
+        const double dt = A.w_dt[w];
+        const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
+        if (mode & FIN_POSITIONS) {
+            for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+                const int t = A.mtype[i];
+                if (!((t == 2 || t == 1) && A.awake[i])) continue;
+                double *p = &A.pos[i * 3], *q = &A.q[i * 4];
+                const double *v = &A.v[i * 3], *om = &A.w[i * 3];
+                for (int c = 0; c < 3; c++) p[c] = p[c] + v[c] * dt;
+                const double ax = om[0], ay = om[1], az = om[2], aw = 0.0;
+                const double bx = q[0], by = q[1], bz = q[2], bw = q[3];
+                double m[4];
+                m[0] = aw * bx + ax * bw + ay * bz - az * by;
+                m[1] = aw * by - ax * bz + ay * bw + az * bx;
+                m[2] = aw * bz + ax * by - ay * bx + az * bw;
+                m[3] = aw * bw - ax * bx - ay * by - az * bz;
+                double s[4];
+                for (int c = 0; c < 4; c++) s[c] = q[c] + (0.5 * m[c]) * dt;
+                const double n = sqrt(((s[0] * s[0] + s[1] * s[1]) + s[2] * s[2]) + s[3] * s[3]);
+                const double d = np_max(n, 1e-12);
+                for (int c = 0; c < 4; c++) q[c] = s[c] / d;
+            }
+        }
+        if (!(mode & FIN_SLEEP)) continue;
+        if (!(A.w_flags[w] & WF_SLEEP)) {
+            for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_island[i] = -1;
+            continue;
+        }
+        __syncthreads();
+        const double lin2 = 0.08 * 0.08, ang2 = 0.25 * 0.25;
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+            const bool dyn_i = A.mtype[i] == 2;
+            const bool slow = dyn_i && speed2(&A.v[i * 3]) < lin2 && speed2(&A.w[i * 3]) < ang2;
+            if (slow) A.timer[i] += dt; else A.timer[i] = 0.0;
+            const bool ready = slow && A.timer[i] > 0.4;
+            A.b_flag[i] = (slow ? BF_SLOW : 0) | (ready ? BF_READY : 0);
+            A.b_parent[i] = i;
+        }
+        __syncthreads();
+        if (world_collides(A, w)) {
+            int c0, c1;
+            world_contacts(A, w, c0, c1);
+            for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+                const int a = A.c_a[k], b = A.c_b[k];
+                const bool da = A.mtype[a] == 2, db = A.mtype[b] == 2;
+                if (da) atomicOr(&A.b_flag[a], BF_CONTACTED);
+                if (db) atomicOr(&A.b_flag[b], BF_CONTACTED);
+                if (da && db) uf_union(A.b_parent, a, b);
+            }
+        }
+        __syncthreads();
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_island[i] = uf_find(A.b_parent, i);
+        __syncthreads();
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+            const int f = ((volatile int *)A.b_flag)[i];
+            if ((f & BF_CONTACTED) && !(f & BF_READY)) atomicOr(&A.b_flag[A.b_island[i]], BF_NOTREADY);
+        }
+        __syncthreads();
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+            const int f = ((volatile int *)A.b_flag)[i];
+            const bool dyn_i = A.mtype[i] == 2;
+            bool to_sleep;
+            if (f & BF_CONTACTED) to_sleep = !(((volatile int *)A.b_flag)[A.b_island[i]] & BF_NOTREADY);
+            else to_sleep = dyn_i && (f & BF_READY);
+            if (!(f & BF_CONTACTED)) A.b_island[i] = -1;
+            if (to_sleep) A.awake[i] = 0;
+            if (dyn_i && !(f & BF_SLOW)) A.awake[i] = 1;
+            if (!A.awake[i] && dyn_i) {
+                for (int c = 0; c < 3; c++) { A.v[i * 3 + c] = 0.0; A.w[i * 3 + c] = 0.0; }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace omi

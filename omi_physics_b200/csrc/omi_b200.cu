@@ -1,0 +1,1241 @@
+// omi_b200: the C ABI (include/omi_b200.h) over the device arena.
+//
+// Host-side duties: own the device buffers and the stream, upload the scene
+// tables, run the step as a CUDA graph, regrow pair/contact capacities when a
+// step reports an overflow (the step is then re-run; nothing was modified),
+// and copy results back for the caller. All compute is in the kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/omi_b200.h"
+#include "kernels2.cuh"
+
+using namespace omi;
+
+namespace {
+
+enum KernelId {
+    KN_REFIT, KN_SORT, KN_PAIR_COUNT, KN_PAIR_SCAN, KN_PAIR_EMIT, KN_NARROW, KN_GJK,
+    KN_CONTACT_SCAN, KN_INTEGRATE_FORCES, KN_COMPACT, KN_SOLVE, KN_CACHE, KN_JOINTS,
+    KN_FINALIZE, KN_COUNT
+};
+const char *kKernelNames[KN_COUNT] = {
+    "refit", "sort", "pair_count", "pair_scan", "pair_emit", "narrow", "gjk_epa",
+    "contact_scan", "integrate_forces", "contact_compact", "solve", "cache_store", "joints",
+    "integrate_positions_sleep"};
+
+struct Buf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct OmiCtx {
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+    int64_t budget = 0;
+    std::vector<Buf> statics;      // scene tables and per-body arrays
+    std::vector<Buf> dyn;          // pair/contact sized buffers
+    std::vector<Buf> cache;        // warm-start cache buffers (preserved on growth)
+    int64_t bytes = 0;
+    Arena A{};
+    bool loaded = false;
+    int max_world_n = 0, max_world_j = 0, sort_cap = 0, sort_block = 256;
+    int solve_block = 128;
+    int cache_cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    int *h_status = nullptr;       // pinned mirror of the status words
+    int64_t launches = 0;
+    std::vector<float> prof_ms;
+    std::vector<uint8_t> h_active;
+    std::vector<int> h_body_off, h_body_n, h_joint_off;
+    bool slots = false;
+    OmiSlotCaps caps{};
+};
+
+namespace {
+
+int fail(OmiCtx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(OmiCtx *c, cudaError_t e, const char *where) {
+    return fail(c, OMI_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e__ = (call);                             \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, #call); \
+    } while (0)
+
+template <class T>
+int alloc(OmiCtx *ctx, std::vector<Buf> &pool, T *&out, size_t n) {
+    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    bytes = (bytes + 255) & ~size_t(255);
+    if (ctx->budget > 0 && ctx->bytes + (int64_t)bytes > ctx->budget)
+        return fail(ctx, OMI_E_OOM, "device budget exceeded allocating " + std::to_string(bytes) + " bytes");
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    e = cudaMemsetAsync(p, 0, bytes, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemset");
+    pool.push_back({p, bytes});
+    ctx->bytes += (int64_t)bytes;
+    out = static_cast<T *>(p);
+    return 0;
+}
+
+template <class T>
+int upload(OmiCtx *ctx, T *&out, const T *src, size_t n) {
+    int rc = alloc(ctx, ctx->statics, out, n);
+    if (rc) return rc;
+    if (src && n) {
+        cudaError_t e = cudaMemcpyAsync(out, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync H2D");
+    }
+    return 0;
+}
+
+void free_pool(OmiCtx *ctx, std::vector<Buf> &pool) {
+    for (auto &b : pool) {
+        cudaFree(b.p);
+        ctx->bytes -= (int64_t)b.bytes;
+    }
+    pool.clear();
+}
+
+void drop_graph(OmiCtx *ctx) {
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+}
+
+int grid_for(int n, int block, int cap) {
+    int g = (n + block - 1) / block;
+    return std::max(1, std::min(g, cap));
+}
+
+int hash_bits_for(int runs) {
+    int bits = 10;
+    while ((1 << bits) < 2 * runs) bits++;
+    return bits;
+}
+
+// (re)allocate the pair/contact-sized buffers; the warm-start cache survives
+int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
+    drop_graph(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    free_pool(ctx, ctx->dyn);
+    Arena &A = ctx->A;
+    A.pair_cap = pair_cap;
+    A.contact_cap = contact_cap;
+    int rc = 0;
+    rc |= alloc(ctx, ctx->dyn, A.pair_a, pair_cap);
+    rc |= alloc(ctx, ctx->dyn, A.pair_b, pair_cap);
+    rc |= alloc(ctx, ctx->dyn, A.pair_solid, pair_cap);
+    rc |= alloc(ctx, ctx->dyn, A.slot_cnt, (size_t)pair_cap + 1);
+    rc |= alloc(ctx, ctx->dyn, A.slot, (size_t)pair_cap * SLOT);
+    rc |= alloc(ctx, ctx->dyn, A.gjk_list, pair_cap);
+    rc |= alloc(ctx, ctx->dyn, A.contact_scan, (size_t)pair_cap + 1);
+    rc |= alloc(ctx, ctx->dyn, A.c_a, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.c_b, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.c_pt, (size_t)contact_cap * 3);
+    rc |= alloc(ctx, ctx->dyn, A.c_n, (size_t)contact_cap * 3);
+    rc |= alloc(ctx, ctx->dyn, A.c_depth, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.c_imp, (size_t)contact_cap * 3);
+    rc |= alloc(ctx, ctx->dyn, A.c_data, (size_t)contact_cap * CD);
+    rc |= alloc(ctx, ctx->dyn, A.c_level, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.c_order, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.c_level_start, 2 * ((size_t)contact_cap + A.W + 1));
+    size_t scan_n = std::max<size_t>((size_t)pair_cap, (size_t)A.NB) / SCAN_TILE + 2;
+    rc |= alloc(ctx, ctx->dyn, A.scan_blocks, scan_n + 1);
+    if (rc) return rc;
+    // warm-start cache: up to one step's contacts plus worlds keeping old ones
+    const int want_cache = 2 * contact_cap;
+    if (want_cache > ctx->cache_cap) {
+        std::vector<Buf> old = ctx->cache;
+        Arena prev = A;
+        const int prev_cap = ctx->cache_cap;
+        ctx->cache.clear();
+        for (int t = 0; t < 2; t++) {
+            rc |= alloc(ctx, ctx->cache, A.cache_a[t], want_cache);
+            rc |= alloc(ctx, ctx->cache, A.cache_b[t], want_cache);
+            rc |= alloc(ctx, ctx->cache, A.cache_pt[t], (size_t)want_cache * 3);
+            rc |= alloc(ctx, ctx->cache, A.cache_imp[t], (size_t)want_cache * 3);
+            rc |= alloc(ctx, ctx->cache, A.hused[t], want_cache);
+        }
+        const int bits = hash_bits_for(want_cache);
+        A.hash_mask = (1 << bits) - 1;
+        for (int t = 0; t < 2; t++) {
+            rc |= alloc(ctx, ctx->cache, A.hkey[t], (size_t)1 << bits);
+            rc |= alloc(ctx, ctx->cache, A.hval[t], (size_t)2 << bits);
+        }
+        if (rc) return rc;
+        for (int t = 0; t < 2; t++) {
+            CK(cudaMemsetAsync(A.hkey[t], 0xff, sizeof(unsigned long long) << bits, ctx->stream));
+            if (prev_cap > 0) {
+                CK(cudaMemcpyAsync(A.cache_a[t], prev.cache_a[t], sizeof(int) * prev_cap, cudaMemcpyDeviceToDevice, ctx->stream));
+                CK(cudaMemcpyAsync(A.cache_b[t], prev.cache_b[t], sizeof(int) * prev_cap, cudaMemcpyDeviceToDevice, ctx->stream));
+                CK(cudaMemcpyAsync(A.cache_pt[t], prev.cache_pt[t], sizeof(double) * 3 * prev_cap, cudaMemcpyDeviceToDevice, ctx->stream));
+                CK(cudaMemcpyAsync(A.cache_imp[t], prev.cache_imp[t], sizeof(double) * 3 * prev_cap, cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+        }
+        CK(cudaMemsetAsync(A.hused_n, 0, sizeof(int) * 4, ctx->stream));
+        ctx->cache_cap = want_cache;
+        cudaStreamSynchronize(ctx->stream);
+        for (auto &b : old) { cudaFree(b.p); ctx->bytes -= (int64_t)b.bytes; }
+        for (int t = 0; t < 2; t++) {
+            k_hash_rebuild<<<std::max(1, A.W), 128, 0, ctx->stream>>>(A, t);
+            ctx->launches++;
+        }
+        CK(cudaGetLastError());
+    }
+    return 0;
+}
+
+void launch_scan(OmiCtx *ctx, const int *in, int *out, int n_const, const int *n_ptr, int cap,
+                 const int *gate_scan, int gate_idx, int gate_cap) {
+    const int tiles = std::max(1, (cap + SCAN_TILE - 1) / SCAN_TILE);
+    k_scan_tiles<<<tiles, 1024, 0, ctx->stream>>>(in, out, n_const, n_ptr, gate_scan, gate_idx, gate_cap, ctx->A.scan_blocks);
+    k_scan_top<<<1, 1024, 0, ctx->stream>>>(ctx->A.scan_blocks, tiles, gate_scan, gate_idx, gate_cap);
+    k_scan_add<<<tiles, 1024, 0, ctx->stream>>>(out, n_const, n_ptr, ctx->A.scan_blocks, tiles, gate_scan, gate_idx, gate_cap);
+    ctx->launches += 3;
+}
+
+constexpr int SM_CAP = 148 * 16;
+
+// the kernels of each stage; `prof` records an event after each stage
+struct Prof {
+    cudaEvent_t ev[KN_COUNT + 1];
+    bool on = false;
+};
+
+void mark(OmiCtx *ctx, Prof *pf, int k) {
+    if (pf && pf->on) cudaEventRecord(pf->ev[k + 1], ctx->stream);
+}
+
+void stage_refit(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    k_refit<<<grid_for(A.NB, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_REFIT);
+}
+
+void stage_broadphase(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    const size_t smem = (size_t)ctx->sort_cap * (2 * sizeof(double) + 2 * sizeof(int));
+    k_sort<<<std::min(A.W, 65535), ctx->sort_block, smem, ctx->stream>>>(A, ctx->sort_cap);
+    ctx->launches++;
+    mark(ctx, pf, KN_SORT);
+    k_pair_count<<<grid_for(A.NB * 32, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_PAIR_COUNT);
+    launch_scan(ctx, A.pair_cnt, A.pair_scan, A.NB, nullptr, A.NB, nullptr, 0, 0);
+    k_pair_check<<<1, 1, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_PAIR_SCAN);
+    k_pair_emit<<<grid_for(A.NB * 32, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_PAIR_EMIT);
+}
+
+void stage_narrow(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    k_narrow<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_NARROW);
+    k_gjk<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_GJK);
+    launch_scan(ctx, A.slot_cnt, A.contact_scan, 0, A.pair_scan + A.NB, A.pair_cap, A.pair_scan, A.NB, A.pair_cap);
+    k_contact_check<<<1, 1, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_CONTACT_SCAN);
+}
+
+void stage_compact(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    k_contact_compact<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_COMPACT);
+}
+
+void stage_solve(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    k_solve<<<std::min(A.W, 65535), ctx->solve_block, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    mark(ctx, pf, KN_SOLVE);
+    k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
+    k_hash_clear<<<grid_for(ctx->cache_cap, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    k_cache_copy<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
+    k_hash_build<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
+    k_flip<<<1, 1, 0, ctx->stream>>>(A);
+    ctx->launches += 5;
+    mark(ctx, pf, KN_CACHE);
+}
+
+void stage_joints(OmiCtx *ctx, Prof *pf, int gated) {
+    Arena &A = ctx->A;
+    if (A.NJ > 0) {
+        k_joints<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A, gated);
+        ctx->launches++;
+    }
+    mark(ctx, pf, KN_JOINTS);
+}
+
+// one full step (world.py:410-430) for every active world
+void enqueue_step(OmiCtx *ctx, Prof *pf) {
+    Arena &A = ctx->A;
+    if (pf && pf->on) cudaEventRecord(pf->ev[0], ctx->stream);
+    stage_refit(ctx, pf);
+    stage_broadphase(ctx, pf);
+    stage_narrow(ctx, pf);
+    k_integrate_forces<<<grid_for(A.NB, 256, SM_CAP), 256, 0, ctx->stream>>>(A, 1);
+    ctx->launches++;
+    mark(ctx, pf, KN_INTEGRATE_FORCES);
+    stage_compact(ctx, pf);
+    stage_solve(ctx, pf);
+    stage_joints(ctx, pf, 1);
+    k_finalize<<<std::min(A.W, 65535), 256, 0, ctx->stream>>>(A, FIN_POSITIONS | FIN_SLEEP | FIN_COUNT | FIN_GATED);
+    ctx->launches++;
+    mark(ctx, pf, KN_FINALIZE);
+}
+
+int reset_status(OmiCtx *ctx) {
+    return cudaMemsetAsync(ctx->A.status, 0, sizeof(int) * ST_WORDS, ctx->stream) == cudaSuccess ? 0 : -1;
+}
+
+int read_status(OmiCtx *ctx) {
+    cudaError_t e = cudaMemcpyAsync(ctx->h_status, ctx->A.status, sizeof(int) * ST_WORDS,
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "status D2H");
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
+    return 0;
+}
+
+// grow after an overflow recorded in the status words
+int grow_for_overflow(OmiCtx *ctx) {
+    int *st = ctx->h_status;
+    int pair_cap = ctx->A.pair_cap, contact_cap = ctx->A.contact_cap;
+    if (st[ST_OVERFLOW] == 1) {
+        const int need = st[ST_PAIRS_NEEDED];
+        pair_cap = std::max(pair_cap * 2, need + need / 2 + 1024);
+        contact_cap = std::max(contact_cap, 2 * pair_cap);
+    } else if (st[ST_OVERFLOW] == 2) {
+        const int need = st[ST_CONTACTS_NEEDED];
+        contact_cap = std::max(contact_cap * 2, need + need / 2 + 1024);
+    }
+    return alloc_dynamic(ctx, pair_cap, contact_cap);
+}
+
+int capture(OmiCtx *ctx) {
+    drop_graph(ctx);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamBeginCapture");
+    const int64_t before = ctx->launches;
+    enqueue_step(ctx, nullptr);
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->launches = before;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+    return 0;
+}
+
+int64_t step_launches(OmiCtx *ctx) {
+    // kernels per captured step (same sequence as enqueue_step)
+    int64_t n = 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 5 + 1;
+    if (ctx->A.NJ > 0) n += 1;
+    return n;
+}
+
+int run_steps(OmiCtx *ctx, int n, bool sync) {
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "omi_step before omi_load");
+    int remaining = n;
+    int guard = 0;
+    while (remaining > 0) {
+        if (reset_status(ctx)) return fail(ctx, OMI_E_CUDA, "status reset");
+        if (!ctx->graph) {
+            int rc = capture(ctx);
+            if (rc) return rc;
+        }
+        for (int s = 0; s < remaining; s++) {
+            cudaError_t e = cudaGraphLaunch(ctx->graph, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphLaunch");
+            ctx->launches += step_launches(ctx);
+        }
+        if (!sync) return 0;
+        int rc = read_status(ctx);
+        if (rc) return rc;
+        const int done = ctx->h_status[ST_STEPS_DONE];
+        remaining -= done;
+        if (remaining > 0) {
+            if (!ctx->h_status[ST_OVERFLOW] || ++guard > 16)
+                return fail(ctx, OMI_E_STATE, "step did not complete (no overflow recorded)");
+            rc = grow_for_overflow(ctx);
+            if (rc) return rc;
+        }
+    }
+    return 0;
+}
+
+template <class T>
+int put(OmiCtx *ctx, T *dst, const T *src, size_t n) {
+    if (!n) return 0;
+    cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "slot upload");
+}
+
+int check_world(OmiCtx *ctx, int w) {
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    if (w < 0 || w >= ctx->A.W) return fail(ctx, OMI_E_ARG, "world index out of range");
+    return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int omi_create(int device, OmiCtx **out) {
+    if (!out) return OMI_E_ARG;
+    *out = nullptr;
+    OmiCtx *ctx = new OmiCtx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaSetDevice"); *out = ctx; return rc; }
+    e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaStreamCreate"); *out = ctx; return rc; }
+    ctx->stream = ctx->own;
+    e = cudaMallocHost(&ctx->h_status, sizeof(int) * ST_WORDS);
+    if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
+    cudaFuncSetAttribute(k_gjk, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * (int)sizeof(EpaWork));
+    cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
+    *out = ctx;
+    return 0;
+}
+
+int omi_destroy(OmiCtx *ctx) {
+    if (!ctx) return 0;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);
+    free_pool(ctx, ctx->dyn);
+    free_pool(ctx, ctx->cache);
+    free_pool(ctx, ctx->statics);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return 0;
+}
+
+const char *omi_last_error(OmiCtx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int omi_set_stream(OmiCtx *ctx, void *stream) {
+    if (!ctx) return OMI_E_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+    return 0;
+}
+
+int omi_set_budget(OmiCtx *ctx, int64_t bytes) {
+    if (!ctx) return OMI_E_ARG;
+    ctx->budget = bytes;
+    return 0;
+}
+
+int64_t omi_device_bytes(OmiCtx *ctx) { return ctx ? ctx->bytes : 0; }
+int64_t omi_launch_count(OmiCtx *ctx) { return ctx ? ctx->launches : 0; }
+const char *omi_kernel_name(int32_t i) { return (i >= 0 && i < KN_COUNT) ? kKernelNames[i] : ""; }
+
+static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const int *joint_n) {
+    if (!ctx || !s) return OMI_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);
+    free_pool(ctx, ctx->dyn);
+    free_pool(ctx, ctx->cache);
+    free_pool(ctx, ctx->statics);
+    ctx->cache_cap = 0;
+    ctx->loaded = false;
+    const int W = s->n_worlds, NB = s->n_bodies;
+    if (W <= 0 || NB < 0 || s->w_body_off[0] != 0 || s->w_body_off[W] != NB)
+        return fail(ctx, OMI_E_ARG, "inconsistent world/body offsets");
+    // validate indices on the host so no kernel can read out of bounds
+    for (int w = 0; w < W; w++) {
+        if (s->w_body_off[w + 1] < s->w_body_off[w]) return fail(ctx, OMI_E_ARG, "world offsets decrease");
+        if (s->w_joint_off[w + 1] < s->w_joint_off[w]) return fail(ctx, OMI_E_ARG, "joint offsets decrease");
+        const int rows = s->w_filter_rows[w];
+        if (rows < 1 || s->w_filter_off[w] < 0 || s->w_filter_off[w] + rows * rows > s->n_filter_bytes)
+            return fail(ctx, OMI_E_ARG, "filter matrix range out of bounds");
+        if (s->w_pf_off[w] < 0 || s->w_pf_n[w] < 0 || s->w_pf_off[w] + s->w_pf_n[w] > s->n_pair_friction)
+            return fail(ctx, OMI_E_ARG, "pair-friction range out of bounds");
+    }
+    if (s->w_joint_off[0] != 0 || s->w_joint_off[W] != s->n_joints)
+        return fail(ctx, OMI_E_ARG, "inconsistent joint offsets");
+    std::vector<int> body_world(NB);
+    std::vector<int8_t> kind(NB, 0);
+    std::vector<double> half((size_t)NB * 3, 0.0);
+    int max_n = 0, max_nc = 0;
+    for (int w = 0; w < W; w++) {
+        const int n = s->w_body_off[w + 1] - s->w_body_off[w];
+        max_n = std::max(max_n, n);
+        if (s->w_flags[w] & OMI_WF_COLLISION) max_nc = std::max(max_nc, n);
+        for (int i = s->w_body_off[w]; i < s->w_body_off[w + 1]; i++) {
+            body_world[i] = w;
+            if (s->filter_row[i] < 0 || s->filter_row[i] >= s->w_filter_rows[w])
+                return fail(ctx, OMI_E_ARG, "filter row out of range");
+        }
+    }
+    for (int i = 0; i < NB; i++) {
+        const int sh = s->shape[i];
+        if (s->motion_type[i] < 0 || s->motion_type[i] > 2) return fail(ctx, OMI_E_ARG, "motion type");
+        if (s->material[i] >= s->n_materials || s->material[i] < -1) return fail(ctx, OMI_E_ARG, "material index out of range");
+        if (sh < 0) continue;
+        if (sh >= s->n_shapes) return fail(ctx, OMI_E_ARG, "shape index out of range");
+        const int t = s->shape_type[sh];
+        if (t == OMI_SHAPE_SPHERE) {
+            kind[i] = 1;
+            for (int c = 0; c < 3; c++) half[i * 3 + c] = s->shape_radius[sh];
+        } else if (t == OMI_SHAPE_BOX) {
+            kind[i] = 2;
+            for (int c = 0; c < 3; c++) half[i * 3 + c] = 0.5 * s->shape_size[sh * 3 + c];
+        } else if (t == OMI_SHAPE_CONVEX) {
+            kind[i] = 3;
+            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
+                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
+                return fail(ctx, OMI_E_ARG, "convex point range out of bounds");
+        } else {
+            return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
+        }
+    }
+    for (int p = 0; p < s->n_pair_friction; p++)
+        if (s->pf_a[p] >= s->n_materials || s->pf_b[p] >= s->n_materials)
+            return fail(ctx, OMI_E_ARG, "pair-friction material out of range");
+    for (int j = 0; j < s->n_joints; j++) {
+        if (s->j_type[j] < 0 || s->j_type[j] > 2) return fail(ctx, OMI_E_ARG, "joint type");
+        if (s->j_a[j] >= NB || s->j_b[j] >= NB) return fail(ctx, OMI_E_ARG, "joint body out of range");
+        if (s->j_type[j] == OMI_JOINT_MOTOR && s->j_a[j] < 0) return fail(ctx, OMI_E_ARG, "motor without a body");
+    }
+    int max_j = 0;
+    for (int w = 0; w < W; w++) max_j = std::max(max_j, s->w_joint_off[w + 1] - s->w_joint_off[w]);
+
+    Arena &A = ctx->A;
+    A = Arena{};
+    A.W = W; A.NB = NB; A.NS = s->n_shapes; A.NM = s->n_materials; A.NJ = s->n_joints;
+    A.NPTS = s->n_points;
+    int rc = 0;
+    // worlds
+    rc |= upload(ctx, const_cast<int *&>(A.w_body_off), s->w_body_off, W + 1);
+    rc |= upload(ctx, const_cast<int *&>(A.w_body_n), body_n, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_joint_n), joint_n, W);
+    ctx->h_body_off.assign(s->w_body_off, s->w_body_off + W + 1);
+    ctx->h_body_n.assign(body_n, body_n + W);
+    ctx->h_joint_off.assign(s->w_joint_off, s->w_joint_off + W + 1);
+    rc |= upload(ctx, const_cast<double *&>(A.w_g), s->w_gravity, (size_t)W * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.w_dt), s->w_dt, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_iters), s->w_iters, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_jiters), s->w_joint_iters, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_flags), s->w_flags, W);
+    ctx->h_active.assign(W, 1);
+    for (int w = 0; w < W; w++) ctx->h_active[w] = (s->w_flags[w] & OMI_WF_ACTIVE) ? 1 : 0;
+    rc |= upload(ctx, const_cast<uint8_t *&>(A.w_active), ctx->h_active.data(), W);
+    rc |= upload(ctx, const_cast<double *&>(A.w_def_damp), s->w_default_damp, (size_t)W * 2);
+    rc |= upload(ctx, const_cast<double *&>(A.w_solver), s->w_solver, (size_t)W * 2);
+    rc |= upload(ctx, const_cast<int *&>(A.w_filter_off), s->w_filter_off, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_filter_rows), s->w_filter_rows, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_pf_off), s->w_pf_off, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_pf_n), s->w_pf_n, W);
+    rc |= upload(ctx, const_cast<int *&>(A.w_joint_off), s->w_joint_off, W + 1);
+    // bodies
+    rc |= upload(ctx, A.pos, s->pos, (size_t)NB * 3);
+    rc |= upload(ctx, A.q, s->q, (size_t)NB * 4);
+    rc |= upload(ctx, A.v, s->v, (size_t)NB * 3);
+    rc |= upload(ctx, A.w, s->w, (size_t)NB * 3);
+    rc |= upload(ctx, A.prev_pos, s->pos, (size_t)NB * 3);
+    rc |= upload(ctx, A.prev_q, s->q, (size_t)NB * 4);
+    rc |= upload(ctx, const_cast<double *&>(A.inv_mass), s->inv_mass, NB);
+    rc |= upload(ctx, const_cast<double *&>(A.inv_inertia), s->inv_inertia, (size_t)NB * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.gf), s->gravity_factor, NB);
+    rc |= upload(ctx, const_cast<double *&>(A.ld), s->lin_damp, NB);
+    rc |= upload(ctx, const_cast<double *&>(A.ad), s->ang_damp, NB);
+    rc |= upload(ctx, const_cast<double *&>(A.qd), s->quad_drag, NB);
+    rc |= upload(ctx, A.timer, s->sleep_timer, NB);
+    rc |= upload(ctx, A.awake, s->awake, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.mtype), s->motion_type, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.shape), s->shape, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.material), s->material, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.material_key), s->material_key, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.filter_row), s->filter_row, NB);
+    rc |= upload(ctx, const_cast<int *&>(A.body_world), body_world.data(), NB);
+    rc |= upload(ctx, const_cast<int8_t *&>(A.kind), kind.data(), NB);
+    rc |= upload(ctx, const_cast<double *&>(A.half), half.data(), (size_t)NB * 3);
+    rc |= alloc(ctx, ctx->statics, A.aabb_min, (size_t)NB * 3);
+    rc |= alloc(ctx, ctx->statics, A.aabb_max, (size_t)NB * 3);
+    rc |= alloc(ctx, ctx->statics, A.invIw, (size_t)NB * 9);
+    // shapes, materials, filters
+    rc |= upload(ctx, const_cast<int *&>(A.shape_type), s->shape_type, s->n_shapes);
+    rc |= upload(ctx, const_cast<double *&>(A.shape_radius), s->shape_radius, s->n_shapes);
+    rc |= upload(ctx, const_cast<double *&>(A.shape_size), s->shape_size, (size_t)s->n_shapes * 3);
+    rc |= upload(ctx, const_cast<int *&>(A.pt_off), s->shape_pt_off, s->n_shapes);
+    rc |= upload(ctx, const_cast<int *&>(A.pt_cnt), s->shape_pt_cnt, s->n_shapes);
+    rc |= upload(ctx, const_cast<double *&>(A.points), s->points, (size_t)s->n_points * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.mat_dynf), s->mat_dynf, s->n_materials);
+    rc |= upload(ctx, const_cast<double *&>(A.mat_rest), s->mat_rest, s->n_materials);
+    rc |= upload(ctx, const_cast<int *&>(A.mat_fcomb), s->mat_fcomb, s->n_materials);
+    rc |= upload(ctx, const_cast<int *&>(A.mat_rcomb), s->mat_rcomb, s->n_materials);
+    rc |= upload(ctx, const_cast<int *&>(A.pf_a), s->pf_a, s->n_pair_friction);
+    rc |= upload(ctx, const_cast<int *&>(A.pf_b), s->pf_b, s->n_pair_friction);
+    rc |= upload(ctx, const_cast<double *&>(A.pf_mu), s->pf_mu, s->n_pair_friction);
+    rc |= upload(ctx, const_cast<uint8_t *&>(A.filter_matrix), s->filter_matrix, s->n_filter_bytes);
+    // joints
+    const int NJ = s->n_joints;
+    rc |= upload(ctx, const_cast<int *&>(A.j_type), s->j_type, NJ);
+    rc |= upload(ctx, const_cast<int *&>(A.j_a), s->j_a, NJ);
+    rc |= upload(ctx, const_cast<int *&>(A.j_b), s->j_b, NJ);
+    rc |= upload(ctx, const_cast<double *&>(A.j_anchor), s->j_anchor, (size_t)NJ * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.j_anchor_b), s->j_anchor_b, (size_t)NJ * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.j_axis), s->j_axis, (size_t)NJ * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.j_target), s->j_target, NJ);
+    rc |= upload(ctx, const_cast<double *&>(A.j_max_force), s->j_max_force, NJ);
+    rc |= upload(ctx, A.j_local_a, s->j_local_a, (size_t)NJ * 3);
+    rc |= upload(ctx, A.j_local_b, s->j_local_b, (size_t)NJ * 3);
+    rc |= upload(ctx, A.j_length, s->j_length, NJ);
+    rc |= upload(ctx, A.j_accum, s->j_accum, NJ);
+    rc |= upload(ctx, A.j_has_local_a, s->j_has_local_a, NJ);
+    rc |= upload(ctx, A.j_has_local_b, s->j_has_local_b, NJ);
+    rc |= upload(ctx, A.j_has_length, s->j_has_length, NJ);
+    rc |= alloc(ctx, ctx->statics, A.j_data, (size_t)NJ * JD);
+    rc |= alloc(ctx, ctx->statics, A.j_level, NJ);
+    rc |= alloc(ctx, ctx->statics, A.j_order, NJ);
+    rc |= alloc(ctx, ctx->statics, A.j_level_start, 2 * ((size_t)NJ + W + 1));
+    // per-body scratch
+    rc |= alloc(ctx, ctx->statics, A.order, NB);
+    rc |= alloc(ctx, ctx->statics, A.sorted_x, NB);
+    for (int t = 0; t < 2; t++) {
+        rc |= alloc(ctx, ctx->statics, A.sort_k[t], NB);
+        rc |= alloc(ctx, ctx->statics, A.sort_v[t], NB);
+    }
+    rc |= alloc(ctx, ctx->statics, A.pair_cnt, NB);
+    rc |= alloc(ctx, ctx->statics, A.pair_scan, (size_t)NB + 1);
+    rc |= alloc(ctx, ctx->statics, A.b_last, NB);
+    rc |= alloc(ctx, ctx->statics, A.b_parent, NB);
+    rc |= alloc(ctx, ctx->statics, A.b_island, NB);
+    rc |= alloc(ctx, ctx->statics, A.b_flag, NB);
+    rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
+    for (int t = 0; t < 2; t++) {
+        rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
+        rc |= alloc(ctx, ctx->statics, A.w_cache_n[t], W);
+    }
+    rc |= alloc(ctx, ctx->statics, A.w_cache_new, W + 1);
+    rc |= alloc(ctx, ctx->statics, A.hused_n, 4);
+    rc |= alloc(ctx, ctx->statics, A.parity, 1);
+    rc |= alloc(ctx, ctx->statics, A.status, ST_WORDS);
+    if (rc) return rc;
+    ctx->max_world_n = max_n;
+    ctx->max_world_j = max_j;
+    ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
+    ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
+    ctx->solve_block = max_n > 1024 ? 256 : 128;
+    const int pair_cap = std::max(4096, 4 * NB);
+    rc = alloc_dynamic(ctx, pair_cap, 2 * pair_cap);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->loaded = true;
+    return 0;
+}
+
+int omi_load(OmiCtx *ctx, const OmiScene *s) {
+    if (!ctx || !s || s->n_worlds <= 0) return OMI_E_ARG;
+    std::vector<int> bn(s->n_worlds), jn(s->n_worlds);
+    for (int w = 0; w < s->n_worlds; w++) {
+        bn[w] = s->w_body_off[w + 1] - s->w_body_off[w];
+        jn[w] = s->w_joint_off[w + 1] - s->w_joint_off[w];
+    }
+    ctx->slots = false;
+    return load_impl(ctx, s, bn.data(), jn.data());
+}
+
+int omi_reserve_slots(OmiCtx *ctx, int32_t n, const OmiSlotCaps *caps) {
+    if (!ctx || !caps || n <= 0 || caps->bodies <= 0 || caps->filter_rows < 1 || caps->shapes < 0 ||
+        caps->materials < 0 || caps->points < 0 || caps->joints < 0 || caps->pair_friction < 0)
+        return fail(ctx, OMI_E_ARG, "bad slot capacities");
+    const OmiSlotCaps c = *caps;
+    const size_t NB = (size_t)n * c.bodies, NS = (size_t)n * std::max(c.shapes, 1);
+    const size_t NM = (size_t)n * std::max(c.materials, 1), NP = (size_t)n * std::max(c.points, 1);
+    const size_t NJ = (size_t)n * c.joints, NF = (size_t)n * c.filter_rows * c.filter_rows;
+    const size_t NPF = (size_t)n * c.pair_friction;
+    if (NB > (1u << 30) || NF > (1u << 30)) return fail(ctx, OMI_E_ARG, "slot arena too large");
+    std::vector<int> body_off(n + 1), joint_off(n + 1), zeros_w(n, 0), frows(n, 1), foff(n), pfoff(n), iters(n, 10);
+    for (int w = 0; w <= n; w++) { body_off[w] = w * c.bodies; joint_off[w] = w * c.joints; }
+    for (int w = 0; w < n; w++) { foff[w] = w * c.filter_rows * c.filter_rows; pfoff[w] = w * c.pair_friction; }
+    std::vector<double> g(3 * n, 0.0), dt(n, 1.0 / 60.0), damp(2 * n, 0.0), solver(2 * n);
+    for (int w = 0; w < n; w++) { solver[2 * w] = 0.5; solver[2 * w + 1] = 0.005; }
+    std::vector<double> zb(NB * 4, 0.0), qb(NB * 4, 0.0);
+    for (size_t i = 0; i < NB; i++) qb[i * 4 + 3] = 1.0;
+    std::vector<int> zi(std::max(NB, NS), 0), neg(std::max(NB, NJ) + 1, -1);
+    std::vector<uint8_t> ones(NB, 1), fm(NF, 1), zu(std::max(NJ, (size_t)1), 0);
+    std::vector<double> zs(std::max({NS, NM, NP, NJ, NPF}) * 3 + 3, 0.0);
+    std::vector<int> zsi(std::max({NS, NM, NJ, NPF}) + 1, 0);
+    OmiScene s{};
+    s.n_worlds = n;
+    s.w_body_off = body_off.data(); s.w_gravity = g.data(); s.w_dt = dt.data();
+    s.w_iters = iters.data(); s.w_joint_iters = iters.data(); s.w_flags = zeros_w.data();
+    s.w_default_damp = damp.data(); s.w_solver = solver.data();
+    s.w_filter_off = foff.data(); s.w_filter_rows = frows.data();
+    s.w_pf_off = pfoff.data(); s.w_pf_n = zeros_w.data(); s.w_joint_off = joint_off.data();
+    s.n_bodies = (int)NB;
+    s.pos = zb.data(); s.q = qb.data(); s.v = zb.data(); s.w = zb.data();
+    s.inv_mass = zb.data(); s.inv_inertia = zb.data(); s.gravity_factor = zb.data();
+    s.lin_damp = zb.data(); s.ang_damp = zb.data(); s.quad_drag = zb.data(); s.sleep_timer = zb.data();
+    s.motion_type = zi.data(); s.shape = neg.data(); s.material = neg.data(); s.material_key = neg.data();
+    s.filter_row = zi.data(); s.awake = ones.data();
+    s.n_shapes = (int)NS; s.shape_type = zsi.data(); s.shape_radius = zs.data(); s.shape_size = zs.data();
+    s.shape_pt_off = zsi.data(); s.shape_pt_cnt = zsi.data(); s.n_points = (int)NP; s.points = zs.data();
+    s.n_materials = (int)NM; s.mat_dynf = zs.data(); s.mat_rest = zs.data(); s.mat_fcomb = zsi.data(); s.mat_rcomb = zsi.data();
+    s.n_pair_friction = (int)NPF; s.pf_a = zsi.data(); s.pf_b = zsi.data(); s.pf_mu = zs.data();
+    s.n_filter_bytes = (int)NF; s.filter_matrix = fm.data();
+    s.n_joints = (int)NJ; s.j_type = zsi.data(); s.j_a = neg.data(); s.j_b = neg.data();
+    s.j_anchor = zs.data(); s.j_anchor_b = zs.data(); s.j_local_a = zs.data(); s.j_local_b = zs.data();
+    s.j_has_local_a = zu.data(); s.j_has_local_b = zu.data(); s.j_length = zs.data(); s.j_has_length = zu.data();
+    s.j_axis = zs.data(); s.j_target = zs.data(); s.j_max_force = zs.data(); s.j_accum = zs.data();
+    // motor rows need a body: empty slots hold point joints between the world and itself
+    int rc = load_impl(ctx, &s, zeros_w.data(), zeros_w.data());
+    if (rc) return rc;
+    ctx->slots = true;
+    ctx->caps = c;
+    return 0;
+}
+
+int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
+    if (!ctx || !o) return OMI_E_ARG;
+    if (!ctx->loaded || !ctx->slots) return fail(ctx, OMI_E_STATE, "omi_reserve_slots first");
+    const OmiSlotCaps &c = ctx->caps;
+    Arena &A = ctx->A;
+    if (slot < 0 || slot >= A.W) return fail(ctx, OMI_E_ARG, "slot out of range");
+    if (o->n_worlds != 1) return fail(ctx, OMI_E_ARG, "one world per slot");
+    const int n = o->n_bodies, ns = o->n_shapes, nm = o->n_materials, np_ = o->n_points;
+    const int nj = o->n_joints, rows = o->w_filter_rows[0], npf = o->n_pair_friction;
+    if (n > c.bodies || ns > c.shapes || nm > c.materials || np_ > c.points || nj > c.joints ||
+        rows > c.filter_rows || rows < 1 || npf > c.pair_friction || o->n_filter_bytes < rows * rows)
+        return fail(ctx, OMI_E_ARG, "world exceeds the slot capacities");
+    const int b0 = slot * c.bodies, s0 = slot * std::max(c.shapes, 1), m0 = slot * std::max(c.materials, 1);
+    const int p0 = slot * std::max(c.points, 1), j0 = slot * c.joints;
+    std::vector<int> shape(n), mat(n), body_world(n, slot);
+    std::vector<int8_t> kind(n, 0);
+    std::vector<double> half((size_t)n * 3, 0.0);
+    for (int i = 0; i < n; i++) {
+        const int sh = o->shape[i];
+        if (o->motion_type[i] < 0 || o->motion_type[i] > 2) return fail(ctx, OMI_E_ARG, "motion type");
+        if (o->filter_row[i] < 0 || o->filter_row[i] >= rows) return fail(ctx, OMI_E_ARG, "filter row");
+        if (o->material[i] >= nm || o->material[i] < -1) return fail(ctx, OMI_E_ARG, "material index");
+        mat[i] = o->material[i] < 0 ? -1 : o->material[i] + m0;
+        shape[i] = sh < 0 ? -1 : sh + s0;
+        if (sh < 0) continue;
+        if (sh >= ns) return fail(ctx, OMI_E_ARG, "shape index");
+        const int t = o->shape_type[sh];
+        if (t == OMI_SHAPE_SPHERE) { kind[i] = 1; for (int k = 0; k < 3; k++) half[i * 3 + k] = o->shape_radius[sh]; }
+        else if (t == OMI_SHAPE_BOX) { kind[i] = 2; for (int k = 0; k < 3; k++) half[i * 3 + k] = 0.5 * o->shape_size[sh * 3 + k]; }
+        else if (t == OMI_SHAPE_CONVEX) {
+            kind[i] = 3;
+            if (o->shape_pt_cnt[sh] < 1 || o->shape_pt_off[sh] < 0 || o->shape_pt_off[sh] + o->shape_pt_cnt[sh] > np_)
+                return fail(ctx, OMI_E_ARG, "convex point range");
+        } else return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
+    }
+    std::vector<int> ptoff(ns);
+    for (int k = 0; k < ns; k++) ptoff[k] = o->shape_pt_off[k] + p0;
+    std::vector<int> ja(nj), jb(nj);
+    for (int j = 0; j < nj; j++) {
+        if (o->j_type[j] < 0 || o->j_type[j] > 2) return fail(ctx, OMI_E_ARG, "joint type");
+        if (o->j_a[j] >= n || o->j_b[j] >= n) return fail(ctx, OMI_E_ARG, "joint body");
+        if (o->j_type[j] == OMI_JOINT_MOTOR && o->j_a[j] < 0) return fail(ctx, OMI_E_ARG, "motor body");
+        ja[j] = o->j_a[j] < 0 ? -1 : o->j_a[j] + b0;
+        jb[j] = o->j_b[j] < 0 ? -1 : o->j_b[j] + b0;
+    }
+    int rc = 0;
+    rc |= put(ctx, A.pos + (size_t)b0 * 3, o->pos, (size_t)n * 3);
+    rc |= put(ctx, A.q + (size_t)b0 * 4, o->q, (size_t)n * 4);
+    rc |= put(ctx, A.prev_pos + (size_t)b0 * 3, o->pos, (size_t)n * 3);
+    rc |= put(ctx, A.prev_q + (size_t)b0 * 4, o->q, (size_t)n * 4);
+    rc |= put(ctx, A.v + (size_t)b0 * 3, o->v, (size_t)n * 3);
+    rc |= put(ctx, A.w + (size_t)b0 * 3, o->w, (size_t)n * 3);
+    rc |= put(ctx, const_cast<double *>(A.inv_mass) + b0, o->inv_mass, n);
+    rc |= put(ctx, const_cast<double *>(A.inv_inertia) + (size_t)b0 * 3, o->inv_inertia, (size_t)n * 3);
+    rc |= put(ctx, const_cast<double *>(A.gf) + b0, o->gravity_factor, n);
+    rc |= put(ctx, const_cast<double *>(A.ld) + b0, o->lin_damp, n);
+    rc |= put(ctx, const_cast<double *>(A.ad) + b0, o->ang_damp, n);
+    rc |= put(ctx, const_cast<double *>(A.qd) + b0, o->quad_drag, n);
+    rc |= put(ctx, A.timer + b0, o->sleep_timer, n);
+    rc |= put(ctx, A.awake + b0, o->awake, n);
+    rc |= put(ctx, const_cast<int *>(A.mtype) + b0, o->motion_type, n);
+    rc |= put(ctx, const_cast<int *>(A.shape) + b0, shape.data(), n);
+    rc |= put(ctx, const_cast<int *>(A.material) + b0, mat.data(), n);
+    rc |= put(ctx, const_cast<int *>(A.material_key) + b0, o->material_key, n);
+    rc |= put(ctx, const_cast<int *>(A.filter_row) + b0, o->filter_row, n);
+    rc |= put(ctx, const_cast<int8_t *>(A.kind) + b0, kind.data(), n);
+    rc |= put(ctx, const_cast<double *>(A.half) + (size_t)b0 * 3, half.data(), (size_t)n * 3);
+    rc |= put(ctx, const_cast<int *>(A.shape_type) + s0, o->shape_type, ns);
+    rc |= put(ctx, const_cast<double *>(A.shape_radius) + s0, o->shape_radius, ns);
+    rc |= put(ctx, const_cast<double *>(A.shape_size) + (size_t)s0 * 3, o->shape_size, (size_t)ns * 3);
+    rc |= put(ctx, const_cast<int *>(A.pt_off) + s0, ptoff.data(), ns);
+    rc |= put(ctx, const_cast<int *>(A.pt_cnt) + s0, o->shape_pt_cnt, ns);
+    rc |= put(ctx, const_cast<double *>(A.points) + (size_t)p0 * 3, o->points, (size_t)np_ * 3);
+    rc |= put(ctx, const_cast<double *>(A.mat_dynf) + m0, o->mat_dynf, nm);
+    rc |= put(ctx, const_cast<double *>(A.mat_rest) + m0, o->mat_rest, nm);
+    rc |= put(ctx, const_cast<int *>(A.mat_fcomb) + m0, o->mat_fcomb, nm);
+    rc |= put(ctx, const_cast<int *>(A.mat_rcomb) + m0, o->mat_rcomb, nm);
+    const int pf0 = slot * c.pair_friction, f0 = slot * c.filter_rows * c.filter_rows;
+    rc |= put(ctx, const_cast<int *>(A.pf_a) + pf0, o->pf_a, npf);
+    rc |= put(ctx, const_cast<int *>(A.pf_b) + pf0, o->pf_b, npf);
+    rc |= put(ctx, const_cast<double *>(A.pf_mu) + pf0, o->pf_mu, npf);
+    rc |= put(ctx, const_cast<uint8_t *>(A.filter_matrix) + f0, o->filter_matrix, (size_t)rows * rows);
+    rc |= put(ctx, const_cast<int *>(A.j_type) + j0, o->j_type, nj);
+    rc |= put(ctx, const_cast<int *>(A.j_a) + j0, ja.data(), nj);
+    rc |= put(ctx, const_cast<int *>(A.j_b) + j0, jb.data(), nj);
+    rc |= put(ctx, const_cast<double *>(A.j_anchor) + (size_t)j0 * 3, o->j_anchor, (size_t)nj * 3);
+    rc |= put(ctx, const_cast<double *>(A.j_anchor_b) + (size_t)j0 * 3, o->j_anchor_b, (size_t)nj * 3);
+    rc |= put(ctx, const_cast<double *>(A.j_axis) + (size_t)j0 * 3, o->j_axis, (size_t)nj * 3);
+    rc |= put(ctx, const_cast<double *>(A.j_target) + j0, o->j_target, nj);
+    rc |= put(ctx, const_cast<double *>(A.j_max_force) + j0, o->j_max_force, nj);
+    rc |= put(ctx, A.j_local_a + (size_t)j0 * 3, o->j_local_a, (size_t)nj * 3);
+    rc |= put(ctx, A.j_local_b + (size_t)j0 * 3, o->j_local_b, (size_t)nj * 3);
+    rc |= put(ctx, A.j_length + j0, o->j_length, nj);
+    rc |= put(ctx, A.j_accum + j0, o->j_accum, nj);
+    rc |= put(ctx, A.j_has_local_a + j0, o->j_has_local_a, nj);
+    rc |= put(ctx, A.j_has_local_b + j0, o->j_has_local_b, nj);
+    rc |= put(ctx, A.j_has_length + j0, o->j_has_length, nj);
+    rc |= put(ctx, const_cast<double *>(A.w_g) + (size_t)slot * 3, o->w_gravity, 3);
+    rc |= put(ctx, const_cast<double *>(A.w_dt) + slot, o->w_dt, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_iters) + slot, o->w_iters, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_jiters) + slot, o->w_joint_iters, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_flags) + slot, o->w_flags, 1);
+    rc |= put(ctx, const_cast<double *>(A.w_def_damp) + (size_t)slot * 2, o->w_default_damp, 2);
+    rc |= put(ctx, const_cast<double *>(A.w_solver) + (size_t)slot * 2, o->w_solver, 2);
+    rc |= put(ctx, const_cast<int *>(A.w_filter_rows) + slot, &rows, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_pf_n) + slot, &npf, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_body_n) + slot, &n, 1);
+    rc |= put(ctx, const_cast<int *>(A.w_joint_n) + slot, &nj, 1);
+    const int zero2[2] = {0, 0};
+    for (int t = 0; t < 2; t++) rc |= put(ctx, A.w_cache_n[t] + slot, zero2, 1);
+    if (rc) return rc;
+    ctx->h_body_n[slot] = n;
+    ctx->h_active[slot] = (o->w_flags[0] & OMI_WF_ACTIVE) ? 1 : 0;
+    rc = put(ctx, const_cast<uint8_t *>(A.w_active) + slot, &ctx->h_active[slot], 1);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_world_rows(OmiCtx *ctx, int32_t w, int32_t *first, int32_t *count) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    if (first) *first = ctx->h_body_off[w];
+    if (count) *count = ctx->h_body_n[w];
+    return 0;
+}
+
+int omi_set_world_params(OmiCtx *ctx, const double *dt, const int32_t *iters, const int32_t *jiters,
+                         const int32_t *flags) {
+    if (!ctx) return OMI_E_ARG;
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    Arena &A = ctx->A;
+    int rc = 0;
+    if (dt) rc |= put(ctx, const_cast<double *>(A.w_dt), dt, A.W);
+    if (iters) rc |= put(ctx, const_cast<int *>(A.w_iters), iters, A.W);
+    if (jiters) rc |= put(ctx, const_cast<int *>(A.w_jiters), jiters, A.W);
+    if (flags) rc |= put(ctx, const_cast<int *>(A.w_flags), flags, A.W);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_set_active(OmiCtx *ctx, const uint8_t *active) {
+    if (!ctx || !active) return OMI_E_ARG;
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    std::memcpy(ctx->h_active.data(), active, ctx->A.W);
+    CK(cudaMemcpyAsync(const_cast<uint8_t *>(ctx->A.w_active), ctx->h_active.data(), ctx->A.W,
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_upload_state(OmiCtx *ctx, int32_t begin, int32_t count, const double *pos, const double *q,
+                     const double *v, const double *w, const uint8_t *awake, const double *timer) {
+    if (!ctx) return OMI_E_ARG;
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    if (begin < 0 || count < 0 || begin + count > ctx->A.NB) return fail(ctx, OMI_E_ARG, "row range");
+    Arena &A = ctx->A;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return src ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream) : cudaSuccess;
+    };
+    CK(cp(A.pos + (size_t)begin * 3, pos, sizeof(double) * 3 * count));
+    CK(cp(A.q + (size_t)begin * 4, q, sizeof(double) * 4 * count));
+    CK(cp(A.v + (size_t)begin * 3, v, sizeof(double) * 3 * count));
+    CK(cp(A.w + (size_t)begin * 3, w, sizeof(double) * 3 * count));
+    CK(cp(A.awake + begin, awake, count));
+    CK(cp(A.timer + begin, timer, sizeof(double) * count));
+    return 0;
+}
+
+int omi_download_state(OmiCtx *ctx, int32_t begin, int32_t count, double *pos, double *q, double *v,
+                       double *w, uint8_t *awake, double *timer, double *amin, double *amax) {
+    if (!ctx) return OMI_E_ARG;
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    if (begin < 0 || count < 0 || begin + count > ctx->A.NB) return fail(ctx, OMI_E_ARG, "row range");
+    Arena &A = ctx->A;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return dst ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) : cudaSuccess;
+    };
+    CK(cp(pos, A.pos + (size_t)begin * 3, sizeof(double) * 3 * count));
+    CK(cp(q, A.q + (size_t)begin * 4, sizeof(double) * 4 * count));
+    CK(cp(v, A.v + (size_t)begin * 3, sizeof(double) * 3 * count));
+    CK(cp(w, A.w + (size_t)begin * 3, sizeof(double) * 3 * count));
+    CK(cp(awake, A.awake + begin, count));
+    CK(cp(timer, A.timer + begin, sizeof(double) * count));
+    CK(cp(amin, A.aabb_min + (size_t)begin * 3, sizeof(double) * 3 * count));
+    CK(cp(amax, A.aabb_max + (size_t)begin * 3, sizeof(double) * 3 * count));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_download_joints(OmiCtx *ctx, double *la, double *lb, uint8_t *hla, uint8_t *hlb,
+                        double *len, uint8_t *hlen, double *accum) {
+    if (!ctx) return OMI_E_ARG;
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+    Arena &A = ctx->A;
+    const size_t J = A.NJ;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return (dst && bytes) ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) : cudaSuccess;
+    };
+    CK(cp(la, A.j_local_a, sizeof(double) * 3 * J));
+    CK(cp(lb, A.j_local_b, sizeof(double) * 3 * J));
+    CK(cp(hla, A.j_has_local_a, J));
+    CK(cp(hlb, A.j_has_local_b, J));
+    CK(cp(len, A.j_length, sizeof(double) * J));
+    CK(cp(hlen, A.j_has_length, J));
+    CK(cp(accum, A.j_accum, sizeof(double) * J));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_step(OmiCtx *ctx, int32_t n) {
+    if (!ctx || n < 0) return OMI_E_ARG;
+    return run_steps(ctx, n, true);
+}
+
+int omi_step_async(OmiCtx *ctx, int32_t n) {
+    if (!ctx || n < 0) return OMI_E_ARG;
+    return run_steps(ctx, n, false);
+}
+
+int omi_sync(OmiCtx *ctx) {
+    if (!ctx) return OMI_E_ARG;
+    int rc = read_status(ctx);
+    if (rc) return rc;
+    if (ctx->h_status[ST_OVERFLOW])
+        return fail(ctx, OMI_E_STATE, "an asynchronous step overflowed its buffers; re-run with omi_step");
+    return 0;
+}
+
+// ---- stage entry points -------------------------------------------------
+#define STAGE_PRELUDE                                                           \
+    if (!ctx) return OMI_E_ARG;                                                 \
+    if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
+
+int omi_integrate_forces(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    k_integrate_forces<<<grid_for(ctx->A.NB, 256, SM_CAP), 256, 0, ctx->stream>>>(ctx->A, 0);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_refit_aabbs(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    stage_refit(ctx, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_broadphase(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    for (int guard = 0; guard < 16; guard++) {
+        if (reset_status(ctx)) return fail(ctx, OMI_E_CUDA, "status reset");
+        stage_broadphase(ctx, nullptr);
+        CK(cudaGetLastError());
+        int rc = read_status(ctx);
+        if (rc) return rc;
+        if (!ctx->h_status[ST_OVERFLOW]) return 0;
+        rc = grow_for_overflow(ctx);
+        if (rc) return rc;
+    }
+    return fail(ctx, OMI_E_STATE, "broadphase did not fit");
+}
+
+int omi_narrowphase(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    for (int guard = 0; guard < 16; guard++) {
+        if (reset_status(ctx)) return fail(ctx, OMI_E_CUDA, "status reset");
+        stage_narrow(ctx, nullptr);
+        stage_compact(ctx, nullptr);
+        CK(cudaGetLastError());
+        int rc = read_status(ctx);
+        if (rc) return rc;
+        if (!ctx->h_status[ST_OVERFLOW]) return 0;
+        rc = grow_for_overflow(ctx);
+        if (rc) return rc;
+        stage_broadphase(ctx, nullptr);
+    }
+    return fail(ctx, OMI_E_STATE, "narrowphase did not fit");
+}
+
+int omi_solve_contacts(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    stage_solve(ctx, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_solve_joints(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    stage_joints(ctx, nullptr, 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_integrate_positions(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    k_finalize<<<std::min(ctx->A.W, 65535), 256, 0, ctx->stream>>>(ctx->A, FIN_POSITIONS);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_update_sleep(OmiCtx *ctx) {
+    STAGE_PRELUDE
+    k_finalize<<<std::min(ctx->A.W, 65535), 256, 0, ctx->stream>>>(ctx->A, FIN_SLEEP);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// ---- results --------------------------------------------------------------
+int omi_counts(OmiCtx *ctx, int32_t *pairs, int32_t *contacts) {
+    STAGE_PRELUDE
+    const int W = ctx->A.W, NB = ctx->A.NB;
+    std::vector<int> off(W + 1), ps(NB + 1);
+    std::vector<int> hoff(ctx->A.W + 1);
+    CK(cudaMemcpyAsync(hoff.data(), ctx->A.w_body_off, sizeof(int) * (W + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ps.data(), ctx->A.pair_scan, sizeof(int) * (NB + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int P = ps[NB];
+    std::vector<int> cs(std::max(P, 0) + 1, 0);
+    if (P >= 0 && P <= ctx->A.pair_cap)
+        CK(cudaMemcpyAsync(cs.data(), ctx->A.contact_scan, sizeof(int) * (P + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int w = 0; w < W; w++) {
+        const int p0 = ps[hoff[w]], p1 = ps[hoff[w + 1]];
+        if (pairs) pairs[w] = p1 - p0;
+        if (contacts) contacts[w] = cs[p1] - cs[p0];
+    }
+    return 0;
+}
+
+static int world_ranges(OmiCtx *ctx, int w, int &p0, int &p1, int &c0, int &c1) {
+    int bo[2];
+    CK(cudaMemcpyAsync(bo, ctx->A.w_body_off + w, sizeof(int) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpyAsync(&p0, ctx->A.pair_scan + bo[0], sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&p1, ctx->A.pair_scan + bo[1], sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpyAsync(&c0, ctx->A.contact_scan + p0, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&c1, ctx->A.contact_scan + p1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_get_pairs(OmiCtx *ctx, int32_t w, int32_t *out, int32_t cap) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    int p0, p1, c0, c1;
+    rc = world_ranges(ctx, w, p0, p1, c0, c1);
+    if (rc) return rc;
+    const int n = p1 - p0;
+    if (n > cap) return fail(ctx, OMI_E_ARG, "pair buffer too small");
+    std::vector<int> a(n), b(n);
+    if (n) {
+        CK(cudaMemcpyAsync(a.data(), ctx->A.pair_a + p0, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(b.data(), ctx->A.pair_b + p0, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    for (int i = 0; i < n; i++) { out[2 * i] = a[i]; out[2 * i + 1] = b[i]; }
+    return n;
+}
+
+int omi_get_contacts(OmiCtx *ctx, int32_t w, int32_t *a, int32_t *b, double *pt, double *nrm,
+                     double *depth, double *imp, int32_t cap) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    int p0, p1, c0, c1;
+    rc = world_ranges(ctx, w, p0, p1, c0, c1);
+    if (rc) return rc;
+    const int n = c1 - c0;
+    if (n > cap) return fail(ctx, OMI_E_ARG, "contact buffer too small");
+    Arena &A = ctx->A;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return (dst && bytes) ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) : cudaSuccess;
+    };
+    CK(cp(a, A.c_a + c0, sizeof(int) * n));
+    CK(cp(b, A.c_b + c0, sizeof(int) * n));
+    CK(cp(pt, A.c_pt + (size_t)c0 * 3, sizeof(double) * 3 * n));
+    CK(cp(nrm, A.c_n + (size_t)c0 * 3, sizeof(double) * 3 * n));
+    CK(cp(depth, A.c_depth + c0, sizeof(double) * n));
+    CK(cp(imp, A.c_imp + (size_t)c0 * 3, sizeof(double) * 3 * n));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return n;
+}
+
+int omi_get_islands(OmiCtx *ctx, int32_t w, int32_t *labels) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    int bo[2];
+    CK(cudaMemcpyAsync(bo, ctx->A.w_body_off + w, sizeof(int) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpyAsync(labels, ctx->A.b_island + bo[0], sizeof(int) * (bo[1] - bo[0]), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_get_cache(OmiCtx *ctx, int32_t w, int32_t *a, int32_t *b, double *pt, double *imp,
+                  int32_t cap) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    Arena &A = ctx->A;
+    int cur = 0, off = 0, n = 0;
+    CK(cudaMemcpyAsync(&cur, A.parity, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpyAsync(&off, A.w_cache_off[cur] + w, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&n, A.w_cache_n[cur] + w, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (n > cap) return fail(ctx, OMI_E_ARG, "cache buffer too small");
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        return (dst && bytes) ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) : cudaSuccess;
+    };
+    CK(cp(a, A.cache_a[cur] + off, sizeof(int) * n));
+    CK(cp(b, A.cache_b[cur] + off, sizeof(int) * n));
+    CK(cp(pt, A.cache_pt[cur] + (size_t)off * 3, sizeof(double) * 3 * n));
+    CK(cp(imp, A.cache_imp[cur] + (size_t)off * 3, sizeof(double) * 3 * n));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return n;
+}
+
+int omi_set_cache(OmiCtx *ctx, int32_t w, int32_t n, const int32_t *a, const int32_t *b,
+                  const double *pt, const double *imp) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!a || !b || !pt || !imp))) return fail(ctx, OMI_E_ARG, "cache arrays");
+    Arena &A = ctx->A;
+    const int W = A.W;
+    for (int i = 0; i < n; i++)
+        if (a[i] < 0 || a[i] >= A.NB || b[i] < 0 || b[i] >= A.NB) return fail(ctx, OMI_E_ARG, "cache body index");
+    CK(cudaStreamSynchronize(ctx->stream));
+    int cur = 0;
+    CK(cudaMemcpy(&cur, A.parity, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> off(W), cnt(W);
+    CK(cudaMemcpy(off.data(), A.w_cache_off[cur], sizeof(int) * W, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cnt.data(), A.w_cache_n[cur], sizeof(int) * W, cudaMemcpyDeviceToHost));
+    // gather every world's entries, replace world w's, lay them out again
+    std::vector<int> ha, hb;
+    std::vector<double> hp, hi;
+    std::vector<int> noff(W), ncnt(W);
+    for (int v = 0; v < W; v++) {
+        noff[v] = (int)ha.size();
+        if (v == w) {
+            ha.insert(ha.end(), a, a + n); hb.insert(hb.end(), b, b + n);
+            hp.insert(hp.end(), pt, pt + 3 * n); hi.insert(hi.end(), imp, imp + 3 * n);
+            ncnt[v] = n;
+            continue;
+        }
+        const int m = cnt[v], o = off[v];
+        const size_t base = ha.size();
+        ha.resize(base + m); hb.resize(base + m); hp.resize((base + m) * 3); hi.resize((base + m) * 3);
+        if (m) {
+            CK(cudaMemcpy(&ha[base], A.cache_a[cur] + o, sizeof(int) * m, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&hb[base], A.cache_b[cur] + o, sizeof(int) * m, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&hp[base * 3], A.cache_pt[cur] + (size_t)o * 3, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&hi[base * 3], A.cache_imp[cur] + (size_t)o * 3, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost));
+        }
+        ncnt[v] = m;
+    }
+    const int total = (int)ha.size();
+    if (total > ctx->cache_cap) {
+        const int want = total;
+        rc = alloc_dynamic(ctx, std::max(ctx->A.pair_cap, want), std::max(ctx->A.contact_cap, want));
+        if (rc) return rc;
+    }
+    if (total) {
+        CK(cudaMemcpy(A.cache_a[cur], ha.data(), sizeof(int) * total, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(A.cache_b[cur], hb.data(), sizeof(int) * total, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(A.cache_pt[cur], hp.data(), sizeof(double) * 3 * total, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(A.cache_imp[cur], hi.data(), sizeof(double) * 3 * total, cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(A.w_cache_off[cur], noff.data(), sizeof(int) * W, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(A.w_cache_n[cur], ncnt.data(), sizeof(int) * W, cudaMemcpyHostToDevice));
+    CK(cudaMemset(A.hkey[cur], 0xff, sizeof(unsigned long long) * ((size_t)A.hash_mask + 1)));
+    CK(cudaMemset(A.hused_n + cur, 0, sizeof(int)));
+    k_hash_rebuild<<<std::min(W, 65535), 128, 0, ctx->stream>>>(A, cur);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out) {
+    STAGE_PRELUDE
+    Prof pf;
+    pf.on = true;
+    for (int i = 0; i <= KN_COUNT; i++) CK(cudaEventCreate(&pf.ev[i]));
+    for (int guard = 0; guard < 16; guard++) {
+        if (reset_status(ctx)) return fail(ctx, OMI_E_CUDA, "status reset");
+        enqueue_step(ctx, &pf);
+        CK(cudaGetLastError());
+        int rc = read_status(ctx);
+        if (rc) return rc;
+        if (ctx->h_status[ST_STEPS_DONE] == 1) break;
+        rc = grow_for_overflow(ctx);
+        if (rc) return rc;
+    }
+    ctx->prof_ms.assign(KN_COUNT, 0.0f);
+    for (int k = 0; k < KN_COUNT; k++) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, pf.ev[k], pf.ev[k + 1]);
+        ctx->prof_ms[k] = t;
+    }
+    for (int i = 0; i <= KN_COUNT; i++) cudaEventDestroy(pf.ev[i]);
+    const int m = std::min<int>(n, KN_COUNT);
+    for (int k = 0; k < m; k++) ms[k] = ctx->prof_ms[k];
+    if (n_out) *n_out = KN_COUNT;
+    return 0;
+}
+
+}  // extern "C"

@@ -219,6 +219,58 @@ def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed:
     return w, dict(dt=1.0 / 240.0, steps=480, name='chain%d' % links)
 
 
+def feature_mix(api=None, backend=None, n: int = 70, seed: int = 11):
+    """Sphere/box mix exercising restitution, every combine mode, a pair-friction
+    override, collision filters, a kinematic mover and a body without collider."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0, default_linear_damping=0.05)
+    rng = np.random.default_rng(seed)
+    g = w.add_material(m.Material(dynamicFriction=0.4, restitution=0.3))
+    bouncy = w.add_material(m.Material(dynamicFriction=0.9, restitution=0.8,
+                                       frictionCombine=m.MINIMUM, restitutionCombine=m.MAXIMUM))
+    slick = w.add_material(m.Material(dynamicFriction=0.1, frictionCombine=m.MULTIPLY))
+    w.set_pair_friction(g, slick, 0.7, 0.65)
+    f_a = w.add_filter(m.CollisionFilter(collisionSystems=('a',), notCollideWithSystems=('b',)))
+    f_b = w.add_filter(m.CollisionFilter(collisionSystems=('b',)))
+    ground = w.add_shape(m.Shape.box((16.0, 1.0, 16.0)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=g),
+               position=(0.0, -0.5, 0.0))
+    kin = w.add_shape(m.Shape.box((2.0, 0.4, 2.0)))
+    w.add_body(m.Motion(type=m.KINEMATIC, linearVelocity=(0.3, 0.0, 0.0),
+                        angularVelocity=(0.0, 0.5, 0.0)),
+               m.Collider(shape=kin, physicsMaterial=g), position=(-2.0, 0.2, 0.0))
+    mats = (g, bouncy, slick, -1)
+    for i in range(n):
+        r = float(rng.uniform(0.2, 0.5))
+        sh = w.add_shape(m.Shape.sphere(r) if i % 3 else
+                         m.Shape.box(tuple(float(x) for x in rng.uniform(0.3, 0.8, 3))))
+        filt = (-1, f_a, f_b)[i % 3]
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=float(rng.uniform(0.5, 3.0)),
+                            linearVelocity=tuple(float(x) for x in rng.normal(0, 1.0, 3)),
+                            linearDamping=float(rng.uniform(0, 0.2)),
+                            angularDamping=float(rng.uniform(0, 0.2)),
+                            quadraticDrag=float(rng.uniform(0, 0.05)),
+                            gravityFactor=float(rng.uniform(0.5, 1.5))),
+                   m.Collider(shape=sh, physicsMaterial=mats[i % 4], collisionFilter=filt),
+                   position=tuple(float(x) for x in rng.uniform((-4, 0.5, -4), (4, 6, 4))))
+    w.add_body(m.Motion(type=m.DYNAMIC), None, position=(9.0, 3.0, 0.0))
+    _set_iterations(w, 6)
+    return w, dict(dt=1.0 / 120.0, steps=120, name='feature_mix')
+
+
+#: the golden-fixture scenes (tests/golden/make_golden.py), by fixture name
+GOLDEN_SCENES = {
+    'pyramid': lambda api=None, backend=None: pyramid(api, backend),
+    'debris': lambda api=None, backend=None: debris(api, backend, n=200, seed=3, extent=6.0,
+                                                    height=8.0, ground=20.0),
+    'convex': lambda api=None, backend=None: convex_pile(api, backend, n=96, seed=5, arena=8.0,
+                                                         height=6.0),
+    'chain': lambda api=None, backend=None: joint_chain(api, backend, links=12, loose=16, seed=2),
+    'spheres': lambda api=None, backend=None: feature_mix(api, backend),
+}
+
+
 def serving_requests(n_worlds: int = 1024, seed: int = 0, rate: float = 200.0,
                      n_min: int = 16, n_max: int = 2048) -> List[dict]:
     """The serving request stream: Poisson arrivals, log-uniform world sizes.

@@ -858,6 +858,38 @@ static int collide_convex(const Proxy *A, const Proxy *B, double *normal, double
     return 1;
 }
 
+/* Test hook: gjk.collide_convex on two proxies given as plain arrays.
+ * kind 1 sphere (r), 2 box (half), 3 convex (m local points). */
+int or_collide_convex(int ka, const double *ca, const double *qa, const double *ha, double ra,
+                      const double *pa, int ma, int kb, const double *cb, const double *qb,
+                      const double *hb, double rb, const double *pb, int mb, double *normal,
+                      double *point, double *depth) {
+    Proxy A, B;
+    double *wa = (double *)malloc(sizeof(double) * 3 * (ma > 0 ? ma : 1));
+    double *wb = (double *)malloc(sizeof(double) * 3 * (mb > 0 ? mb : 1));
+    const int ks[2] = {ka, kb};
+    const double *cs[2] = {ca, cb}, *qs[2] = {qa, qb}, *hs[2] = {ha, hb}, *ps[2] = {pa, pb};
+    const double rs[2] = {ra, rb};
+    const int ms[2] = {ma, mb};
+    Proxy *P[2] = {&A, &B};
+    double *W[2] = {wa, wb};
+    for (int e = 0; e < 2; e++) {
+        Proxy *p = P[e];
+        p->kind = ks[e];
+        or_quat_to_matrix(qs[e], p->R);
+        for (int c = 0; c < 3; c++) { p->center[c] = cs[e][c]; p->half[c] = hs[e][c]; }
+        p->radius = rs[e];
+        p->m = ms[e];
+        for (int i = 0; i < ms[e]; i++)
+            for (int c = 0; c < 3; c++)
+                W[e][i * 3 + c] = dot_blas(&ps[e][i * 3], &p->R[c * 3]) + p->center[c];
+        p->world = W[e];
+    }
+    int r = collide_convex(&A, &B, normal, point, depth);
+    free(wa); free(wb);
+    return r;
+}
+
 static void make_proxy(const OrWorld *w, int i, Proxy *p, double *scratch) {
     int si = w->collider_shape[i];
     int t = w->shape_type[si];

@@ -32,52 +32,9 @@ from omi_physics_b200 import scenes              # noqa: E402
 
 API = SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=rmodel, joints=rjoints)
 
-SCENES = {
-    'pyramid': (lambda: scenes.pyramid(API), 50, (0, 3, 12, 30, 44)),
-    'debris': (lambda: scenes.debris(API, n=200, seed=3, extent=6.0, height=8.0, ground=20.0),
-               240, (0, 90, 150, 239)),
-    'convex': (lambda: scenes.convex_pile(API, n=96, seed=5, arena=8.0, height=6.0), 180,
-               (0, 100, 140, 179)),
-    'chain': (lambda: scenes.joint_chain(API, links=12, loose=16, seed=2), 140, (0, 60, 139)),
-    'spheres': (lambda: _spheres(), 120, (0, 60, 119)),
-}
-
-
-def _spheres():
-    """Sphere/box mix with restitution, combine modes, a pair override and a filter."""
-    m = rmodel
-    w = ref.PhysicsWorld(fixed_dt=1.0 / 120.0, default_linear_damping=0.05)
-    rng = np.random.default_rng(11)
-    g = w.add_material(m.Material(dynamicFriction=0.4, restitution=0.3))
-    bouncy = w.add_material(m.Material(dynamicFriction=0.9, restitution=0.8,
-                                       frictionCombine=m.MINIMUM, restitutionCombine=m.MAXIMUM))
-    slick = w.add_material(m.Material(dynamicFriction=0.1, frictionCombine=m.MULTIPLY))
-    w.set_pair_friction(g, slick, 0.7, 0.65)
-    f_a = w.add_filter(m.CollisionFilter(collisionSystems=('a',), notCollideWithSystems=('b',)))
-    f_b = w.add_filter(m.CollisionFilter(collisionSystems=('b',)))
-    ground = w.add_shape(m.Shape.box((16.0, 1.0, 16.0)))
-    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=g),
-               position=(0.0, -0.5, 0.0))
-    kin = w.add_shape(m.Shape.box((2.0, 0.4, 2.0)))
-    w.add_body(m.Motion(type=m.KINEMATIC, linearVelocity=(0.3, 0.0, 0.0),
-                        angularVelocity=(0.0, 0.5, 0.0)),
-               m.Collider(shape=kin, physicsMaterial=g), position=(-2.0, 0.2, 0.0))
-    mats = (g, bouncy, slick, -1)
-    for i in range(70):
-        r = float(rng.uniform(0.2, 0.5))
-        sh = w.add_shape(m.Shape.sphere(r) if i % 3 else m.Shape.box(tuple(rng.uniform(0.3, 0.8, 3))))
-        filt = (-1, f_a, f_b)[i % 3]
-        w.add_body(m.Motion(type=m.DYNAMIC, mass=float(rng.uniform(0.5, 3.0)),
-                            linearVelocity=tuple(rng.normal(0, 1.0, 3)),
-                            linearDamping=float(rng.uniform(0, 0.2)),
-                            angularDamping=float(rng.uniform(0, 0.2)),
-                            quadraticDrag=float(rng.uniform(0, 0.05)),
-                            gravityFactor=float(rng.uniform(0.5, 1.5))),
-                   m.Collider(shape=sh, physicsMaterial=mats[i % 4], collisionFilter=filt),
-                   position=tuple(rng.uniform((-4, 0.5, -4), (4, 6, 4))))
-    w.add_body(m.Motion(type=m.DYNAMIC), None, position=(9.0, 3.0, 0.0))   # no collider
-    w._collision.solver.velocity_iterations = 6
-    return w, dict(dt=1.0 / 120.0, steps=120, name='spheres')
+STEPS = {'pyramid': (50, (0, 3, 12, 30, 44)), 'debris': (240, (0, 90, 150, 239)),
+         'convex': (180, (0, 100, 140, 179)), 'chain': (140, (0, 60, 139)),
+         'spheres': (120, (0, 60, 119))}
 
 
 def snapshot_init(w):
@@ -89,8 +46,8 @@ def snapshot_init(w):
 
 
 def main():
-    for name, (build, steps, checkpoints) in SCENES.items():
-        w, meta = build()
+    for name, (steps, checkpoints) in STEPS.items():
+        w, meta = scenes.GOLDEN_SCENES[name](API)
         dt = meta['dt']
         data = snapshot_init(w)
         rec = {}
