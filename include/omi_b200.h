@@ -204,6 +204,41 @@ int omi_get_contacts(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double 
                      double *normal, double *depth, double *impulse, int32_t cap);
 /* sleep-island label per body of one world (-1 = not in contact) */
 int omi_get_islands(OmiCtx *ctx, int32_t world, int32_t *labels);
+/*
+ * Allocation-free sweep-and-prune for one world. (This entry point has no
+ * counterpart in the reference.) It is for callers that must not allocate
+ * device memory: an engine whose memory is fully reserved up front by its own
+ * pool, a real-time loop where cudaMalloc/cudaFree would synchronise the
+ * device mid-frame, or code running where the allocator is unavailable. It
+ * computes the same pair list, in the same order, as omi_broadphase
+ * (broadphase.py:243-294) for AABBs the caller already holds on the device.
+ *
+ * All array arguments are DEVICE pointers owned by the caller: aabb_min and
+ * aabb_max (n*3 doubles), motion_type (n ints), optionally filter_row (n ints,
+ * rows of the filter_rows x filter_rows collides_with matrix filter_matrix;
+ * both NULL when every pair collides), the output pairs (2*pair_cap ints,
+ * (min, max) body indices) and n_pairs (1 int: the full pair count, which may
+ * exceed pair_cap; pairs past pair_cap are not written). Work is enqueued on
+ * `stream` (a cudaStream_t, NULL = default) and the call returns without
+ * waiting; read n_pairs after the stream is synchronised.
+ *
+ * Scratch lives in a fixed device array inside this library (about 0.8 MB,
+ * held by every GPU that loads the library until the process exits), so
+ * n_bodies may not exceed OMI_NOALLOC_MAX_BODIES: larger worlds are refused
+ * with OMI_E_ARG and a message in err (err_cap bytes, may be NULL). The first
+ * call on each device looks that array's device address up (once per device,
+ * with the device current); make that first call before any stream capture.
+ * Every call shares the one array, so calls whose work overlaps on the GPU
+ * (other streams, other host threads) race and must be serialised by the
+ * caller. No call allocates or frees memory.
+ */
+#define OMI_NOALLOC_MAX_BODIES 16384
+int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aabb_max,
+                            const int32_t *motion_type, const int32_t *filter_row,
+                            const uint8_t *filter_matrix, int32_t filter_rows, int32_t n_bodies,
+                            int32_t *pairs, int32_t pair_cap, int32_t *n_pairs, void *stream,
+                            char *err, int32_t err_cap);
+
 /* per-kernel device time (ms) of the last profiled step, see omi_profile_step */
 int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out);
 const char *omi_kernel_name(int32_t i);

@@ -107,7 +107,14 @@ PROTOTYPES = {
     'omi_profile_step': (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, I]),
     'omi_kernel_name': (C.c_char_p, [C.c_int32]),
     'omi_launch_count': (C.c_int64, [C.c_void_p]),
+    'omi_sweep_pairs_noalloc': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                          C.c_int32, C.c_void_p, C.c_void_p, C.c_char_p,
+                                          C.c_int32]),
 }
+
+#: the fixed body limit of omi_sweep_pairs_noalloc (OMI_NOALLOC_MAX_BODIES)
+NOALLOC_MAX_BODIES = 16384
 
 _LIB = None
 

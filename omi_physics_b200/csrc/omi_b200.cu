@@ -1239,3 +1239,184 @@ int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free sweep-and-prune (omi_sweep_pairs_noalloc)
+//
+// For callers that cannot allocate device memory. Its scratch is this fixed
+// file-scope device array; in host code `g_noalloc_scratch` is only a host-side
+// stand-in for the symbol, so its device address is looked up with
+// cudaGetSymbolAddress (once per device) and that address is what the kernels
+// receive. Reuses the arena's sort, window-count and scan kernels through an
+// Arena whose pointers all lie in the array or in the caller's buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int NA_MAX = OMI_NOALLOC_MAX_BODIES;
+constexpr size_t NA_TILES = NA_MAX / SCAN_TILE + 2;
+// layout (bytes), each block 256-aligned
+constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t NA_OFF_SORTK0 = 0;
+constexpr size_t NA_OFF_SORTK1 = NA_OFF_SORTK0 + na_align(sizeof(double) * NA_MAX);
+constexpr size_t NA_OFF_SORTV0 = NA_OFF_SORTK1 + na_align(sizeof(double) * NA_MAX);
+constexpr size_t NA_OFF_SORTV1 = NA_OFF_SORTV0 + na_align(sizeof(int) * NA_MAX);
+constexpr size_t NA_OFF_ORDER = NA_OFF_SORTV1 + na_align(sizeof(int) * NA_MAX);
+constexpr size_t NA_OFF_SORTX = NA_OFF_ORDER + na_align(sizeof(int) * NA_MAX);
+constexpr size_t NA_OFF_CNT = NA_OFF_SORTX + na_align(sizeof(double) * NA_MAX);
+constexpr size_t NA_OFF_SCAN = NA_OFF_CNT + na_align(sizeof(int) * NA_MAX);
+constexpr size_t NA_OFF_ZERO = NA_OFF_SCAN + na_align(sizeof(int) * (NA_MAX + 1));   // body_world / filter rows
+constexpr size_t NA_OFF_TILES = NA_OFF_ZERO + na_align(sizeof(int) * NA_MAX);
+constexpr size_t NA_OFF_WORLD = NA_OFF_TILES + na_align(sizeof(int) * (NA_TILES + 1));
+// world tables: body_off[2], body_n[1], flags[1], filter_off[1], filter_rows[1], active byte, filter byte
+constexpr size_t NA_BYTES = NA_OFF_WORLD + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+struct NaDevice {
+    bool ready = false;
+    unsigned char *base = nullptr;
+};
+NaDevice g_na_dev[64];
+
+void na_err(char *err, int cap, const std::string &msg) {
+    if (err && cap > 0) {
+        std::snprintf(err, (size_t)cap, "%s", msg.c_str());
+    }
+}
+
+// world table and zeroed per-row arrays for a one-world arena of n rows
+__global__ void k_noalloc_init(unsigned char *base, int n, int filter_rows, int own_filter) {
+    int *world = reinterpret_cast<int *>(base + NA_OFF_WORLD);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        world[0] = 0;                 // body_off[0]
+        world[1] = n;                 // body_off[1]
+        world[2] = n;                 // body_n
+        world[3] = WF_COLLISION;      // flags
+        world[4] = 0;                 // filter_off
+        world[5] = filter_rows;       // filter_rows
+        base[NA_OFF_WORLD + 24] = 1;  // active
+        base[NA_OFF_WORLD + 25] = 1;  // default filter matrix: everything collides
+    }
+    int *zero = reinterpret_cast<int *>(base + NA_OFF_ZERO);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) zero[i] = 0;
+    (void)own_filter;
+}
+
+// write pairs in the reference's order into the caller's interleaved buffer
+__global__ void k_noalloc_emit(Arena A, int *pairs, int cap, int *n_pairs) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_pairs = A.pair_scan[A.NB];
+    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.NB; e += nwarps) {
+        const int a = A.order[e];
+        const int endk = window_end(A, 0, A.NB, A.aabb_max[a * 3]);
+        int out = A.pair_scan[e];
+        for (int base = e + 1; base < endk; base += 32) {
+            const int kj = base + lane;
+            int b = -1;
+            bool keep = false;
+            if (kj < endk) { b = A.order[kj]; keep = pair_keep(A, 0, a, b); }
+            const unsigned m = __ballot_sync(FULL, keep);
+            if (keep) {
+                const int slot = out + __popc(m & ((1u << lane) - 1u));
+                if (slot < cap) {
+                    pairs[2 * slot] = a < b ? a : b;
+                    pairs[2 * slot + 1] = a < b ? b : a;
+                }
+            }
+            out += __popc(m);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aabb_max,
+                                       const int32_t *motion_type, const int32_t *filter_row,
+                                       const uint8_t *filter_matrix, int32_t filter_rows,
+                                       int32_t n, int32_t *pairs, int32_t pair_cap,
+                                       int32_t *n_pairs, void *stream_v, char *err,
+                                       int32_t err_cap) {
+    if (n < 0 || n > NA_MAX) {
+        na_err(err, err_cap, "omi_sweep_pairs_noalloc: " + std::to_string(n) +
+                                 " bodies exceeds the fixed scratch limit of " +
+                                 std::to_string(NA_MAX) + " (OMI_NOALLOC_MAX_BODIES)");
+        return OMI_E_ARG;
+    }
+    if (!aabb_min || !aabb_max || !motion_type || !n_pairs || pair_cap < 0 || (pair_cap > 0 && !pairs)) {
+        na_err(err, err_cap, "omi_sweep_pairs_noalloc: null buffer or negative pair_cap");
+        return OMI_E_ARG;
+    }
+    if ((filter_row == nullptr) != (filter_matrix == nullptr) || (filter_row && filter_rows < 1)) {
+        na_err(err, err_cap, "omi_sweep_pairs_noalloc: filter_row and filter_matrix go together");
+        return OMI_E_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+        return OMI_E_CUDA;
+    }
+    NaDevice &nd = g_na_dev[dev];
+    if (!nd.ready) {   // set-up, once per device, with that device current
+        void *addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+        if (e != cudaSuccess || !addr) {
+            na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaGetSymbolAddress: ") +
+                                     cudaGetErrorString(e));
+            return OMI_E_CUDA;
+        }
+        e = cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
+        if (e != cudaSuccess) {
+            na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaFuncSetAttribute: ") +
+                                     cudaGetErrorString(e));
+            return OMI_E_CUDA;
+        }
+        nd.base = static_cast<unsigned char *>(addr);
+        nd.ready = true;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream_v);
+    unsigned char *base = nd.base;
+    int *world = reinterpret_cast<int *>(base + NA_OFF_WORLD);
+    Arena A{};
+    A.W = 1;
+    A.NB = n;
+    A.pair_cap = pair_cap;
+    A.w_body_off = world;
+    A.w_body_n = world + 2;
+    A.w_flags = world + 3;
+    A.w_filter_off = world + 4;
+    A.w_filter_rows = world + 5;
+    A.w_active = base + NA_OFF_WORLD + 24;
+    A.body_world = reinterpret_cast<int *>(base + NA_OFF_ZERO);
+    A.aabb_min = const_cast<double *>(aabb_min);
+    A.aabb_max = const_cast<double *>(aabb_max);
+    A.mtype = motion_type;
+    A.filter_row = filter_row ? filter_row : reinterpret_cast<int *>(base + NA_OFF_ZERO);
+    A.filter_matrix = filter_matrix ? filter_matrix : base + NA_OFF_WORLD + 25;
+    A.sort_k[0] = reinterpret_cast<double *>(base + NA_OFF_SORTK0);
+    A.sort_k[1] = reinterpret_cast<double *>(base + NA_OFF_SORTK1);
+    A.sort_v[0] = reinterpret_cast<int *>(base + NA_OFF_SORTV0);
+    A.sort_v[1] = reinterpret_cast<int *>(base + NA_OFF_SORTV1);
+    A.order = reinterpret_cast<int *>(base + NA_OFF_ORDER);
+    A.sorted_x = reinterpret_cast<double *>(base + NA_OFF_SORTX);
+    A.pair_cnt = reinterpret_cast<int *>(base + NA_OFF_CNT);
+    A.pair_scan = reinterpret_cast<int *>(base + NA_OFF_SCAN);
+    int *tiles = reinterpret_cast<int *>(base + NA_OFF_TILES);
+    const int rows = filter_row ? filter_rows : 1;
+    k_noalloc_init<<<grid_for(std::max(n, 1), 256, 64), 256, 0, st>>>(base, n, rows, filter_row != nullptr);
+    const int sort_cap = std::min(std::max(n, 1), 8192);
+    k_sort<<<1, n > 2048 ? 1024 : 256, (size_t)sort_cap * 24, st>>>(A, sort_cap);
+    k_pair_count<<<grid_for(std::max(n, 1) * 32, 256, 148 * 16), 256, 0, st>>>(A);
+    const int ntiles = std::max(1, (n + SCAN_TILE - 1) / SCAN_TILE);
+    k_scan_tiles<<<ntiles, 1024, 0, st>>>(A.pair_cnt, A.pair_scan, n, nullptr, nullptr, 0, 0, tiles);
+    k_scan_top<<<1, 1024, 0, st>>>(tiles, ntiles, nullptr, 0, 0);
+    k_scan_add<<<ntiles, 1024, 0, st>>>(A.pair_scan, n, nullptr, tiles, ntiles, nullptr, 0, 0);
+    k_noalloc_emit<<<grid_for(std::max(n, 1) * 32, 256, 148 * 16), 256, 0, st>>>(A, pairs, pair_cap, n_pairs);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: launch: ") + cudaGetErrorString(e));
+        return OMI_E_CUDA;
+    }
+    return 0;
+}
