@@ -239,6 +239,10 @@ int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aabb_max,
                             int32_t *pairs, int32_t pair_cap, int32_t *n_pairs, void *stream,
                             char *err, int32_t err_cap);
 
+/* Gauss-Seidel depth (number of dependency levels of one sweep) of each
+ * world's contacts in the last step (n_worlds ints; diagnostics). */
+int omi_world_levels(OmiCtx *ctx, int32_t *levels);
+
 /* per-kernel device time (ms) of the last profiled step, see omi_profile_step */
 int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out);
 const char *omi_kernel_name(int32_t i);

@@ -104,6 +104,7 @@ PROTOTYPES = {
     'omi_get_pairs': (C.c_int, [C.c_void_p, C.c_int32, I, C.c_int32]),
     'omi_get_contacts': (C.c_int, [C.c_void_p, C.c_int32, I, I, D, D, D, D, C.c_int32]),
     'omi_get_islands': (C.c_int, [C.c_void_p, C.c_int32, I]),
+    'omi_world_levels': (C.c_int, [C.c_void_p, I]),
     'omi_profile_step': (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, I]),
     'omi_kernel_name': (C.c_char_p, [C.c_int32]),
     'omi_launch_count': (C.c_int64, [C.c_void_p]),

@@ -157,6 +157,12 @@ class WorldBatch:
         lab = lab[:n]
         return np.where(lab >= 0, lab - self.offsets[i], -1)
 
+    def levels(self) -> np.ndarray:
+        """Gauss-Seidel depth of each world's contacts in the last step."""
+        out = np.zeros(len(self.worlds), np.int32)
+        self.ctx.call('world_levels', ptr(out, I))
+        return out
+
     def set_cache(self, i: int, a, b, point, impulse) -> None:
         off = self.offsets[i]
         a = np.ascontiguousarray(np.asarray(a, np.int32) + off)

@@ -6,9 +6,18 @@
 
 namespace omi {
 
-// per-contact prepared solver row (AoS, CD doubles): rA, rB, n, t1, t2,
-// nMass, t1Mass, t2Mass, vBias, friction, inv mass a, inv mass b
-constexpr int CD = 24;
+// per-contact prepared solver row (AoS, CD doubles, 16-byte multiple).
+// The first C_PART doubles vary per contact (arms, effective masses, bias,
+// depth); the rest is the same for every contact of one body pair (normal and
+// tangent basis, friction, inverse masses, world inverse inertia of both
+// bodies, the pair, dynamic flags), so a sweep loads it once per pair.
+constexpr int CD = 44;
+constexpr int C_PART = 12;
+enum { C_RA = 0, C_RB = 3, C_NM = 6, C_T1M = 7, C_T2M = 8, C_VB = 9, C_DEPTH = 10,
+       R_N = 12, R_T1 = 15, R_T2 = 18, R_FRIC = 21, R_IMA = 22, R_IMB = 23, R_IA = 24, R_IB = 33,
+       R_AB = 42, R_FLAGS = 43 };
+// most contacts one body pair produces (box-box manifolds are reduced to 4)
+constexpr int RUN_MAX = 4;
 // per-joint prepared row: invIa(9) invIb(9) rA(3) rB(3) K/LU(9) piv(3) bias(3)
 // n(3) mass bias_s
 constexpr int JD = 48;
@@ -90,6 +99,12 @@ struct Arena {
     int *c_a, *c_b;
     double *c_pt, *c_n, *c_depth, *c_imp, *c_data;
     int *c_level, *c_order, *c_level_start;
+    int *w_levels;                  // Gauss-Seidel depth of each world's contact runs
+    int *w_runs;                    // runs (consecutive contacts of one body pair) per world
+    int *run_k, *run_n, *run_a, *run_b;   // per run: first contact (world-local), count, dynamic bodies (-1 otherwise)
+    unsigned *run_mask;             // per run: earlier runs of its 32-run batch it shares a body with
+    int max_passes;                 // sweep passes the level buffers are sized for (warm start + iterations)
+    const int *w_sched;             // worlds ordered largest first (per-world kernels)
 
     // per-body scratch
     int *b_last, *b_parent, *b_island;

@@ -472,7 +472,7 @@ __device__ __forceinline__ void world_contacts(const Arena &A, int w, int &c0, i
 // Computed by one warp, 32 constraints per batch.
 // ---------------------------------------------------------------------------
 __device__ inline int warp_levels(int n, const int *ea, const int *eb, const int *mtype,
-                                  int *last, int *level) {
+                                  int *last, int *level, int last_base = 0) {
     const int lane = threadIdx.x & 31;
     int maxl = -1;
     for (int base = 0; base < n; base += 32) {
@@ -481,8 +481,8 @@ __device__ inline int warp_levels(int n, const int *ea, const int *eb, const int
         const int a = valid ? ea[k] : -1, b = valid ? eb[k] : -1;
         const bool da = a >= 0 && mtype[a] == 2, db = b >= 0 && mtype[b] == 2;
         int lvl = 0;
-        if (da) lvl = max(lvl, ((volatile int *)last)[a] + 1);
-        if (db) lvl = max(lvl, ((volatile int *)last)[b] + 1);
+        if (da) lvl = max(lvl, ((volatile int *)last)[a - last_base] + 1);
+        if (db) lvl = max(lvl, ((volatile int *)last)[b - last_base] + 1);
         unsigned conflict = 0;
         for (int j = 0; j < 32; j++) {
             const int aj = __shfl_sync(FULL, a, j), bj = __shfl_sync(FULL, b, j);
@@ -495,8 +495,8 @@ __device__ inline int warp_levels(int n, const int *ea, const int *eb, const int
         }
         if (valid) {
             level[k] = lvl;
-            if (da) atomicMax(&last[a], lvl);
-            if (db) atomicMax(&last[b], lvl);
+            if (da) atomicMax(&last[a - last_base], lvl);
+            if (db) atomicMax(&last[b - last_base], lvl);
             maxl = max(maxl, lvl);
         }
         __syncwarp();
@@ -556,28 +556,6 @@ __device__ __forceinline__ void rel_vel(const double *lv, const double *av, int 
         (lv[a * 3 + 1] + av[a * 3 + 2] * rA[0] - av[a * 3] * rA[2]);
     z = (lv[b * 3 + 2] + av[b * 3] * rB[1] - av[b * 3 + 1] * rB[0]) -
         (lv[a * 3 + 2] + av[a * 3] * rA[1] - av[a * 3 + 1] * rA[0]);
-}
-
-// _apply_w (_solver_native.pyx:132-151); only dynamic bodies are written
-__device__ __forceinline__ void apply_impulse(const Arena &A, double *lv, double *av, int a, int b,
-                                              double ima, double imb, const double *rA,
-                                              const double *rB, double Px, double Py, double Pz) {
-    if (A.mtype[a] == 2) {
-        const double *I = &A.invIw[a * 9];
-        lv[a * 3] -= ima * Px; lv[a * 3 + 1] -= ima * Py; lv[a * 3 + 2] -= ima * Pz;
-        const double cx = rA[1] * Pz - rA[2] * Py, cy = rA[2] * Px - rA[0] * Pz, cz = rA[0] * Py - rA[1] * Px;
-        av[a * 3] -= I[0] * cx + I[1] * cy + I[2] * cz;
-        av[a * 3 + 1] -= I[3] * cx + I[4] * cy + I[5] * cz;
-        av[a * 3 + 2] -= I[6] * cx + I[7] * cy + I[8] * cz;
-    }
-    if (A.mtype[b] == 2) {
-        const double *I = &A.invIw[b * 9];
-        lv[b * 3] += imb * Px; lv[b * 3 + 1] += imb * Py; lv[b * 3 + 2] += imb * Pz;
-        const double cx = rB[1] * Pz - rB[2] * Py, cy = rB[2] * Px - rB[0] * Pz, cz = rB[0] * Py - rB[1] * Px;
-        av[b * 3] += I[0] * cx + I[1] * cy + I[2] * cz;
-        av[b * 3 + 1] += I[3] * cx + I[4] * cy + I[5] * cz;
-        av[b * 3 + 2] += I[6] * cx + I[7] * cy + I[8] * cz;
-    }
 }
 
 // _effmass (_solver_native.pyx:154-176)
@@ -668,108 +646,65 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
     const double inv = ln > 1e-12 ? 1.0 / ln : 0.0;
     t1x *= inv; t1y *= inv; t1z *= inv;
     const double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
-    D[0] = rA[0]; D[1] = rA[1]; D[2] = rA[2];
-    D[3] = rB[0]; D[4] = rB[1]; D[5] = rB[2];
-    D[6] = nx; D[7] = ny; D[8] = nz;
-    D[9] = t1x; D[10] = t1y; D[11] = t1z;
-    D[12] = t2x; D[13] = t2y; D[14] = t2z;
-    D[15] = effmass(A, rA, rB, nx, ny, nz, a, b, ima, imb);
-    D[16] = effmass(A, rA, rB, t1x, t1y, t1z, a, b, ima, imb);
-    D[17] = effmass(A, rA, rB, t2x, t2y, t2z, a, b, ima, imb);
+    D[C_RA] = rA[0]; D[C_RA + 1] = rA[1]; D[C_RA + 2] = rA[2];
+    D[C_RB] = rB[0]; D[C_RB + 1] = rB[1]; D[C_RB + 2] = rB[2];
+    D[R_N] = nx; D[R_N + 1] = ny; D[R_N + 2] = nz;
+    D[R_T1] = t1x; D[R_T1 + 1] = t1y; D[R_T1 + 2] = t1z;
+    D[R_T2] = t2x; D[R_T2 + 1] = t2y; D[R_T2 + 2] = t2z;
+    D[C_NM] = effmass(A, rA, rB, nx, ny, nz, a, b, ima, imb);
+    D[C_T1M] = effmass(A, rA, rB, t1x, t1y, t1z, a, b, ima, imb);
+    D[C_T2M] = effmass(A, rA, rB, t2x, t2y, t2z, a, b, ima, imb);
     double dvx, dvy, dvz;
     rel_vel(A.v, A.w, a, b, rA, rB, dvx, dvy, dvz);
     const double vn0 = dvx * nx + dvy * ny + dvz * nz;
-    D[18] = vn0 < -A.w_solver[w * 2] ? -rest * vn0 : 0.0;
-    D[19] = fric;
-    D[20] = ima;
-    D[21] = imb;
+    D[C_VB] = vn0 < -A.w_solver[w * 2] ? -rest * vn0 : 0.0;
+    D[C_DEPTH] = A.c_depth[k];
+    D[11] = 0.0;
+    D[R_FRIC] = fric;
+    D[R_IMA] = ima;
+    D[R_IMB] = imb;
+    int2 *ab = reinterpret_cast<int2 *>(&D[R_AB]);
+    *ab = make_int2(a, b);
+    int2 *fl = reinterpret_cast<int2 *>(&D[R_FLAGS]);
+    *fl = make_int2((A.mtype[a] == 2 ? 1 : 0) | (A.mtype[b] == 2 ? 2 : 0), 0);
+    for (int q = 0; q < 9; q++) { D[R_IA + q] = A.invIw[a * 9 + q]; D[R_IB + q] = A.invIw[b * 9 + q]; }
 }
 
-__device__ inline void warm_contact(const Arena &A, int k) {
-    const int a = A.c_a[k], b = A.c_b[k];
-    const double *D = &A.c_data[(size_t)k * CD];
-    const double n = A.c_imp[k * 3], t0 = A.c_imp[k * 3 + 1], t1 = A.c_imp[k * 3 + 2];
-    apply_impulse(A, A.v, A.w, a, b, D[20], D[21], &D[0], &D[3],
-                  n * D[6] + t0 * D[9] + t1 * D[12],
-                  n * D[7] + t0 * D[10] + t1 * D[13],
-                  n * D[8] + t0 * D[11] + t1 * D[14]);
-}
+// ---- the solver as four launches -------------------------------------------
+// k_wake     one warp per world: _wake_sleepers (solver.py:321-337)
+// k_prep     one thread per contact, every world at once: material combine,
+//            warm-start seed, arms, tangent basis, effective masses, bias
+// k_levels   one warp per world: Gauss-Seidel levels and their buckets
+// k_iterate  one warp per world: warm start (or the first iteration) fused
+//            with the split-impulse position pass, then the remaining
+//            velocity iterations; __syncwarp between levels, the next
+//            level's contact rows prefetched before each barrier
+constexpr int SOLVE_WARPS = 4;   // warps (worlds) per block of the per-world kernels
 
-// one velocity-iteration update of contact k (_solver_native.pyx:259-295)
-__device__ inline void solve_contact(const Arena &A, int k) {
-    const int a = A.c_a[k], b = A.c_b[k];
-    const double *D = &A.c_data[(size_t)k * CD];
-    double *lv = A.v, *av = A.w;
-    const double *rA = &D[0], *rB = &D[3];
-    const double nx = D[6], ny = D[7], nz = D[8];
-    const double ima = D[20], imb = D[21];
-    double *imp = &A.c_imp[k * 3];
-    double dvx, dvy, dvz;
-    rel_vel(lv, av, a, b, rA, rB, dvx, dvy, dvz);
-    const double vn = dvx * nx + dvy * ny + dvz * nz;
-    double nw = imp[0] - D[15] * (vn - D[18]);
-    if (nw < 0.0) nw = 0.0;
-    double dL = nw - imp[0];
-    imp[0] = nw;
-    apply_impulse(A, lv, av, a, b, ima, imb, rA, rB, dL * nx, dL * ny, dL * nz);
-    const double maxf = D[19] * nw;
-    rel_vel(lv, av, a, b, rA, rB, dvx, dvy, dvz);
-    double vt = dvx * D[9] + dvy * D[10] + dvz * D[11];
-    double nt = imp[1] - D[16] * vt;
-    if (nt > maxf) nt = maxf; else if (nt < -maxf) nt = -maxf;
-    dL = nt - imp[1];
-    imp[1] = nt;
-    apply_impulse(A, lv, av, a, b, ima, imb, rA, rB, dL * D[9], dL * D[10], dL * D[11]);
-    vt = dvx * D[12] + dvy * D[13] + dvz * D[14];
-    nt = imp[2] - D[17] * vt;
-    if (nt > maxf) nt = maxf; else if (nt < -maxf) nt = -maxf;
-    dL = nt - imp[2];
-    imp[2] = nt;
-    apply_impulse(A, lv, av, a, b, ima, imb, rA, rB, dL * D[12], dL * D[13], dL * D[14]);
-}
+__device__ __forceinline__ int warp_global_id() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int warp_count() { return (gridDim.x * blockDim.x) >> 5; }
 
-// split-impulse position pass (_solver_native.pyx:297-312)
-__device__ inline void position_contact(const Arena &A, int k, double slop) {
-    const double vn = A.c_depth[k] - slop;
-    if (vn <= 0.0) return;
-    const double *D = &A.c_data[(size_t)k * CD];
-    const double ima = D[20], imb = D[21];
-    if (ima + imb <= 1e-12) return;
-    const double dL = 0.8 * vn / (ima + imb);
-    const int a = A.c_a[k], b = A.c_b[k];
-    if (A.mtype[a] == 2)
-        for (int c = 0; c < 3; c++) A.pos[a * 3 + c] -= ima * dL * D[6 + c];
-    if (A.mtype[b] == 2)
-        for (int c = 0; c < 3; c++) A.pos[b * 3 + c] += imb * dL * D[6 + c];
-}
-
-__global__ void k_solve(Arena A) {
-    __shared__ int s_flag, s_D;
+__global__ void k_wake(Arena A) {
     if (overflowed(A)) return;
-    const int cur = *A.parity;
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const double thr = 0.15 * 0.15;
+    for (int w = warp_global_id(); w < A.W; w += warp_count()) {
         if (!world_collides(A, w)) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
-        const int K = c1 - c0;
-        if (K == 0) continue;                       // solver.py:197-198
-        const bool warm = (A.w_flags[w] & WF_WARM) != 0;
-        const double thr = 0.15 * 0.15;
-        // ---- _wake_sleepers (solver.py:321-337)
-        if (threadIdx.x == 0) s_flag = 0;
-        __syncthreads();
-        for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+        if (c1 == c0) continue;
+        bool cascade = false;
+        for (int k = c0 + lane; k < c1; k += 32) {
             const int e[2] = {A.c_a[k], A.c_b[k]};
             for (int j = 0; j < 2; j++) {
                 const int x = e[j];
-                if (A.mtype[x] == 2 && !A.awake[x] && speed2(&A.v[x * 3]) > thr) s_flag = 1;
+                cascade |= A.mtype[x] == 2 && !A.awake[x] && speed2(&A.v[x * 3]) > thr;
             }
         }
-        __syncthreads();
-        if (s_flag) {
+        if (__any_sync(FULL, cascade)) {
             // a body asleep at the start could wake and then wake others:
             // resolve in the reference's sequential contact order
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 atomicAdd(&A.status[ST_CASCADE], 1);
                 for (int k = c0; k < c1; k++) {
                     const int a = A.c_a[k], b = A.c_b[k];
@@ -785,7 +720,7 @@ __global__ void k_solve(Arena A) {
             }
         } else {
             // no woken body can wake another: order does not matter
-            for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+            for (int k = c0 + lane; k < c1; k += 32) {
                 const int a = A.c_a[k], b = A.c_b[k];
                 const int ta = A.mtype[a], tb = A.mtype[b];
                 if (!A.awake[b] && (ta == 1 || (ta == 2 && A.awake[a] && speed2(&A.v[a * 3]) > thr)))
@@ -794,42 +729,549 @@ __global__ void k_solve(Arena A) {
                     wake_body(A, a);
             }
         }
-        __syncthreads();
-        // ---- per-contact prep (parallel; reads velocities before any impulse)
-        for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) prep_contact(A, w, k, warm, cur);
-        const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
-        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_last[i] = -1;
-        __syncthreads();
-        // ---- Gauss-Seidel levels
-        if (threadIdx.x < 32) {
-            const int D = warp_levels(K, A.c_a + c0, A.c_b + c0, A.mtype, A.b_last, A.c_level + c0);
-            if (threadIdx.x == 0) s_D = D;
+        __syncwarp();
+    }
+}
+
+__global__ void k_prep(Arena A) {
+    if (overflowed(A)) return;
+    const int cur = *A.parity;
+    const int Ktot = A.contact_scan[A.pair_scan[A.NB]];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ktot; k += gridDim.x * blockDim.x) {
+        const int w = A.body_world[A.c_a[k]];
+        if (!world_collides(A, w)) continue;
+        prep_contact(A, w, k, (A.w_flags[w] & WF_WARM) != 0, cur);
+    }
+}
+
+// bucket constraints by level inside one warp: ls[0..D] = level starts
+__device__ inline void bucket_levels_warp(int n, int D, const int *level, int *ls, int *cursor,
+                                          int *order) {
+    const int lane = threadIdx.x & 31;
+    for (int l = lane; l <= D; l += 32) { ls[l] = 0; cursor[l] = 0; }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) atomicAdd(&ls[level[k] + 1], 1);
+    __syncwarp();
+    // exclusive scan of ls[1..D] in chunks of 32 with a carry
+    int carry = 0;
+    for (int base = 1; base <= D; base += 32) {
+        const int i = base + lane;
+        int x = i <= D ? ls[i] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
         }
-        __syncthreads();
-        const int D = s_D;
-        int *ls = A.c_level_start + c0 + w;
-        int *cursor = A.c_level_start + (A.contact_cap + A.W + 1) + c0 + w;
-        int *order = A.c_order + c0;
-        bucket_levels(K, D, A.c_level + c0, ls, cursor, order);
-        // ---- warm start, iterations, position pass, level by level
-        if (warm) {
-            for (int l = 0; l < D; l++) {
-                for (int j = ls[l] + threadIdx.x; j < ls[l + 1]; j += blockDim.x) warm_contact(A, c0 + order[j]);
-                __syncthreads();
+        if (i <= D) ls[i] = x + carry;
+        carry += __shfl_sync(FULL, x, 31);
+        __syncwarp();
+    }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+        const int l = level[k];
+        order[ls[l] + atomicAdd(&cursor[l], 1)] = k;
+    }
+    __syncwarp();
+}
+
+// Levels over the whole sequence of sweep passes. The Gauss-Seidel unit is a
+// run (the consecutive contacts of one body pair) and the sequence is every
+// pass of the reference's solve in order: the warm start (when on), then each
+// velocity iteration, each visiting the runs in contact order. Entry (p, r)
+// must follow every earlier entry sharing a dynamic body with it - within its
+// pass and in earlier passes - and nothing else, so a run of pass p+1 may
+// start while unrelated runs of pass p are still pending. The split-impulse
+// position pass rides along pass 0 (it reads and writes only positions, which
+// no velocity pass touches, and pass 0 orders the runs as the position pass
+// does). Entries are encoded (p << 24) | r.
+constexpr int PASS_SHIFT = 24;
+
+__device__ __forceinline__ int world_passes(const Arena &A, int w) {
+    const int p = ((A.w_flags[w] & WF_WARM) ? 1 : 0) + A.w_iters[w];
+    return p > 0 ? p : 1;
+}
+
+// one pass of levels over R runs; pass 0 also records each run's conflict
+// mask (earlier lanes of its batch sharing a dynamic body), later passes
+// reuse it and walk only the lanes that are conflict sources
+__device__ inline int warp_levels_pass(const Arena &A, int c0, int R, int pass, int *last, int last_base,
+                                       int *level_out) {
+    const int lane = threadIdx.x & 31;
+    const int *ra = A.run_a + c0, *rb = A.run_b + c0;
+    unsigned *rmask = A.run_mask + c0;
+    int maxl = -1;
+    // this batch's run bodies (and, after pass 0, conflict masks), loaded one batch ahead
+    int a = lane < R ? ra[lane] : -1, b = lane < R ? rb[lane] : -1;
+    unsigned mnext = (pass > 0 && lane < R) ? rmask[lane] : 0u;
+    for (int base = 0; base < R; base += 32) {
+        const int r = base + lane;
+        const bool valid = r < R;
+        const int rn = r + 32;
+        const int an = rn < R ? ra[rn] : -1, bn = rn < R ? rb[rn] : -1;
+        const unsigned mn = (pass > 0 && rn < R) ? rmask[rn] : 0u;
+        int lvl = 0;
+        if (a >= 0) lvl = max(lvl, ((volatile int *)last)[a - last_base] + 1);
+        if (b >= 0) lvl = max(lvl, ((volatile int *)last)[b - last_base] + 1);
+        unsigned mask;
+        if (pass == 0) {
+            mask = 0;
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int aj = __shfl_sync(FULL, a, j), bj = __shfl_sync(FULL, b, j);
+                const bool c = j < lane && ((a >= 0 && (a == aj || a == bj)) || (b >= 0 && (b == aj || b == bj)));
+                mask |= (c ? 1u : 0u) << j;
+            }
+            if (valid) rmask[r] = mask;
+        } else {
+            mask = mnext;
+        }
+        unsigned src = __reduce_or_sync(FULL, mask);
+        while (src) {
+            const int j = __ffs(src) - 1;
+            src &= src - 1;
+            const int lj = __shfl_sync(FULL, lvl, j);
+            if ((mask >> j) & 1u) lvl = max(lvl, lj + 1);
+        }
+        if (valid) {
+            level_out[r] = lvl;
+            if (a >= 0) atomicMax(&last[a - last_base], lvl);
+            if (b >= 0) atomicMax(&last[b - last_base], lvl);
+            maxl = max(maxl, lvl);
+        }
+        __syncwarp();
+        a = an; b = bn; mnext = mn;
+    }
+    for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(FULL, maxl, o));
+    return maxl + 1;
+}
+
+// bucket entries by level inside one warp: ls[0..D] = level starts; the
+// entries of pass p are level[p*R + r], stored in order as (p << 24) | r.
+// Counting runs in shared memory (`sc`, `scap` ints) when the levels fit.
+__device__ inline void bucket_entries_warp(int R, int P, int D, const int *level, int *ls, int *cursor,
+                                           int *order, int *sc, int scap) {
+    const int lane = threadIdx.x & 31;
+    const bool shared_counts = D + 1 <= scap;
+    int *cnt = shared_counts ? sc : cursor;
+    for (int l = lane; l <= D; l += 32) cnt[l] = 0;
+    __syncwarp();
+    const int N = R * P;
+    for (int e = lane; e < N; e += 32) atomicAdd(&cnt[level[e]], 1);
+    __syncwarp();
+    // exclusive scan into ls, reset cnt as the fill cursor
+    int carry = 0;
+    for (int base = 0; base <= D; base += 32) {
+        const int i = base + lane;
+        const int v = i < D ? cnt[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (i <= D) ls[i] = x - v + carry;
+        carry += __shfl_sync(FULL, x, 31);
+        __syncwarp();
+        if (i <= D) cnt[i] = 0;
+    }
+    __syncwarp();
+    for (int p = 0, e0 = 0; p < P; p++, e0 += R)
+        for (int r = lane; r < R; r += 32) {
+            const int l = level[e0 + r];
+            order[ls[l] + atomicAdd(&cnt[l], 1)] = (p << PASS_SHIFT) | r;
+        }
+    __syncwarp();
+}
+
+// per-warp shared slice for `last` (worlds up to `last_cap` bodies; larger
+// ones use the global per-body array)
+constexpr int LEVEL_COUNT_CAP = 4096;   // per-warp shared level counters
+
+__global__ void k_levels(Arena A, int last_cap) {
+    extern __shared__ int last_smem[];
+    if (overflowed(A)) return;
+    const int lane = threadIdx.x & 31;
+    int *my_last = last_smem + (threadIdx.x >> 5) * (last_cap + LEVEL_COUNT_CAP);
+    int *my_counts = my_last + last_cap;
+    for (int wi = warp_global_id(); wi < A.W; wi += warp_count()) {
+        const int w = A.w_sched[wi];
+        if (!world_collides(A, w)) continue;
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        const int K = c1 - c0;
+        if (K == 0) { if (lane == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; } continue; }
+        // runs in contact order; level bodies: the dynamic ones
+        int R = 0;
+        for (int base = 0; base < K; base += 32) {
+            const int k = base + lane;
+            bool start = false;
+            int a = -1, b = -1;
+            if (k < K) {
+                a = A.c_a[c0 + k];
+                b = A.c_b[c0 + k];
+                start = k == 0 || a != A.c_a[c0 + k - 1] || b != A.c_b[c0 + k - 1];
+            }
+            const unsigned m = __ballot_sync(FULL, start);
+            if (start) {
+                const int r = R + __popc(m & ((1u << lane) - 1u));
+                A.run_k[c0 + r] = k;
+                A.run_a[c0 + r] = A.mtype[a] == 2 ? a : -1;
+                A.run_b[c0 + r] = A.mtype[b] == 2 ? b : -1;
+            }
+            R += __popc(m);
+        }
+        __syncwarp();
+        for (int r = lane; r < R; r += 32) {
+            const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
+            A.run_n[c0 + r] = end - A.run_k[c0 + r];
+        }
+        const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+        int *last = nb <= last_cap ? my_last : A.b_last + b0;
+        for (int i = lane; i < nb; i += 32) last[i] = -1;
+        __syncwarp();
+        const int P = world_passes(A, w);
+        const size_t e0 = (size_t)c0 * A.max_passes;
+        int D = 0;
+        for (int p = 0; p < P; p++) D = max(D, warp_levels_pass(A, c0, R, p, last, b0, A.c_level + e0 + (size_t)p * R));
+        int *ls = A.c_level_start + e0 + w;
+        int *cursor = A.c_level_start + ((size_t)A.contact_cap * A.max_passes + A.W + 1) + e0 + w;
+        bucket_entries_warp(R, P, D, A.c_level + e0, ls, cursor, A.c_order + e0, my_counts, LEVEL_COUNT_CAP);
+        if (lane == 0) { A.w_levels[w] = D; A.w_runs[w] = R; }
+    }
+}
+
+// asynchronous 16-byte-chunk copy into shared memory
+__device__ __forceinline__ void async_copy(double *dst, const double *src, int chunks) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    for (int q = 0; q < chunks; q++)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s + 16 * q), "l"(src + 2 * q));
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// a lane's buffer for one run: the first contact's whole row, then the
+// per-contact part of the others
+constexpr int RUNBUF = CD + (RUN_MAX - 1) * C_PART;
+
+__device__ __forceinline__ void run_prefetch(const Arena &A, int k0, int n, double *dst) {
+    async_copy(dst, &A.c_data[(size_t)k0 * CD], CD / 2);
+    for (int i = 1; i < n && i < RUN_MAX; i++)
+        async_copy(dst + CD + (i - 1) * C_PART, &A.c_data[(size_t)(k0 + i) * CD], C_PART / 2);
+}
+
+// Velocities of one world, staged for the sweeps: in shared memory when the
+// world fits (six doubles per body: linear then angular), else the global
+// arrays. The two bodies of a pair are always distinct, so keeping their
+// velocities (and, in the first pass, positions) in registers across all of
+// the pair's contacts and storing them once gives exactly the arithmetic of
+// updating memory after every impulse.
+struct VelView {
+    double *s;       // shared staging (nullptr: global)
+    int b0;
+};
+
+__device__ __forceinline__ void vel_load(const Arena &A, const VelView &V, int i, double *lv, double *av) {
+    if (V.s) {
+        const double *p = &V.s[(i - V.b0) * 6];
+        lv[0] = p[0]; lv[1] = p[1]; lv[2] = p[2]; av[0] = p[3]; av[1] = p[4]; av[2] = p[5];
+    } else {
+        lv[0] = A.v[i * 3]; lv[1] = A.v[i * 3 + 1]; lv[2] = A.v[i * 3 + 2];
+        av[0] = A.w[i * 3]; av[1] = A.w[i * 3 + 1]; av[2] = A.w[i * 3 + 2];
+    }
+}
+__device__ __forceinline__ void vel_store(const Arena &A, const VelView &V, int i, const double *lv,
+                                          const double *av) {
+    if (V.s) {
+        double *p = &V.s[(i - V.b0) * 6];
+        p[0] = lv[0]; p[1] = lv[1]; p[2] = lv[2]; p[3] = av[0]; p[4] = av[1]; p[5] = av[2];
+    } else {
+        A.v[i * 3] = lv[0]; A.v[i * 3 + 1] = lv[1]; A.v[i * 3 + 2] = lv[2];
+        A.w[i * 3] = av[0]; A.w[i * 3 + 1] = av[1]; A.w[i * 3 + 2] = av[2];
+    }
+}
+
+// the per-pair part of a run's row
+struct PairRow {
+    int a, b;
+    bool da, db;
+    double n[3], t1[3], t2[3], fric, ima, imb, Ia[9], Ib[9];
+};
+// the per-contact part
+struct ContactRow {
+    double rA[3], rB[3], nM, t1M, t2M, vB, depth;
+};
+
+__device__ __forceinline__ void load_pair(const double *src, PairRow &r) {
+    const int2 ab = *reinterpret_cast<const int2 *>(&src[R_AB]);
+    r.a = ab.x; r.b = ab.y;
+    const int fl = reinterpret_cast<const int2 *>(&src[R_FLAGS])->x;
+    r.da = (fl & 1) != 0; r.db = (fl & 2) != 0;
+    for (int q = 0; q < 3; q++) { r.n[q] = src[R_N + q]; r.t1[q] = src[R_T1 + q]; r.t2[q] = src[R_T2 + q]; }
+    r.fric = src[R_FRIC]; r.ima = src[R_IMA]; r.imb = src[R_IMB];
+    for (int q = 0; q < 9; q++) { r.Ia[q] = src[R_IA + q]; r.Ib[q] = src[R_IB + q]; }
+}
+__device__ __forceinline__ void load_contact(const double *src, ContactRow &c) {
+    for (int q = 0; q < 3; q++) { c.rA[q] = src[C_RA + q]; c.rB[q] = src[C_RB + q]; }
+    c.nM = src[C_NM]; c.t1M = src[C_T1M]; c.t2M = src[C_T2M]; c.vB = src[C_VB]; c.depth = src[C_DEPTH];
+}
+
+struct PairVel {
+    double la[3], aa[3], lb[3], ab[3];
+};
+
+// _apply_w (_solver_native.pyx:132-151) on the register copies
+__device__ __forceinline__ void pair_apply(PairVel &s, const PairRow &r, const ContactRow &c, double Px,
+                                           double Py, double Pz) {
+    if (r.da) {
+        s.la[0] -= r.ima * Px; s.la[1] -= r.ima * Py; s.la[2] -= r.ima * Pz;
+        const double cx = c.rA[1] * Pz - c.rA[2] * Py, cy = c.rA[2] * Px - c.rA[0] * Pz, cz = c.rA[0] * Py - c.rA[1] * Px;
+        s.aa[0] -= r.Ia[0] * cx + r.Ia[1] * cy + r.Ia[2] * cz;
+        s.aa[1] -= r.Ia[3] * cx + r.Ia[4] * cy + r.Ia[5] * cz;
+        s.aa[2] -= r.Ia[6] * cx + r.Ia[7] * cy + r.Ia[8] * cz;
+    }
+    if (r.db) {
+        s.lb[0] += r.imb * Px; s.lb[1] += r.imb * Py; s.lb[2] += r.imb * Pz;
+        const double cx = c.rB[1] * Pz - c.rB[2] * Py, cy = c.rB[2] * Px - c.rB[0] * Pz, cz = c.rB[0] * Py - c.rB[1] * Px;
+        s.ab[0] += r.Ib[0] * cx + r.Ib[1] * cy + r.Ib[2] * cz;
+        s.ab[1] += r.Ib[3] * cx + r.Ib[4] * cy + r.Ib[5] * cz;
+        s.ab[2] += r.Ib[6] * cx + r.Ib[7] * cy + r.Ib[8] * cz;
+    }
+}
+
+__device__ __forceinline__ void pair_rel_vel(const PairVel &s, const ContactRow &c, double &x, double &y, double &z) {
+    x = (s.lb[0] + s.ab[1] * c.rB[2] - s.ab[2] * c.rB[1]) - (s.la[0] + s.aa[1] * c.rA[2] - s.aa[2] * c.rA[1]);
+    y = (s.lb[1] + s.ab[2] * c.rB[0] - s.ab[0] * c.rB[2]) - (s.la[1] + s.aa[2] * c.rA[0] - s.aa[0] * c.rA[2]);
+    z = (s.lb[2] + s.ab[0] * c.rB[1] - s.ab[1] * c.rB[0]) - (s.la[2] + s.aa[0] * c.rA[1] - s.aa[1] * c.rA[0]);
+}
+
+// warm start of one contact (_solver_native.pyx:250-256)
+__device__ __forceinline__ void contact_warm(PairVel &s, const PairRow &r, const ContactRow &c, const double *imp) {
+    const double n = imp[0], t0 = imp[1], t1 = imp[2];
+    pair_apply(s, r, c, n * r.n[0] + t0 * r.t1[0] + t1 * r.t2[0],
+               n * r.n[1] + t0 * r.t1[1] + t1 * r.t2[1],
+               n * r.n[2] + t0 * r.t1[2] + t1 * r.t2[2]);
+}
+
+// one velocity-iteration update (_solver_native.pyx:259-295); imp in/out
+__device__ __forceinline__ void contact_solve(PairVel &s, const PairRow &r, const ContactRow &c, double *imp) {
+    double dvx, dvy, dvz;
+    pair_rel_vel(s, c, dvx, dvy, dvz);
+    const double vn = dvx * r.n[0] + dvy * r.n[1] + dvz * r.n[2];
+    const double old = imp[0];
+    double nw = old - c.nM * (vn - c.vB);
+    if (nw < 0.0) nw = 0.0;
+    double dL = nw - old;
+    pair_apply(s, r, c, dL * r.n[0], dL * r.n[1], dL * r.n[2]);
+    const double maxf = r.fric * nw;
+    pair_rel_vel(s, c, dvx, dvy, dvz);
+    double vt = dvx * r.t1[0] + dvy * r.t1[1] + dvz * r.t1[2];
+    const double o1 = imp[1];
+    double n1 = o1 - c.t1M * vt;
+    if (n1 > maxf) n1 = maxf; else if (n1 < -maxf) n1 = -maxf;
+    dL = n1 - o1;
+    pair_apply(s, r, c, dL * r.t1[0], dL * r.t1[1], dL * r.t1[2]);
+    vt = dvx * r.t2[0] + dvy * r.t2[1] + dvz * r.t2[2];
+    const double o2 = imp[2];
+    double n2 = o2 - c.t2M * vt;
+    if (n2 > maxf) n2 = maxf; else if (n2 < -maxf) n2 = -maxf;
+    dL = n2 - o2;
+    pair_apply(s, r, c, dL * r.t2[0], dL * r.t2[1], dL * r.t2[2]);
+    imp[0] = nw; imp[1] = n1; imp[2] = n2;
+}
+
+// split-impulse position pass of one contact (_solver_native.pyx:297-312)
+__device__ __forceinline__ void contact_position(double *pa, double *pb, const PairRow &r, const ContactRow &c,
+                                                 double slop) {
+    const double vn = c.depth - slop;
+    if (vn <= 0.0) return;
+    if (r.ima + r.imb <= 1e-12) return;
+    const double dL = 0.8 * vn / (r.ima + r.imb);
+    if (r.da)
+        for (int q = 0; q < 3; q++) pa[q] -= r.ima * dL * r.n[q];
+    if (r.db)
+        for (int q = 0; q < 3; q++) pb[q] += r.imb * dL * r.n[q];
+}
+
+// One warp per block, walking the pipelined levels. Dynamic shared memory:
+// each lane's two run buffers (the next level's run is copied in with
+// cp.async while this level runs), then the world's staged state - its
+// bodies' velocities, and its contacts' impulses when they fit too (worlds
+// above the capacity sweep on the global arrays).
+// shared memory of one sweep block, in doubles (227 KB)
+constexpr int SWEEP_SMEM_DOUBLES = 29056;
+
+struct ImpView {
+    double *s;       // shared staging (nullptr: global c_imp)
+    int c0;
+};
+__device__ __forceinline__ double *imp_ptr(const Arena &A, const ImpView &I, int k) {
+    return I.s ? &I.s[(k - I.c0) * 3] : &A.c_imp[k * 3];
+}
+
+// one pass over one run (all its contacts, in order) by one lane
+__device__ __forceinline__ void run_pass(const Arena &A, const VelView &V, const ImpView &I, const double *buf,
+                                         int k0, int n, bool vel, bool warm_pass, bool pos_pass, double slop) {
+    PairRow r;
+    load_pair(buf, r);
+    PairVel s;
+    vel_load(A, V, r.a, s.la, s.aa);
+    vel_load(A, V, r.b, s.lb, s.ab);
+    double pa[3], pb[3];
+    if (pos_pass) {
+        for (int q = 0; q < 3; q++) { pa[q] = A.pos[r.a * 3 + q]; pb[q] = A.pos[r.b * 3 + q]; }
+    }
+#pragma unroll
+    for (int i = 0; i < RUN_MAX; i++) {
+        if (i < n) {
+            ContactRow c;
+            load_contact(i == 0 ? buf : buf + CD + (i - 1) * C_PART, c);
+            if (vel) {
+                double *ip = imp_ptr(A, I, k0 + i);
+                double imp[3] = {ip[0], ip[1], ip[2]};
+                if (warm_pass) contact_warm(s, r, c, imp);
+                else {
+                    contact_solve(s, r, c, imp);
+                    ip[0] = imp[0]; ip[1] = imp[1]; ip[2] = imp[2];
+                }
+            }
+            if (pos_pass) contact_position(pa, pb, r, c, slop);
+        }
+    }
+    if (r.da) vel_store(A, V, r.a, s.la, s.aa);
+    if (r.db) vel_store(A, V, r.b, s.lb, s.ab);
+    if (pos_pass) {
+        if (r.da) for (int q = 0; q < 3; q++) A.pos[r.a * 3 + q] = pa[q];
+        if (r.db) for (int q = 0; q < 3; q++) A.pos[r.b * 3 + q] = pb[q];
+    }
+}
+
+// a run too long for the lane buffer or in a level wider than a warp: the
+// same pass straight from global memory, contact by contact
+__device__ inline void run_pass_direct(const Arena &A, const VelView &V, const ImpView &I, int k0, int n,
+                                       bool vel, bool warm_pass, bool pos_pass, double slop) {
+    PairRow r;
+    load_pair(&A.c_data[(size_t)k0 * CD], r);
+    PairVel s;
+    vel_load(A, V, r.a, s.la, s.aa);
+    vel_load(A, V, r.b, s.lb, s.ab);
+    double pa[3], pb[3];
+    if (pos_pass) for (int q = 0; q < 3; q++) { pa[q] = A.pos[r.a * 3 + q]; pb[q] = A.pos[r.b * 3 + q]; }
+    for (int i = 0; i < n; i++) {
+        ContactRow c;
+        load_contact(&A.c_data[(size_t)(k0 + i) * CD], c);
+        if (vel) {
+            double *ip = imp_ptr(A, I, k0 + i);
+            double imp[3] = {ip[0], ip[1], ip[2]};
+            if (warm_pass) contact_warm(s, r, c, imp);
+            else {
+                contact_solve(s, r, c, imp);
+                ip[0] = imp[0]; ip[1] = imp[1]; ip[2] = imp[2];
             }
         }
-        const int iters = A.w_iters[w];
-        for (int it = 0; it < iters; it++) {
-            for (int l = 0; l < D; l++) {
-                for (int j = ls[l] + threadIdx.x; j < ls[l + 1]; j += blockDim.x) solve_contact(A, c0 + order[j]);
-                __syncthreads();
+        if (pos_pass) contact_position(pa, pb, r, c, slop);
+    }
+    if (r.da) vel_store(A, V, r.a, s.la, s.aa);
+    if (r.db) vel_store(A, V, r.b, s.lb, s.ab);
+    if (pos_pass) {
+        if (r.da) for (int q = 0; q < 3; q++) A.pos[r.a * 3 + q] = pa[q];
+        if (r.db) for (int q = 0; q < 3; q++) A.pos[r.b * 3 + q] = pb[q];
+    }
+}
+
+// SWEEP_WARPS warps per block sweep one world's pipelined levels together
+// (__syncthreads between levels); every entry of a level touches its own
+// dynamic bodies. Shared memory: the world's staged velocities and, when they
+// fit too, its impulses; then, room permitting, each thread's buffer for the
+// next level's run (copied with cp.async while this level runs).
+constexpr int SWEEP_WARPS = 4;
+constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
+
+__global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
+    extern __shared__ __align__(16) double smem_d[];
+    if (overflowed(A)) return;
+    const int tid = threadIdx.x;
+    for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
+        const int w = A.w_sched[wi];
+        if (!world_collides(A, w)) continue;
+        const int D = A.w_levels[w];
+        if (D == 0) continue;
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        const int K = c1 - c0;
+        const size_t e0 = (size_t)c0 * A.max_passes;
+        const int *ls = A.c_level_start + e0 + w;
+        const int *order = A.c_order + e0;
+        const int *run_k = A.run_k + c0, *run_n = A.run_n + c0;
+        const bool warm = (A.w_flags[w] & WF_WARM) != 0;
+        const bool vel = warm || A.w_iters[w] > 0;
+        const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+        int used = 0;
+        VelView V;
+        V.b0 = b0;
+        V.s = nb * 6 <= smem_doubles ? smem_d : nullptr;
+        if (V.s) used = (nb * 6 + 1) & ~1;
+        ImpView I;
+        I.c0 = c0;
+        I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
+        if (I.s) used = (used + K * 3 + 1) & ~1;
+        const bool prefetch = used + SWEEP_THREADS * 2 * RUNBUF <= smem_doubles;
+        double *runbuf = smem_d + used + tid * 2 * RUNBUF;
+        if (V.s) {
+            for (int i = tid; i < nb; i += SWEEP_THREADS) {
+                double lv[3], av[3];
+                lv[0] = A.v[(b0 + i) * 3]; lv[1] = A.v[(b0 + i) * 3 + 1]; lv[2] = A.v[(b0 + i) * 3 + 2];
+                av[0] = A.w[(b0 + i) * 3]; av[1] = A.w[(b0 + i) * 3 + 1]; av[2] = A.w[(b0 + i) * 3 + 2];
+                vel_store(A, V, b0 + i, lv, av);
             }
         }
+        if (I.s)
+            for (int i = tid; i < K * 3; i += SWEEP_THREADS) I.s[i] = A.c_imp[c0 * 3 + i];
+        __syncthreads();
         const double slop = A.w_solver[w * 2 + 1];
-        for (int l = 0; l < D; l++) {
-            for (int j = ls[l] + threadIdx.x; j < ls[l + 1]; j += blockDim.x) position_contact(A, c0 + order[j], slop);
-            __syncthreads();
+        int ecur = ls[0] + tid < ls[1] ? order[ls[0] + tid] : -1;
+        if (prefetch && ecur >= 0) {
+            const int r = ecur & ((1 << PASS_SHIFT) - 1);
+            run_prefetch(A, c0 + run_k[r], run_n[r], runbuf);
         }
+        if (prefetch) async_commit();
+        for (int l = 0; l < D; l++) {
+            const int enext = (l + 1 < D && ls[l + 1] + tid < ls[l + 2]) ? order[ls[l + 1] + tid] : -1;
+            double *buf_cur = runbuf + (l & 1) * RUNBUF, *buf_nxt = runbuf + ((l + 1) & 1) * RUNBUF;
+            if (prefetch) {
+                if (enext >= 0) {
+                    const int r = enext & ((1 << PASS_SHIFT) - 1);
+                    run_prefetch(A, c0 + run_k[r], run_n[r], buf_nxt);
+                }
+                async_commit();
+                async_wait_prev();      // this level's run has landed
+            }
+            if (ecur >= 0) {
+                const int r = ecur & ((1 << PASS_SHIFT) - 1), p = ecur >> PASS_SHIFT;
+                const int k0 = c0 + run_k[r], n = run_n[r];
+                const bool pos_pass = (p == 0), warm_pass = warm && p == 0;
+                if (prefetch && n <= RUN_MAX) run_pass(A, V, I, buf_cur, k0, n, vel, warm_pass, pos_pass, slop);
+                else run_pass_direct(A, V, I, k0, n, vel, warm_pass, pos_pass, slop);
+            }
+            for (int j = ls[l] + tid + SWEEP_THREADS; j < ls[l + 1]; j += SWEEP_THREADS) {   // wider levels
+                const int e = order[j];
+                const int r = e & ((1 << PASS_SHIFT) - 1), p = e >> PASS_SHIFT;
+                run_pass_direct(A, V, I, c0 + run_k[r], run_n[r], vel, warm && p == 0, p == 0, slop);
+            }
+            __syncthreads();
+            ecur = enext;
+        }
+        if (prefetch) async_wait_all();
+        if (V.s) {
+            for (int i = tid; i < nb; i += SWEEP_THREADS) {
+                if (A.mtype[b0 + i] != 2) continue;
+                double lv[3], av[3];
+                vel_load(A, V, b0 + i, lv, av);
+                A.v[(b0 + i) * 3] = lv[0]; A.v[(b0 + i) * 3 + 1] = lv[1]; A.v[(b0 + i) * 3 + 2] = lv[2];
+                A.w[(b0 + i) * 3] = av[0]; A.w[(b0 + i) * 3 + 1] = av[1]; A.w[(b0 + i) * 3 + 2] = av[2];
+            }
+        }
+        if (I.s)
+            for (int i = tid; i < K * 3; i += SWEEP_THREADS) A.c_imp[c0 * 3 + i] = I.s[i];
+        __syncthreads();
     }
 }
 

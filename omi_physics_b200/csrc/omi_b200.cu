@@ -21,13 +21,13 @@ namespace {
 
 enum KernelId {
     KN_REFIT, KN_SORT, KN_PAIR_COUNT, KN_PAIR_SCAN, KN_PAIR_EMIT, KN_NARROW, KN_GJK,
-    KN_CONTACT_SCAN, KN_INTEGRATE_FORCES, KN_COMPACT, KN_SOLVE, KN_CACHE, KN_JOINTS,
-    KN_FINALIZE, KN_COUNT
+    KN_CONTACT_SCAN, KN_INTEGRATE_FORCES, KN_COMPACT, KN_WAKE, KN_PREP, KN_LEVELS, KN_SOLVE,
+    KN_CACHE, KN_JOINTS, KN_FINALIZE, KN_COUNT
 };
 const char *kKernelNames[KN_COUNT] = {
     "refit", "sort", "pair_count", "pair_scan", "pair_emit", "narrow", "gjk_epa",
-    "contact_scan", "integrate_forces", "contact_compact", "solve", "cache_store", "joints",
-    "integrate_positions_sleep"};
+    "contact_scan", "integrate_forces", "contact_compact", "wake", "prep", "levels", "solve",
+    "cache_store", "joints", "integrate_positions_sleep"};
 
 struct Buf {
     void *p = nullptr;
@@ -49,6 +49,8 @@ struct OmiCtx {
     bool loaded = false;
     int max_world_n = 0, max_world_j = 0, sort_cap = 0, sort_block = 256;
     int solve_block = 128;
+    int stage_cap = 0;             // bodies whose level scan keeps `last` in shared memory
+    int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
     cudaGraphExec_t graph = nullptr;
     int *h_status = nullptr;       // pinned mirror of the status words
@@ -118,6 +120,11 @@ void drop_graph(OmiCtx *ctx) {
     ctx->graph = nullptr;
 }
 
+int passes_of(int flags, int iters) {
+    const int p = ((flags & OMI_WF_WARM) ? 1 : 0) + std::max(iters, 0);
+    return std::max(p, 1);
+}
+
 int grid_for(int n, int block, int cap) {
     int g = (n + block - 1) / block;
     return std::max(1, std::min(g, cap));
@@ -152,9 +159,15 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.c_depth, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.c_imp, (size_t)contact_cap * 3);
     rc |= alloc(ctx, ctx->dyn, A.c_data, (size_t)contact_cap * CD);
-    rc |= alloc(ctx, ctx->dyn, A.c_level, contact_cap);
-    rc |= alloc(ctx, ctx->dyn, A.c_order, contact_cap);
-    rc |= alloc(ctx, ctx->dyn, A.c_level_start, 2 * ((size_t)contact_cap + A.W + 1));
+    const size_t entries = (size_t)contact_cap * A.max_passes;
+    rc |= alloc(ctx, ctx->dyn, A.c_level, entries);
+    rc |= alloc(ctx, ctx->dyn, A.c_order, entries);
+    rc |= alloc(ctx, ctx->dyn, A.c_level_start, 2 * (entries + A.W + 1));
+    rc |= alloc(ctx, ctx->dyn, A.run_mask, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_k, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_n, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_a, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_b, contact_cap);
     size_t scan_n = std::max<size_t>((size_t)pair_cap, (size_t)A.NB) / SCAN_TILE + 2;
     rc |= alloc(ctx, ctx->dyn, A.scan_blocks, scan_n + 1);
     if (rc) return rc;
@@ -270,8 +283,16 @@ void stage_compact(OmiCtx *ctx, Prof *pf) {
 
 void stage_solve(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
-    k_solve<<<std::min(A.W, 65535), ctx->solve_block, 0, ctx->stream>>>(A);
-    ctx->launches++;
+    const int wb = 32 * SOLVE_WARPS;
+    const int wg = std::max(1, (A.W + SOLVE_WARPS - 1) / SOLVE_WARPS);
+    k_wake<<<wg, wb, 0, ctx->stream>>>(A);
+    mark(ctx, pf, KN_WAKE);
+    k_prep<<<grid_for(A.contact_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    mark(ctx, pf, KN_PREP);
+    k_levels<<<wg, wb, (size_t)SOLVE_WARPS * (ctx->stage_cap + LEVEL_COUNT_CAP) * sizeof(int), ctx->stream>>>(A, ctx->stage_cap);
+    mark(ctx, pf, KN_LEVELS);
+    k_iterate<<<std::min(A.W, 65535), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
+    ctx->launches += 4;
     mark(ctx, pf, KN_SOLVE);
     k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
     k_hash_clear<<<grid_for(ctx->cache_cap, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
@@ -355,7 +376,7 @@ int capture(OmiCtx *ctx) {
 
 int64_t step_launches(OmiCtx *ctx) {
     // kernels per captured step (same sequence as enqueue_step)
-    int64_t n = 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 5 + 1;
+    int64_t n = 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
     if (ctx->A.NJ > 0) n += 1;
     return n;
 }
@@ -424,6 +445,8 @@ int omi_create(int device, OmiCtx **out) {
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
     cudaFuncSetAttribute(k_gjk, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * (int)sizeof(EpaWork));
     cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
+    cudaFuncSetAttribute(k_iterate, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM_DOUBLES * (int)sizeof(double));
+    cudaFuncSetAttribute(k_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_WARPS * (3584 + LEVEL_COUNT_CAP) * (int)sizeof(int));
     *out = ctx;
     return 0;
 }
@@ -546,6 +569,12 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->h_body_off.assign(s->w_body_off, s->w_body_off + W + 1);
     ctx->h_body_n.assign(body_n, body_n + W);
     ctx->h_joint_off.assign(s->w_joint_off, s->w_joint_off + W + 1);
+    {
+        std::vector<int> sched(W);
+        for (int w = 0; w < W; w++) sched[w] = w;
+        std::stable_sort(sched.begin(), sched.end(), [&](int x, int y) { return body_n[x] > body_n[y]; });
+        rc |= upload(ctx, const_cast<int *&>(A.w_sched), sched.data(), W);
+    }
     rc |= upload(ctx, const_cast<double *&>(A.w_g), s->w_gravity, (size_t)W * 3);
     rc |= upload(ctx, const_cast<double *&>(A.w_dt), s->w_dt, W);
     rc |= upload(ctx, const_cast<int *&>(A.w_iters), s->w_iters, W);
@@ -636,6 +665,8 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.b_parent, NB);
     rc |= alloc(ctx, ctx->statics, A.b_island, NB);
     rc |= alloc(ctx, ctx->statics, A.b_flag, NB);
+    rc |= alloc(ctx, ctx->statics, A.w_levels, W);
+    rc |= alloc(ctx, ctx->statics, A.w_runs, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
@@ -651,6 +682,13 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
     ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
     ctx->solve_block = max_n > 1024 ? 256 : 128;
+    ctx->stage_cap = std::min(std::max(max_nc, 1), 3584);
+    // velocities (6 per body) and impulses of the largest world, then run
+    // buffers; small worlds need little, the largest take the whole 227 KB
+    ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
+                                                (int64_t)std::max(max_nc, 1) * 6 * 3 + SWEEP_THREADS * 2 * RUNBUF);
+    A.max_passes = 1;
+    for (int w = 0; w < W; w++) A.max_passes = std::max(A.max_passes, passes_of(s->w_flags[w], s->w_iters[w]));
     const int pair_cap = std::max(4096, 4 * NB);
     rc = alloc_dynamic(ctx, pair_cap, 2 * pair_cap);
     if (rc) return rc;
@@ -733,6 +771,14 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
     if (n > c.bodies || ns > c.shapes || nm > c.materials || np_ > c.points || nj > c.joints ||
         rows > c.filter_rows || rows < 1 || npf > c.pair_friction || o->n_filter_bytes < rows * rows)
         return fail(ctx, OMI_E_ARG, "world exceeds the slot capacities");
+    {
+        const int need = passes_of(o->w_flags[0], o->w_iters[0]);
+        if (need > A.max_passes) {
+            A.max_passes = need;
+            const int rc0 = alloc_dynamic(ctx, A.pair_cap, A.contact_cap);
+            if (rc0) return rc0;
+        }
+    }
     const int b0 = slot * c.bodies, s0 = slot * std::max(c.shapes, 1), m0 = slot * std::max(c.materials, 1);
     const int p0 = slot * std::max(c.points, 1), j0 = slot * c.joints;
     std::vector<int> shape(n), mat(n), body_world(n, slot);
@@ -833,6 +879,14 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
     for (int t = 0; t < 2; t++) rc |= put(ctx, A.w_cache_n[t] + slot, zero2, 1);
     if (rc) return rc;
     ctx->h_body_n[slot] = n;
+    {
+        std::vector<int> sched(A.W);
+        for (int w = 0; w < A.W; w++) sched[w] = w;
+        std::stable_sort(sched.begin(), sched.end(),
+                         [&](int x, int y) { return ctx->h_body_n[x] > ctx->h_body_n[y]; });
+        rc |= put(ctx, const_cast<int *>(A.w_sched), sched.data(), A.W);
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     ctx->h_active[slot] = (o->w_flags[0] & OMI_WF_ACTIVE) ? 1 : 0;
     rc = put(ctx, const_cast<uint8_t *>(A.w_active) + slot, &ctx->h_active[slot], 1);
     if (rc) return rc;
@@ -853,6 +907,19 @@ int omi_set_world_params(OmiCtx *ctx, const double *dt, const int32_t *iters, co
     if (!ctx) return OMI_E_ARG;
     if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "no scene loaded");
     Arena &A = ctx->A;
+    if (iters || flags) {
+        std::vector<int> cur_it(A.W), cur_fl(A.W);
+        CK(cudaMemcpy(cur_it.data(), A.w_iters, sizeof(int) * A.W, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(cur_fl.data(), A.w_flags, sizeof(int) * A.W, cudaMemcpyDeviceToHost));
+        int need = 1;
+        for (int w = 0; w < A.W; w++)
+            need = std::max(need, passes_of(flags ? flags[w] : cur_fl[w], iters ? iters[w] : cur_it[w]));
+        if (need > A.max_passes) {
+            A.max_passes = need;
+            const int rc0 = alloc_dynamic(ctx, A.pair_cap, A.contact_cap);
+            if (rc0) return rc0;
+        }
+    }
     int rc = 0;
     if (dt) rc |= put(ctx, const_cast<double *>(A.w_dt), dt, A.W);
     if (iters) rc |= put(ctx, const_cast<int *>(A.w_iters), iters, A.W);
@@ -1113,6 +1180,14 @@ int omi_get_contacts(OmiCtx *ctx, int32_t w, int32_t *a, int32_t *b, double *pt,
     CK(cp(imp, A.c_imp + (size_t)c0 * 3, sizeof(double) * 3 * n));
     CK(cudaStreamSynchronize(ctx->stream));
     return n;
+}
+
+int omi_world_levels(OmiCtx *ctx, int32_t *levels) {
+    STAGE_PRELUDE
+    if (!levels) return fail(ctx, OMI_E_ARG, "null output");
+    CK(cudaMemcpyAsync(levels, ctx->A.w_levels, sizeof(int) * ctx->A.W, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
 }
 
 int omi_get_islands(OmiCtx *ctx, int32_t w, int32_t *labels) {
