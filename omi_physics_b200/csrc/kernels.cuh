@@ -883,58 +883,193 @@ __device__ inline void bucket_entries_warp(int R, int P, int D, const int *level
 
 // per-warp shared slice for `last` (worlds up to `last_cap` bodies; larger
 // ones use the global per-body array)
-constexpr int LEVEL_COUNT_CAP = 4096;   // per-warp shared level counters
+// ---------------------------------------------------------------------------
+// Gauss-Seidel levels of one world (one block per world).
+//
+// The sequential sweep visits (pass p, run r) in the order p-major, r-minor.
+// Entry (p, r) must follow the latest earlier entry that touches each of its
+// dynamic bodies: the previous run of that body in the same pass, or, for the
+// body's first run of the pass, its last run of pass p - 1. Its level is the
+// longest such chain ending at it; entries of one level touch disjoint
+// dynamic bodies and any order among them gives the sequential result.
+// (Every run has a dynamic body - the broadphase keeps no pair of two static
+// or kinematic bodies - so (p - 1, r) is always on a chain into (p, r).)
+//
+// In shared memory: per run and side (two arrays), a predecessor code (>= 0: the run of
+// the same pass; < 0 and not LEVEL_NONE: -(run of the previous pass) - 1),
+// found from per-body run buckets; then the levels by in-place max-plus
+// relaxation from zero. Each thread owns a contiguous stretch of entries in
+// sweep order, so chains inside a stretch settle in one round; the stretch
+// length is odd, so a warp's 32 stretches start in 32 different shared-memory
+// banks. Values only grow and stay below the true levels, and a round without
+// change is the fixed point (at most D + 1 rounds). Worlds whose tables exceed the shared
+// memory take the warp-sequential scan instead.
+// ---------------------------------------------------------------------------
+constexpr int LEVEL_THREADS = 1024;
+constexpr int LEVEL_SMEM_INTS = 56 * 1024;
+constexpr int LEVEL_NONE = -2147483647 - 1;
 
-__global__ void k_levels(Arena A, int last_cap) {
-    extern __shared__ int last_smem[];
+__device__ __forceinline__ int run_pred_code(const int *list, int s, int e, int r) {
+    int pred = -1, mx = -1;
+    for (int j = s; j < e; j++) {
+        const int q = list[j];
+        if (q < r && q > pred) pred = q;
+        mx = max(mx, q);
+    }
+    return pred >= 0 ? pred : -(mx + 1);
+}
+
+// block-wide exclusive scan of cnt[0..n) into out[0..n) (out may be global);
+// cnt is cleared for use as a fill cursor
+__device__ inline void block_scan_reset(int *cnt, int *out, int n, int *sh) {
+    int carry = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? cnt[i] : 0;
+        int tot;
+        const int x = block_exclusive_scan(v, sh, &tot);
+        if (i < n) { out[i] = carry + x; cnt[i] = 0; }
+        carry += tot;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints) {
+    extern __shared__ int lsm[];
+    __shared__ int scan_sh[33];
     if (overflowed(A)) return;
-    const int lane = threadIdx.x & 31;
-    int *my_last = last_smem + (threadIdx.x >> 5) * (last_cap + LEVEL_COUNT_CAP);
-    int *my_counts = my_last + last_cap;
-    for (int wi = warp_global_id(); wi < A.W; wi += warp_count()) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
         if (!world_collides(A, w)) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
         const int K = c1 - c0;
-        if (K == 0) { if (lane == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; } continue; }
-        // runs in contact order; level bodies: the dynamic ones
+        if (K == 0) {
+            if (tid == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; }
+            continue;
+        }
+        // runs: maximal stretches of consecutive contacts of one pair
         int R = 0;
-        for (int base = 0; base < K; base += 32) {
-            const int k = base + lane;
-            bool start = false;
-            int a = -1, b = -1;
+        for (int base = 0; base < K; base += T) {
+            const int k = base + tid;
+            int start = 0, a = -1, b = -1;
             if (k < K) {
                 a = A.c_a[c0 + k];
                 b = A.c_b[c0 + k];
                 start = k == 0 || a != A.c_a[c0 + k - 1] || b != A.c_b[c0 + k - 1];
             }
-            const unsigned m = __ballot_sync(FULL, start);
+            int tot;
+            const int r = R + block_exclusive_scan(start, scan_sh, &tot);
             if (start) {
-                const int r = R + __popc(m & ((1u << lane) - 1u));
                 A.run_k[c0 + r] = k;
                 A.run_a[c0 + r] = A.mtype[a] == 2 ? a : -1;
                 A.run_b[c0 + r] = A.mtype[b] == 2 ? b : -1;
             }
-            R += __popc(m);
+            R += tot;
         }
-        __syncwarp();
-        for (int r = lane; r < R; r += 32) {
+        __syncthreads();
+        for (int r = tid; r < R; r += T) {
             const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
             A.run_n[c0 + r] = end - A.run_k[c0 + r];
         }
-        const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
-        int *last = nb <= last_cap ? my_last : A.b_last + b0;
-        for (int i = lane; i < nb; i += 32) last[i] = -1;
-        __syncwarp();
         const int P = world_passes(A, w);
+        const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+        const int N = P * R;
         const size_t e0 = (size_t)c0 * A.max_passes;
-        int D = 0;
-        for (int p = 0; p < P; p++) D = max(D, warp_levels_pass(A, c0, R, p, last, b0, A.c_level + e0 + (size_t)p * R));
         int *ls = A.c_level_start + e0 + w;
+        int *order = A.c_order + e0;
         int *cursor = A.c_level_start + ((size_t)A.contact_cap * A.max_passes + A.W + 1) + e0 + w;
-        bucket_entries_warp(R, P, D, A.c_level + e0, ls, cursor, A.c_order + e0, my_counts, LEVEL_COUNT_CAP);
-        if (lane == 0) { A.w_levels[w] = D; A.w_runs[w] = R; }
+        int D = 0;
+        if (2 * R + max(2 * nb + 1 + 2 * R, N) <= smem_ints) {
+            int *code_a = lsm, *code_b = lsm + R;    // per run
+            int *cnt = lsm + 2 * R;          // per body, then the fill cursor
+            int *bstart = cnt + nb;          // nb + 1
+            int *list = bstart + nb + 1;     // 2R run indices, bucketed by body
+            int *lvl = lsm + 2 * R;          // N levels (after the buckets are done)
+            for (int i = tid; i < nb; i += T) cnt[i] = 0;
+            __syncthreads();
+            for (int r = tid; r < R; r += T) {
+                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+                if (a >= 0) atomicAdd(&cnt[a - b0], 1);
+                if (b >= 0) atomicAdd(&cnt[b - b0], 1);
+            }
+            __syncthreads();
+            block_scan_reset(cnt, bstart, nb, scan_sh);
+            if (tid == 0) bstart[nb] = 2 * R;     // unused tail: only bodies' own ranges are read
+            for (int r = tid; r < R; r += T) {
+                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+                if (a >= 0) list[bstart[a - b0] + atomicAdd(&cnt[a - b0], 1)] = r;
+                if (b >= 0) list[bstart[b - b0] + atomicAdd(&cnt[b - b0], 1)] = r;
+            }
+            __syncthreads();
+            for (int r = tid; r < R; r += T) {
+                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+                int ca = LEVEL_NONE, cb = LEVEL_NONE;
+                if (a >= 0) ca = run_pred_code(list, bstart[a - b0], bstart[a - b0] + cnt[a - b0], r);
+                if (b >= 0) cb = run_pred_code(list, bstart[b - b0], bstart[b - b0] + cnt[b - b0], r);
+                code_a[r] = ca;
+                code_b[r] = cb;
+            }
+            __syncthreads();
+            for (int e = tid; e < N; e += T) lvl[e] = 0;
+            __syncthreads();
+            const int ch = ((N + T - 1) / T) | 1;
+            const int e_lo = min(N, tid * ch), e_hi = min(N, e_lo + ch);
+            volatile int *vl = lvl;
+            for (int round = 0; round <= N; round++) {
+                int changed = 0;
+                int p = e_lo / R, r = e_lo - p * R;
+                for (int e = e_lo; e < e_hi; e++) {
+                    const int ca = code_a[r], cb = code_b[r];
+                    int v = 0;
+                    if (ca >= 0) v = vl[p * R + ca] + 1;
+                    else if (ca != LEVEL_NONE && p > 0) v = vl[(p - 1) * R - ca - 1] + 1;
+                    if (cb >= 0) v = max(v, vl[p * R + cb] + 1);
+                    else if (cb != LEVEL_NONE && p > 0) v = max(v, vl[(p - 1) * R - cb - 1] + 1);
+                    if (v != vl[e]) { vl[e] = v; changed = 1; }
+                    if (++r == R) { r = 0; p++; }
+                }
+                if (!__syncthreads_or(changed)) break;
+            }
+            int mx = -1;
+            for (int e = e_lo; e < e_hi; e++) mx = max(mx, lvl[e]);
+            mx = __reduce_max_sync(FULL, mx);
+            if ((tid & 31) == 0) scan_sh[tid >> 5] = mx;
+            __syncthreads();
+            if (tid < 32) {
+                int m = tid < (T >> 5) ? scan_sh[tid] : -1;
+                m = __reduce_max_sync(FULL, m);
+                if (tid == 0) scan_sh[32] = m + 1;
+            }
+            __syncthreads();
+            D = scan_sh[32];
+            // bucket the entries by level; order inside a level is free
+            int *lc = D + 1 <= 2 * R ? lsm : cursor;
+            for (int l = tid; l <= D; l += T) lc[l] = 0;
+            __syncthreads();
+            for (int e = e_lo; e < e_hi; e++) atomicAdd(&lc[lvl[e]], 1);
+            __syncthreads();
+            block_scan_reset(lc, ls, D + 1, scan_sh);
+            {
+                int p = e_lo / R, r = e_lo - p * R;
+                for (int e = e_lo; e < e_hi; e++) {
+                    const int l = lvl[e];
+                    order[ls[l] + atomicAdd(&lc[l], 1)] = (p << PASS_SHIFT) | r;
+                    if (++r == R) { r = 0; p++; }
+                }
+            }
+        } else if (tid < 32) {
+            // warp-sequential scan with `last` in global memory
+            int *last = A.b_last + b0;
+            for (int i = tid; i < nb; i += 32) last[i] = -1;
+            __syncwarp();
+            for (int p = 0; p < P; p++)
+                D = max(D, warp_levels_pass(A, c0, R, p, last, b0, A.c_level + e0 + (size_t)p * R));
+            bucket_entries_warp(R, P, D, A.c_level + e0, ls, cursor, order, lsm, smem_ints);
+        }
+        if (tid == 0) { A.w_levels[w] = D; A.w_runs[w] = R; }
+        __syncthreads();
     }
 }
 

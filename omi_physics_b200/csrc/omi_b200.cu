@@ -49,7 +49,7 @@ struct OmiCtx {
     bool loaded = false;
     int max_world_n = 0, max_world_j = 0, sort_cap = 0, sort_block = 256;
     int solve_block = 128;
-    int stage_cap = 0;             // bodies whose level scan keeps `last` in shared memory
+    int level_ints = 0;            // shared ints of one k_levels block
     int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
     cudaGraphExec_t graph = nullptr;
@@ -289,7 +289,7 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     mark(ctx, pf, KN_WAKE);
     k_prep<<<grid_for(A.contact_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
     mark(ctx, pf, KN_PREP);
-    k_levels<<<wg, wb, (size_t)SOLVE_WARPS * (ctx->stage_cap + LEVEL_COUNT_CAP) * sizeof(int), ctx->stream>>>(A, ctx->stage_cap);
+    k_levels<<<std::min(A.W, 65535), LEVEL_THREADS, (size_t)ctx->level_ints * sizeof(int), ctx->stream>>>(A, ctx->level_ints);
     mark(ctx, pf, KN_LEVELS);
     k_iterate<<<std::min(A.W, 65535), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
     ctx->launches += 4;
@@ -446,7 +446,7 @@ int omi_create(int device, OmiCtx **out) {
     cudaFuncSetAttribute(k_gjk, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * (int)sizeof(EpaWork));
     cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
     cudaFuncSetAttribute(k_iterate, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM_DOUBLES * (int)sizeof(double));
-    cudaFuncSetAttribute(k_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, SOLVE_WARPS * (3584 + LEVEL_COUNT_CAP) * (int)sizeof(int));
+    cudaFuncSetAttribute(k_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, LEVEL_SMEM_INTS * (int)sizeof(int));
     *out = ctx;
     return 0;
 }
@@ -682,7 +682,8 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
     ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
     ctx->solve_block = max_n > 1024 ? 256 : 128;
-    ctx->stage_cap = std::min(std::max(max_nc, 1), 3584);
+    // level tables of the largest world: about 2 + P ints per run, runs ~1.5 per body
+    ctx->level_ints = (int)std::min<int64_t>(LEVEL_SMEM_INTS, 32 * (int64_t)std::max(max_nc, 1) + 1024);
     // velocities (6 per body) and impulses of the largest world, then run
     // buffers; small worlds need little, the largest take the whole 227 KB
     ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
