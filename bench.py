@@ -50,6 +50,9 @@ def parse():
     ap.add_argument('--preroll', type=int, default=240,
                     help='steps every world is advanced before timing (settled piles)')
     ap.add_argument('--no-extras', action='store_true')
+    ap.add_argument('--serve-requests', type=int, default=None,
+                    help='requests in the serving run (default: --worlds; 0 skips it)')
+    ap.add_argument('--serve-slots', type=int, default=96, help='slots per size class')
     return ap.parse_args()
 
 
@@ -306,11 +309,41 @@ def run_ours(args, rank, world, local):
            'd2h_bytes_per_step': h2d, 'path': 'omi_upload_state + omi_step + omi_download_state, pinned'}
 
     extras = {}
+    n_serve = args.worlds if args.serve_requests is None else args.serve_requests
+    if not args.no_extras and n_serve > 0:
+        extras['serving'] = serving_run(n_serve, args.seed + 1000 * rank, args.serve_slots, stream)
+        barrier(world)
     if not args.no_extras and rank == 0:
         extras['plain'] = plain_per_world(worlds, reqs, args.plain_sample, local, args.preroll)
     return dict(value=value, ms=ms_max, N=total_N, P=P, K=K, launches=launches, setup_s=setup_s,
                 ticks=ticks, roofline=roofline, e2e=e2e, clocks=clk.summary(), extras=extras,
                 NB=NB)
+
+
+SERVE_BUDGET = 120 * 10 ** 9
+
+
+def serving_run(n_requests, seed, per_class, stream):
+    """The request loop: Poisson arrivals (200/s), each world admitted into a
+    free slot of its size class under the HBM budget, stepped with every other
+    resident world once per tick until its 60-600 steps are done."""
+    from omi_physics_b200 import scenes
+    from omi_physics_b200.serving import Server, size_classes
+    reqs = scenes.serving_requests(n_requests, seed=seed)
+    srv = Server(size_classes(2048, per_class=per_class), budget_bytes=SERVE_BUDGET,
+                 stream=stream.cuda_stream)
+    for r in reqs:
+        w, meta = scenes.serving_world(r)
+        srv.submit(w, r['steps'], dt=meta['dt'], arrival=r['arrival'])
+    srv.ctx.call('step', 1)         # capture the step graph while every slot is empty
+    st = srv.run(clock='wall').summary()
+    srv.close()
+    st.update(requests=n_requests, arrival_rate_per_s=200.0, slots=srv.W,
+              slot_classes='bodies 33..2049 (powers of two + ground), %d each' % per_class,
+              budget_bytes=SERVE_BUDGET,
+              note='wall-clock ticks: admit (omi_load_world) + one omi_step of all resident '
+                   'worlds + retire (state download); body-steps/s is bounded by the arrival rate')
+    return st
 
 
 def plain_per_world(worlds, reqs, sample, device, preroll):
@@ -433,6 +466,8 @@ def main():
             'dynamic_bodies': res['N'], 'rows': res['NB'], 'pairs': res['P'], 'contacts': res['K'],
         }
         ex = res['extras']
+        if 'serving' in ex:
+            line['serving'] = ex['serving']
         if 'plain' in ex:
             line['plain_per_world'] = ex['plain']
             line['batched_over_plain'] = res['value'] / world / ex['plain']['value']

@@ -129,6 +129,9 @@ typedef struct OmiSlotCaps {
     int32_t bodies, shapes, materials, points, joints, filter_rows, pair_friction;
 } OmiSlotCaps;
 int omi_reserve_slots(OmiCtx *ctx, int32_t n_slots, const OmiSlotCaps *caps);
+/* The same with capacities per slot (caps[n_slots]): slots of several size
+ * classes in one arena, so small requests do not hold large slots. */
+int omi_reserve_slots_each(OmiCtx *ctx, int32_t n_slots, const OmiSlotCaps *caps);
 /* Admit one world (an OmiScene with n_worlds == 1, local indices) into a
  * slot: its tables and state are copied in, its warm-start cache cleared and
  * the slot activated when OMI_WF_ACTIVE is set. No reallocation, no graph

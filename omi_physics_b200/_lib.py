@@ -82,6 +82,7 @@ PROTOTYPES = {
     'omi_set_active': (C.c_int, [C.c_void_p, U8]),
     'omi_set_world_params': (C.c_int, [C.c_void_p, D, I, I, I]),
     'omi_reserve_slots': (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(OmiSlotCaps)]),
+    'omi_reserve_slots_each': (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(OmiSlotCaps)]),
     'omi_load_world': (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(OmiScene)]),
     'omi_world_rows': (C.c_int, [C.c_void_p, C.c_int32, I, I]),
     'omi_upload_state': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, D, D, D, D, U8, D]),

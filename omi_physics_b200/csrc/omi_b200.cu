@@ -36,6 +36,12 @@ struct Buf {
 
 }  // namespace
 
+// Serving slots: per-slot capacities and the first row of each of its tables.
+struct SlotTable {
+    std::vector<OmiSlotCaps> caps;
+    std::vector<int64_t> b0, s0, m0, p0, j0, f0, pf0;   // n + 1 prefix sums
+};
+
 struct OmiCtx {
     int device = 0;
     cudaStream_t own = nullptr, stream = nullptr;
@@ -59,7 +65,7 @@ struct OmiCtx {
     std::vector<uint8_t> h_active;
     std::vector<int> h_body_off, h_body_n, h_joint_off;
     bool slots = false;
-    OmiSlotCaps caps{};
+    SlotTable slot;                // capacities and table offsets of each slot
 };
 
 namespace {
@@ -709,19 +715,35 @@ int omi_load(OmiCtx *ctx, const OmiScene *s) {
     return load_impl(ctx, s, bn.data(), jn.data());
 }
 
-int omi_reserve_slots(OmiCtx *ctx, int32_t n, const OmiSlotCaps *caps) {
-    if (!ctx || !caps || n <= 0 || caps->bodies <= 0 || caps->filter_rows < 1 || caps->shapes < 0 ||
-        caps->materials < 0 || caps->points < 0 || caps->joints < 0 || caps->pair_friction < 0)
-        return fail(ctx, OMI_E_ARG, "bad slot capacities");
-    const OmiSlotCaps c = *caps;
-    const size_t NB = (size_t)n * c.bodies, NS = (size_t)n * std::max(c.shapes, 1);
-    const size_t NM = (size_t)n * std::max(c.materials, 1), NP = (size_t)n * std::max(c.points, 1);
-    const size_t NJ = (size_t)n * c.joints, NF = (size_t)n * c.filter_rows * c.filter_rows;
-    const size_t NPF = (size_t)n * c.pair_friction;
-    if (NB > (1u << 30) || NF > (1u << 30)) return fail(ctx, OMI_E_ARG, "slot arena too large");
+int omi_reserve_slots_each(OmiCtx *ctx, int32_t n, const OmiSlotCaps *caps) {
+    if (!ctx || !caps || n <= 0) return fail(ctx, OMI_E_ARG, "bad slot capacities");
+    for (int w = 0; w < n; w++) {
+        const OmiSlotCaps &c = caps[w];
+        if (c.bodies <= 0 || c.filter_rows < 1 || c.shapes < 0 || c.materials < 0 || c.points < 0 ||
+            c.joints < 0 || c.pair_friction < 0 || c.bodies > (1 << 24) || c.filter_rows > 4096)
+            return fail(ctx, OMI_E_ARG, "bad slot capacities");
+    }
+    // per-slot table offsets: prefix sums of the capacities (empty tables keep one row)
+    SlotTable t;
+    t.caps.assign(caps, caps + n);
+    for (auto *v : {&t.b0, &t.s0, &t.m0, &t.p0, &t.j0, &t.f0, &t.pf0}) v->assign(n + 1, 0);
+    for (int w = 0; w < n; w++) {
+        const OmiSlotCaps &c = caps[w];
+        t.b0[w + 1] = t.b0[w] + c.bodies;
+        t.s0[w + 1] = t.s0[w] + std::max(c.shapes, 1);
+        t.m0[w + 1] = t.m0[w] + std::max(c.materials, 1);
+        t.p0[w + 1] = t.p0[w] + std::max(c.points, 1);
+        t.j0[w + 1] = t.j0[w] + c.joints;
+        t.f0[w + 1] = t.f0[w] + (int64_t)c.filter_rows * c.filter_rows;
+        t.pf0[w + 1] = t.pf0[w] + c.pair_friction;
+    }
+    if (t.b0[n] > (1 << 30) || t.f0[n] > (1 << 30) || t.s0[n] > (1 << 30) || t.p0[n] > (1 << 30) ||
+        t.j0[n] > (1 << 30) || t.m0[n] > (1 << 30) || t.pf0[n] > (1 << 30))
+        return fail(ctx, OMI_E_ARG, "slot arena too large");
+    const size_t NB = t.b0[n], NS = t.s0[n], NM = t.m0[n], NP = t.p0[n], NJ = t.j0[n], NF = t.f0[n], NPF = t.pf0[n];
     std::vector<int> body_off(n + 1), joint_off(n + 1), zeros_w(n, 0), frows(n, 1), foff(n), pfoff(n), iters(n, 10);
-    for (int w = 0; w <= n; w++) { body_off[w] = w * c.bodies; joint_off[w] = w * c.joints; }
-    for (int w = 0; w < n; w++) { foff[w] = w * c.filter_rows * c.filter_rows; pfoff[w] = w * c.pair_friction; }
+    for (int w = 0; w <= n; w++) { body_off[w] = (int)t.b0[w]; joint_off[w] = (int)t.j0[w]; }
+    for (int w = 0; w < n; w++) { foff[w] = (int)t.f0[w]; pfoff[w] = (int)t.pf0[w]; }
     std::vector<double> g(3 * n, 0.0), dt(n, 1.0 / 60.0), damp(2 * n, 0.0), solver(2 * n);
     for (int w = 0; w < n; w++) { solver[2 * w] = 0.5; solver[2 * w + 1] = 0.005; }
     std::vector<double> zb(NB * 4, 0.0), qb(NB * 4, 0.0);
@@ -752,20 +774,27 @@ int omi_reserve_slots(OmiCtx *ctx, int32_t n, const OmiSlotCaps *caps) {
     s.j_anchor = zs.data(); s.j_anchor_b = zs.data(); s.j_local_a = zs.data(); s.j_local_b = zs.data();
     s.j_has_local_a = zu.data(); s.j_has_local_b = zu.data(); s.j_length = zs.data(); s.j_has_length = zu.data();
     s.j_axis = zs.data(); s.j_target = zs.data(); s.j_max_force = zs.data(); s.j_accum = zs.data();
-    // motor rows need a body: empty slots hold point joints between the world and itself
+    // empty slots: no live bodies, no joints, inactive
     int rc = load_impl(ctx, &s, zeros_w.data(), zeros_w.data());
     if (rc) return rc;
     ctx->slots = true;
-    ctx->caps = c;
+    ctx->slot = std::move(t);
     return 0;
+}
+
+int omi_reserve_slots(OmiCtx *ctx, int32_t n, const OmiSlotCaps *caps) {
+    if (!ctx || !caps || n <= 0) return fail(ctx, OMI_E_ARG, "bad slot capacities");
+    std::vector<OmiSlotCaps> each(n, *caps);
+    return omi_reserve_slots_each(ctx, n, each.data());
 }
 
 int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
     if (!ctx || !o) return OMI_E_ARG;
     if (!ctx->loaded || !ctx->slots) return fail(ctx, OMI_E_STATE, "omi_reserve_slots first");
-    const OmiSlotCaps &c = ctx->caps;
     Arena &A = ctx->A;
     if (slot < 0 || slot >= A.W) return fail(ctx, OMI_E_ARG, "slot out of range");
+    const SlotTable &T = ctx->slot;
+    const OmiSlotCaps &c = T.caps[slot];
     if (o->n_worlds != 1) return fail(ctx, OMI_E_ARG, "one world per slot");
     const int n = o->n_bodies, ns = o->n_shapes, nm = o->n_materials, np_ = o->n_points;
     const int nj = o->n_joints, rows = o->w_filter_rows[0], npf = o->n_pair_friction;
@@ -780,8 +809,8 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
             if (rc0) return rc0;
         }
     }
-    const int b0 = slot * c.bodies, s0 = slot * std::max(c.shapes, 1), m0 = slot * std::max(c.materials, 1);
-    const int p0 = slot * std::max(c.points, 1), j0 = slot * c.joints;
+    const int b0 = (int)T.b0[slot], s0 = (int)T.s0[slot], m0 = (int)T.m0[slot];
+    const int p0 = (int)T.p0[slot], j0 = (int)T.j0[slot];
     std::vector<int> shape(n), mat(n), body_world(n, slot);
     std::vector<int8_t> kind(n, 0);
     std::vector<double> half((size_t)n * 3, 0.0);
@@ -845,7 +874,7 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
     rc |= put(ctx, const_cast<double *>(A.mat_rest) + m0, o->mat_rest, nm);
     rc |= put(ctx, const_cast<int *>(A.mat_fcomb) + m0, o->mat_fcomb, nm);
     rc |= put(ctx, const_cast<int *>(A.mat_rcomb) + m0, o->mat_rcomb, nm);
-    const int pf0 = slot * c.pair_friction, f0 = slot * c.filter_rows * c.filter_rows;
+    const int pf0 = (int)T.pf0[slot], f0 = (int)T.f0[slot];
     rc |= put(ctx, const_cast<int *>(A.pf_a) + pf0, o->pf_a, npf);
     rc |= put(ctx, const_cast<int *>(A.pf_b) + pf0, o->pf_b, npf);
     rc |= put(ctx, const_cast<double *>(A.pf_mu) + pf0, o->pf_mu, npf);

@@ -1,0 +1,293 @@
+"""Continuous-batching request loop over device-resident worlds.
+
+A :class:`Server` reserves one arena of *slots* in size classes (per-slot
+capacities, ``omi_reserve_slots_each``) under an HBM budget
+(``omi_set_budget``: the reservation fails with :class:`OutOfBudget` above it).
+Requests - a world plus a step count - queue on arrival. Every tick:
+
+1. admit queued requests that have arrived, in arrival order, each into the
+   smallest free slot whose capacities hold it (``omi_load_world``: no
+   reallocation, no graph rebuild - the other slots keep stepping);
+2. step every active slot once, all worlds in the same launches (the
+   captured CUDA graph of ``omi_step``);
+3. retire worlds whose steps are done: their rows are copied back into the
+   request's world columns and the slot is freed.
+
+Worlds never interact, so a world's result does not depend on what else is
+resident: stepping it here gives the same state as stepping it alone.
+
+The admission policy (:class:`SlotPool`) is plain Python so it can be tested
+without a GPU.
+"""
+import bisect
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from ._lib import D, I, U8, Context, OmiSlotCaps, ptr
+from .arena import pack_worlds
+
+
+@dataclass(frozen=True)
+class SlotClass:
+    """``count`` slots, each able to hold a world within these capacities."""
+    bodies: int
+    count: int
+    shapes: int = -1            # -1: same as bodies
+    materials: int = -1         # -1: same as bodies
+    points: int = 0
+    joints: int = 0
+    filter_rows: int = 8
+    pair_friction: int = 16
+
+    def caps(self) -> OmiSlotCaps:
+        return OmiSlotCaps(self.bodies, self.shapes if self.shapes >= 0 else self.bodies,
+                           self.materials if self.materials >= 0 else self.bodies, self.points,
+                           self.joints, self.filter_rows, self.pair_friction)
+
+
+def need_of(scene) -> tuple:
+    """Capacities one packed single-world scene needs, in OmiSlotCaps order."""
+    return (int(scene.n_bodies), int(scene.n_shapes), int(scene.n_materials), int(scene.n_points),
+            int(scene.n_joints), int(scene.w_filter_rows[0]), int(scene.n_pair_friction))
+
+
+def fits(caps: OmiSlotCaps, need: tuple) -> bool:
+    have = (caps.bodies, caps.shapes, caps.materials, caps.points, caps.joints, caps.filter_rows,
+            caps.pair_friction)
+    return all(n <= h for n, h in zip(need, have))
+
+
+def size_classes(max_bodies: int, per_class: int, min_bodies: int = 32, **kw) -> List[SlotClass]:
+    """Power-of-two body classes (plus one row for a ground body) up to ``max_bodies``."""
+    out, b = [], min_bodies
+    while True:
+        out.append(SlotClass(bodies=b + 1, count=per_class, **kw))
+        if b >= max_bodies:
+            return out
+        b *= 2
+
+
+class SlotPool:
+    """Free slots per class; a request takes the smallest free slot that fits."""
+
+    def __init__(self, caps: Sequence[OmiSlotCaps]):
+        self.caps = list(caps)
+        order = sorted(range(len(self.caps)), key=lambda s: (self.caps[s].bodies, s))
+        self._order = order                      # slots by capacity
+        self._bodies = [self.caps[s].bodies for s in order]
+        self.free = set(range(len(self.caps)))
+
+    def take(self, need: tuple) -> Optional[int]:
+        """A free slot holding ``need`` (smallest capacity first), or None."""
+        start = bisect.bisect_left(self._bodies, need[0])
+        for j in range(start, len(self._order)):
+            s = self._order[j]
+            if s in self.free and fits(self.caps[s], need):
+                self.free.discard(s)
+                return s
+        return None
+
+    def give_back(self, slot: int) -> None:
+        if slot in self.free:
+            raise ValueError('slot %d is already free' % slot)
+        self.free.add(slot)
+
+    def could_ever_fit(self, need: tuple) -> bool:
+        return any(fits(c, need) for c in self.caps)
+
+
+@dataclass
+class Request:
+    """One simulation request: ``steps`` steps of ``world`` at ``dt``."""
+    rid: int
+    world: object
+    steps: int
+    dt: float
+    arrival: float = 0.0
+    packed: object = None
+    need: tuple = ()
+    bodies: int = 0                 # dynamic bodies (the body-steps it contributes per step)
+    slot: int = -1
+    admitted_at: float = -1.0
+    finished_at: float = -1.0
+    done: int = 0
+
+
+@dataclass
+class ServeStats:
+    ticks: int = 0
+    tick_ms: List[float] = field(default_factory=list)      # wall time of each tick
+    step_ms: List[float] = field(default_factory=list)      # device time of each tick's step
+    body_steps: int = 0
+    wall_s: float = 0.0
+    completed: int = 0
+    peak_active: int = 0
+    wait_ms: List[float] = field(default_factory=list)      # arrival -> admission
+    device_bytes: int = 0
+
+    def summary(self) -> dict:
+        def pct(xs, q):
+            return float(np.percentile(xs, q)) if len(xs) else None
+        return {
+            'ticks': self.ticks, 'completed': self.completed, 'peak_active': self.peak_active,
+            'body_steps': self.body_steps, 'wall_s': self.wall_s,
+            'body_steps_per_s': self.body_steps / self.wall_s if self.wall_s > 0 else 0.0,
+            'tick_ms_p50': pct(self.tick_ms, 50), 'tick_ms_p99': pct(self.tick_ms, 99),
+            'step_ms_p50': pct(self.step_ms, 50), 'step_ms_p99': pct(self.step_ms, 99),
+            'wait_ms_p50': pct(self.wait_ms, 50), 'wait_ms_p99': pct(self.wait_ms, 99),
+            'device_bytes': self.device_bytes,
+        }
+
+
+class Server:
+    """Slots in HBM, requests admitted as slots free up, one step per tick."""
+
+    def __init__(self, classes: Sequence[SlotClass], device: int = 0,
+                 budget_bytes: Optional[int] = None, stream=None):
+        self.ctx = Context(device)
+        if stream is not None:
+            self.ctx.call('set_stream', stream)
+        self.stream = stream
+        if budget_bytes:
+            self.ctx.call('set_budget', int(budget_bytes))
+        caps = [c.caps() for c in classes for _ in range(c.count)]
+        arr = (OmiSlotCaps * len(caps))(*caps)
+        self.ctx.call('reserve_slots_each', len(caps), arr)
+        self.pool = SlotPool(caps)
+        self.W = len(caps)
+        self.active = np.zeros(self.W, np.uint8)
+        self.resident: Dict[int, Request] = {}
+        self.queue: List[Request] = []
+        self.finished: Dict[int, Request] = {}
+        self.stats = ServeStats(device_bytes=self.ctx.device_bytes())
+        self._next_rid = 0
+        self._events = None
+
+    # -- requests ---------------------------------------------------------------
+    def submit(self, world, steps: int, dt: float = None, arrival: float = 0.0) -> Request:
+        dt = float(world.fixed_dt if dt is None else dt)
+        packed = pack_worlds([world], [dt], active=True)
+        req = Request(self._next_rid, world, int(steps), dt, float(arrival), packed,
+                      need_of(packed.scene), int(np.count_nonzero(world.motion_type == 2)))
+        if not self.pool.could_ever_fit(req.need):
+            raise ValueError('request %d needs %s, larger than every slot class' % (req.rid, req.need))
+        self._next_rid += 1
+        i = len(self.queue)
+        while i > 0 and self.queue[i - 1].arrival > req.arrival:
+            i -= 1
+        self.queue.insert(i, req)
+        return req
+
+    def _admit(self, now: float) -> int:
+        n = 0
+        keep = []
+        for req in self.queue:
+            if req.arrival > now:
+                keep.append(req)
+                continue
+            slot = self.pool.take(req.need)
+            if slot is None:
+                keep.append(req)
+                continue
+            self.ctx.call('load_world', slot, C.byref(req.packed.scene))
+            req.slot, req.admitted_at = slot, now
+            self.active[slot] = 1
+            self.resident[slot] = req
+            self.stats.wait_ms.append(max(0.0, now - req.arrival) * 1e3)
+            n += 1
+        self.queue = keep
+        return n
+
+    def _retire(self, now: float) -> int:
+        done = [s for s, r in self.resident.items() if r.done >= r.steps]
+        if not done:
+            return 0
+        for s in done:
+            req = self.resident.pop(s)
+            self._download(req)
+            req.finished_at = now
+            self.active[s] = 0
+            self.pool.give_back(s)
+            self.finished[req.rid] = req
+            self.stats.completed += 1
+        self.ctx.call('set_active', ptr(self.active, U8))
+        return len(done)
+
+    def _download(self, req: Request) -> None:
+        first, n = C.c_int32(), C.c_int32()
+        self.ctx.call('world_rows', req.slot, C.byref(first), C.byref(n))
+        w = req.world
+        self.ctx.call('download_state', first.value, n.value, ptr(w._position, D),
+                      ptr(w._orientation, D), ptr(w._linear_velocity, D),
+                      ptr(w._angular_velocity, D), ptr(w._awake.view(np.uint8), U8),
+                      ptr(w._sleep_timer, D), ptr(w._aabb_min, D), ptr(w._aabb_max, D))
+        w.time += req.steps * req.dt
+
+    # -- ticks ------------------------------------------------------------------
+    def tick(self, now: float) -> None:
+        """Admit, step every resident world once, retire finished ones."""
+        t = time.perf_counter()
+        self._admit(now)
+        if self.resident:
+            ev = self._step_events()
+            if ev is not None:
+                ev[0].record(self._torch_stream)
+            self.ctx.call('step', 1)
+            if ev is not None:
+                ev[1].record(self._torch_stream)
+                ev[1].synchronize()
+                self.stats.step_ms.append(ev[0].elapsed_time(ev[1]))
+            for r in self.resident.values():
+                r.done += 1
+                self.stats.body_steps += r.bodies
+            self.stats.peak_active = max(self.stats.peak_active, len(self.resident))
+            self.stats.ticks += 1
+        self._retire(now)
+        self.stats.tick_ms.append((time.perf_counter() - t) * 1e3)
+
+    def _step_events(self):
+        """CUDA events on the library's stream, when it is a torch stream."""
+        if self._events is None:
+            self._events = False
+            if self.stream is not None:
+                try:
+                    import torch
+                    self._torch_stream = torch.cuda.ExternalStream(self.stream)
+                    self._events = True
+                except Exception:
+                    pass
+        if not self._events:
+            return None
+        import torch
+        return (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+
+    def run(self, clock: str = 'wall', max_ticks: int = None) -> ServeStats:
+        """Serve until every submitted request is done.
+
+        ``clock='wall'``: arrivals are seconds after the start of the loop,
+        and an idle server sleeps until the next arrival. ``clock='ticks'``:
+        arrivals are tick numbers (deterministic, for tests).
+        """
+        t0 = time.perf_counter()
+        k = 0
+        while self.queue or self.resident:
+            if clock == 'wall':
+                now = time.perf_counter() - t0
+                if not self.resident and self.queue and self.queue[0].arrival > now:
+                    time.sleep(min(self.queue[0].arrival - now, 0.05))
+                    continue
+            else:
+                now = float(k)
+            self.tick(now)
+            k += 1
+            if max_ticks is not None and k >= max_ticks:
+                break
+        self.stats.wall_s = time.perf_counter() - t0
+        return self.stats
+
+    def close(self):
+        self.ctx.close()
