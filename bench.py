@@ -33,6 +33,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from omi_physics_b200.shard import barrier, max_over_ranks, sum_over_ranks  # noqa: E402
+
 MEASURED = os.path.join(ROOT, 'MEASURED_PEAKS.json')
 FALLBACK_HBM = 6650.0
 
@@ -71,32 +73,6 @@ def dist_init(n):
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device('cuda', local))
     return rank, world, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device='cuda')
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device='cuda')
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
 
 
 # ---------------------------------------------------------------------------

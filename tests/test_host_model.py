@@ -1,0 +1,73 @@
+"""Host side without a GPU: the package's PhysicsWorld mirror builds the same
+columns as the reference (pinned by the golden fixtures' ``init/*``
+snapshots, which the reference wrote), arena packing remaps indices per
+world, and features outside the device step are rejected loudly."""
+import numpy as np
+import pytest
+
+from golden_util import SCENES, load
+from omi_physics_b200 import scenes
+from omi_physics_b200._lib import UnsupportedFeature
+from omi_physics_b200.arena import check_supported, pack_worlds
+from omi_physics_b200.backend import CudaBackend, select_backend
+
+COLUMNS = ('position', 'orientation', 'linear_velocity', 'angular_velocity', 'inv_inertia',
+           'inv_mass', 'mass', 'gravity_factor', 'linear_damping', 'angular_damping',
+           'quadratic_drag', 'sleep_timer', 'motion_type', 'collider_shape', 'collider_material',
+           'collider_filter', 'trigger_shape', 'awake')
+
+
+@pytest.mark.parametrize('scene', SCENES)
+def test_mirror_world_columns_equal_reference_init(scene):
+    g = load(scene)
+    w, _ = scenes.GOLDEN_SCENES[scene]()
+    n = w.body_count
+    assert n == len(g['init/position'])
+    for col in COLUMNS:
+        mine = np.asarray(getattr(w, '_' + col)[:n])
+        ref = g['init/' + col]
+        assert np.array_equal(mine, ref.astype(mine.dtype)), col
+
+
+def test_pack_two_worlds_offsets_and_remaps():
+    a, _ = scenes.GOLDEN_SCENES['pyramid']()
+    b, _ = scenes.GOLDEN_SCENES['chain']()
+    p = pack_worlds([a, b], [1 / 60, 1 / 240])
+    s = p.scene
+    na, nb = a.body_count, b.body_count
+    assert s.n_worlds == 2 and s.n_bodies == na + nb
+    off = p.arrays['w_body_off']
+    assert list(off) == [0, na, na + nb]
+    shape = p.arrays['shape']
+    ok = shape[na:] >= 0
+    assert np.array_equal(shape[na:][ok] - len(a.shapes), np.asarray(b._collider_shape[:nb])[ok])
+    ja = p.arrays['j_a']
+    assert s.n_joints == len(b.joint_constraints)
+    assert ((ja < 0) | ((ja >= na) & (ja < na + nb))).all()     # chain joints index world b's rows
+    assert np.array_equal(p.arrays['w_dt'], [1 / 60, 1 / 240])
+
+
+def test_unsupported_features_raise():
+    from omi_physics_b200 import model
+    w, _ = scenes.GOLDEN_SCENES['pyramid']()
+    cap = w.add_shape(model.Shape.capsule(1.0, 0.3))
+    w.add_body(model.Motion(type=model.DYNAMIC), model.Collider(shape=cap), position=(0, 5, 0))
+    with pytest.raises(UnsupportedFeature):
+        check_supported(w)
+    with pytest.raises(UnsupportedFeature):
+        CudaBackend().attach(w)
+    w2, _ = scenes.GOLDEN_SCENES['pyramid']()
+    s = w2.add_shape(model.Shape.box((1, 1, 1)))
+    w2.add_body(model.Motion(type=model.STATIC), trigger=model.Trigger(shape=s), position=(0, 9, 0))
+    with pytest.raises(UnsupportedFeature):
+        check_supported(w2)
+    w3, _ = scenes.GOLDEN_SCENES['pyramid']()
+    w3.add_gravity_volume(object())
+    with pytest.raises(UnsupportedFeature):
+        check_supported(w3)
+
+
+def test_select_backend_has_no_fallback():
+    assert isinstance(select_backend('cuda'), CudaBackend)
+    with pytest.raises(ValueError):
+        select_backend('numpy')

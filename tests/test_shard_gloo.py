@@ -1,0 +1,81 @@
+"""Multi-GPU host logic on CPU: whole-world shards and the cross-rank
+bookkeeping (max step time, sums, gathers) over gloo with two ranks."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from omi_physics_b200.shard import plan_shards
+
+
+def test_plan_shards_partition_and_balance():
+    rng = np.random.default_rng(0)
+    sizes = np.exp(rng.uniform(np.log(16), np.log(2048), size=101)).astype(int)
+    for n in (1, 2, 3, 8):
+        sh = plan_shards(sizes, n)
+        flat = sorted(i for s in sh for i in s)
+        assert flat == list(range(len(sizes)))            # disjoint, complete
+        loads = [int(sizes[s].sum()) for s in sh]
+        assert max(loads) - min(loads) <= int(sizes.max())  # LPT bound
+        assert plan_shards(sizes, n) == sh                # deterministic
+
+
+def test_plan_shards_edge_cases():
+    assert plan_shards([], 3) == [[], [], []]
+    assert plan_shards([5], 2) == [[0], []]
+    with pytest.raises(ValueError):
+        plan_shards([1, 2], 0)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(('127.0.0.1', 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world_size, port, sizes, out):
+    import datetime
+    import torch.distributed as dist
+    from omi_physics_b200 import shard
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world_size,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        mine = shard.local_shard(sizes, rank, world_size)
+        bodies = int(np.asarray(sizes)[mine].sum())
+        fake_ms = 10.0 + rank            # rank 1 is the slow one
+        shard.barrier(world_size)
+        t = shard.max_over_ranks(fake_ms, world_size)
+        total = shard.sum_over_ranks(bodies, world_size)
+        got = shard.gather_to_rank0(mine, world_size)
+        out.put((rank, t, total, got))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_over_gloo():
+    import torch.multiprocessing as mp
+    sizes = [300, 17, 2048, 64, 999, 128, 5, 700]
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, sizes, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(2):
+        r, t, total, got = q.get(timeout=120)
+        res[r] = (t, total, got)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0][0] == res[1][0] == 11.0
+    assert res[0][1] == res[1][1] == float(sum(sizes))
+    assert res[1][2] is None
+    gathered = res[0][2]
+    assert sorted(i for s in gathered for i in s) == list(range(len(sizes)))
+    assert gathered == plan_shards(sizes, 2)
