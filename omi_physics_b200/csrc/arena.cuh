@@ -33,6 +33,7 @@ enum {
     ST_CASCADE = 4,      // wake cascades resolved sequentially (diagnostic)
     ST_GJK_ITEMS = 5,    // convex pairs routed to GJK/EPA in the last step
     ST_CONTACTS_NEEDED = 6,
+    ST_SWEEP_TIMEOUT = 7, // a sweep wait ran out (never expected; the step is reported failed)
     ST_WORDS = 8
 };
 
@@ -99,10 +100,13 @@ struct Arena {
     int *c_a, *c_b;
     double *c_pt, *c_n, *c_depth, *c_imp, *c_data;
     int *c_level, *c_order, *c_level_start;
-    int *w_levels;                  // Gauss-Seidel depth of each world's contact runs
+    int *w_levels;                  // sweep length of each world in contact-solve slots
     int *w_runs;                    // runs (consecutive contacts of one body pair) per world
     int *run_k, *run_n, *run_a, *run_b;   // per run: first contact (world-local), count, dynamic bodies (-1 otherwise)
-    unsigned *run_mask;             // per run: earlier runs of its 32-run batch it shares a body with
+    int *run_pa, *run_pb;           // per run and side: the entry it follows (predecessor code, k_levels)
+    int *run_done;                  // per run: sweep passes completed (when not in shared memory)
+    int *w_batches;                 // sweep batches per world (k_levels -> k_iterate)
+    int *lv_scratch;                // k_levels tables of worlds too large for shared memory
     int max_passes;                 // sweep passes the level buffers are sized for (warm start + iterations)
     const int *w_sched;             // worlds ordered largest first (per-world kernels)
 

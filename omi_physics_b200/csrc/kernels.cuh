@@ -773,141 +773,57 @@ __device__ inline void bucket_levels_warp(int n, int D, const int *level, int *l
     __syncwarp();
 }
 
-// Levels over the whole sequence of sweep passes. The Gauss-Seidel unit is a
-// run (the consecutive contacts of one body pair) and the sequence is every
-// pass of the reference's solve in order: the warm start (when on), then each
-// velocity iteration, each visiting the runs in contact order. Entry (p, r)
-// must follow every earlier entry sharing a dynamic body with it - within its
-// pass and in earlier passes - and nothing else, so a run of pass p+1 may
-// start while unrelated runs of pass p are still pending. The split-impulse
-// position pass rides along pass 0 (it reads and writes only positions, which
-// no velocity pass touches, and pass 0 orders the runs as the position pass
-// does). Entries are encoded (p << 24) | r.
+// The sweep sequence. The Gauss-Seidel unit is a run (the consecutive
+// contacts of one body pair) and the sequence is every pass of the
+// reference's solve in order: the warm start (when on), then each velocity
+// iteration, each visiting the runs in contact order. Entry (p, r) must
+// follow the latest earlier entry that shares a dynamic body with it - the
+// previous run of that body in the same pass, or, for the body's first run of
+// the pass, its last run of pass p - 1 - and nothing else, so a run of pass
+// p+1 may start while unrelated runs of pass p are still pending. The
+// split-impulse position pass rides along pass 0 (it reads and writes only
+// positions, which no velocity pass touches, and pass 0 orders the runs as the
+// position pass does). Entries are encoded (p << 24) | r. Every run has a
+// dynamic body (the broadphase keeps no pair of two static or kinematic
+// bodies), so (p - 1, r) is always on a chain into (p, r).
 constexpr int PASS_SHIFT = 24;
+constexpr int PASS_MASK = (1 << PASS_SHIFT) - 1;
 
 __device__ __forceinline__ int world_passes(const Arena &A, int w) {
     const int p = ((A.w_flags[w] & WF_WARM) ? 1 : 0) + A.w_iters[w];
     return p > 0 ? p : 1;
 }
 
-// one pass of levels over R runs; pass 0 also records each run's conflict
-// mask (earlier lanes of its batch sharing a dynamic body), later passes
-// reuse it and walk only the lanes that are conflict sources
-__device__ inline int warp_levels_pass(const Arena &A, int c0, int R, int pass, int *last, int last_base,
-                                       int *level_out) {
-    const int lane = threadIdx.x & 31;
-    const int *ra = A.run_a + c0, *rb = A.run_b + c0;
-    unsigned *rmask = A.run_mask + c0;
-    int maxl = -1;
-    // this batch's run bodies (and, after pass 0, conflict masks), loaded one batch ahead
-    int a = lane < R ? ra[lane] : -1, b = lane < R ? rb[lane] : -1;
-    unsigned mnext = (pass > 0 && lane < R) ? rmask[lane] : 0u;
-    for (int base = 0; base < R; base += 32) {
-        const int r = base + lane;
-        const bool valid = r < R;
-        const int rn = r + 32;
-        const int an = rn < R ? ra[rn] : -1, bn = rn < R ? rb[rn] : -1;
-        const unsigned mn = (pass > 0 && rn < R) ? rmask[rn] : 0u;
-        int lvl = 0;
-        if (a >= 0) lvl = max(lvl, ((volatile int *)last)[a - last_base] + 1);
-        if (b >= 0) lvl = max(lvl, ((volatile int *)last)[b - last_base] + 1);
-        unsigned mask;
-        if (pass == 0) {
-            mask = 0;
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const int aj = __shfl_sync(FULL, a, j), bj = __shfl_sync(FULL, b, j);
-                const bool c = j < lane && ((a >= 0 && (a == aj || a == bj)) || (b >= 0 && (b == aj || b == bj)));
-                mask |= (c ? 1u : 0u) << j;
-            }
-            if (valid) rmask[r] = mask;
-        } else {
-            mask = mnext;
-        }
-        unsigned src = __reduce_or_sync(FULL, mask);
-        while (src) {
-            const int j = __ffs(src) - 1;
-            src &= src - 1;
-            const int lj = __shfl_sync(FULL, lvl, j);
-            if ((mask >> j) & 1u) lvl = max(lvl, lj + 1);
-        }
-        if (valid) {
-            level_out[r] = lvl;
-            if (a >= 0) atomicMax(&last[a - last_base], lvl);
-            if (b >= 0) atomicMax(&last[b - last_base], lvl);
-            maxl = max(maxl, lvl);
-        }
-        __syncwarp();
-        a = an; b = bn; mnext = mn;
-    }
-    for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(FULL, maxl, o));
-    return maxl + 1;
-}
-
-// bucket entries by level inside one warp: ls[0..D] = level starts; the
-// entries of pass p are level[p*R + r], stored in order as (p << 24) | r.
-// Counting runs in shared memory (`sc`, `scap` ints) when the levels fit.
-__device__ inline void bucket_entries_warp(int R, int P, int D, const int *level, int *ls, int *cursor,
-                                           int *order, int *sc, int scap) {
-    const int lane = threadIdx.x & 31;
-    const bool shared_counts = D + 1 <= scap;
-    int *cnt = shared_counts ? sc : cursor;
-    for (int l = lane; l <= D; l += 32) cnt[l] = 0;
-    __syncwarp();
-    const int N = R * P;
-    for (int e = lane; e < N; e += 32) atomicAdd(&cnt[level[e]], 1);
-    __syncwarp();
-    // exclusive scan into ls, reset cnt as the fill cursor
-    int carry = 0;
-    for (int base = 0; base <= D; base += 32) {
-        const int i = base + lane;
-        const int v = i < D ? cnt[i] : 0;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
-        }
-        if (i <= D) ls[i] = x - v + carry;
-        carry += __shfl_sync(FULL, x, 31);
-        __syncwarp();
-        if (i <= D) cnt[i] = 0;
-    }
-    __syncwarp();
-    for (int p = 0, e0 = 0; p < P; p++, e0 += R)
-        for (int r = lane; r < R; r += 32) {
-            const int l = level[e0 + r];
-            order[ls[l] + atomicAdd(&cnt[l], 1)] = (p << PASS_SHIFT) | r;
-        }
-    __syncwarp();
-}
-
-// per-warp shared slice for `last` (worlds up to `last_cap` bodies; larger
-// ones use the global per-body array)
 // ---------------------------------------------------------------------------
-// Gauss-Seidel levels of one world (one block per world).
+// Sweep schedule of one world (one block per world).
 //
-// The sequential sweep visits (pass p, run r) in the order p-major, r-minor.
-// Entry (p, r) must follow the latest earlier entry that touches each of its
-// dynamic bodies: the previous run of that body in the same pass, or, for the
-// body's first run of the pass, its last run of pass p - 1. Its level is the
-// longest such chain ending at it; entries of one level touch disjoint
-// dynamic bodies and any order among them gives the sequential result.
-// (Every run has a dynamic body - the broadphase keeps no pair of two static
-// or kinematic bodies - so (p - 1, r) is always on a chain into (p, r).)
+// Per run and side, a predecessor code (>= 0: that run of the same pass;
+// < 0 and not LEVEL_NONE: -(run of the previous pass) - 1), found from
+// per-body run buckets and stored for the sweep. Then each entry's earliest
+// start slot in units of contact solves: t(e) = max over its predecessors d
+// of t(d) + n(d), n the run's contact count - the as-soon-as-possible start
+// when a run takes n slots. Slots come from in-place max-plus relaxation from
+// zero: each thread owns a contiguous stretch of entries in sweep order, so
+// chains inside a stretch settle in one round (the stretch length is odd, so
+// a warp's 32 stretches start in 32 different shared-memory banks); values
+// only grow and stay below the fixed point, and a round without change is it.
 //
-// In shared memory: per run and side (two arrays), a predecessor code (>= 0: the run of
-// the same pass; < 0 and not LEVEL_NONE: -(run of the previous pass) - 1),
-// found from per-body run buckets; then the levels by in-place max-plus
-// relaxation from zero. Each thread owns a contiguous stretch of entries in
-// sweep order, so chains inside a stretch settle in one round; the stretch
-// length is odd, so a warp's 32 stretches start in 32 different shared-memory
-// banks. Values only grow and stay below the true levels, and a round without
-// change is the fixed point (at most D + 1 rounds). Worlds whose tables exceed the shared
-// memory take the warp-sequential scan instead.
+// Entries are then ordered by (start slot, class) - class: pass 0 or not,
+// one contact or more, so a warp's lanes mostly take the same path - and
+// cut into batches of at most 32 entries of one key. Entries of one slot
+// never depend on each other (a dependency adds n >= 1 slots), so the lanes
+// of a batch are independent and every predecessor of a batch lies in an
+// earlier batch. Batch q is stored as start | (count - 1) << BATCH_SHIFT
+// (count 32 sets the sign bit: decode with an unsigned shift).
+//
+// Tables live in shared memory when they fit, else in a global scratch area
+// of the same layout.
 // ---------------------------------------------------------------------------
 constexpr int LEVEL_THREADS = 1024;
 constexpr int LEVEL_SMEM_INTS = 56 * 1024;
 constexpr int LEVEL_NONE = -2147483647 - 1;
+constexpr int SLOT_CLASSES = 4;
+constexpr int BATCH_SHIFT = 27;
 
 __device__ __forceinline__ int run_pred_code(const int *list, int s, int e, int r) {
     int pred = -1, mx = -1;
@@ -934,6 +850,37 @@ __device__ inline void block_scan_reset(int *cnt, int *out, int n, int *sh) {
     __syncthreads();
 }
 
+// block-wide maximum (every thread gets it)
+__device__ inline int block_max(int v, int *sh) {
+    v = __reduce_max_sync(FULL, v);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int m = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : -2147483647;
+        m = __reduce_max_sync(FULL, m);
+        if (threadIdx.x == 0) sh[32] = m;
+    }
+    __syncthreads();
+    const int r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// start slot bound by one predecessor code of entry (p, .), or 0
+__device__ __forceinline__ int pred_slot(volatile const int *t, const int *rn, int code, int p, int R) {
+    if (code >= 0) return t[p * R + code] + rn[code];
+    if (code != LEVEL_NONE && p > 0) {
+        const int x = -code - 1;
+        return t[(p - 1) * R + x] + rn[x];
+    }
+    return 0;
+}
+
+// global scratch of world w when its tables exceed the shared memory
+__device__ __forceinline__ size_t level_scratch_offset(const Arena &A, int c0, int b0, int w) {
+    return (size_t)(5 + A.max_passes) * c0 + 2 * (size_t)b0 + 2 * (size_t)w;
+}
+
 __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints) {
     extern __shared__ int lsm[];
     __shared__ int scan_sh[33];
@@ -946,7 +893,7 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
         world_contacts(A, w, c0, c1);
         const int K = c1 - c0;
         if (K == 0) {
-            if (tid == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; }
+            if (tid == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; A.w_batches[w] = 0; }
             continue;
         }
         // runs: maximal stretches of consecutive contacts of one pair
@@ -969,128 +916,134 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
             R += tot;
         }
         __syncthreads();
-        for (int r = tid; r < R; r += T) {
-            const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
-            A.run_n[c0 + r] = end - A.run_k[c0 + r];
-        }
         const int P = world_passes(A, w);
         const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
         const int N = P * R;
         const size_t e0 = (size_t)c0 * A.max_passes;
-        int *ls = A.c_level_start + e0 + w;
-        int *order = A.c_order + e0;
-        int *cursor = A.c_level_start + ((size_t)A.contact_cap * A.max_passes + A.W + 1) + e0 + w;
-        int D = 0;
-        if (2 * R + max(2 * nb + 1 + 2 * R, N) <= smem_ints) {
-            int *code_a = lsm, *code_b = lsm + R;    // per run
-            int *cnt = lsm + 2 * R;          // per body, then the fill cursor
-            int *bstart = cnt + nb;          // nb + 1
-            int *list = bstart + nb + 1;     // 2R run indices, bucketed by body
-            int *lvl = lsm + 2 * R;          // N levels (after the buckets are done)
-            for (int i = tid; i < nb; i += T) cnt[i] = 0;
-            __syncthreads();
-            for (int r = tid; r < R; r += T) {
-                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
-                if (a >= 0) atomicAdd(&cnt[a - b0], 1);
-                if (b >= 0) atomicAdd(&cnt[b - b0], 1);
-            }
-            __syncthreads();
-            block_scan_reset(cnt, bstart, nb, scan_sh);
-            if (tid == 0) bstart[nb] = 2 * R;     // unused tail: only bodies' own ranges are read
-            for (int r = tid; r < R; r += T) {
-                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
-                if (a >= 0) list[bstart[a - b0] + atomicAdd(&cnt[a - b0], 1)] = r;
-                if (b >= 0) list[bstart[b - b0] + atomicAdd(&cnt[b - b0], 1)] = r;
-            }
-            __syncthreads();
-            for (int r = tid; r < R; r += T) {
-                const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
-                int ca = LEVEL_NONE, cb = LEVEL_NONE;
-                if (a >= 0) ca = run_pred_code(list, bstart[a - b0], bstart[a - b0] + cnt[a - b0], r);
-                if (b >= 0) cb = run_pred_code(list, bstart[b - b0], bstart[b - b0] + cnt[b - b0], r);
-                code_a[r] = ca;
-                code_b[r] = cb;
-            }
-            __syncthreads();
-            for (int e = tid; e < N; e += T) lvl[e] = 0;
-            __syncthreads();
-            const int ch = ((N + T - 1) / T) | 1;
-            const int e_lo = min(N, tid * ch), e_hi = min(N, e_lo + ch);
-            volatile int *vl = lvl;
-            for (int round = 0; round <= N; round++) {
-                int changed = 0;
-                int p = e_lo / R, r = e_lo - p * R;
-                for (int e = e_lo; e < e_hi; e++) {
-                    const int ca = code_a[r], cb = code_b[r];
-                    int v = 0;
-                    if (ca >= 0) v = vl[p * R + ca] + 1;
-                    else if (ca != LEVEL_NONE && p > 0) v = vl[(p - 1) * R - ca - 1] + 1;
-                    if (cb >= 0) v = max(v, vl[p * R + cb] + 1);
-                    else if (cb != LEVEL_NONE && p > 0) v = max(v, vl[(p - 1) * R - cb - 1] + 1);
-                    if (v != vl[e]) { vl[e] = v; changed = 1; }
-                    if (++r == R) { r = 0; p++; }
-                }
-                if (!__syncthreads_or(changed)) break;
-            }
-            int mx = -1;
-            for (int e = e_lo; e < e_hi; e++) mx = max(mx, lvl[e]);
-            mx = __reduce_max_sync(FULL, mx);
-            if ((tid & 31) == 0) scan_sh[tid >> 5] = mx;
-            __syncthreads();
-            if (tid < 32) {
-                int m = tid < (T >> 5) ? scan_sh[tid] : -1;
-                m = __reduce_max_sync(FULL, m);
-                if (tid == 0) scan_sh[32] = m + 1;
-            }
-            __syncthreads();
-            D = scan_sh[32];
-            // bucket the entries by level; order inside a level is free
-            int *lc = D + 1 <= 2 * R ? lsm : cursor;
-            for (int l = tid; l <= D; l += T) lc[l] = 0;
-            __syncthreads();
-            for (int e = e_lo; e < e_hi; e++) atomicAdd(&lc[lvl[e]], 1);
-            __syncthreads();
-            block_scan_reset(lc, ls, D + 1, scan_sh);
-            {
-                int p = e_lo / R, r = e_lo - p * R;
-                for (int e = e_lo; e < e_hi; e++) {
-                    const int l = lvl[e];
-                    order[ls[l] + atomicAdd(&lc[l], 1)] = (p << PASS_SHIFT) | r;
-                    if (++r == R) { r = 0; p++; }
-                }
-            }
-        } else if (tid < 32) {
-            // warp-sequential scan with `last` in global memory
-            int *last = A.b_last + b0;
-            for (int i = tid; i < nb; i += 32) last[i] = -1;
-            __syncwarp();
-            for (int p = 0; p < P; p++)
-                D = max(D, warp_levels_pass(A, c0, R, p, last, b0, A.c_level + e0 + (size_t)p * R));
-            bucket_entries_warp(R, P, D, A.c_level + e0, ls, cursor, order, lsm, smem_ints);
+        const bool in_smem = 3 * R + max(2 * nb + 1 + 2 * R, N) <= smem_ints;
+        int *tab = in_smem ? lsm : A.lv_scratch + level_scratch_offset(A, c0, b0, w);
+        int *code_a = tab, *code_b = tab + R, *rn = tab + 2 * R;
+        int *cnt = tab + 3 * R;              // per body, then the fill cursor
+        int *bstart = cnt + nb;              // nb + 1
+        int *list = bstart + nb + 1;         // 2R run indices, bucketed by body
+        int *slot = tab + 3 * R;             // N start slots (after the buckets are done)
+        for (int r = tid; r < R; r += T) {
+            const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
+            const int n = end - A.run_k[c0 + r];
+            A.run_n[c0 + r] = n;
+            rn[r] = n;
         }
-        if (tid == 0) { A.w_levels[w] = D; A.w_runs[w] = R; }
+        for (int i = tid; i < nb; i += T) cnt[i] = 0;
+        __syncthreads();
+        for (int r = tid; r < R; r += T) {
+            const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+            if (a >= 0) atomicAdd(&cnt[a - b0], 1);
+            if (b >= 0) atomicAdd(&cnt[b - b0], 1);
+        }
+        __syncthreads();
+        block_scan_reset(cnt, bstart, nb, scan_sh);
+        for (int r = tid; r < R; r += T) {
+            const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+            if (a >= 0) list[bstart[a - b0] + atomicAdd(&cnt[a - b0], 1)] = r;
+            if (b >= 0) list[bstart[b - b0] + atomicAdd(&cnt[b - b0], 1)] = r;
+        }
+        __syncthreads();
+        for (int r = tid; r < R; r += T) {
+            const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+            int ca = LEVEL_NONE, cb = LEVEL_NONE;
+            if (a >= 0) ca = run_pred_code(list, bstart[a - b0], bstart[a - b0] + cnt[a - b0], r);
+            if (b >= 0) cb = run_pred_code(list, bstart[b - b0], bstart[b - b0] + cnt[b - b0], r);
+            code_a[r] = ca;
+            code_b[r] = cb;
+            A.run_pa[c0 + r] = ca;
+            A.run_pb[c0 + r] = cb;
+        }
+        __syncthreads();
+        for (int e = tid; e < N; e += T) slot[e] = 0;
+        __syncthreads();
+        const int ch = ((N + T - 1) / T) | 1;
+        const int e_lo = min(N, tid * ch), e_hi = min(N, e_lo + ch);
+        volatile int *vs = slot;
+        for (int round = 0; round <= N; round++) {
+            int changed = 0;
+            int p = e_lo / R, r = e_lo - p * R;
+            for (int e = e_lo; e < e_hi; e++) {
+                const int v = max(pred_slot(vs, rn, code_a[r], p, R), pred_slot(vs, rn, code_b[r], p, R));
+                if (v != vs[e]) { vs[e] = v; changed = 1; }
+                if (++r == R) { r = 0; p++; }
+            }
+            if (!__syncthreads_or(changed)) break;
+        }
+        int smax = 0, dmax = 0;
+        {
+            int p = e_lo / R, r = e_lo - p * R;
+            for (int e = e_lo; e < e_hi; e++) {
+                smax = max(smax, slot[e] + 1);
+                dmax = max(dmax, slot[e] + rn[r]);
+                if (++r == R) { r = 0; p++; }
+            }
+        }
+        const int S = block_max(smax, scan_sh);          // distinct start slots
+        const int Dw = block_max(dmax, scan_sh);         // slots of the whole sweep
+        // order by (slot, class); counters in the code arrays when they fit
+        // keys and batches live in regions of K * max_passes (+ 1) ints; S <= P * K
+        const int C = (int64_t)SLOT_CLASSES * S <= (int64_t)K * A.max_passes ? SLOT_CLASSES : 1;
+        const int NK = C * S;
+        int *ls = A.c_level_start + e0 + w;
+        int *cursor = A.c_level_start + ((size_t)A.contact_cap * A.max_passes + A.W + 1) + e0 + w;
+        int *kc = NK <= 2 * R ? tab : cursor;
+        for (int k = tid; k < NK; k += T) kc[k] = 0;
+        __syncthreads();
+        {
+            int p = e_lo / R, r = e_lo - p * R;
+            for (int e = e_lo; e < e_hi; e++) {
+                const int cls = C == 1 ? 0 : (p == 0 ? 2 : 0) + (rn[r] > 1 ? 1 : 0);
+                atomicAdd(&kc[slot[e] * C + cls], 1);
+                if (++r == R) { r = 0; p++; }
+            }
+        }
+        __syncthreads();
+        block_scan_reset(kc, ls, NK, scan_sh);
+        int *order = A.c_order + e0;
+        {
+            int p = e_lo / R, r = e_lo - p * R;
+            for (int e = e_lo; e < e_hi; e++) {
+                const int cls = C == 1 ? 0 : (p == 0 ? 2 : 0) + (rn[r] > 1 ? 1 : 0);
+                const int k = slot[e] * C + cls;
+                order[ls[k] + atomicAdd(&kc[k], 1)] = (p << PASS_SHIFT) | r;
+                if (++r == R) { r = 0; p++; }
+            }
+        }
+        __syncthreads();
+        // batches: ceil(count / 32) per key, written after the slots are no
+        // longer needed (they may share the global scratch's neighbourhood)
+        for (int k = tid; k < NK; k += T) kc[k] = (kc[k] + 31) >> 5;
+        __syncthreads();
+        int nbatch = 0;
+        {
+            int carry = 0;
+            for (int base = 0; base < NK; base += T) {
+                const int k = base + tid;
+                const int v = k < NK ? kc[k] : 0;
+                int tot;
+                const int x = block_exclusive_scan(v, scan_sh, &tot);
+                if (k < NK) kc[k] = carry + x;
+                carry += tot;
+            }
+            nbatch = carry;
+        }
+        __syncthreads();
+        int *batch = A.c_level + e0;
+        for (int k = tid; k < NK; k += T) {
+            const int s0 = ls[k];
+            const int c = (k + 1 < NK ? ls[k + 1] : N) - s0;
+            const int q0 = kc[k];
+            for (int j = 0; 32 * j < c; j++)
+                batch[q0 + j] = (s0 + 32 * j) | ((min(32, c - 32 * j) - 1) << BATCH_SHIFT);
+        }
+        if (tid == 0) { A.w_levels[w] = Dw; A.w_runs[w] = R; A.w_batches[w] = nbatch; }
         __syncthreads();
     }
-}
-
-// asynchronous 16-byte-chunk copy into shared memory
-__device__ __forceinline__ void async_copy(double *dst, const double *src, int chunks) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    for (int q = 0; q < chunks; q++)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s + 16 * q), "l"(src + 2 * q));
-}
-__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// a lane's buffer for one run: the first contact's whole row, then the
-// per-contact part of the others
-constexpr int RUNBUF = CD + (RUN_MAX - 1) * C_PART;
-
-__device__ __forceinline__ void run_prefetch(const Arena &A, int k0, int n, double *dst) {
-    async_copy(dst, &A.c_data[(size_t)k0 * CD], CD / 2);
-    for (int i = 1; i < n && i < RUN_MAX; i++)
-        async_copy(dst + CD + (i - 1) * C_PART, &A.c_data[(size_t)(k0 + i) * CD], C_PART / 2);
 }
 
 // Velocities of one world, staged for the sweeps: in shared memory when the
@@ -1226,13 +1179,9 @@ __device__ __forceinline__ void contact_position(double *pa, double *pb, const P
         for (int q = 0; q < 3; q++) pb[q] += r.imb * dL * r.n[q];
 }
 
-// One warp per block, walking the pipelined levels. Dynamic shared memory:
-// each lane's two run buffers (the next level's run is copied in with
-// cp.async while this level runs), then the world's staged state - its
-// bodies' velocities, and its contacts' impulses when they fit too (worlds
-// above the capacity sweep on the global arrays).
-// shared memory of one sweep block, in doubles (227 KB)
-constexpr int SWEEP_SMEM_DOUBLES = 29056;
+// dynamic shared memory of one sweep block, in doubles: 227 KB less room for
+// the block's static shared variables
+constexpr int SWEEP_SMEM_DOUBLES = 29056 - 8;
 
 struct ImpView {
     double *s;       // shared staging (nullptr: global c_imp)
@@ -1242,57 +1191,45 @@ __device__ __forceinline__ double *imp_ptr(const Arena &A, const ImpView &I, int
     return I.s ? &I.s[(k - I.c0) * 3] : &A.c_imp[k * 3];
 }
 
-// one pass over one run (all its contacts, in order) by one lane
-__device__ __forceinline__ void run_pass(const Arena &A, const VelView &V, const ImpView &I, const double *buf,
-                                         int k0, int n, bool vel, bool warm_pass, bool pos_pass, double slop) {
-    PairRow r;
-    load_pair(buf, r);
-    PairVel s;
-    vel_load(A, V, r.a, s.la, s.aa);
-    vel_load(A, V, r.b, s.lb, s.ab);
-    double pa[3], pb[3];
-    if (pos_pass) {
-        for (int q = 0; q < 3; q++) { pa[q] = A.pos[r.a * 3 + q]; pb[q] = A.pos[r.b * 3 + q]; }
-    }
+// the first contact's whole row (pair part included), read-only path
+__device__ __forceinline__ void load_row(const Arena &A, int k, double *row) {
+    const double2 *g = reinterpret_cast<const double2 *>(&A.c_data[(size_t)k * CD]);
 #pragma unroll
-    for (int i = 0; i < RUN_MAX; i++) {
-        if (i < n) {
-            ContactRow c;
-            load_contact(i == 0 ? buf : buf + CD + (i - 1) * C_PART, c);
-            if (vel) {
-                double *ip = imp_ptr(A, I, k0 + i);
-                double imp[3] = {ip[0], ip[1], ip[2]};
-                if (warm_pass) contact_warm(s, r, c, imp);
-                else {
-                    contact_solve(s, r, c, imp);
-                    ip[0] = imp[0]; ip[1] = imp[1]; ip[2] = imp[2];
-                }
-            }
-            if (pos_pass) contact_position(pa, pb, r, c, slop);
-        }
-    }
-    if (r.da) vel_store(A, V, r.a, s.la, s.aa);
-    if (r.db) vel_store(A, V, r.b, s.lb, s.ab);
-    if (pos_pass) {
-        if (r.da) for (int q = 0; q < 3; q++) A.pos[r.a * 3 + q] = pa[q];
-        if (r.db) for (int q = 0; q < 3; q++) A.pos[r.b * 3 + q] = pb[q];
+    for (int q = 0; q < CD / 2; q++) {
+        const double2 t = __ldg(g + q);
+        row[2 * q] = t.x;
+        row[2 * q + 1] = t.y;
     }
 }
 
-// a run too long for the lane buffer or in a level wider than a warp: the
-// same pass straight from global memory, contact by contact
-__device__ inline void run_pass_direct(const Arena &A, const VelView &V, const ImpView &I, int k0, int n,
-                                       bool vel, bool warm_pass, bool pos_pass, double slop) {
+// One pass over one run (all its contacts, in order) by one thread; row0 is
+// the first contact's row, the next contact's part is loaded while the
+// current one is solved.
+__device__ __forceinline__ void run_pass(const Arena &A, const VelView &V, const ImpView &I, const double *row0,
+                                         int k0, int n, bool vel, bool warm_pass, bool pos_pass, double slop) {
     PairRow r;
-    load_pair(&A.c_data[(size_t)k0 * CD], r);
+    load_pair(row0, r);
     PairVel s;
     vel_load(A, V, r.a, s.la, s.aa);
     vel_load(A, V, r.b, s.lb, s.ab);
     double pa[3], pb[3];
-    if (pos_pass) for (int q = 0; q < 3; q++) { pa[q] = A.pos[r.a * 3 + q]; pb[q] = A.pos[r.b * 3 + q]; }
+    if (pos_pass)
+        for (int q = 0; q < 3; q++) { pa[q] = A.pos[r.a * 3 + q]; pb[q] = A.pos[r.b * 3 + q]; }
+    double cur[C_PART];
+#pragma unroll
+    for (int q = 0; q < C_PART; q++) cur[q] = row0[q];
     for (int i = 0; i < n; i++) {
         ContactRow c;
-        load_contact(&A.c_data[(size_t)(k0 + i) * CD], c);
+        load_contact(cur, c);
+        if (i + 1 < n) {
+            const double2 *g = reinterpret_cast<const double2 *>(&A.c_data[(size_t)(k0 + i + 1) * CD]);
+#pragma unroll
+            for (int q = 0; q < C_PART / 2; q++) {
+                const double2 t = __ldg(g + q);
+                cur[2 * q] = t.x;
+                cur[2 * q + 1] = t.y;
+            }
+        }
         if (vel) {
             double *ip = imp_ptr(A, I, k0 + i);
             double imp[3] = {ip[0], ip[1], ip[2]};
@@ -1312,44 +1249,85 @@ __device__ inline void run_pass_direct(const Arena &A, const VelView &V, const I
     }
 }
 
-// SWEEP_WARPS warps per block sweep one world's pipelined levels together
-// (__syncthreads between levels); every entry of a level touches its own
-// dynamic bodies. Shared memory: the world's staged velocities and, when they
-// fit too, its impulses; then, room permitting, each thread's buffer for the
-// next level's run (copied with cp.async while this level runs).
-constexpr int SWEEP_WARPS = 4;
+// block-scope acquire / release on a generic address (shared or global)
+__device__ __forceinline__ int ld_acquire_cta(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cta.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cta(int *p, int v) {
+    asm volatile("st.release.cta.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// polls before a wait gives up: ~40x the longest legitimate wait (a whole
+// world's sweep)
+constexpr int SPIN_LIMIT = 1 << 22;
+
+// wait until the predecessor named by `code` of an entry of pass p is done
+// (done[x] counts the passes of run x completed). A wait that runs out sets
+// *abort, which ends every later wait of the block at once, so a broken
+// schedule costs one timeout, not one per entry; returns false then.
+__device__ __forceinline__ bool wait_pred(const int *done, int code, int p, volatile int *abort) {
+    int x, need;
+    if (code >= 0) { x = code; need = p + 1; }
+    else if (code != LEVEL_NONE && p > 0) { x = -code - 1; need = p; }
+    else return true;
+    for (int it = 0; it < SPIN_LIMIT; it++) {
+        if (ld_acquire_cta(&done[x]) >= need) return true;
+        if (*abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// The sweep: SWEEP_WARPS warps per world pull batches in schedule order from
+// a shared counter. Each lane reads its run's first row, waits until the
+// runs it follows have finished the passes it needs (acquire), solves the
+// run and publishes done[r] = p + 1 (release). Every predecessor sits in an
+// earlier batch, already taken by a running warp, so the waits end; a wait
+// that still runs out records ST_SWEEP_TIMEOUT (the host reports the step as
+// failed) and the lane goes on. Shared memory: the per-run pass counters,
+// the world's velocities and, when they fit too, its contacts' impulses
+// (worlds beyond the capacity use the global arrays).
+// ---------------------------------------------------------------------------
+constexpr int SWEEP_WARPS = 8;
 constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
 
 __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
     extern __shared__ __align__(16) double smem_d[];
+    __shared__ int next_batch;
+    __shared__ int abort_flag;
     if (overflowed(A)) return;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
         if (!world_collides(A, w)) continue;
-        const int D = A.w_levels[w];
-        if (D == 0) continue;
+        const int NBt = A.w_batches[w];
+        if (NBt == 0) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
-        const int K = c1 - c0;
+        const int K = c1 - c0, R = A.w_runs[w];
         const size_t e0 = (size_t)c0 * A.max_passes;
-        const int *ls = A.c_level_start + e0 + w;
-        const int *order = A.c_order + e0;
+        const int *batch = A.c_level + e0, *order = A.c_order + e0;
         const int *run_k = A.run_k + c0, *run_n = A.run_n + c0;
+        const int *run_pa = A.run_pa + c0, *run_pb = A.run_pb + c0;
         const bool warm = (A.w_flags[w] & WF_WARM) != 0;
         const bool vel = warm || A.w_iters[w] > 0;
         const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
         int used = 0;
+        const int done_d = ((R + 3) >> 2) << 1;        // R ints, in doubles, 16-byte multiple
+        int *done;
+        if (done_d <= smem_doubles) { done = reinterpret_cast<int *>(smem_d); used = done_d; }
+        else done = A.run_done + c0;
         VelView V;
         V.b0 = b0;
-        V.s = nb * 6 <= smem_doubles ? smem_d : nullptr;
-        if (V.s) used = (nb * 6 + 1) & ~1;
+        V.s = used + nb * 6 <= smem_doubles ? smem_d + used : nullptr;
+        if (V.s) used = (used + nb * 6 + 1) & ~1;
         ImpView I;
         I.c0 = c0;
         I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
-        if (I.s) used = (used + K * 3 + 1) & ~1;
-        const bool prefetch = used + SWEEP_THREADS * 2 * RUNBUF <= smem_doubles;
-        double *runbuf = smem_d + used + tid * 2 * RUNBUF;
+        for (int r = tid; r < R; r += SWEEP_THREADS) done[r] = 0;
         if (V.s) {
             for (int i = tid; i < nb; i += SWEEP_THREADS) {
                 double lv[3], av[3];
@@ -1360,41 +1338,32 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_dou
         }
         if (I.s)
             for (int i = tid; i < K * 3; i += SWEEP_THREADS) I.s[i] = A.c_imp[c0 * 3 + i];
+        if (tid == 0) { next_batch = 0; abort_flag = 0; }
         __syncthreads();
         const double slop = A.w_solver[w * 2 + 1];
-        int ecur = ls[0] + tid < ls[1] ? order[ls[0] + tid] : -1;
-        if (prefetch && ecur >= 0) {
-            const int r = ecur & ((1 << PASS_SHIFT) - 1);
-            run_prefetch(A, c0 + run_k[r], run_n[r], runbuf);
-        }
-        if (prefetch) async_commit();
-        for (int l = 0; l < D; l++) {
-            const int enext = (l + 1 < D && ls[l + 1] + tid < ls[l + 2]) ? order[ls[l + 1] + tid] : -1;
-            double *buf_cur = runbuf + (l & 1) * RUNBUF, *buf_nxt = runbuf + ((l + 1) & 1) * RUNBUF;
-            if (prefetch) {
-                if (enext >= 0) {
-                    const int r = enext & ((1 << PASS_SHIFT) - 1);
-                    run_prefetch(A, c0 + run_k[r], run_n[r], buf_nxt);
-                }
-                async_commit();
-                async_wait_prev();      // this level's run has landed
-            }
-            if (ecur >= 0) {
-                const int r = ecur & ((1 << PASS_SHIFT) - 1), p = ecur >> PASS_SHIFT;
+        bool ok = true;
+        for (;;) {
+            int q = 0;
+            if (lane == 0) q = atomicAdd(&next_batch, 1);
+            q = __shfl_sync(FULL, q, 0);
+            if (q >= NBt) break;
+            const int bq = batch[q];
+            const int start = bq & ((1 << BATCH_SHIFT) - 1), cnt = (int)((unsigned)bq >> BATCH_SHIFT) + 1;
+            if (lane < cnt) {
+                const int e = order[start + lane];
+                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
                 const int k0 = c0 + run_k[r], n = run_n[r];
-                const bool pos_pass = (p == 0), warm_pass = warm && p == 0;
-                if (prefetch && n <= RUN_MAX) run_pass(A, V, I, buf_cur, k0, n, vel, warm_pass, pos_pass, slop);
-                else run_pass_direct(A, V, I, k0, n, vel, warm_pass, pos_pass, slop);
+                double row0[CD];
+                load_row(A, k0, row0);
+                ok &= wait_pred(done, run_pa[r], p, &abort_flag);
+                ok &= wait_pred(done, run_pb[r], p, &abort_flag);
+                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                st_release_cta(&done[r], p + 1);
             }
-            for (int j = ls[l] + tid + SWEEP_THREADS; j < ls[l + 1]; j += SWEEP_THREADS) {   // wider levels
-                const int e = order[j];
-                const int r = e & ((1 << PASS_SHIFT) - 1), p = e >> PASS_SHIFT;
-                run_pass_direct(A, V, I, c0 + run_k[r], run_n[r], vel, warm && p == 0, p == 0, slop);
-            }
-            __syncthreads();
-            ecur = enext;
+            __syncwarp();
         }
-        if (prefetch) async_wait_all();
+        if (!ok) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+        __syncthreads();
         if (V.s) {
             for (int i = tid; i < nb; i += SWEEP_THREADS) {
                 if (A.mtype[b0 + i] != 2) continue;

@@ -166,10 +166,15 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.c_imp, (size_t)contact_cap * 3);
     rc |= alloc(ctx, ctx->dyn, A.c_data, (size_t)contact_cap * CD);
     const size_t entries = (size_t)contact_cap * A.max_passes;
+    if (entries >= ((size_t)1 << 27)) return fail(ctx, OMI_E_ARG, "contact capacity x sweep passes exceeds 2^27");
     rc |= alloc(ctx, ctx->dyn, A.c_level, entries);
     rc |= alloc(ctx, ctx->dyn, A.c_order, entries);
     rc |= alloc(ctx, ctx->dyn, A.c_level_start, 2 * (entries + A.W + 1));
-    rc |= alloc(ctx, ctx->dyn, A.run_mask, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_pa, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_pb, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_done, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.lv_scratch,
+                (size_t)(5 + A.max_passes) * contact_cap + 2 * (size_t)A.NB + 2 * (size_t)A.W + 64);
     rc |= alloc(ctx, ctx->dyn, A.run_k, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_n, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_a, contact_cap);
@@ -405,6 +410,7 @@ int run_steps(OmiCtx *ctx, int n, bool sync) {
         if (!sync) return 0;
         int rc = read_status(ctx);
         if (rc) return rc;
+        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_STATE, "contact sweep wait timed out");
         const int done = ctx->h_status[ST_STEPS_DONE];
         remaining -= done;
         if (remaining > 0) {
@@ -449,10 +455,20 @@ int omi_create(int device, OmiCtx **out) {
     ctx->stream = ctx->own;
     e = cudaMallocHost(&ctx->h_status, sizeof(int) * ST_WORDS);
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
-    cudaFuncSetAttribute(k_gjk, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * (int)sizeof(EpaWork));
-    cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
-    cudaFuncSetAttribute(k_iterate, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM_DOUBLES * (int)sizeof(double));
-    cudaFuncSetAttribute(k_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, LEVEL_SMEM_INTS * (int)sizeof(int));
+    const struct { const void *fn; int bytes; const char *name; } smem[] = {
+        {(const void *)k_gjk, 4 * (int)sizeof(EpaWork), "k_gjk"},
+        {(const void *)k_sort, 8192 * 24, "k_sort"},
+        {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
+        {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
+    };
+    for (const auto &f : smem) {
+        e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
+        if (e != cudaSuccess) {
+            int rc = cuda_fail(ctx, e, (std::string("cudaFuncSetAttribute ") + f.name).c_str());
+            *out = ctx;
+            return rc;
+        }
+    }
     *out = ctx;
     return 0;
 }
@@ -673,6 +689,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.b_flag, NB);
     rc |= alloc(ctx, ctx->statics, A.w_levels, W);
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
+    rc |= alloc(ctx, ctx->statics, A.w_batches, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
@@ -690,10 +707,10 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->solve_block = max_n > 1024 ? 256 : 128;
     // level tables of the largest world: about 2 + P ints per run, runs ~1.5 per body
     ctx->level_ints = (int)std::min<int64_t>(LEVEL_SMEM_INTS, 32 * (int64_t)std::max(max_nc, 1) + 1024);
-    // velocities (6 per body) and impulses of the largest world, then run
-    // buffers; small worlds need little, the largest take the whole 227 KB
+    // the largest world's per-run pass counters (~1.5 runs per body), velocities
+    // (6 per body) and impulses (~2 contacts per body, 3 each)
     ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
-                                                (int64_t)std::max(max_nc, 1) * 6 * 3 + SWEEP_THREADS * 2 * RUNBUF);
+                                                (int64_t)std::max(max_nc, 1) * 14 + 64);
     A.max_passes = 1;
     for (int w = 0; w < W; w++) A.max_passes = std::max(A.max_passes, passes_of(s->w_flags[w], s->w_iters[w]));
     const int pair_cap = std::max(4096, 4 * NB);
@@ -1045,6 +1062,7 @@ int omi_sync(OmiCtx *ctx) {
     if (rc) return rc;
     if (ctx->h_status[ST_OVERFLOW])
         return fail(ctx, OMI_E_STATE, "an asynchronous step overflowed its buffers; re-run with omi_step");
+    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_STATE, "contact sweep wait timed out");
     return 0;
 }
 
