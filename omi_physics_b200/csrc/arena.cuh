@@ -99,14 +99,15 @@ struct Arena {
     // contacts
     int *c_a, *c_b;
     double *c_pt, *c_n, *c_depth, *c_imp, *c_data;
-    int *c_level, *c_order, *c_level_start;
-    int *w_levels;                  // sweep length of each world in contact-solve slots
+    int *c_order;                   // per world: the sweep's work ring (when not in shared memory)
+    int *w_levels;                  // critical path of each world's last sweep, in contact solves
     int *w_runs;                    // runs (consecutive contacts of one body pair) per world
     int *run_k, *run_n, *run_a, *run_b;   // per run: first contact (world-local), count, dynamic bodies (-1 otherwise)
-    int *run_pa, *run_pb;           // per run and side: the entry it follows (predecessor code, k_levels)
-    int *run_done;                  // per run: sweep passes completed (when not in shared memory)
-    int *w_batches;                 // sweep batches per world (k_levels -> k_iterate)
-    int *lv_scratch;                // k_levels tables of worlds too large for shared memory
+    int *run_pa, *run_pb;           // per run and side: predecessor code (k_levels)
+    int *run_sa, *run_sb;           // per run and side: successor code (k_levels)
+    int *run_kn, *run_need;         // per run: first contact | count << 24; need counts (k_levels)
+    int *run_done, *run_tend;       // per run: sweep arrivals, finish slot (when not in shared memory)
+    int *lv_scratch;                // k_levels buckets of worlds too large for shared memory
     int max_passes;                 // sweep passes the level buffers are sized for (warm start + iterations)
     const int *w_sched;             // worlds ordered largest first (per-world kernels)
 

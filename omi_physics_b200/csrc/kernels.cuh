@@ -795,44 +795,31 @@ __device__ __forceinline__ int world_passes(const Arena &A, int w) {
 }
 
 // ---------------------------------------------------------------------------
-// Sweep schedule of one world (one block per world).
+// Sweep dependencies of one world (one block per world).
 //
-// Per run and side, a predecessor code (>= 0: that run of the same pass;
-// < 0 and not LEVEL_NONE: -(run of the previous pass) - 1), found from
-// per-body run buckets and stored for the sweep. Then each entry's earliest
-// start slot in units of contact solves: t(e) = max over its predecessors d
-// of t(d) + n(d), n the run's contact count - the as-soon-as-possible start
-// when a run takes n slots. Slots come from in-place max-plus relaxation from
-// zero: each thread owns a contiguous stretch of entries in sweep order, so
-// chains inside a stretch settle in one round (the stretch length is odd, so
-// a warp's 32 stretches start in 32 different shared-memory banks); values
-// only grow and stay below the fixed point, and a round without change is it.
-//
-// Entries are then ordered by (start slot, class) - class: pass 0 or not,
-// one contact or more, so a warp's lanes mostly take the same path - and
-// cut into batches of at most 32 entries of one key. Entries of one slot
-// never depend on each other (a dependency adds n >= 1 slots), so the lanes
-// of a batch are independent and every predecessor of a batch lies in an
-// earlier batch. Batch q is stored as start | (count - 1) << BATCH_SHIFT
-// (count 32 sets the sign bit: decode with an unsigned shift).
-//
-// Tables live in shared memory when they fit, else in a global scratch area
-// of the same layout.
+// Per run and side (a dynamic body), two codes found from per-body run
+// buckets: the predecessor - the previous run of that body in the same pass
+// (code >= 0), or, for the body's first run of a pass, its last run of the
+// previous pass (code -(run) - 1) - and the successor - the next run of that
+// body in the same pass (>= 0), or, for its last run, its first run of the
+// next pass (-(run) - 1). LEVEL_NONE marks a side without a dynamic body.
+// The sweep itself runs the resulting graph as a dataflow.
 // ---------------------------------------------------------------------------
-constexpr int LEVEL_THREADS = 1024;
+constexpr int LEVEL_THREADS = 256;
 constexpr int LEVEL_SMEM_INTS = 56 * 1024;
 constexpr int LEVEL_NONE = -2147483647 - 1;
-constexpr int SLOT_CLASSES = 4;
-constexpr int BATCH_SHIFT = 27;
 
-__device__ __forceinline__ int run_pred_code(const int *list, int s, int e, int r) {
-    int pred = -1, mx = -1;
+__device__ __forceinline__ void run_link_codes(const int *list, int s, int e, int r, int &pred, int &succ) {
+    int pv = -1, nx = 0x7fffffff, mn = 0x7fffffff, mx = -1;
     for (int j = s; j < e; j++) {
         const int q = list[j];
-        if (q < r && q > pred) pred = q;
+        if (q < r && q > pv) pv = q;
+        if (q > r && q < nx) nx = q;
+        mn = min(mn, q);
         mx = max(mx, q);
     }
-    return pred >= 0 ? pred : -(mx + 1);
+    pred = pv >= 0 ? pv : -(mx + 1);
+    succ = nx != 0x7fffffff ? nx : -(mn + 1);
 }
 
 // block-wide exclusive scan of cnt[0..n) into out[0..n) (out may be global);
@@ -850,35 +837,9 @@ __device__ inline void block_scan_reset(int *cnt, int *out, int n, int *sh) {
     __syncthreads();
 }
 
-// block-wide maximum (every thread gets it)
-__device__ inline int block_max(int v, int *sh) {
-    v = __reduce_max_sync(FULL, v);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        int m = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : -2147483647;
-        m = __reduce_max_sync(FULL, m);
-        if (threadIdx.x == 0) sh[32] = m;
-    }
-    __syncthreads();
-    const int r = sh[32];
-    __syncthreads();
-    return r;
-}
-
-// start slot bound by one predecessor code of entry (p, .), or 0
-__device__ __forceinline__ int pred_slot(volatile const int *t, const int *rn, int code, int p, int R) {
-    if (code >= 0) return t[p * R + code] + rn[code];
-    if (code != LEVEL_NONE && p > 0) {
-        const int x = -code - 1;
-        return t[(p - 1) * R + x] + rn[x];
-    }
-    return 0;
-}
-
-// global scratch of world w when its tables exceed the shared memory
+// global scratch of world w when its buckets exceed the shared memory
 __device__ __forceinline__ size_t level_scratch_offset(const Arena &A, int c0, int b0, int w) {
-    return (size_t)(5 + A.max_passes) * c0 + 2 * (size_t)b0 + 2 * (size_t)w;
+    return 3 * (size_t)c0 + 2 * (size_t)b0 + 2 * (size_t)w;
 }
 
 __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints) {
@@ -892,8 +853,11 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
         int c0, c1;
         world_contacts(A, w, c0, c1);
         const int K = c1 - c0;
-        if (K == 0) {
-            if (tid == 0) { A.w_levels[w] = 0; A.w_runs[w] = 0; A.w_batches[w] = 0; }
+        if (K == 0 || K >= (1 << 24)) {            // run_kn packs contact offsets in 24 bits
+            if (tid == 0) {
+                A.w_runs[w] = 0;
+                if (K) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+            }
             continue;
         }
         // runs: maximal stretches of consecutive contacts of one pair
@@ -916,22 +880,14 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
             R += tot;
         }
         __syncthreads();
-        const int P = world_passes(A, w);
         const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
-        const int N = P * R;
-        const size_t e0 = (size_t)c0 * A.max_passes;
-        const bool in_smem = 3 * R + max(2 * nb + 1 + 2 * R, N) <= smem_ints;
-        int *tab = in_smem ? lsm : A.lv_scratch + level_scratch_offset(A, c0, b0, w);
-        int *code_a = tab, *code_b = tab + R, *rn = tab + 2 * R;
-        int *cnt = tab + 3 * R;              // per body, then the fill cursor
+        const bool in_smem = 2 * nb + 1 + 2 * R <= smem_ints;
+        int *cnt = in_smem ? lsm : A.lv_scratch + level_scratch_offset(A, c0, b0, w);
         int *bstart = cnt + nb;              // nb + 1
         int *list = bstart + nb + 1;         // 2R run indices, bucketed by body
-        int *slot = tab + 3 * R;             // N start slots (after the buckets are done)
         for (int r = tid; r < R; r += T) {
             const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
-            const int n = end - A.run_k[c0 + r];
-            A.run_n[c0 + r] = n;
-            rn[r] = n;
+            A.run_n[c0 + r] = end - A.run_k[c0 + r];
         }
         for (int i = tid; i < nb; i += T) cnt[i] = 0;
         __syncthreads();
@@ -950,98 +906,19 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
         __syncthreads();
         for (int r = tid; r < R; r += T) {
             const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
-            int ca = LEVEL_NONE, cb = LEVEL_NONE;
-            if (a >= 0) ca = run_pred_code(list, bstart[a - b0], bstart[a - b0] + cnt[a - b0], r);
-            if (b >= 0) cb = run_pred_code(list, bstart[b - b0], bstart[b - b0] + cnt[b - b0], r);
-            code_a[r] = ca;
-            code_b[r] = cb;
-            A.run_pa[c0 + r] = ca;
-            A.run_pb[c0 + r] = cb;
+            int pa = LEVEL_NONE, pb = LEVEL_NONE, sa = LEVEL_NONE, sb = LEVEL_NONE;
+            if (a >= 0) run_link_codes(list, bstart[a - b0], bstart[a - b0] + cnt[a - b0], r, pa, sa);
+            if (b >= 0) run_link_codes(list, bstart[b - b0], bstart[b - b0] + cnt[b - b0], r, pb, sb);
+            A.run_pa[c0 + r] = pa;
+            A.run_pb[c0 + r] = pb;
+            A.run_sa[c0 + r] = sa;
+            A.run_sb[c0 + r] = sb;
+            // packed for the sweep: first contact | count << 24, and the
+            // same-pass / all-pass predecessor counts
+            A.run_kn[c0 + r] = A.run_k[c0 + r] | (A.run_n[c0 + r] << 24);
+            A.run_need[c0 + r] = ((pa >= 0) + (pb >= 0)) | (((pa != LEVEL_NONE) + (pb != LEVEL_NONE)) << 2);
         }
-        __syncthreads();
-        for (int e = tid; e < N; e += T) slot[e] = 0;
-        __syncthreads();
-        const int ch = ((N + T - 1) / T) | 1;
-        const int e_lo = min(N, tid * ch), e_hi = min(N, e_lo + ch);
-        volatile int *vs = slot;
-        for (int round = 0; round <= N; round++) {
-            int changed = 0;
-            int p = e_lo / R, r = e_lo - p * R;
-            for (int e = e_lo; e < e_hi; e++) {
-                const int v = max(pred_slot(vs, rn, code_a[r], p, R), pred_slot(vs, rn, code_b[r], p, R));
-                if (v != vs[e]) { vs[e] = v; changed = 1; }
-                if (++r == R) { r = 0; p++; }
-            }
-            if (!__syncthreads_or(changed)) break;
-        }
-        int smax = 0, dmax = 0;
-        {
-            int p = e_lo / R, r = e_lo - p * R;
-            for (int e = e_lo; e < e_hi; e++) {
-                smax = max(smax, slot[e] + 1);
-                dmax = max(dmax, slot[e] + rn[r]);
-                if (++r == R) { r = 0; p++; }
-            }
-        }
-        const int S = block_max(smax, scan_sh);          // distinct start slots
-        const int Dw = block_max(dmax, scan_sh);         // slots of the whole sweep
-        // order by (slot, class); counters in the code arrays when they fit
-        // keys and batches live in regions of K * max_passes (+ 1) ints; S <= P * K
-        const int C = (int64_t)SLOT_CLASSES * S <= (int64_t)K * A.max_passes ? SLOT_CLASSES : 1;
-        const int NK = C * S;
-        int *ls = A.c_level_start + e0 + w;
-        int *cursor = A.c_level_start + ((size_t)A.contact_cap * A.max_passes + A.W + 1) + e0 + w;
-        int *kc = NK <= 2 * R ? tab : cursor;
-        for (int k = tid; k < NK; k += T) kc[k] = 0;
-        __syncthreads();
-        {
-            int p = e_lo / R, r = e_lo - p * R;
-            for (int e = e_lo; e < e_hi; e++) {
-                const int cls = C == 1 ? 0 : (p == 0 ? 2 : 0) + (rn[r] > 1 ? 1 : 0);
-                atomicAdd(&kc[slot[e] * C + cls], 1);
-                if (++r == R) { r = 0; p++; }
-            }
-        }
-        __syncthreads();
-        block_scan_reset(kc, ls, NK, scan_sh);
-        int *order = A.c_order + e0;
-        {
-            int p = e_lo / R, r = e_lo - p * R;
-            for (int e = e_lo; e < e_hi; e++) {
-                const int cls = C == 1 ? 0 : (p == 0 ? 2 : 0) + (rn[r] > 1 ? 1 : 0);
-                const int k = slot[e] * C + cls;
-                order[ls[k] + atomicAdd(&kc[k], 1)] = (p << PASS_SHIFT) | r;
-                if (++r == R) { r = 0; p++; }
-            }
-        }
-        __syncthreads();
-        // batches: ceil(count / 32) per key, written after the slots are no
-        // longer needed (they may share the global scratch's neighbourhood)
-        for (int k = tid; k < NK; k += T) kc[k] = (kc[k] + 31) >> 5;
-        __syncthreads();
-        int nbatch = 0;
-        {
-            int carry = 0;
-            for (int base = 0; base < NK; base += T) {
-                const int k = base + tid;
-                const int v = k < NK ? kc[k] : 0;
-                int tot;
-                const int x = block_exclusive_scan(v, scan_sh, &tot);
-                if (k < NK) kc[k] = carry + x;
-                carry += tot;
-            }
-            nbatch = carry;
-        }
-        __syncthreads();
-        int *batch = A.c_level + e0;
-        for (int k = tid; k < NK; k += T) {
-            const int s0 = ls[k];
-            const int c = (k + 1 < NK ? ls[k + 1] : N) - s0;
-            const int q0 = kc[k];
-            for (int j = 0; 32 * j < c; j++)
-                batch[q0 + j] = (s0 + 32 * j) | ((min(32, c - 32 * j) - 1) << BATCH_SHIFT);
-        }
-        if (tid == 0) { A.w_levels[w] = Dw; A.w_runs[w] = R; A.w_batches[w] = nbatch; }
+        if (tid == 0) A.w_runs[w] = R;
         __syncthreads();
     }
 }
@@ -1258,68 +1135,103 @@ __device__ __forceinline__ int ld_acquire_cta(const int *p) {
 __device__ __forceinline__ void st_release_cta(int *p, int v) {
     asm volatile("st.release.cta.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
-// polls before a wait gives up: ~40x the longest legitimate wait (a whole
-// world's sweep)
+// polls before a wait gives up: far beyond any legitimate wait (a whole
+// world's sweep); one timeout sets the block's abort flag and ends every
+// other wait at once
 constexpr int SPIN_LIMIT = 1 << 22;
 
-// wait until the predecessor named by `code` of an entry of pass p is done
-// (done[x] counts the passes of run x completed). A wait that runs out sets
-// *abort, which ends every later wait of the block at once, so a broken
-// schedule costs one timeout, not one per entry; returns false then.
-__device__ __forceinline__ bool wait_pred(const int *done, int code, int p, volatile int *abort) {
-    int x, need;
-    if (code >= 0) { x = code; need = p + 1; }
-    else if (code != LEVEL_NONE && p > 0) { x = -code - 1; need = p; }
-    else return true;
-    for (int it = 0; it < SPIN_LIMIT; it++) {
-        if (ld_acquire_cta(&done[x]) >= need) return true;
-        if (*abort) return false;
-    }
-    *abort = 1;
-    return false;
+// predecessors entry (p, r) waits for: on each side, a same-pass predecessor
+// always counts, a previous-pass one only after pass 0. Runs count their
+// arrivals cumulatively over the passes, so entry (p, r) is ready when
+// arrivals reach need_first + p * need_rest (run_need packs both).
+__device__ __forceinline__ int need_of(int pk, int p) { return (pk & 3) + p * (pk >> 2); }
+
+// The per-world work ring: one slot per entry (each entry becomes ready
+// exactly once), 0 = not yet published, else entry + 1.
+struct SweepQueue {
+    int *ring;
+    int *head, *tail;
+};
+
+__device__ __forceinline__ void sweep_push(const Arena &A, const SweepQueue &Q, int N, int c0, int e,
+                                           const int *kn, volatile int *abort) {
+    const int pos = atomicAdd(Q.tail, 1);
+    if (pos >= N) { *abort = 1; return; }          // never with a consistent graph
+    st_release_cta(&Q.ring[pos], e + 1);
+    // then warm L1 with the entry's contact rows for whichever lane claims it
+    const int v = kn[e & PASS_MASK];
+    const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+    const char *row = reinterpret_cast<const char *>(&A.c_data[(size_t)k0 * CD]);
+    for (int off = 0; off < n * (int)(CD * sizeof(double)); off += 128) prefetch_l1(row + off);
 }
 
 // ---------------------------------------------------------------------------
-// The sweep: SWEEP_WARPS warps per world pull batches in schedule order from
-// a shared counter. Each lane reads its run's first row, waits until the
-// runs it follows have finished the passes it needs (acquire), solves the
-// run and publishes done[r] = p + 1 (release). Every predecessor sits in an
-// earlier batch, already taken by a running warp, so the waits end; a wait
-// that still runs out records ST_SWEEP_TIMEOUT (the host reports the step as
-// failed) and the lane goes on. Shared memory: the per-run pass counters,
-// the world's velocities and, when they fit too, its contacts' impulses
-// (worlds beyond the capacity use the global arrays).
+// The sweep as a dataflow over the world's entries (SWEEP_WARPS warps per
+// world). Entries whose predecessors are all done sit in the work ring; a
+// warp claims up to 32 published ones at a time (CAS on the head), each lane
+// solves its run, records the finish slot (for the critical-path length),
+// then (after a release fence) counts itself into each successor's arrivals -
+// the arrival that completes a successor fences again (acquire) and
+// publishes it to the ring (release store), then prefetches its contact rows
+// into L1. Everything an entry reads was written
+// by entries that happen-before it through those release/acquire chains.
+// Every wait is bounded; a timeout records ST_SWEEP_TIMEOUT and the host
+// reports the step as failed. Shared memory, as far as it goes: the per-run
+// arrival counts, finish slots, packed (contact, count) and need counts, the
+// world's velocities, its contacts' impulses, then the work ring (else the
+// global arrays).
 // ---------------------------------------------------------------------------
 constexpr int SWEEP_WARPS = 8;
 constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
 
 __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
     extern __shared__ __align__(16) double smem_d[];
-    __shared__ int next_batch;
-    __shared__ int abort_flag;
+    __shared__ int q_head, q_tail, abort_flag, crit;
     if (overflowed(A)) return;
     const int tid = threadIdx.x, lane = tid & 31;
+    volatile int *abort = &abort_flag;
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
         if (!world_collides(A, w)) continue;
-        const int NBt = A.w_batches[w];
-        if (NBt == 0) continue;
+        const int R = A.w_runs[w];
+        if (R == 0) { if (tid == 0) A.w_levels[w] = 0; continue; }
         int c0, c1;
         world_contacts(A, w, c0, c1);
-        const int K = c1 - c0, R = A.w_runs[w];
-        const size_t e0 = (size_t)c0 * A.max_passes;
-        const int *batch = A.c_level + e0, *order = A.c_order + e0;
-        const int *run_k = A.run_k + c0, *run_n = A.run_n + c0;
+        const int K = c1 - c0;
+        const int P = world_passes(A, w);
+        const int N = P * R;
         const int *run_pa = A.run_pa + c0, *run_pb = A.run_pb + c0;
+        const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
         const bool warm = (A.w_flags[w] & WF_WARM) != 0;
         const bool vel = warm || A.w_iters[w] > 0;
         const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+        // shared memory carve-up (doubles, 16-byte multiples): per-run arrival
+        // counts, finish slots, packed (contact, count) and need counts; then
+        // velocities, impulses and the work ring as far as they fit
         int used = 0;
-        const int done_d = ((R + 3) >> 2) << 1;        // R ints, in doubles, 16-byte multiple
-        int *done;
-        if (done_d <= smem_doubles) { done = reinterpret_cast<int *>(smem_d); used = done_d; }
-        else done = A.run_done + c0;
+        const int runs_d = ((4 * R + 3) >> 2) << 1;
+        int *arrived, *tend, *kn, *needpk;
+        if (runs_d <= smem_doubles) {
+            arrived = reinterpret_cast<int *>(smem_d);
+            tend = arrived + R;
+            kn = tend + R;
+            needpk = kn + R;
+            used = runs_d;
+            for (int r = tid; r < R; r += SWEEP_THREADS) {
+                kn[r] = A.run_kn[c0 + r];
+                needpk[r] = A.run_need[c0 + r];
+            }
+        } else {
+            arrived = A.run_done + c0;
+            tend = A.run_tend + c0;
+            kn = A.run_kn + c0;
+            needpk = A.run_need + c0;
+        }
         VelView V;
         V.b0 = b0;
         V.s = used + nb * 6 <= smem_doubles ? smem_d + used : nullptr;
@@ -1327,7 +1239,14 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_dou
         ImpView I;
         I.c0 = c0;
         I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
-        for (int r = tid; r < R; r += SWEEP_THREADS) done[r] = 0;
+        if (I.s) used = (used + K * 3 + 1) & ~1;
+        SweepQueue Q;
+        Q.ring = used + ((N + 1) >> 1) <= smem_doubles ? reinterpret_cast<int *>(smem_d + used)
+                                                        : A.c_order + (size_t)c0 * A.max_passes;
+        Q.head = &q_head;
+        Q.tail = &q_tail;
+        for (int r = tid; r < R; r += SWEEP_THREADS) { arrived[r] = 0; tend[r] = 0; }
+        for (int e = tid; e < N; e += SWEEP_THREADS) Q.ring[e] = 0;
         if (V.s) {
             for (int i = tid; i < nb; i += SWEEP_THREADS) {
                 double lv[3], av[3];
@@ -1338,32 +1257,82 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_dou
         }
         if (I.s)
             for (int i = tid; i < K * 3; i += SWEEP_THREADS) I.s[i] = A.c_imp[c0 * 3 + i];
-        if (tid == 0) { next_batch = 0; abort_flag = 0; }
+        if (tid == 0) { q_head = 0; q_tail = 0; abort_flag = 0; crit = 0; }
+        __syncthreads();
+        // entries with no predecessor: pass-0 runs that start both bodies' chains
+        for (int r = tid; r < R; r += SWEEP_THREADS)
+            if ((needpk[r] & 3) == 0) sweep_push(A, Q, N, c0, r, kn, abort);
         __syncthreads();
         const double slop = A.w_solver[w * 2 + 1];
-        bool ok = true;
+        int my_crit = 0;
         for (;;) {
-            int q = 0;
-            if (lane == 0) q = atomicAdd(&next_batch, 1);
-            q = __shfl_sync(FULL, q, 0);
-            if (q >= NBt) break;
-            const int bq = batch[q];
-            const int start = bq & ((1 << BATCH_SHIFT) - 1), cnt = (int)((unsigned)bq >> BATCH_SHIFT) + 1;
+            // lane 0 claims up to 32 published-or-pending ring positions
+            int lo = 0, cnt = 0;
+            if (lane == 0) {
+                for (int it = 0;; it++) {
+                    const int h = *(volatile int *)Q.head;
+                    if (h >= N || *abort) { cnt = -1; break; }
+                    const int t = min(*(volatile int *)Q.tail, N);
+                    if (t > h) {
+                        const int want = min(t - h, 32);
+                        if (atomicCAS(Q.head, h, h + want) == h) { lo = h; cnt = want; break; }
+                        continue;
+                    }
+                    if (it >= SPIN_LIMIT) { *abort = 1; cnt = -1; break; }
+                    __nanosleep(32);
+                }
+            }
+            cnt = __shfl_sync(FULL, cnt, 0);
+            lo = __shfl_sync(FULL, lo, 0);
+            if (cnt < 0) break;
             if (lane < cnt) {
-                const int e = order[start + lane];
-                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
-                const int k0 = c0 + run_k[r], n = run_n[r];
-                double row0[CD];
-                load_row(A, k0, row0);
-                ok &= wait_pred(done, run_pa[r], p, &abort_flag);
-                ok &= wait_pred(done, run_pb[r], p, &abort_flag);
-                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
-                st_release_cta(&done[r], p + 1);
+                int e1 = 0;
+                for (int it = 0; it < SPIN_LIMIT; it++) {     // the pusher is between its two steps
+                    e1 = ld_acquire_cta(&Q.ring[lo + lane]);
+                    if (e1 || *abort) break;
+                }
+                if (e1 == 0) *abort = 1;
+                else {
+                    const int e = e1 - 1;
+                    const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
+                    const int v = kn[r];
+                    const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+                    double row0[CD];
+                    load_row(A, k0, row0);
+                    // codes for the finish slot and the successors, read before the solve
+                    const int ca = __ldg(run_pa + r), cb = __ldg(run_pb + r);
+                    const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                    int t0 = 0;
+                    if (ca >= 0) t0 = tend[ca]; else if (ca != LEVEL_NONE && p > 0) t0 = tend[-ca - 1];
+                    if (cb >= 0) t0 = max(t0, tend[cb]); else if (cb != LEVEL_NONE && p > 0) t0 = max(t0, tend[-cb - 1]);
+                    run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                    tend[r] = t0 + n;
+                    my_crit = max(my_crit, t0 + n);
+                    // release this entry's writes, then count into the successors
+                    fence_acq_rel_cta();
+                    const int sides[2] = {sa, sb};
+#pragma unroll
+                    for (int sd = 0; sd < 2; sd++) {
+                        const int sc = sides[sd];
+                        int ps, rs;
+                        if (sc >= 0) { ps = p; rs = sc; }
+                        else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
+                        else continue;
+                        if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
+                            fence_acq_rel_cta();             // acquire the other arrivals' writes
+                            sweep_push(A, Q, N, c0, (ps << PASS_SHIFT) | rs, kn, abort);
+                        }
+                    }
+                }
             }
             __syncwarp();
         }
-        if (!ok) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+        atomicMax(&crit, my_crit);
         __syncthreads();
+        if (tid == 0) {
+            A.w_levels[w] = crit;
+            if (abort_flag || q_head < N) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+        }
         if (V.s) {
             for (int i = tid; i < nb; i += SWEEP_THREADS) {
                 if (A.mtype[b0 + i] != 2) continue;

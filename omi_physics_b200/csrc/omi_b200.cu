@@ -166,15 +166,17 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.c_imp, (size_t)contact_cap * 3);
     rc |= alloc(ctx, ctx->dyn, A.c_data, (size_t)contact_cap * CD);
     const size_t entries = (size_t)contact_cap * A.max_passes;
-    if (entries >= ((size_t)1 << 27)) return fail(ctx, OMI_E_ARG, "contact capacity x sweep passes exceeds 2^27");
-    rc |= alloc(ctx, ctx->dyn, A.c_level, entries);
+    if (entries >= ((size_t)1 << 31) - 2) return fail(ctx, OMI_E_ARG, "contact capacity x sweep passes exceeds 2^31");
     rc |= alloc(ctx, ctx->dyn, A.c_order, entries);
-    rc |= alloc(ctx, ctx->dyn, A.c_level_start, 2 * (entries + A.W + 1));
     rc |= alloc(ctx, ctx->dyn, A.run_pa, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_pb, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_sa, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_sb, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_kn, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.run_need, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_done, contact_cap);
-    rc |= alloc(ctx, ctx->dyn, A.lv_scratch,
-                (size_t)(5 + A.max_passes) * contact_cap + 2 * (size_t)A.NB + 2 * (size_t)A.W + 64);
+    rc |= alloc(ctx, ctx->dyn, A.run_tend, contact_cap);
+    rc |= alloc(ctx, ctx->dyn, A.lv_scratch, 3 * (size_t)contact_cap + 2 * (size_t)A.NB + 2 * (size_t)A.W + 64);
     rc |= alloc(ctx, ctx->dyn, A.run_k, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_n, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_a, contact_cap);
@@ -689,7 +691,6 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.b_flag, NB);
     rc |= alloc(ctx, ctx->statics, A.w_levels, W);
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
-    rc |= alloc(ctx, ctx->statics, A.w_batches, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
@@ -705,14 +706,15 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
     ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
     ctx->solve_block = max_n > 1024 ? 256 : 128;
-    // level tables of the largest world: about 2 + P ints per run, runs ~1.5 per body
-    ctx->level_ints = (int)std::min<int64_t>(LEVEL_SMEM_INTS, 32 * (int64_t)std::max(max_nc, 1) + 1024);
-    // the largest world's per-run pass counters (~1.5 runs per body), velocities
-    // (6 per body) and impulses (~2 contacts per body, 3 each)
-    ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
-                                                (int64_t)std::max(max_nc, 1) * 14 + 64);
+    // body buckets of the largest world: 2 ints per body + 2 per run (~1.5 runs per body)
+    ctx->level_ints = (int)std::min<int64_t>(LEVEL_SMEM_INTS, 8 * (int64_t)std::max(max_nc, 1) + 1024);
     A.max_passes = 1;
     for (int w = 0; w < W; w++) A.max_passes = std::max(A.max_passes, passes_of(s->w_flags[w], s->w_iters[w]));
+    // the largest world's per-run tables (4 ints, ~1.5 runs per body),
+    // velocities (6 per body), impulses (~2 contacts per body, 3 each) and work
+    // ring (~1.5 runs per body x passes)
+    ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
+                                                (int64_t)std::max(max_nc, 1) * (16 + A.max_passes) + 64);
     const int pair_cap = std::max(4096, 4 * NB);
     rc = alloc_dynamic(ctx, pair_cap, 2 * pair_cap);
     if (rc) return rc;
