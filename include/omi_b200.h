@@ -242,8 +242,11 @@ int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aabb_max,
                             int32_t *pairs, int32_t pair_cap, int32_t *n_pairs, void *stream,
                             char *err, int32_t err_cap);
 
-/* Gauss-Seidel depth (number of dependency levels of one sweep) of each
- * world's contacts in the last step (n_worlds ints; diagnostics). */
+/* Critical path of each world's last contact sweep (n_worlds ints;
+ * diagnostics): the longest chain of runs that must follow one another,
+ * weighted by their contact counts - the sequential sweep's length in contact
+ * solves, after independent runs are overlapped. No counterpart in the
+ * reference (whose sweep is the full sequence). */
 int omi_world_levels(OmiCtx *ctx, int32_t *levels);
 
 /* per-kernel device time (ms) of the last profiled step, see omi_profile_step */

@@ -158,7 +158,7 @@ class WorldBatch:
         return np.where(lab >= 0, lab - self.offsets[i], -1)
 
     def levels(self) -> np.ndarray:
-        """Gauss-Seidel depth of each world's contacts in the last step."""
+        """Critical path of each world's last contact sweep, in contact solves."""
         out = np.zeros(len(self.worlds), np.int32)
         self.ctx.call('world_levels', ptr(out, I))
         return out

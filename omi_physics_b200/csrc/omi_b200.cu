@@ -412,7 +412,7 @@ int run_steps(OmiCtx *ctx, int n, bool sync) {
         if (!sync) return 0;
         int rc = read_status(ctx);
         if (rc) return rc;
-        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_STATE, "contact sweep wait timed out");
+        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out");
         const int done = ctx->h_status[ST_STEPS_DONE];
         remaining -= done;
         if (remaining > 0) {
@@ -1064,7 +1064,7 @@ int omi_sync(OmiCtx *ctx) {
     if (rc) return rc;
     if (ctx->h_status[ST_OVERFLOW])
         return fail(ctx, OMI_E_STATE, "an asynchronous step overflowed its buffers; re-run with omi_step");
-    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_STATE, "contact sweep wait timed out");
+    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out");
     return 0;
 }
 
