@@ -108,6 +108,7 @@ struct Arena {
     int *run_kn, *run_need;         // per run: first contact | count << 24; need counts (k_levels)
     int *run_done, *run_tend;       // per run: sweep arrivals, finish slot (when not in shared memory)
     int *lv_scratch;                // k_levels buckets of worlds too large for shared memory
+    int *sweep_next;                // next schedule index the sweep blocks take (reset by k_levels)
     int max_passes;                 // sweep passes the level buffers are sized for (warm start + iterations)
     const int *w_sched;             // worlds ordered largest first (per-world kernels)
 

@@ -845,6 +845,7 @@ __device__ __forceinline__ size_t level_scratch_offset(const Arena &A, int c0, i
 __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints) {
     extern __shared__ int lsm[];
     __shared__ int scan_sh[33];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *A.sweep_next = 0;   // the sweep's world counter
     if (overflowed(A)) return;
     const int tid = threadIdx.x, T = blockDim.x;
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
@@ -1188,162 +1189,229 @@ __device__ __forceinline__ void sweep_push(const Arena &A, const SweepQueue &Q, 
 // ---------------------------------------------------------------------------
 constexpr int SWEEP_WARPS = 8;
 constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
+constexpr int SWEEP_GROUP = SWEEP_THREADS / 2;    // a half block sweeps one small world
 
+// barrier over the `n` threads of barrier `id` (0 = the whole block)
+__device__ __forceinline__ void group_sync(int id, int n) {
+    if (id == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// per-group shared scalars of the sweep
+struct SweepShared {
+    int head, tail, abort, crit;
+};
+
+// shared-memory doubles one world's sweep would like (tables, velocities,
+// impulses, work ring)
+__device__ __forceinline__ int sweep_want(const Arena &A, int w) {
+    const int R = A.w_runs[w];
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int N = world_passes(A, w) * R;
+    return 2 * R + 6 * A.w_body_n[w] + 3 * (c1 - c0) + (N + 1) / 2 + 8;
+}
+
+// One world's sweep by the `gn` threads of a group (gtid = thread index in it,
+// bar = its barrier id; 0 when the group is the whole block).
+__device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doubles, int gtid, int gn, int bar,
+                            SweepShared &sh) {
+    const int lane = gtid & 31;
+    volatile int *abort = &sh.abort;
+    const int R = A.w_runs[w];
+    if (R == 0) {
+        if (gtid == 0) A.w_levels[w] = 0;
+        return;
+    }
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int K = c1 - c0;
+    const int P = world_passes(A, w);
+    const int N = P * R;
+    const int *run_pa = A.run_pa + c0, *run_pb = A.run_pb + c0;
+    const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
+    const bool warm = (A.w_flags[w] & WF_WARM) != 0;
+    const bool vel = warm || A.w_iters[w] > 0;
+    const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+    // shared memory carve-up (doubles, 16-byte multiples): per-run arrival
+    // counts, finish slots, packed (contact, count) and need counts; then
+    // velocities, impulses and the work ring as far as they fit
+    int used = 0;
+    const int runs_d = ((4 * R + 3) >> 2) << 1;
+    int *arrived, *tend, *kn, *needpk;
+    if (runs_d <= smem_doubles) {
+        arrived = reinterpret_cast<int *>(smem_d);
+        tend = arrived + R;
+        kn = tend + R;
+        needpk = kn + R;
+        used = runs_d;
+        for (int r = gtid; r < R; r += gn) {
+            kn[r] = A.run_kn[c0 + r];
+            needpk[r] = A.run_need[c0 + r];
+        }
+    } else {
+        arrived = A.run_done + c0;
+        tend = A.run_tend + c0;
+        kn = A.run_kn + c0;
+        needpk = A.run_need + c0;
+    }
+    VelView V;
+    V.b0 = b0;
+    V.s = used + nb * 6 <= smem_doubles ? smem_d + used : nullptr;
+    if (V.s) used = (used + nb * 6 + 1) & ~1;
+    ImpView I;
+    I.c0 = c0;
+    I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
+    if (I.s) used = (used + K * 3 + 1) & ~1;
+    SweepQueue Q;
+    Q.ring = used + ((N + 1) >> 1) <= smem_doubles ? reinterpret_cast<int *>(smem_d + used)
+                                                    : A.c_order + (size_t)c0 * A.max_passes;
+    Q.head = &sh.head;
+    Q.tail = &sh.tail;
+    for (int r = gtid; r < R; r += gn) { arrived[r] = 0; tend[r] = 0; }
+    for (int e = gtid; e < N; e += gn) Q.ring[e] = 0;
+    if (V.s) {
+        for (int i = gtid; i < nb; i += gn) {
+            double lv[3], av[3];
+            lv[0] = A.v[(b0 + i) * 3]; lv[1] = A.v[(b0 + i) * 3 + 1]; lv[2] = A.v[(b0 + i) * 3 + 2];
+            av[0] = A.w[(b0 + i) * 3]; av[1] = A.w[(b0 + i) * 3 + 1]; av[2] = A.w[(b0 + i) * 3 + 2];
+            vel_store(A, V, b0 + i, lv, av);
+        }
+    }
+    if (I.s)
+        for (int i = gtid; i < K * 3; i += gn) I.s[i] = A.c_imp[c0 * 3 + i];
+    if (gtid == 0) { sh.head = 0; sh.tail = 0; sh.abort = 0; sh.crit = 0; }
+    group_sync(bar, gn);
+    // entries with no predecessor: pass-0 runs that start both bodies' chains
+    for (int r = gtid; r < R; r += gn)
+        if ((needpk[r] & 3) == 0) sweep_push(A, Q, N, c0, r, kn, abort);
+    group_sync(bar, gn);
+    const double slop = A.w_solver[w * 2 + 1];
+    int my_crit = 0;
+    for (;;) {
+        // lane 0 claims up to 32 published-or-pending ring positions
+        int lo = 0, cnt = 0;
+        if (lane == 0) {
+            for (int it = 0;; it++) {
+                const int h = *(volatile int *)Q.head;
+                if (h >= N || *abort) { cnt = -1; break; }
+                const int t = min(*(volatile int *)Q.tail, N);
+                if (t > h) {
+                    const int want = min(t - h, 32);
+                    if (atomicCAS(Q.head, h, h + want) == h) { lo = h; cnt = want; break; }
+                    continue;
+                }
+                if (it >= SPIN_LIMIT) { *abort = 1; cnt = -1; break; }
+                __nanosleep(32);
+            }
+        }
+        cnt = __shfl_sync(FULL, cnt, 0);
+        lo = __shfl_sync(FULL, lo, 0);
+        if (cnt < 0) break;
+        if (lane < cnt) {
+            int e1 = 0;
+            for (int it = 0; it < SPIN_LIMIT; it++) {     // the pusher is between its two steps
+                e1 = ld_acquire_cta(&Q.ring[lo + lane]);
+                if (e1 || *abort) break;
+            }
+            if (e1 == 0) *abort = 1;
+            else {
+                const int e = e1 - 1;
+                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
+                const int v = kn[r];
+                const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+                double row0[CD];
+                load_row(A, k0, row0);
+                // codes for the finish slot and the successors, read before the solve
+                const int ca = __ldg(run_pa + r), cb = __ldg(run_pb + r);
+                const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                int t0 = 0;
+                if (ca >= 0) t0 = tend[ca]; else if (ca != LEVEL_NONE && p > 0) t0 = tend[-ca - 1];
+                if (cb >= 0) t0 = max(t0, tend[cb]); else if (cb != LEVEL_NONE && p > 0) t0 = max(t0, tend[-cb - 1]);
+                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                tend[r] = t0 + n;
+                my_crit = max(my_crit, t0 + n);
+                // release this entry's writes, then count into the successors
+                fence_acq_rel_cta();
+                const int sides[2] = {sa, sb};
+#pragma unroll
+                for (int sd = 0; sd < 2; sd++) {
+                    const int sc = sides[sd];
+                    int ps, rs;
+                    if (sc >= 0) { ps = p; rs = sc; }
+                    else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
+                    else continue;
+                    if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
+                        fence_acq_rel_cta();             // acquire the other arrivals' writes
+                        sweep_push(A, Q, N, c0, (ps << PASS_SHIFT) | rs, kn, abort);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    atomicMax(&sh.crit, my_crit);
+    group_sync(bar, gn);
+    if (gtid == 0) {
+        A.w_levels[w] = sh.crit;
+        if (sh.abort || sh.head < N) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+    }
+    if (V.s) {
+        for (int i = gtid; i < nb; i += gn) {
+            if (A.mtype[b0 + i] != 2) continue;
+            double lv[3], av[3];
+            vel_load(A, V, b0 + i, lv, av);
+            A.v[(b0 + i) * 3] = lv[0]; A.v[(b0 + i) * 3 + 1] = lv[1]; A.v[(b0 + i) * 3 + 2] = lv[2];
+            A.w[(b0 + i) * 3] = av[0]; A.w[(b0 + i) * 3 + 1] = av[1]; A.w[(b0 + i) * 3 + 2] = av[2];
+        }
+    }
+    if (I.s)
+        for (int i = gtid; i < K * 3; i += gn) A.c_imp[c0 * 3 + i] = I.s[i];
+    group_sync(bar, gn);
+}
+
+// Persistent sweep blocks take worlds in schedule order (largest first) from
+// a counter k_levels reset. A world whose wanted shared memory exceeds half
+// of the block's gets the whole block; otherwise the block takes two worlds
+// and each half sweeps one (all later worlds are no larger).
 __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
     extern __shared__ __align__(16) double smem_d[];
-    __shared__ int q_head, q_tail, abort_flag, crit;
+    __shared__ SweepShared sh[2];
+    __shared__ int pick[3];               // mode (0 done, 1 whole, 2 halves), world per group
     if (overflowed(A)) return;
-    const int tid = threadIdx.x, lane = tid & 31;
-    volatile int *abort = &abort_flag;
-    for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
-        const int w = A.w_sched[wi];
-        if (!world_collides(A, w)) continue;
-        const int R = A.w_runs[w];
-        if (R == 0) { if (tid == 0) A.w_levels[w] = 0; continue; }
-        int c0, c1;
-        world_contacts(A, w, c0, c1);
-        const int K = c1 - c0;
-        const int P = world_passes(A, w);
-        const int N = P * R;
-        const int *run_pa = A.run_pa + c0, *run_pb = A.run_pb + c0;
-        const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
-        const bool warm = (A.w_flags[w] & WF_WARM) != 0;
-        const bool vel = warm || A.w_iters[w] > 0;
-        const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
-        // shared memory carve-up (doubles, 16-byte multiples): per-run arrival
-        // counts, finish slots, packed (contact, count) and need counts; then
-        // velocities, impulses and the work ring as far as they fit
-        int used = 0;
-        const int runs_d = ((4 * R + 3) >> 2) << 1;
-        int *arrived, *tend, *kn, *needpk;
-        if (runs_d <= smem_doubles) {
-            arrived = reinterpret_cast<int *>(smem_d);
-            tend = arrived + R;
-            kn = tend + R;
-            needpk = kn + R;
-            used = runs_d;
-            for (int r = tid; r < R; r += SWEEP_THREADS) {
-                kn[r] = A.run_kn[c0 + r];
-                needpk[r] = A.run_need[c0 + r];
-            }
-        } else {
-            arrived = A.run_done + c0;
-            tend = A.run_tend + c0;
-            kn = A.run_kn + c0;
-            needpk = A.run_need + c0;
-        }
-        VelView V;
-        V.b0 = b0;
-        V.s = used + nb * 6 <= smem_doubles ? smem_d + used : nullptr;
-        if (V.s) used = (used + nb * 6 + 1) & ~1;
-        ImpView I;
-        I.c0 = c0;
-        I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
-        if (I.s) used = (used + K * 3 + 1) & ~1;
-        SweepQueue Q;
-        Q.ring = used + ((N + 1) >> 1) <= smem_doubles ? reinterpret_cast<int *>(smem_d + used)
-                                                        : A.c_order + (size_t)c0 * A.max_passes;
-        Q.head = &q_head;
-        Q.tail = &q_tail;
-        for (int r = tid; r < R; r += SWEEP_THREADS) { arrived[r] = 0; tend[r] = 0; }
-        for (int e = tid; e < N; e += SWEEP_THREADS) Q.ring[e] = 0;
-        if (V.s) {
-            for (int i = tid; i < nb; i += SWEEP_THREADS) {
-                double lv[3], av[3];
-                lv[0] = A.v[(b0 + i) * 3]; lv[1] = A.v[(b0 + i) * 3 + 1]; lv[2] = A.v[(b0 + i) * 3 + 2];
-                av[0] = A.w[(b0 + i) * 3]; av[1] = A.w[(b0 + i) * 3 + 1]; av[2] = A.w[(b0 + i) * 3 + 2];
-                vel_store(A, V, b0 + i, lv, av);
-            }
-        }
-        if (I.s)
-            for (int i = tid; i < K * 3; i += SWEEP_THREADS) I.s[i] = A.c_imp[c0 * 3 + i];
-        if (tid == 0) { q_head = 0; q_tail = 0; abort_flag = 0; crit = 0; }
-        __syncthreads();
-        // entries with no predecessor: pass-0 runs that start both bodies' chains
-        for (int r = tid; r < R; r += SWEEP_THREADS)
-            if ((needpk[r] & 3) == 0) sweep_push(A, Q, N, c0, r, kn, abort);
-        __syncthreads();
-        const double slop = A.w_solver[w * 2 + 1];
-        int my_crit = 0;
-        for (;;) {
-            // lane 0 claims up to 32 published-or-pending ring positions
-            int lo = 0, cnt = 0;
-            if (lane == 0) {
-                for (int it = 0;; it++) {
-                    const int h = *(volatile int *)Q.head;
-                    if (h >= N || *abort) { cnt = -1; break; }
-                    const int t = min(*(volatile int *)Q.tail, N);
-                    if (t > h) {
-                        const int want = min(t - h, 32);
-                        if (atomicCAS(Q.head, h, h + want) == h) { lo = h; cnt = want; break; }
-                        continue;
-                    }
-                    if (it >= SPIN_LIMIT) { *abort = 1; cnt = -1; break; }
-                    __nanosleep(32);
-                }
-            }
-            cnt = __shfl_sync(FULL, cnt, 0);
-            lo = __shfl_sync(FULL, lo, 0);
-            if (cnt < 0) break;
-            if (lane < cnt) {
-                int e1 = 0;
-                for (int it = 0; it < SPIN_LIMIT; it++) {     // the pusher is between its two steps
-                    e1 = ld_acquire_cta(&Q.ring[lo + lane]);
-                    if (e1 || *abort) break;
-                }
-                if (e1 == 0) *abort = 1;
-                else {
-                    const int e = e1 - 1;
-                    const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
-                    const int v = kn[r];
-                    const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
-                    double row0[CD];
-                    load_row(A, k0, row0);
-                    // codes for the finish slot and the successors, read before the solve
-                    const int ca = __ldg(run_pa + r), cb = __ldg(run_pb + r);
-                    const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
-                    int t0 = 0;
-                    if (ca >= 0) t0 = tend[ca]; else if (ca != LEVEL_NONE && p > 0) t0 = tend[-ca - 1];
-                    if (cb >= 0) t0 = max(t0, tend[cb]); else if (cb != LEVEL_NONE && p > 0) t0 = max(t0, tend[-cb - 1]);
-                    run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
-                    tend[r] = t0 + n;
-                    my_crit = max(my_crit, t0 + n);
-                    // release this entry's writes, then count into the successors
-                    fence_acq_rel_cta();
-                    const int sides[2] = {sa, sb};
-#pragma unroll
-                    for (int sd = 0; sd < 2; sd++) {
-                        const int sc = sides[sd];
-                        int ps, rs;
-                        if (sc >= 0) { ps = p; rs = sc; }
-                        else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
-                        else continue;
-                        if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
-                            fence_acq_rel_cta();             // acquire the other arrivals' writes
-                            sweep_push(A, Q, N, c0, (ps << PASS_SHIFT) | rs, kn, abort);
-                        }
-                    }
-                }
-            }
-            __syncwarp();
-        }
-        atomicMax(&crit, my_crit);
-        __syncthreads();
+    const int tid = threadIdx.x;
+    const int half = (smem_doubles / 2) & ~1;
+    for (;;) {
         if (tid == 0) {
-            A.w_levels[w] = crit;
-            if (abort_flag || q_head < N) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
-        }
-        if (V.s) {
-            for (int i = tid; i < nb; i += SWEEP_THREADS) {
-                if (A.mtype[b0 + i] != 2) continue;
-                double lv[3], av[3];
-                vel_load(A, V, b0 + i, lv, av);
-                A.v[(b0 + i) * 3] = lv[0]; A.v[(b0 + i) * 3 + 1] = lv[1]; A.v[(b0 + i) * 3 + 2] = lv[2];
-                A.w[(b0 + i) * 3] = av[0]; A.w[(b0 + i) * 3 + 1] = av[1]; A.w[(b0 + i) * 3 + 2] = av[2];
+            int mode = 0, w0 = -1, w1 = -1;
+            for (;;) {
+                const int wi = atomicAdd(A.sweep_next, 1);
+                if (wi >= A.W) break;
+                const int w = A.w_sched[wi];
+                if (!world_collides(A, w)) continue;
+                w0 = w;
+                if (sweep_want(A, w) > half) { mode = 1; break; }
+                mode = 2;
+                for (;;) {
+                    const int wj = atomicAdd(A.sweep_next, 1);
+                    if (wj >= A.W) break;
+                    const int x = A.w_sched[wj];
+                    if (world_collides(A, x)) { w1 = x; break; }
+                }
+                break;
             }
+            pick[0] = mode; pick[1] = w0; pick[2] = w1;
         }
-        if (I.s)
-            for (int i = tid; i < K * 3; i += SWEEP_THREADS) A.c_imp[c0 * 3 + i] = I.s[i];
+        __syncthreads();
+        const int mode = pick[0];
+        if (mode == 0) break;
+        if (mode == 1) {
+            sweep_world(A, pick[1], smem_d, smem_doubles, tid, SWEEP_THREADS, 0, sh[0]);
+        } else {
+            const int g = tid / SWEEP_GROUP;
+            const int w = pick[1 + g];
+            if (w >= 0) sweep_world(A, w, smem_d + g * half, half, tid - g * SWEEP_GROUP, SWEEP_GROUP, 1 + g, sh[g]);
+        }
         __syncthreads();
     }
 }

@@ -56,6 +56,7 @@ struct OmiCtx {
     int max_world_n = 0, max_world_j = 0, sort_cap = 0, sort_block = 256;
     int solve_block = 128;
     int level_ints = 0;            // shared ints of one k_levels block
+    int sm_count = 148;            // multiprocessors of the device (persistent sweep grid)
     int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
     cudaGraphExec_t graph = nullptr;
@@ -304,7 +305,7 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     mark(ctx, pf, KN_PREP);
     k_levels<<<std::min(A.W, 65535), LEVEL_THREADS, (size_t)ctx->level_ints * sizeof(int), ctx->stream>>>(A, ctx->level_ints);
     mark(ctx, pf, KN_LEVELS);
-    k_iterate<<<std::min(A.W, 65535), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
+    k_iterate<<<std::min(A.W, ctx->sm_count), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
     ctx->launches += 4;
     mark(ctx, pf, KN_SOLVE);
     k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
@@ -455,6 +456,8 @@ int omi_create(int device, OmiCtx **out) {
     e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaStreamCreate"); *out = ctx; return rc; }
     ctx->stream = ctx->own;
+    e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaDeviceGetAttribute"); *out = ctx; return rc; }
     e = cudaMallocHost(&ctx->h_status, sizeof(int) * ST_WORDS);
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
     const struct { const void *fn; int bytes; const char *name; } smem[] = {
@@ -692,6 +695,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.w_levels, W);
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
+    rc |= alloc(ctx, ctx->statics, A.sweep_next, 1);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
         rc |= alloc(ctx, ctx->statics, A.w_cache_n[t], W);
