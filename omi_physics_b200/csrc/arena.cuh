@@ -84,6 +84,9 @@ struct Arena {
     // broadphase
     int *order;              // sorted global body index per row (per world range)
     double *sorted_x;
+    double *srt_box;         // per sorted row: lo/hi x, y, z and 2 pad (8 doubles)
+    int *srt_info;           // per sorted row: motion type | filter row << 2
+    int *pair_end;           // per sorted row: end of its sweep window
     double *sort_k[2];
     int *sort_v[2];
     int *pair_cnt, *pair_scan;      // NB, NB+1

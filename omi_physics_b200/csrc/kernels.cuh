@@ -88,6 +88,8 @@ __device__ __forceinline__ bool key_less(double ka, int va, double kb, int vb) {
     return ka < kb || (!(kb < ka) && va < vb);
 }
 
+// ROWS: also write each sorted row's box (the step's broadphase reads them)
+template <bool ROWS>
 __global__ void k_sort(Arena A, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem[];
     for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
@@ -133,8 +135,16 @@ __global__ void k_sort(Arena A, int smem_cap) {
             int *tv = v0; v0 = v1; v1 = tv;
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            A.order[off + i] = off + v0[i];
+            const int body = off + v0[i];
+            A.order[off + i] = body;
             A.sorted_x[off + i] = k0[i];
+            if (!ROWS) continue;
+            // the row's box in sorted order, so the sweep windows read rows contiguously
+            double4 *row = reinterpret_cast<double4 *>(&A.srt_box[(size_t)(off + i) * 8]);
+            const double *lo = &A.aabb_min[body * 3], *hi = &A.aabb_max[body * 3];
+            row[0] = make_double4(lo[0], hi[0], lo[1], hi[1]);
+            row[1] = make_double4(lo[2], hi[2], 0.0, 0.0);
+            A.srt_info[off + i] = A.mtype[body] | (A.filter_row[body] << 2);
         }
         __syncthreads();
     }
@@ -145,7 +155,10 @@ __global__ void k_sort(Arena A, int smem_cap) {
 // candidates are rows k+1 .. searchsorted(lo_sx, hi_sx[k], 'right')-1; keep
 // y/z overlap (>=), at least one dynamic body and interacting filters. One
 // warp per sorted row; lanes test 32 candidates at a time and a ballot keeps
-// the reference's k-major, then kj, order.
+// the reference's k-major, then kj, order. The step's kernels read the rows'
+// boxes in sorted order (written by k_sort) and the count pass records each
+// window's end for the emit pass; the helpers below serve the
+// allocation-free entry point, which reads the caller's boxes in place.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool pair_keep(const Arena &A, int w, int a, int b) {
     const double *la = &A.aabb_min[a * 3], *ha = &A.aabb_max[a * 3];
@@ -168,7 +181,9 @@ __device__ __forceinline__ int window_end(const Arena &A, int off, int end_w, do
     return lo;
 }
 
-__global__ void k_pair_count(Arena A) {
+// the count pass on boxes read in place (no sorted rows, no recorded window
+// ends): the allocation-free entry point's form
+__global__ void k_pair_count_boxes(Arena A) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.NB; e += nwarps) {
@@ -188,6 +203,66 @@ __global__ void k_pair_count(Arena A) {
     }
 }
 
+
+// first row k in [lo, hi) with !(sorted_x[k] <= hx), else hi - the binary
+// search above done 32-ary by a warp (one load per lane per step, ~3 steps)
+__device__ __forceinline__ int window_end_warp(const double *sx, int lo, int hi, double hx) {
+    const int lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const int step = (hi - lo + 31) >> 5;
+        const int k = lo + lane * step;
+        const bool t = k < hi ? !(sx[k] <= hx) : true;
+        const unsigned m = __ballot_sync(FULL, t);
+        const int f = m ? __ffs(m) - 1 : 32;
+        const int nlo = f > 0 ? lo + (f - 1) * step + 1 : lo;
+        const int nhi = f < 32 ? min(hi, lo + f * step) : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    const bool t = lo + lane < hi ? !(sx[lo + lane] <= hx) : true;
+    const unsigned m = __ballot_sync(FULL, t);
+    return m ? min(hi, lo + __ffs(m) - 1) : hi;      // m == 0: 32 rows left, none past hx
+}
+
+// pair_keep on sorted rows: `ra`/`rb` are the rows' boxes (lo/hi x, y, z),
+// `ia`/`ib` their motion type | filter row << 2
+__device__ __forceinline__ bool row_keep(const Arena &A, int w, const double4 &a0, const double4 &a1, int ia,
+                                         const double4 &b0, const double4 &b1, int ib) {
+    bool keep = (a0.w >= b0.z) & (b0.w >= a0.z) & (a1.y >= b1.x) & (b1.y >= a1.x);
+    keep &= ((ia & 3) == 2) | ((ib & 3) == 2);
+    if (keep) {
+        const int rows = A.w_filter_rows[w];
+        keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 2) * rows + (ib >> 2)] != 0;
+    }
+    return keep;
+}
+
+__global__ void k_pair_count(Arena A) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.NB; e += nwarps) {
+        const int w = A.body_world[e];
+        int cnt = 0, endk = e + 1;
+        if (world_collides(A, w) && e - A.w_body_off[w] < A.w_body_n[w]) {
+            const int off = A.w_body_off[w], end_w = off + A.w_body_n[w];
+            const double4 *ra = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)e * 8]);
+            const double4 a0 = ra[0], a1 = ra[1];
+            const int ia = A.srt_info[e];
+            endk = window_end_warp(A.sorted_x, off, end_w, a0.y);
+            for (int base = e + 1; base < endk; base += 32) {
+                const int kj = base + lane;
+                bool keep = false;
+                if (kj < endk) {
+                    const double4 *rb = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)kj * 8]);
+                    keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], A.srt_info[kj]);
+                }
+                cnt += __popc(__ballot_sync(FULL, keep));
+            }
+        }
+        if (lane == 0) { A.pair_cnt[e] = cnt; A.pair_end[e] = endk; }
+    }
+}
+
 __global__ void k_pair_emit(Arena A) {
     if (pairs_over(A)) return;
     const int lane = threadIdx.x & 31;
@@ -195,15 +270,22 @@ __global__ void k_pair_emit(Arena A) {
     for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.NB; e += nwarps) {
         const int w = A.body_world[e];
         if (!world_collides(A, w) || e - A.w_body_off[w] >= A.w_body_n[w]) continue;
-        const int off = A.w_body_off[w], end_w = off + A.w_body_n[w];
+        const int endk = A.pair_end[e];
+        if (endk <= e + 1) continue;
         const int a = A.order[e];
-        const int endk = window_end(A, off, end_w, A.aabb_max[a * 3]);
+        const double4 *ra = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)e * 8]);
+        const double4 a0 = ra[0], a1 = ra[1];
+        const int ia = A.srt_info[e];
         int out = A.pair_scan[e];
         for (int base = e + 1; base < endk; base += 32) {
             const int kj = base + lane;
             int b = -1;
             bool keep = false;
-            if (kj < endk) { b = A.order[kj]; keep = pair_keep(A, w, a, b); }
+            if (kj < endk) {
+                const double4 *rb = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)kj * 8]);
+                keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], A.srt_info[kj]);
+                if (keep) b = A.order[kj];
+            }
             const unsigned m = __ballot_sync(FULL, keep);
             if (keep) {
                 const int slot = out + __popc(m & ((1u << lane) - 1u));
@@ -1059,7 +1141,7 @@ __device__ __forceinline__ void contact_position(double *pa, double *pb, const P
 
 // dynamic shared memory of one sweep block, in doubles: 227 KB less room for
 // the block's static shared variables
-constexpr int SWEEP_SMEM_DOUBLES = 29056 - 8;
+constexpr int SWEEP_SMEM_DOUBLES = 29056 - 16;
 
 struct ImpView {
     double *s;       // shared staging (nullptr: global c_imp)
@@ -1189,7 +1271,6 @@ __device__ __forceinline__ void sweep_push(const Arena &A, const SweepQueue &Q, 
 // ---------------------------------------------------------------------------
 constexpr int SWEEP_WARPS = 8;
 constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
-constexpr int SWEEP_GROUP = SWEEP_THREADS / 2;    // a half block sweeps one small world
 
 // barrier over the `n` threads of barrier `id` (0 = the whole block)
 __device__ __forceinline__ void group_sync(int id, int n) {
@@ -1371,47 +1452,49 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
 }
 
 // Persistent sweep blocks take worlds in schedule order (largest first) from
-// a counter k_levels reset. A world whose wanted shared memory exceeds half
-// of the block's gets the whole block; otherwise the block takes two worlds
-// and each half sweeps one (all later worlds are no larger).
+// a counter k_levels reset. The first world taken decides the split: G = 1,
+// 2 or 4 groups, the largest G whose share of the block's shared memory
+// still holds everything that world wants; the block then takes G - 1 more
+// worlds (all later worlds are no larger) and each group sweeps one.
+constexpr int SWEEP_MAX_GROUPS = 4;
+
 __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
     extern __shared__ __align__(16) double smem_d[];
-    __shared__ SweepShared sh[2];
-    __shared__ int pick[3];               // mode (0 done, 1 whole, 2 halves), world per group
+    __shared__ SweepShared sh[SWEEP_MAX_GROUPS];
+    __shared__ int pick[1 + SWEEP_MAX_GROUPS];    // groups (0: done), world per group
     if (overflowed(A)) return;
     const int tid = threadIdx.x;
-    const int half = (smem_doubles / 2) & ~1;
     for (;;) {
         if (tid == 0) {
-            int mode = 0, w0 = -1, w1 = -1;
+            int G = 0;
+            for (int g = 0; g < SWEEP_MAX_GROUPS; g++) pick[1 + g] = -1;
             for (;;) {
                 const int wi = atomicAdd(A.sweep_next, 1);
                 if (wi >= A.W) break;
                 const int w = A.w_sched[wi];
                 if (!world_collides(A, w)) continue;
-                w0 = w;
-                if (sweep_want(A, w) > half) { mode = 1; break; }
-                mode = 2;
-                for (;;) {
-                    const int wj = atomicAdd(A.sweep_next, 1);
-                    if (wj >= A.W) break;
-                    const int x = A.w_sched[wj];
-                    if (world_collides(A, x)) { w1 = x; break; }
+                const int want = sweep_want(A, w);
+                G = want <= ((smem_doubles / 4) & ~1) ? 4 : (want <= ((smem_doubles / 2) & ~1) ? 2 : 1);
+                pick[1] = w;
+                for (int g = 1; g < G; g++) {
+                    for (;;) {
+                        const int wj = atomicAdd(A.sweep_next, 1);
+                        if (wj >= A.W) break;
+                        const int x = A.w_sched[wj];
+                        if (world_collides(A, x)) { pick[1 + g] = x; break; }
+                    }
                 }
                 break;
             }
-            pick[0] = mode; pick[1] = w0; pick[2] = w1;
+            pick[0] = G;
         }
         __syncthreads();
-        const int mode = pick[0];
-        if (mode == 0) break;
-        if (mode == 1) {
-            sweep_world(A, pick[1], smem_d, smem_doubles, tid, SWEEP_THREADS, 0, sh[0]);
-        } else {
-            const int g = tid / SWEEP_GROUP;
-            const int w = pick[1 + g];
-            if (w >= 0) sweep_world(A, w, smem_d + g * half, half, tid - g * SWEEP_GROUP, SWEEP_GROUP, 1 + g, sh[g]);
-        }
+        const int G = pick[0];
+        if (G == 0) break;
+        const int gn = SWEEP_THREADS / G, g = tid / gn;
+        const int share = (smem_doubles / G) & ~1;
+        const int w = pick[1 + g];
+        if (w >= 0) sweep_world(A, w, smem_d + g * share, share, tid - g * gn, gn, G == 1 ? 0 : 1 + g, sh[g]);
         __syncthreads();
     }
 }

@@ -259,7 +259,7 @@ void stage_refit(OmiCtx *ctx, Prof *pf) {
 void stage_broadphase(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
     const size_t smem = (size_t)ctx->sort_cap * (2 * sizeof(double) + 2 * sizeof(int));
-    k_sort<<<std::min(A.W, 65535), ctx->sort_block, smem, ctx->stream>>>(A, ctx->sort_cap);
+    k_sort<true><<<std::min(A.W, 65535), ctx->sort_block, smem, ctx->stream>>>(A, ctx->sort_cap);
     ctx->launches++;
     mark(ctx, pf, KN_SORT);
     k_pair_count<<<grid_for(A.NB * 32, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
@@ -462,7 +462,7 @@ int omi_create(int device, OmiCtx **out) {
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
     const struct { const void *fn; int bytes; const char *name; } smem[] = {
         {(const void *)k_gjk, 4 * (int)sizeof(EpaWork), "k_gjk"},
-        {(const void *)k_sort, 8192 * 24, "k_sort"},
+        {(const void *)k_sort<true>, 8192 * 24, "k_sort"},
         {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
     };
@@ -682,6 +682,9 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     // per-body scratch
     rc |= alloc(ctx, ctx->statics, A.order, NB);
     rc |= alloc(ctx, ctx->statics, A.sorted_x, NB);
+    rc |= alloc(ctx, ctx->statics, A.srt_box, (size_t)NB * 8);
+    rc |= alloc(ctx, ctx->statics, A.srt_info, NB);
+    rc |= alloc(ctx, ctx->statics, A.pair_end, NB);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.sort_k[t], NB);
         rc |= alloc(ctx, ctx->statics, A.sort_v[t], NB);
@@ -1495,7 +1498,7 @@ extern "C" int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aab
                                      cudaGetErrorString(e));
             return OMI_E_CUDA;
         }
-        e = cudaFuncSetAttribute(k_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
+        e = cudaFuncSetAttribute(k_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
         if (e != cudaSuccess) {
             na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaFuncSetAttribute: ") +
                                      cudaGetErrorString(e));
@@ -1535,8 +1538,8 @@ extern "C" int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aab
     const int rows = filter_row ? filter_rows : 1;
     k_noalloc_init<<<grid_for(std::max(n, 1), 256, 64), 256, 0, st>>>(base, n, rows, filter_row != nullptr);
     const int sort_cap = std::min(std::max(n, 1), 8192);
-    k_sort<<<1, n > 2048 ? 1024 : 256, (size_t)sort_cap * 24, st>>>(A, sort_cap);
-    k_pair_count<<<grid_for(std::max(n, 1) * 32, 256, 148 * 16), 256, 0, st>>>(A);
+    k_sort<false><<<1, n > 2048 ? 1024 : 256, (size_t)sort_cap * 24, st>>>(A, sort_cap);
+    k_pair_count_boxes<<<grid_for(std::max(n, 1) * 32, 256, 148 * 16), 256, 0, st>>>(A);
     const int ntiles = std::max(1, (n + SCAN_TILE - 1) / SCAN_TILE);
     k_scan_tiles<<<ntiles, 1024, 0, st>>>(A.pair_cnt, A.pair_scan, n, nullptr, nullptr, 0, 0, tiles);
     k_scan_top<<<1, 1024, 0, st>>>(tiles, ntiles, nullptr, 0, 0);

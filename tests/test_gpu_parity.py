@@ -100,3 +100,32 @@ def test_joint_chain_trajectory_within_tolerance():
     st = o.state()
     assert float(np.max(np.abs(w.position - st['position']))) < 1e-6
     assert float(np.max(np.abs(w.orientation - st['orientation']))) < 1e-6
+
+
+def test_serving_mix_batch_matches_oracle_per_world():
+    """64 worlds of the serving mix (uneven sizes) stepped together for 120 steps:
+    every world's pairs, poses, velocities and sleep flags equal the oracle's
+    for that world alone, bit for bit."""
+    reqs = scenes.serving_requests(64, seed=0)
+    worlds, dts = [], []
+    for r in reqs:
+        w, meta = scenes.serving_world(r)
+        worlds.append(w)
+        dts.append(meta['dt'])
+    b = WorldBatch(worlds, dts=dts)
+    b.step(120)
+    b.sync_to_host()
+    for i, r in enumerate(reqs):
+        w0, meta = scenes.serving_world(r)
+        o = pyoracle.OracleWorld.from_world(w0)
+        for _ in range(120):
+            o.step(meta['dt'])
+        st = o.state()
+        w = worlds[i]
+        n = w.body_count
+        assert np.array_equal(b.pairs(i), o.pairs()), (i, 'pairs')
+        assert np.array_equal(w._position[:n], st['position']), (i, 'position')
+        assert np.array_equal(w._orientation[:n], st['orientation']), (i, 'orientation')
+        assert np.array_equal(w._linear_velocity[:n], st['linear_velocity']), (i, 'v')
+        assert np.array_equal(w._angular_velocity[:n], st['angular_velocity']), (i, 'w')
+        assert np.array_equal(w._awake[:n], st['awake']), (i, 'awake')
