@@ -97,6 +97,7 @@ struct Arena {
     int *slot_cnt;                  // pair_cap (+1 scratch)
     double *slot;                   // pair_cap * SLOT
     int *gjk_list, *gjk_n;
+    int *clip_list, *clip_n;        // touching box-box pairs awaiting face clipping
     int *contact_scan;              // pair_cap + 1
 
     // contacts

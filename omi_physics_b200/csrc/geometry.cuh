@@ -225,9 +225,11 @@ __device__ inline int clip_faces(const double *ca, const double *Ra, const doubl
     return reduce4(allp, alld, nc, out_p, out_d);
 }
 
-__device__ inline int box_box(const double *ca, const double *Ra, const double *ha,
-                              const double *cb, const double *Rb, const double *hb,
-                              double *normal, double *pts, double *deps) {
+// the separating-axis part of box_box: false when separated, else the
+// contact normal (A -> B) and the minimum overlap
+__device__ inline bool box_box_sat(const double *ca, const double *Ra, const double *ha,
+                                   const double *cb, const double *Rb, const double *hb,
+                                   double *normal, double &depth) {
     const double d0 = cb[0] - ca[0], d1 = cb[1] - ca[1], d2 = cb[2] - ca[2];
     double best_depth = 1e300, bx = 0.0, by = 0.0, bz = 0.0;
     normal[0] = normal[1] = normal[2] = 0.0;
@@ -255,7 +257,7 @@ __device__ inline int box_box(const double *ca, const double *Ra, const double *
                      fabs(a0 * Rb[2] + a1 * Rb[5] + a2 * Rb[8]) * hb[2]);
         double proj = a0 * d0 + a1 * d1 + a2 * d2;
         double overlap = ra + rb - fabs(proj);
-        if (overlap < 0.0) return 0;
+        if (overlap < 0.0) return false;
         if (overlap < best_depth) {
             best_depth = overlap;
             if (proj >= 0.0) { bx = a0; by = a1; bz = a2; }
@@ -263,7 +265,16 @@ __device__ inline int box_box(const double *ca, const double *Ra, const double *
         }
     }
     normal[0] = bx; normal[1] = by; normal[2] = bz;
-    return clip_faces(ca, Ra, ha, cb, Rb, hb, normal, best_depth, pts, deps);
+    depth = best_depth;
+    return true;
+}
+
+__device__ inline int box_box(const double *ca, const double *Ra, const double *ha,
+                              const double *cb, const double *Rb, const double *hb,
+                              double *normal, double *pts, double *deps) {
+    double depth;
+    if (!box_box_sat(ca, Ra, ha, cb, Rb, hb, normal, depth)) return 0;
+    return clip_faces(ca, Ra, ha, cb, Rb, hb, normal, depth, pts, deps);
 }
 
 // _collide_native.pyx:285-299

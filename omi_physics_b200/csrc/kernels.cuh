@@ -35,7 +35,7 @@ __device__ __forceinline__ bool dyn(const Arena &A, int i) { return A.mtype[i] =
 // einsum('nij,nkj->nik', R*invI, R) (solver.py:215-220), one thread per body
 // ---------------------------------------------------------------------------
 __global__ void k_refit(Arena A) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.gjk_n[0] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.gjk_n[0] = 0; A.clip_n[0] = 0; }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.NB; i += gridDim.x * blockDim.x) {
         int w = A.body_world[i];
         if (!world_collides(A, w) || i - A.w_body_off[w] >= A.w_body_n[w]) continue;
@@ -144,7 +144,8 @@ __global__ void k_sort(Arena A, int smem_cap) {
             const double *lo = &A.aabb_min[body * 3], *hi = &A.aabb_max[body * 3];
             row[0] = make_double4(lo[0], hi[0], lo[1], hi[1]);
             row[1] = make_double4(lo[2], hi[2], 0.0, 0.0);
-            A.srt_info[off + i] = A.mtype[body] | (A.filter_row[body] << 2);
+            A.srt_info[off + i] = A.mtype[body] | (A.shape[body] >= 0 ? 4 : 0) | (A.awake[body] ? 8 : 0) |
+                                  (A.filter_row[body] << 4);
         }
         __syncthreads();
     }
@@ -225,14 +226,15 @@ __device__ __forceinline__ int window_end_warp(const double *sx, int lo, int hi,
 }
 
 // pair_keep on sorted rows: `ra`/`rb` are the rows' boxes (lo/hi x, y, z),
-// `ia`/`ib` their motion type | filter row << 2
+// `ia`/`ib` their info words: motion type (bits 0-1), has a shape (2), awake
+// (3), filter row (4-)
 __device__ __forceinline__ bool row_keep(const Arena &A, int w, const double4 &a0, const double4 &a1, int ia,
                                          const double4 &b0, const double4 &b1, int ib) {
     bool keep = (a0.w >= b0.z) & (b0.w >= a0.z) & (a1.y >= b1.x) & (b1.y >= a1.x);
     keep &= ((ia & 3) == 2) | ((ib & 3) == 2);
     if (keep) {
         const int rows = A.w_filter_rows[w];
-        keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 2) * rows + (ib >> 2)] != 0;
+        keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 4) * rows + (ib >> 4)] != 0;
     }
     return keep;
 }
@@ -279,23 +281,23 @@ __global__ void k_pair_emit(Arena A) {
         int out = A.pair_scan[e];
         for (int base = e + 1; base < endk; base += 32) {
             const int kj = base + lane;
-            int b = -1;
+            int b = -1, ib = 0;
             bool keep = false;
             if (kj < endk) {
                 const double4 *rb = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)kj * 8]);
-                keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], A.srt_info[kj]);
+                ib = A.srt_info[kj];
+                keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], ib);
                 if (keep) b = A.order[kj];
             }
             const unsigned m = __ballot_sync(FULL, keep);
             if (keep) {
                 const int slot = out + __popc(m & ((1u << lane) - 1u));
-                const int p = a < b ? a : b, q = a < b ? b : a;
-                A.pair_a[slot] = p;
-                A.pair_b[slot] = q;
+                A.pair_a[slot] = a < b ? a : b;
+                A.pair_b[slot] = a < b ? b : a;
                 // solid-pair filter (world.py:663-670): both colliders and an awake mover
-                const bool mp = (A.mtype[p] == 2 && A.awake[p]) || A.mtype[p] == 1;
-                const bool mq = (A.mtype[q] == 2 && A.awake[q]) || A.mtype[q] == 1;
-                A.pair_solid[slot] = (A.shape[p] >= 0 && A.shape[q] >= 0 && (mp || mq)) ? 1 : 0;
+                const bool ma = ((ia & 3) == 2 && (ia & 8)) || (ia & 3) == 1;
+                const bool mb = ((ib & 3) == 2 && (ib & 8)) || (ib & 3) == 1;
+                A.pair_solid[slot] = ((ia & 4) && (ib & 4) && (ma || mb)) ? 1 : 0;
             }
             out += __popc(m);
         }
@@ -452,7 +454,13 @@ __global__ void k_narrow(Arena A) {
                 quat_to_matrix(&A.q[a * 4], Ra);
                 quat_to_matrix(&A.q[b * 4], Rb);
                 if (ka == 2 && kb == 2) {
-                    cnt = box_box(pa, Ra, ha, pb, Rb, hb, nrm, pts, dep);
+                    // separating axes here; the touching pairs (about a third)
+                    // clip their faces in k_clip, away from the separated ones
+                    double depth;
+                    if (box_box_sat(pa, Ra, ha, pb, Rb, hb, nrm, depth)) {
+                        s[0] = nrm[0]; s[1] = nrm[1]; s[2] = nrm[2]; s[3] = depth;
+                        A.clip_list[atomicAdd(A.clip_n, 1)] = p;
+                    }
                 } else if (ka == 1 && kb == 1) {
                     cnt = sphere_sphere(pa, ha[0], pb, hb[0], nrm, pts, dep);
                 } else if (ka == 1 && kb == 2) {
@@ -468,6 +476,33 @@ __global__ void k_narrow(Arena A) {
                         s[5 + j * 4] = pts[j * 3 + 2]; s[6 + j * 4] = dep[j];
                     }
                 }
+            }
+        }
+        A.slot_cnt[p] = cnt;
+    }
+}
+
+// face clipping of the touching box-box pairs k_narrow found
+// (_collide_native.pyx:79-263), one thread per pair, into the pair's slot
+__global__ void k_clip(Arena A) {
+    if (pairs_over(A)) return;
+    const int n = *A.clip_n;
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n; it += gridDim.x * blockDim.x) {
+        const int p = A.clip_list[it];
+        const int a = A.pair_a[p], b = A.pair_b[p];
+        double *s = &A.slot[(size_t)p * SLOT];
+        double nrm[3] = {s[0], s[1], s[2]};
+        const double depth = s[3];
+        double Ra[9], Rb[9], pts[12], dep[4];
+        quat_to_matrix(&A.q[a * 4], Ra);
+        quat_to_matrix(&A.q[b * 4], Rb);
+        const int cnt = clip_faces(&A.pos[a * 3], Ra, &A.half[a * 3], &A.pos[b * 3], Rb, &A.half[b * 3], nrm, depth,
+                                   pts, dep);
+        if (cnt) {
+            s[0] = nrm[0]; s[1] = nrm[1]; s[2] = nrm[2];
+            for (int j = 0; j < cnt; j++) {
+                s[3 + j * 4] = pts[j * 3]; s[4 + j * 4] = pts[j * 3 + 1];
+                s[5 + j * 4] = pts[j * 3 + 2]; s[6 + j * 4] = dep[j];
             }
         }
         A.slot_cnt[p] = cnt;

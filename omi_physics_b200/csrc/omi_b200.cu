@@ -157,6 +157,7 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.pair_solid, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.slot_cnt, (size_t)pair_cap + 1);
     rc |= alloc(ctx, ctx->dyn, A.slot, (size_t)pair_cap * SLOT);
+    rc |= alloc(ctx, ctx->dyn, A.clip_list, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.gjk_list, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.contact_scan, (size_t)pair_cap + 1);
     rc |= alloc(ctx, ctx->dyn, A.c_a, contact_cap);
@@ -277,7 +278,8 @@ void stage_broadphase(OmiCtx *ctx, Prof *pf) {
 void stage_narrow(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
     k_narrow<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
-    ctx->launches++;
+    k_clip<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    ctx->launches += 2;
     mark(ctx, pf, KN_NARROW);
     k_gjk<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
     ctx->launches++;
@@ -390,7 +392,7 @@ int capture(OmiCtx *ctx) {
 
 int64_t step_launches(OmiCtx *ctx) {
     // kernels per captured step (same sequence as enqueue_step)
-    int64_t n = 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
+    int64_t n = 1 + 1 + 1 + 3 + 1 + 2 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
     if (ctx->A.NJ > 0) n += 1;
     return n;
 }
@@ -698,6 +700,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.w_levels, W);
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
+    rc |= alloc(ctx, ctx->statics, A.clip_n, 1);
     rc |= alloc(ctx, ctx->statics, A.sweep_next, 1);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.w_cache_off[t], W);
