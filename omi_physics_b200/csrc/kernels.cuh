@@ -791,11 +791,10 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
 // k_wake     one warp per world: _wake_sleepers (solver.py:321-337)
 // k_prep     one thread per contact, every world at once: material combine,
 //            warm-start seed, arms, tangent basis, effective masses, bias
-// k_levels   one warp per world: Gauss-Seidel levels and their buckets
-// k_iterate  one warp per world: warm start (or the first iteration) fused
-//            with the split-impulse position pass, then the remaining
-//            velocity iterations; __syncwarp between levels, the next
-//            level's contact rows prefetched before each barrier
+// k_levels   one block per world: runs and their predecessor / successor links
+// k_iterate  persistent blocks, 1, 2 or 4 worlds each: every pass of every
+//            run (warm start fused with the split-impulse position pass,
+//            then the velocity iterations) as a dataflow
 constexpr int SOLVE_WARPS = 4;   // warps (worlds) per block of the per-world kernels
 
 __device__ __forceinline__ int warp_global_id() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
@@ -1254,9 +1253,6 @@ __device__ __forceinline__ void st_release_cta(int *p, int v) {
     asm volatile("st.release.cta.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
-__device__ __forceinline__ void prefetch_l1(const void *p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
 
 // polls before a wait gives up: far beyond any legitimate wait (a whole
 // world's sweep); one timeout sets the block's abort flag and ends every
@@ -1276,16 +1272,10 @@ struct SweepQueue {
     int *head, *tail;
 };
 
-__device__ __forceinline__ void sweep_push(const Arena &A, const SweepQueue &Q, int N, int c0, int e,
-                                           const int *kn, volatile int *abort) {
+__device__ __forceinline__ void sweep_push(const SweepQueue &Q, int N, int e, volatile int *abort) {
     const int pos = atomicAdd(Q.tail, 1);
     if (pos >= N) { *abort = 1; return; }          // never with a consistent graph
     st_release_cta(&Q.ring[pos], e + 1);
-    // then warm L1 with the entry's contact rows for whichever lane claims it
-    const int v = kn[e & PASS_MASK];
-    const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
-    const char *row = reinterpret_cast<const char *>(&A.c_data[(size_t)k0 * CD]);
-    for (int off = 0; off < n * (int)(CD * sizeof(double)); off += 128) prefetch_l1(row + off);
 }
 
 // ---------------------------------------------------------------------------
@@ -1295,8 +1285,8 @@ __device__ __forceinline__ void sweep_push(const Arena &A, const SweepQueue &Q, 
 // solves its run, records the finish slot (for the critical-path length),
 // then (after a release fence) counts itself into each successor's arrivals -
 // the arrival that completes a successor fences again (acquire) and
-// publishes it to the ring (release store), then prefetches its contact rows
-// into L1. Everything an entry reads was written
+// publishes it to the ring (release store). (Prefetching the successor's rows
+// into L1 at publication cost more than it saved.) Everything an entry reads was written
 // by entries that happen-before it through those release/acquire chains.
 // Every wait is bounded; a timeout records ST_SWEEP_TIMEOUT and the host
 // reports the step as failed. Shared memory, as far as it goes: the per-run
@@ -1400,7 +1390,7 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
     group_sync(bar, gn);
     // entries with no predecessor: pass-0 runs that start both bodies' chains
     for (int r = gtid; r < R; r += gn)
-        if ((needpk[r] & 3) == 0) sweep_push(A, Q, N, c0, r, kn, abort);
+        if ((needpk[r] & 3) == 0) sweep_push(Q, N, r, abort);
     group_sync(bar, gn);
     const double slop = A.w_solver[w * 2 + 1];
     int my_crit = 0;
@@ -1438,13 +1428,14 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
                 const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
                 double row0[CD];
                 load_row(A, k0, row0);
-                // codes for the finish slot and the successors, read before the solve
+                // codes for the finish slot and the successors, loaded during the solve
                 const int ca = __ldg(run_pa + r), cb = __ldg(run_pb + r);
                 const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                // finish slot (critical-path diagnostics), off the solve's path
                 int t0 = 0;
                 if (ca >= 0) t0 = tend[ca]; else if (ca != LEVEL_NONE && p > 0) t0 = tend[-ca - 1];
                 if (cb >= 0) t0 = max(t0, tend[cb]); else if (cb != LEVEL_NONE && p > 0) t0 = max(t0, tend[-cb - 1]);
-                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
                 tend[r] = t0 + n;
                 my_crit = max(my_crit, t0 + n);
                 // release this entry's writes, then count into the successors
@@ -1459,7 +1450,7 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
                     else continue;
                     if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
                         fence_acq_rel_cta();             // acquire the other arrivals' writes
-                        sweep_push(A, Q, N, c0, (ps << PASS_SHIFT) | rs, kn, abort);
+                        sweep_push(Q, N, (ps << PASS_SHIFT) | rs, abort);
                     }
                 }
             }
