@@ -1175,7 +1175,7 @@ __device__ __forceinline__ void contact_position(double *pa, double *pb, const P
 
 // dynamic shared memory of one sweep block, in doubles: 227 KB less room for
 // the block's static shared variables
-constexpr int SWEEP_SMEM_DOUBLES = 29056 - 16;
+constexpr int SWEEP_SMEM_DOUBLES = 29056 - 80;
 
 struct ImpView {
     double *s;       // shared staging (nullptr: global c_imp)
@@ -1265,17 +1265,31 @@ constexpr int SPIN_LIMIT = 1 << 22;
 // arrivals reach need_first + p * need_rest (run_need packs both).
 __device__ __forceinline__ int need_of(int pk, int p) { return (pk & 3) + p * (pk >> 2); }
 
-// The per-world work ring: one slot per entry (each entry becomes ready
-// exactly once), 0 = not yet published, else entry + 1.
-struct SweepQueue {
-    int *ring;
-    int *head, *tail;
+// Ready entries go to one ring per class - pass 0 or not x run length 1-4 -
+// so a warp claims entries that take the same path through the solve for
+// the same number of contacts. Class c's ring is ring[base[c] ..) with exactly
+// as many slots as the class has entries.
+constexpr int SWEEP_CLASSES = 8;
+// (a block shared by small worlds has few ready entries at a time: there a
+// single ring keeps claims large)
+__device__ __forceinline__ int entry_class(int p, int n, bool classes) {
+    return classes ? (p == 0 ? 4 : 0) + min(n, 4) - 1 : 0;
+}
+
+// per-group shared scalars of the sweep
+struct SweepShared {
+    int head[SWEEP_CLASSES], tail[SWEEP_CLASSES], size[SWEEP_CLASSES], base[SWEEP_CLASSES];
+    int claimed, abort, crit;
+    bool classes;
 };
 
-__device__ __forceinline__ void sweep_push(const SweepQueue &Q, int N, int e, volatile int *abort) {
-    const int pos = atomicAdd(Q.tail, 1);
-    if (pos >= N) { *abort = 1; return; }          // never with a consistent graph
-    st_release_cta(&Q.ring[pos], e + 1);
+// The per-world work rings: one slot per entry (each entry becomes ready
+// exactly once), 0 = not yet published, else entry + 1.
+__device__ __forceinline__ void sweep_push(int *ring, SweepShared &sh, int e, int n, volatile int *abort) {
+    const int c = entry_class(e >> PASS_SHIFT, n, sh.classes);
+    const int pos = atomicAdd(&sh.tail[c], 1);
+    if (pos >= sh.size[c]) { *abort = 1; return; }    // never with a consistent graph
+    st_release_cta(&ring[sh.base[c] + pos], e + 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -1303,10 +1317,6 @@ __device__ __forceinline__ void group_sync(int id, int n) {
     else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
-// per-group shared scalars of the sweep
-struct SweepShared {
-    int head, tail, abort, crit;
-};
 
 // shared-memory doubles one world's sweep would like (tables, velocities,
 // impulses, work ring)
@@ -1369,13 +1379,19 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
     I.c0 = c0;
     I.s = (V.s && used + K * 3 <= smem_doubles) ? smem_d + used : nullptr;
     if (I.s) used = (used + K * 3 + 1) & ~1;
-    SweepQueue Q;
-    Q.ring = used + ((N + 1) >> 1) <= smem_doubles ? reinterpret_cast<int *>(smem_d + used)
-                                                    : A.c_order + (size_t)c0 * A.max_passes;
-    Q.head = &sh.head;
-    Q.tail = &sh.tail;
-    for (int r = gtid; r < R; r += gn) { arrived[r] = 0; tend[r] = 0; }
-    for (int e = gtid; e < N; e += gn) Q.ring[e] = 0;
+    int *ring = used + ((N + 1) >> 1) <= smem_doubles ? reinterpret_cast<int *>(smem_d + used)
+                                                       : A.c_order + (size_t)c0 * A.max_passes;
+    if (gtid < SWEEP_CLASSES) { sh.head[gtid] = 0; sh.tail[gtid] = 0; sh.size[gtid] = 0; }
+    if (gtid == 0) sh.classes = bar == 0;              // the whole block on one world
+    group_sync(bar, gn);
+    for (int r = gtid; r < R; r += gn) {
+        arrived[r] = 0;
+        tend[r] = 0;
+        const int n = A.run_kn[c0 + r] >> 24;
+        atomicAdd(&sh.size[entry_class(0, n, sh.classes)], 1);
+        if (P > 1) atomicAdd(&sh.size[entry_class(1, n, sh.classes)], P - 1);
+    }
+    for (int e = gtid; e < N; e += gn) ring[e] = 0;
     if (V.s) {
         for (int i = gtid; i < nb; i += gn) {
             double lv[3], av[3];
@@ -1386,27 +1402,42 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
     }
     if (I.s)
         for (int i = gtid; i < K * 3; i += gn) I.s[i] = A.c_imp[c0 * 3 + i];
-    if (gtid == 0) { sh.head = 0; sh.tail = 0; sh.abort = 0; sh.crit = 0; }
+    group_sync(bar, gn);
+    if (gtid == 0) {
+        int acc = 0;
+        for (int c = 0; c < SWEEP_CLASSES; c++) { sh.base[c] = acc; acc += sh.size[c]; }
+        sh.claimed = 0; sh.abort = 0; sh.crit = 0;
+    }
     group_sync(bar, gn);
     // entries with no predecessor: pass-0 runs that start both bodies' chains
     for (int r = gtid; r < R; r += gn)
-        if ((needpk[r] & 3) == 0) sweep_push(Q, N, r, abort);
+        if ((needpk[r] & 3) == 0) sweep_push(ring, sh, r, kn[r] >> 24, abort);
     group_sync(bar, gn);
     const double slop = A.w_solver[w * 2 + 1];
     int my_crit = 0;
     for (;;) {
-        // lane 0 claims up to 32 published-or-pending ring positions
+        // lane 0 claims up to 32 published-or-pending positions of one class
         int lo = 0, cnt = 0;
         if (lane == 0) {
+            const int first = (gtid >> 5) & (SWEEP_CLASSES - 1);
             for (int it = 0;; it++) {
-                const int h = *(volatile int *)Q.head;
-                if (h >= N || *abort) { cnt = -1; break; }
-                const int t = min(*(volatile int *)Q.tail, N);
-                if (t > h) {
-                    const int want = min(t - h, 32);
-                    if (atomicCAS(Q.head, h, h + want) == h) { lo = h; cnt = want; break; }
-                    continue;
+                if (*(volatile int *)&sh.claimed >= N || *abort) { cnt = -1; break; }
+                bool got = false;
+                for (int j = 0; j < SWEEP_CLASSES && !got; j++) {
+                    const int c = (first + j) & (SWEEP_CLASSES - 1);
+                    const int h = *(volatile int *)&sh.head[c];
+                    const int t = min(*(volatile int *)&sh.tail[c], sh.size[c]);
+                    if (t > h) {
+                        const int want = min(t - h, 32);
+                        if (atomicCAS(&sh.head[c], h, h + want) == h) {
+                            atomicAdd(&sh.claimed, want);
+                            lo = sh.base[c] + h;
+                            cnt = want;
+                            got = true;
+                        }
+                    }
                 }
+                if (got) break;
                 if (it >= SPIN_LIMIT) { *abort = 1; cnt = -1; break; }
                 __nanosleep(32);
             }
@@ -1417,7 +1448,7 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
         if (lane < cnt) {
             int e1 = 0;
             for (int it = 0; it < SPIN_LIMIT; it++) {     // the pusher is between its two steps
-                e1 = ld_acquire_cta(&Q.ring[lo + lane]);
+                e1 = ld_acquire_cta(&ring[lo + lane]);
                 if (e1 || *abort) break;
             }
             if (e1 == 0) *abort = 1;
@@ -1450,7 +1481,7 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
                     else continue;
                     if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
                         fence_acq_rel_cta();             // acquire the other arrivals' writes
-                        sweep_push(Q, N, (ps << PASS_SHIFT) | rs, abort);
+                        sweep_push(ring, sh, (ps << PASS_SHIFT) | rs, kn[rs] >> 24, abort);
                     }
                 }
             }
@@ -1461,7 +1492,7 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
     group_sync(bar, gn);
     if (gtid == 0) {
         A.w_levels[w] = sh.crit;
-        if (sh.abort || sh.head < N) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+        if (sh.abort || sh.claimed < N) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
     }
     if (V.s) {
         for (int i = gtid; i < nb; i += gn) {
