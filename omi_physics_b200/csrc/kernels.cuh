@@ -1509,50 +1509,63 @@ __device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doub
 }
 
 // Persistent sweep blocks take worlds in schedule order (largest first) from
-// a counter k_levels reset. The first world taken decides the split: G = 1,
-// 2 or 4 groups, the largest G whose share of the block's shared memory
-// still holds everything that world wants; the block then takes G - 1 more
-// worlds (all later worlds are no larger) and each group sweeps one.
+// a counter k_levels reset. While the worlds taken need the whole block's
+// shared memory, the block sweeps them one at a time. The first world whose
+// needs fit a half (or a quarter) splits the block into 2 (or 4) groups for
+// good: every later world is no larger, so from then on each group takes its
+// own next world as soon as it is done, with no block-wide barrier between
+// worlds.
 constexpr int SWEEP_MAX_GROUPS = 4;
+
+// next colliding world of the schedule, or -1
+__device__ __forceinline__ int sweep_take(const Arena &A) {
+    for (;;) {
+        const int wi = atomicAdd(A.sweep_next, 1);
+        if (wi >= A.W) return -1;
+        const int w = A.w_sched[wi];
+        if (world_collides(A, w)) return w;
+    }
+}
 
 __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
     extern __shared__ __align__(16) double smem_d[];
     __shared__ SweepShared sh[SWEEP_MAX_GROUPS];
-    __shared__ int pick[1 + SWEEP_MAX_GROUPS];    // groups (0: done), world per group
+    __shared__ int pick[1 + SWEEP_MAX_GROUPS];    // split (0: done), world per group
     if (overflowed(A)) return;
     const int tid = threadIdx.x;
+    int G;
     for (;;) {
         if (tid == 0) {
-            int G = 0;
-            for (int g = 0; g < SWEEP_MAX_GROUPS; g++) pick[1 + g] = -1;
-            for (;;) {
-                const int wi = atomicAdd(A.sweep_next, 1);
-                if (wi >= A.W) break;
-                const int w = A.w_sched[wi];
-                if (!world_collides(A, w)) continue;
+            const int w = sweep_take(A);
+            int g = 0;
+            if (w >= 0) {
                 const int want = sweep_want(A, w);
-                G = want <= ((smem_doubles / 4) & ~1) ? 4 : (want <= ((smem_doubles / 2) & ~1) ? 2 : 1);
-                pick[1] = w;
-                for (int g = 1; g < G; g++) {
-                    for (;;) {
-                        const int wj = atomicAdd(A.sweep_next, 1);
-                        if (wj >= A.W) break;
-                        const int x = A.w_sched[wj];
-                        if (world_collides(A, x)) { pick[1 + g] = x; break; }
-                    }
-                }
-                break;
+                g = want <= ((smem_doubles / 4) & ~1) ? 4 : (want <= ((smem_doubles / 2) & ~1) ? 2 : 1);
             }
-            pick[0] = G;
+            pick[0] = g;
+            pick[1] = w;
         }
         __syncthreads();
-        const int G = pick[0];
-        if (G == 0) break;
-        const int gn = SWEEP_THREADS / G, g = tid / gn;
-        const int share = (smem_doubles / G) & ~1;
-        const int w = pick[1 + g];
-        if (w >= 0) sweep_world(A, w, smem_d + g * share, share, tid - g * gn, gn, G == 1 ? 0 : 1 + g, sh[g]);
+        G = pick[0];
+        if (G == 0) return;
+        if (G > 1) break;
+        sweep_world(A, pick[1], smem_d, smem_doubles, tid, SWEEP_THREADS, 0, sh[0]);
         __syncthreads();
+    }
+    // split for good: group g sweeps its own worlds on named barrier 1 + g
+    const int gn = SWEEP_THREADS / G, g = tid / gn, gtid = tid - g * gn;
+    const int share = (smem_doubles / G) & ~1;
+    int w = g == 0 ? pick[1] : -1;
+    for (;;) {
+        if (w < 0) {
+            group_sync(1 + g, gn);                 // everyone has read the previous pick
+            if (gtid == 0) pick[1 + g] = sweep_take(A);
+            group_sync(1 + g, gn);
+            w = pick[1 + g];
+            if (w < 0) return;
+        }
+        sweep_world(A, w, smem_d + g * share, share, gtid, gn, 1 + g, sh[g]);
+        w = -1;
     }
 }
 
