@@ -394,13 +394,20 @@ __device__ inline void uf_union(int *parent, int a, int b) {
     }
 }
 
-__global__ void k_finalize(Arena A, int mode) {
+// Per body of the world: flags and union-find parents, in shared memory when
+// the world has at most `cap` bodies (indices local to the world), else in
+// the global arrays. Roots are each island's smallest index (uf_union links
+// the larger root under the smaller), so labels do not depend on which of
+// the two is used.
+__global__ void k_finalize(Arena A, int mode, int cap) {
+    extern __shared__ int fsm[];
     if ((mode & FIN_GATED) && overflowed(A)) return;
     if ((mode & FIN_COUNT) && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.status[ST_STEPS_DONE], 1);
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
+    for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
+        const int w = A.w_sched[wi];
         if (!A.w_active[w]) continue;
         const double dt = A.w_dt[w];
-        const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
+        const int b0 = A.w_body_off[w], nb = A.w_body_n[w], b1 = b0 + nb;
         if (mode & FIN_POSITIONS) {
             for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
                 const int t = A.mtype[i];
@@ -427,6 +434,9 @@ __global__ void k_finalize(Arena A, int mode) {
             for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_island[i] = -1;
             continue;
         }
+        const bool local = nb <= cap;
+        int *flag = local ? fsm : A.b_flag + b0;          // indexed by i - b0
+        int *parent = local ? fsm + cap : A.b_parent + b0;
         __syncthreads();
         const double lin2 = 0.08 * 0.08, ang2 = 0.25 * 0.25;
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
@@ -434,8 +444,8 @@ __global__ void k_finalize(Arena A, int mode) {
             const bool slow = dyn_i && speed2(&A.v[i * 3]) < lin2 && speed2(&A.w[i * 3]) < ang2;
             if (slow) A.timer[i] += dt; else A.timer[i] = 0.0;
             const bool ready = slow && A.timer[i] > 0.4;
-            A.b_flag[i] = (slow ? BF_SLOW : 0) | (ready ? BF_READY : 0);
-            A.b_parent[i] = i;
+            flag[i - b0] = (slow ? BF_SLOW : 0) | (ready ? BF_READY : 0);
+            parent[i - b0] = i - b0;
         }
         __syncthreads();
         if (world_collides(A, w)) {
@@ -444,24 +454,24 @@ __global__ void k_finalize(Arena A, int mode) {
             for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
                 const int a = A.c_a[k], b = A.c_b[k];
                 const bool da = A.mtype[a] == 2, db = A.mtype[b] == 2;
-                if (da) atomicOr(&A.b_flag[a], BF_CONTACTED);
-                if (db) atomicOr(&A.b_flag[b], BF_CONTACTED);
-                if (da && db) uf_union(A.b_parent, a, b);
+                if (da) atomicOr(&flag[a - b0], BF_CONTACTED);
+                if (db) atomicOr(&flag[b - b0], BF_CONTACTED);
+                if (da && db) uf_union(parent, a - b0, b - b0);
             }
         }
         __syncthreads();
-        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_island[i] = uf_find(A.b_parent, i);
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) A.b_island[b0 + i] = b0 + uf_find(parent, i);
         __syncthreads();
-        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-            const int f = ((volatile int *)A.b_flag)[i];
-            if ((f & BF_CONTACTED) && !(f & BF_READY)) atomicOr(&A.b_flag[A.b_island[i]], BF_NOTREADY);
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+            const int f = ((volatile int *)flag)[i];
+            if ((f & BF_CONTACTED) && !(f & BF_READY)) atomicOr(&flag[A.b_island[b0 + i] - b0], BF_NOTREADY);
         }
         __syncthreads();
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-            const int f = ((volatile int *)A.b_flag)[i];
+            const int f = ((volatile int *)flag)[i - b0];
             const bool dyn_i = A.mtype[i] == 2;
             bool to_sleep;
-            if (f & BF_CONTACTED) to_sleep = !(((volatile int *)A.b_flag)[A.b_island[i]] & BF_NOTREADY);
+            if (f & BF_CONTACTED) to_sleep = !(((volatile int *)flag)[A.b_island[i] - b0] & BF_NOTREADY);
             else to_sleep = dyn_i && (f & BF_READY);
             if (!(f & BF_CONTACTED)) A.b_island[i] = -1;
             if (to_sleep) A.awake[i] = 0;

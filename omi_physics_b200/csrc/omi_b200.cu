@@ -57,6 +57,7 @@ struct OmiCtx {
     int solve_block = 128;
     int level_ints = 0;            // shared ints of one k_levels block
     int sm_count = 148;            // multiprocessors of the device (persistent sweep grid)
+    int fin_cap = 1;               // bodies whose sleep flags / islands k_finalize keeps in shared memory
     int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
     cudaGraphExec_t graph = nullptr;
@@ -341,7 +342,7 @@ void enqueue_step(OmiCtx *ctx, Prof *pf) {
     stage_compact(ctx, pf);
     stage_solve(ctx, pf);
     stage_joints(ctx, pf, 1);
-    k_finalize<<<std::min(A.W, 65535), 256, 0, ctx->stream>>>(A, FIN_POSITIONS | FIN_SLEEP | FIN_COUNT | FIN_GATED);
+    k_finalize<<<std::min(A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(A, FIN_POSITIONS | FIN_SLEEP | FIN_COUNT | FIN_GATED, ctx->fin_cap);
     ctx->launches++;
     mark(ctx, pf, KN_FINALIZE);
 }
@@ -467,6 +468,7 @@ int omi_create(int device, OmiCtx **out) {
         {(const void *)k_sort<true>, 8192 * 24, "k_sort"},
         {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
+        {(const void *)k_finalize, 2 * 8192 * (int)sizeof(int), "k_finalize"},
     };
     for (const auto &f : smem) {
         e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
@@ -716,6 +718,8 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
     ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
     ctx->solve_block = max_n > 1024 ? 256 : 128;
+    // sleep flags and union-find parents of the largest world (two ints per body, <= 64 KB)
+    ctx->fin_cap = std::min(std::max(max_n, 1), 8192);
     // body buckets of the largest world: 2 ints per body + 2 per run (~1.5 runs per body)
     ctx->level_ints = (int)std::min<int64_t>(LEVEL_SMEM_INTS, 8 * (int64_t)std::max(max_nc, 1) + 1024);
     A.max_passes = 1;
@@ -1150,7 +1154,7 @@ int omi_solve_joints(OmiCtx *ctx) {
 
 int omi_integrate_positions(OmiCtx *ctx) {
     STAGE_PRELUDE
-    k_finalize<<<std::min(ctx->A.W, 65535), 256, 0, ctx->stream>>>(ctx->A, FIN_POSITIONS);
+    k_finalize<<<std::min(ctx->A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(ctx->A, FIN_POSITIONS, ctx->fin_cap);
     ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1159,7 +1163,7 @@ int omi_integrate_positions(OmiCtx *ctx) {
 
 int omi_update_sleep(OmiCtx *ctx) {
     STAGE_PRELUDE
-    k_finalize<<<std::min(ctx->A.W, 65535), 256, 0, ctx->stream>>>(ctx->A, FIN_SLEEP);
+    k_finalize<<<std::min(ctx->A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(ctx->A, FIN_SLEEP, ctx->fin_cap);
     ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
