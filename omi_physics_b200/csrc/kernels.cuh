@@ -1318,14 +1318,13 @@ __device__ __forceinline__ void group_sync(int id, int n) {
 }
 
 
-// shared-memory doubles one world's sweep would like (tables, velocities,
-// impulses, work ring)
+// shared-memory doubles one world's sweep wants: per-run tables, velocities
+// and impulses (the work ring - one store and one load per entry - may
+// live in global memory)
 __device__ __forceinline__ int sweep_want(const Arena &A, int w) {
-    const int R = A.w_runs[w];
     int c0, c1;
     world_contacts(A, w, c0, c1);
-    const int N = world_passes(A, w) * R;
-    return 2 * R + 6 * A.w_body_n[w] + 3 * (c1 - c0) + (N + 1) / 2 + 8;
+    return 2 * A.w_runs[w] + 6 * A.w_body_n[w] + 3 * (c1 - c0) + 8;
 }
 
 // One world's sweep by the `gn` threads of a group (gtid = thread index in it,
