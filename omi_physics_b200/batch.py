@@ -185,6 +185,37 @@ class WorldBatch:
             off = self.offsets[i]
             return dict(a=a[:n] - off, b=b[:n] - off, point=pt[:n], impulse=imp[:n])
 
+    # -- snapshot / restore ------------------------------------------------------
+    def snapshot(self, i: int) -> dict:
+        """World ``i``'s resident state and warm-start cache, as host arrays.
+
+        Restoring it (here or into another batch holding the same world) and
+        stepping gives exactly what stepping on from here would: pose,
+        velocities, sleep state and the solver's warm-start impulses
+        (solver.py:91, 272-278) are all the step carries over.
+        """
+        w = self.worlds[i]
+        n = w.body_count
+        self.download_state(i)
+        snap = {name: np.array(getattr(w, '_' + name)[:n], copy=True)
+                for name in ('position', 'orientation', 'linear_velocity', 'angular_velocity',
+                             'awake', 'sleep_timer')}
+        snap['cache'] = self.cache(i)
+        snap['time'] = w.time
+        return snap
+
+    def restore(self, i: int, snap: dict) -> None:
+        """Put a :meth:`snapshot` back into world ``i`` (host columns and device)."""
+        w = self.worlds[i]
+        n = w.body_count
+        for name in ('position', 'orientation', 'linear_velocity', 'angular_velocity', 'awake',
+                     'sleep_timer'):
+            getattr(w, '_' + name)[:n] = snap[name]
+        w.time = snap['time']
+        self.upload_state(i)
+        c = snap['cache']
+        self.set_cache(i, c['a'], c['b'], c['point'], c['impulse'])
+
     def profile(self) -> dict:
         """Per-stage device milliseconds of one eagerly launched step."""
         return self.ctx.profile_step()

@@ -227,6 +227,55 @@ class Server:
                       ptr(w._sleep_timer, D), ptr(w._aabb_min, D), ptr(w._aabb_max, D))
         w.time += req.steps * req.dt
 
+    # -- snapshot / restore of resident worlds -----------------------------------
+    def _rows(self, slot: int):
+        first, n = C.c_int32(), C.c_int32()
+        self.ctx.call('world_rows', slot, C.byref(first), C.byref(n))
+        return first.value, n.value
+
+    def snapshot(self, req: Request) -> dict:
+        """A resident request's state, warm-start cache and progress (host arrays)."""
+        if req.slot < 0 or self.resident.get(req.slot) is not req:
+            raise ValueError('request %d is not resident' % req.rid)
+        first, n = self._rows(req.slot)
+        cols = {k: np.zeros((n, d)) for k, d in (('pos', 3), ('q', 4), ('v', 3), ('w', 3))}
+        awake = np.zeros(n, np.uint8)
+        timer = np.zeros(n)
+        self.ctx.call('download_state', first, n, ptr(cols['pos'], D), ptr(cols['q'], D),
+                      ptr(cols['v'], D), ptr(cols['w'], D), ptr(awake, U8), ptr(timer, D), None, None)
+        cap = 1 << 12
+        while True:
+            a = np.zeros(cap, np.int32); b = np.zeros(cap, np.int32)
+            pt = np.zeros((cap, 3)); imp = np.zeros((cap, 3))
+            rc = self.ctx.lib.omi_get_cache(self.ctx.h, req.slot, ptr(a, I), ptr(b, I), ptr(pt, D),
+                                            ptr(imp, D), cap)
+            if rc == -2 and cap < (1 << 26):
+                cap *= 8
+                continue
+            k = self.ctx.check(rc, 'omi_get_cache')
+            break
+        return dict(cols, awake=awake, timer=timer, done=req.done,
+                    cache=dict(a=a[:k] - first, b=b[:k] - first, point=pt[:k], impulse=imp[:k]))
+
+    def restore(self, req: Request, snap: dict) -> None:
+        """Put a :meth:`snapshot` back into the request's slot; stepping on gives
+        exactly what stepping on from the snapshot would have."""
+        if req.slot < 0 or self.resident.get(req.slot) is not req:
+            raise ValueError('request %d is not resident' % req.rid)
+        first, n = self._rows(req.slot)
+        pos, q, v, w = (np.ascontiguousarray(snap[k], 'd') for k in ('pos', 'q', 'v', 'w'))
+        awake = np.ascontiguousarray(snap['awake'], np.uint8)
+        timer = np.ascontiguousarray(snap['timer'], 'd')
+        self.ctx.call('upload_state', first, n, ptr(pos, D), ptr(q, D), ptr(v, D), ptr(w, D),
+                      ptr(awake, U8), ptr(timer, D))
+        c = snap['cache']
+        a = np.ascontiguousarray(np.asarray(c['a'], np.int32) + first)
+        b = np.ascontiguousarray(np.asarray(c['b'], np.int32) + first)
+        pt = np.ascontiguousarray(c['point'], 'd').reshape(-1, 3)
+        imp = np.ascontiguousarray(c['impulse'], 'd').reshape(-1, 3)
+        self.ctx.call('set_cache', req.slot, len(a), ptr(a, I), ptr(b, I), ptr(pt, D), ptr(imp, D))
+        req.done = int(snap['done'])
+
     # -- ticks ------------------------------------------------------------------
     def tick(self, now: float) -> None:
         """Admit, step every resident world once, retire finished ones."""
