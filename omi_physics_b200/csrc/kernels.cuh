@@ -675,13 +675,11 @@ __device__ __forceinline__ void rel_vel(const double *lv, const double *av, int 
         (lv[a * 3 + 2] + av[a * 3] * rA[1] - av[a * 3 + 1] * rA[0]);
 }
 
-// _effmass (_solver_native.pyx:154-176)
-__device__ __forceinline__ double effmass(const Arena &A, const double *ra, const double *rb,
-                                          double dx, double dy, double dz, int a, int b,
-                                          double ima, double imb) {
+// _effmass (_solver_native.pyx:154-176); Ia / Ib: the bodies' world inverse inertias
+__device__ __forceinline__ double effmass(const double *Ia, const double *Ib, const double *ra, const double *rb,
+                                          double dx, double dy, double dz, double ima, double imb) {
     const double ax = ra[1] * dz - ra[2] * dy, ay = ra[2] * dx - ra[0] * dz, az = ra[0] * dy - ra[1] * dx;
     const double bx = rb[1] * dz - rb[2] * dy, by = rb[2] * dx - rb[0] * dz, bz = rb[0] * dy - rb[1] * dx;
-    const double *Ia = &A.invIw[a * 9], *Ib = &A.invIw[b * 9];
     double kk = ima + imb;
     double wx = Ia[0] * ax + Ia[1] * ay + Ia[2] * az;
     double wy = Ia[3] * ax + Ia[4] * ay + Ia[5] * az;
@@ -704,7 +702,7 @@ __device__ __forceinline__ double speed2(const double *v) {
 }
 
 // contact prep: material combine, warm-start seed, arms, basis, masses, bias
-__device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int cur) {
+__device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int cur, double *D) {
     const int a = A.c_a[k], b = A.c_b[k];
     double fa, ra_, fb, rb_;
     int fca, rca, fcb, rcb;
@@ -751,8 +749,9 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
         }
     }
     A.c_imp[k * 3] = n0; A.c_imp[k * 3 + 1] = t0; A.c_imp[k * 3 + 2] = t1v;
-    double *D = &A.c_data[(size_t)k * CD];
     const double ima = A.inv_mass[a], imb = A.inv_mass[b];
+    double Ia[9], Ib[9];
+    for (int q = 0; q < 9; q++) { Ia[q] = A.invIw[a * 9 + q]; Ib[q] = A.invIw[b * 9 + q]; }
     double rA[3], rB[3];
     for (int c = 0; c < 3; c++) { rA[c] = pt[c] - A.pos[a * 3 + c]; rB[c] = pt[c] - A.pos[b * 3 + c]; }
     const double nx = A.c_n[k * 3], ny = A.c_n[k * 3 + 1], nz = A.c_n[k * 3 + 2];
@@ -768,9 +767,9 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
     D[R_N] = nx; D[R_N + 1] = ny; D[R_N + 2] = nz;
     D[R_T1] = t1x; D[R_T1 + 1] = t1y; D[R_T1 + 2] = t1z;
     D[R_T2] = t2x; D[R_T2 + 1] = t2y; D[R_T2 + 2] = t2z;
-    D[C_NM] = effmass(A, rA, rB, nx, ny, nz, a, b, ima, imb);
-    D[C_T1M] = effmass(A, rA, rB, t1x, t1y, t1z, a, b, ima, imb);
-    D[C_T2M] = effmass(A, rA, rB, t2x, t2y, t2z, a, b, ima, imb);
+    D[C_NM] = effmass(Ia, Ib, rA, rB, nx, ny, nz, ima, imb);
+    D[C_T1M] = effmass(Ia, Ib, rA, rB, t1x, t1y, t1z, ima, imb);
+    D[C_T2M] = effmass(Ia, Ib, rA, rB, t2x, t2y, t2z, ima, imb);
     double dvx, dvy, dvz;
     rel_vel(A.v, A.w, a, b, rA, rB, dvx, dvy, dvz);
     const double vn0 = dvx * nx + dvy * ny + dvz * nz;
@@ -784,7 +783,7 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
     *ab = make_int2(a, b);
     int2 *fl = reinterpret_cast<int2 *>(&D[R_FLAGS]);
     *fl = make_int2((A.mtype[a] == 2 ? 1 : 0) | (A.mtype[b] == 2 ? 2 : 0), 0);
-    for (int q = 0; q < 9; q++) { D[R_IA + q] = A.invIw[a * 9 + q]; D[R_IB + q] = A.invIw[b * 9 + q]; }
+    for (int q = 0; q < 9; q++) { D[R_IA + q] = Ia[q]; D[R_IB + q] = Ib[q]; }
 }
 
 // ---- the solver as four launches -------------------------------------------
@@ -849,14 +848,34 @@ __global__ void k_wake(Arena A) {
     }
 }
 
-__global__ void k_prep(Arena A) {
+// one thread per contact; the block's rows (consecutive contacts) are built
+// in shared memory and written out with coalesced stores
+constexpr int PREP_THREADS = 128;
+
+__global__ void __launch_bounds__(PREP_THREADS) k_prep(Arena A) {
+    extern __shared__ __align__(16) double rows[];        // PREP_THREADS * CD
+    __shared__ unsigned char valid[PREP_THREADS];
     if (overflowed(A)) return;
     const int cur = *A.parity;
     const int Ktot = A.contact_scan[A.pair_scan[A.NB]];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ktot; k += gridDim.x * blockDim.x) {
-        const int w = A.body_world[A.c_a[k]];
-        if (!world_collides(A, w)) continue;
-        prep_contact(A, w, k, (A.w_flags[w] & WF_WARM) != 0, cur);
+    for (int base = blockIdx.x * PREP_THREADS; base < Ktot; base += gridDim.x * PREP_THREADS) {
+        const int k = base + threadIdx.x;
+        bool ok = false;
+        if (k < Ktot) {
+            const int w = A.body_world[A.c_a[k]];
+            if (world_collides(A, w)) {
+                prep_contact(A, w, k, (A.w_flags[w] & WF_WARM) != 0, cur, rows + threadIdx.x * CD);
+                ok = true;
+            }
+        }
+        valid[threadIdx.x] = ok;
+        __syncthreads();
+        const int n = min(PREP_THREADS, Ktot - base);
+        double2 *dst = reinterpret_cast<double2 *>(&A.c_data[(size_t)base * CD]);
+        const double2 *src = reinterpret_cast<const double2 *>(rows);
+        for (int i = threadIdx.x; i < n * (CD / 2); i += PREP_THREADS)
+            if (valid[i / (CD / 2)]) dst[i] = src[i];
+        __syncthreads();
     }
 }
 

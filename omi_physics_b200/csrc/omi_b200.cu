@@ -304,7 +304,7 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     const int wg = std::max(1, (A.W + SOLVE_WARPS - 1) / SOLVE_WARPS);
     k_wake<<<wg, wb, 0, ctx->stream>>>(A);
     mark(ctx, pf, KN_WAKE);
-    k_prep<<<grid_for(A.contact_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    k_prep<<<grid_for(A.contact_cap, PREP_THREADS, SM_CAP), PREP_THREADS, (size_t)PREP_THREADS * CD * sizeof(double), ctx->stream>>>(A);
     mark(ctx, pf, KN_PREP);
     k_levels<<<std::min(A.W, 65535), LEVEL_THREADS, (size_t)ctx->level_ints * sizeof(int), ctx->stream>>>(A, ctx->level_ints);
     mark(ctx, pf, KN_LEVELS);
@@ -469,6 +469,7 @@ int omi_create(int device, OmiCtx **out) {
         {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
         {(const void *)k_finalize, 2 * 8192 * (int)sizeof(int), "k_finalize"},
+        {(const void *)k_prep, PREP_THREADS * CD * (int)sizeof(double), "k_prep"},
     };
     for (const auto &f : smem) {
         e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
