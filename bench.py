@@ -55,6 +55,8 @@ def parse():
     ap.add_argument('--serve-requests', type=int, default=None,
                     help='requests in the serving run (default: --worlds; 0 skips it)')
     ap.add_argument('--serve-slots', type=int, default=96, help='slots per size class')
+    ap.add_argument('--groups', type=int, default=4,
+                    help='worlds are stepped as this many concurrent groups (one context + stream each)')
     return ap.parse_args()
 
 
@@ -169,72 +171,80 @@ STAGE_GROUPS = {
 
 def run_ours(args, rank, world, local):
     import torch
-    from omi_physics_b200 import WorldBatch
-    from omi_physics_b200._lib import D, U8, ptr
+    from omi_physics_b200.groups import WorldGroups
+    from omi_physics_b200._lib import D, U8, OmiError, ptr
     torch.cuda.set_device(local)
     t0 = time.time()
     reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
-    batch = WorldBatch(worlds, device=local)
-    batch.step(args.preroll)
+    grp = WorldGroups(worlds, groups=args.groups, device=local)
+    grp.step(args.preroll)
     setup_s = time.time() - t0
     N = dynamic_bodies(worlds)
-    NB = batch.packed.n_bodies
-    # a dedicated stream shared with the library: the CUDA events below are
-    # recorded on the very stream the step kernels are launched on
-    stream = torch.cuda.Stream(device=local)
-    torch.cuda.set_stream(stream)
-    assert stream.cuda_stream != 0
-    batch.ctx.call('set_stream', stream.cuda_stream)
+    NB = sum(b.packed.n_bodies for b in grp.batches)
+    # one torch stream per group, shared with the library, and a main stream
+    # whose events bracket every group's work
+    streams = [torch.cuda.Stream(device=local) for _ in range(len(grp))]
+    grp.set_streams([s.cuda_stream for s in streams])
+    main = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(main)
+
+    def timed_steps(n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for s in streams:
+            s.wait_event(e0)
+        grp.step_async(n)
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            main.wait_event(ev)
+        e1.record(main)
+        return e0, e1
 
     # ---- device-resident batched steps (the headline) ----
-    batch.step(args.warmup)
+    grp.step(args.warmup)
     torch.cuda.synchronize()
     barrier(world)
-    from omi_physics_b200._lib import OmiError
     for attempt in range(4):
-        launches0 = batch.ctx.launches()
+        launches0 = grp.launches()
         with ClockSampler(local) as clk:
             torch.cuda.synchronize()
             barrier(world)
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
-            batch.step_async(args.steps)
-            ev1.record(stream)
+            ev0, ev1 = timed_steps(args.steps)
             torch.cuda.synchronize()
             barrier(world)
         try:
-            batch.sync()          # raises if a step overflowed its buffers (then it did nothing)
+            grp.sync()            # raises if a step overflowed its buffers (then it did nothing)
             ok = 1.0
         except OmiError:
             ok = 0.0
         if max_over_ranks(1.0 - ok, world) == 0.0:
             break
-        batch.step(1)             # synchronous step regrows the buffers; time again
+        grp.step(1)               # synchronous steps regrow the buffers; time again
     ms = ev0.elapsed_time(ev1)
-    launches = batch.ctx.launches() - launches0
+    launches = grp.launches() - launches0
     ms_max = max_over_ranks(ms, world)
     total_N = sum_over_ranks(N, world)
     value = total_N * args.steps / (ms_max / 1e3)
-    pairs, contacts = batch.counts()
+    pairs, contacts = grp.counts()
     P, K = int(pairs.sum()), int(contacts.sum())
 
-    # per-step tick latency distribution (graph replay, synchronised per tick)
+    # per-step tick latency distribution (every world one step, synchronised per tick)
     ticks = []
     for _ in range(max(10, min(args.steps, 50))):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        batch.step_async(1)
-        b.record(stream)
+        a, b = timed_steps(1)
         b.synchronize()
         ticks.append(a.elapsed_time(b))
-    batch.sync()
+    grp.sync()
 
-    # ---- roofline: per-stage device time of eagerly launched steps ----
+    # ---- roofline: per-stage device time of eagerly launched steps (groups one
+    # after another, so the sums are the stage times of the whole mix) ----
     prof = {}
     n_prof = 5
     for _ in range(n_prof):
-        for k, v in batch.profile().items():
-            prof[k] = prof.get(k, 0.0) + v / n_prof
+        for bt in grp.batches:
+            for k, v in bt.profile().items():
+                prof[k] = prof.get(k, 0.0) + v / n_prof
     groups = {g: sum(prof.get(k, 0.0) for k in ks) for g, ks in STAGE_GROUPS.items()}
     dominant = max(groups, key=groups.get)
     dom_ms = groups[dominant]
@@ -257,32 +267,28 @@ def run_ours(args, rank, world, local):
                 'stage_ms': {k: round(v, 4) for k, v in groups.items()},
                 'kernel_group_ms': {k: round(v, 4) for k, v in prof.items()}}
 
-    # ---- e2e: whole-arena state through pinned host buffers every step ----
-    pin = {name: torch.empty(shape, dtype=dt, pin_memory=True).numpy() for name, shape, dt in (
-        ('pos', (NB, 3), torch.float64), ('q', (NB, 4), torch.float64),
-        ('v', (NB, 3), torch.float64), ('w', (NB, 3), torch.float64),
-        ('awake', (NB,), torch.uint8), ('timer', (NB,), torch.float64))}
-    c = batch.ctx
-    c.call('download_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
-           ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D), None, None)
-    h2d = sum(a.nbytes for a in pin.values())
+    # ---- e2e: every group's state through pinned host buffers every step ----
+    def pinned(shape, dtype=np.float64):
+        return torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.uint8,
+                           pin_memory=True).numpy()
+    bufs = grp.host_buffers(alloc=pinned)
+    for bt, h in zip(grp.batches, bufs):
+        nb = bt.packed.n_bodies
+        bt.ctx.call('download_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D),
+                    ptr(h['w'], D), ptr(h['awake'], U8), ptr(h['timer'], D), None, None)
+    h2d = sum(a.nbytes for h in bufs for a in h.values())
     e2e_steps = max(3, min(args.steps, 20))
-
-    def e2e_step():
-        c.call('upload_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
-               ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D))
-        c.call('step', 1)
-        c.call('download_state', 0, NB, ptr(pin['pos'], D), ptr(pin['q'], D), ptr(pin['v'], D),
-               ptr(pin['w'], D), ptr(pin['awake'], U8), ptr(pin['timer'], D), None, None)
-
-    e2e_step()
+    grp.step_from_host(bufs, 1)
     barrier(world)
     t = time.perf_counter()
     for _ in range(e2e_steps):
-        e2e_step()
+        grp.step_from_host(bufs, 1)
     e2e_s = max_over_ranks(time.perf_counter() - t, world)
     e2e = {'value': total_N * e2e_steps / e2e_s, 'unit': 'body-steps/s', 'h2d_bytes_per_step': h2d,
-           'd2h_bytes_per_step': h2d, 'path': 'omi_upload_state + omi_step + omi_download_state, pinned'}
+           'd2h_bytes_per_step': h2d,
+           'path': 'per group: omi_upload_state + omi_step + omi_download_state from pinned memory, '
+                   'the groups concurrently'}
+    stream = main
 
     extras = {}
     n_serve = args.worlds if args.serve_requests is None else args.serve_requests
@@ -291,6 +297,7 @@ def run_ours(args, rank, world, local):
         barrier(world)
     if not args.no_extras and rank == 0:
         extras['plain'] = plain_per_world(worlds, reqs, args.plain_sample, local, args.preroll)
+    grp.close()
     return dict(value=value, ms=ms_max, N=total_N, P=P, K=K, launches=launches, setup_s=setup_s,
                 ticks=ticks, roofline=roofline, e2e=e2e, clocks=clk.summary(), extras=extras,
                 NB=NB)
@@ -406,7 +413,8 @@ def main():
     config = {'workload': 'serving-mix', 'worlds_per_gpu': args.worlds,
               'bodies': 'log-uniform [16,2048] per world, debris contents', 'dt': '1/120 s',
               'iterations': 8, 'l2': 'inputs larger than L2 (arena state > 126 MB)',
-              'parallelism': 'world-sharded x%d (no data-path collective)' % world}
+              'parallelism': 'world-sharded x%d (no data-path collective)' % world,
+              'groups_per_gpu': args.groups}
     if args.impl == 'reference':
         if rank == 0:
             budget = max(5.0, args.cpu_sample_s)

@@ -110,3 +110,37 @@ def test_serving_snapshot_restore():
     for k in ('pos', 'q', 'v', 'w', 'awake', 'timer'):
         assert np.array_equal(later[k], again[k]), k
     srv.close()
+
+
+def test_world_groups_equal_one_batch():
+    from omi_physics_b200.groups import WorldGroups
+    reqs = scenes.serving_requests(16, seed=9, n_min=16, n_max=256)
+    one = [scenes.serving_world(r)[0] for r in reqs]
+    many = [scenes.serving_world(r)[0] for r in reqs]
+    b = WorldBatch(one)
+    g = WorldGroups(many, groups=3)
+    b.step(30)
+    g.step(20)
+    g.step_async(10)
+    g.sync()
+    b.sync_to_host()
+    g.sync_to_host()
+    for w1, w2 in zip(one, many):
+        n = w1.body_count
+        for col in COLS:
+            assert np.array_equal(getattr(w1, col)[:n], getattr(w2, col)[:n]), col
+    # the host round trip of the groups equals plain steps too
+    bufs = g.host_buffers()
+    from omi_physics_b200._lib import D, U8, ptr
+    for bt, h in zip(g.batches, bufs):
+        nb = bt.packed.n_bodies
+        bt.ctx.call('download_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D), ptr(h['w'], D),
+                    ptr(h['awake'], U8), ptr(h['timer'], D), None, None)
+    g.step_from_host(bufs, 2)
+    b.step(2)
+    b.sync_to_host()
+    g.sync_to_host()
+    for w1, w2 in zip(one, many):
+        n = w1.body_count
+        assert np.array_equal(w1._position[:n], w2._position[:n])
+    g.close()

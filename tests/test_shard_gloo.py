@@ -79,3 +79,15 @@ def test_two_ranks_over_gloo():
     gathered = res[0][2]
     assert sorted(i for s in gathered for i in s) == list(range(len(sizes)))
     assert gathered == plan_shards(sizes, 2)
+
+
+def test_plan_groups_complete_and_balanced():
+    from omi_physics_b200.groups import plan_groups
+    rng = np.random.default_rng(3)
+    sizes = np.exp(rng.uniform(np.log(16), np.log(2048), size=257)).astype(int)
+    for g in (1, 2, 4, 8):
+        plan = plan_groups(sizes, g)
+        assert sorted(i for grp in plan for i in grp) == list(range(len(sizes)))
+        loads = [int(sizes[grp].sum()) for grp in plan]
+        assert max(loads) - min(loads) <= 2 * int(sizes.max())
+    assert plan_groups([5, 3], 4) == [[0], [1]]        # no empty groups
