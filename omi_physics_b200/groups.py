@@ -87,18 +87,21 @@ class WorldGroups:
                         'w': alloc((nb, 3)), 'awake': alloc((nb,), np.uint8), 'timer': alloc((nb,))})
         return out
 
-    def step_from_host(self, bufs, n: int = 1) -> None:
-        """Upload each group's state from ``bufs``, step ``n`` times, download
-        it back - the groups concurrently, so copies overlap kernels."""
+    def step_from_host(self, bufs, n: int = 1, rounds: int = 1) -> None:
+        """``rounds`` times per group: upload its state from ``bufs``, step ``n``
+        times, download it back. The groups run concurrently and independently
+        (no barrier between rounds), so one group's copies overlap the others'
+        kernels."""
         def run(pair):
             b, h = pair
             nb = b.packed.n_bodies
             c = b.ctx
-            c.call('upload_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D), ptr(h['w'], D),
-                   ptr(h['awake'], U8), ptr(h['timer'], D))
-            c.call('step', int(n))
-            c.call('download_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D),
-                   ptr(h['w'], D), ptr(h['awake'], U8), ptr(h['timer'], D), None, None)
+            for _ in range(rounds):
+                c.call('upload_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D), ptr(h['w'], D),
+                       ptr(h['awake'], U8), ptr(h['timer'], D))
+                c.call('step', int(n))
+                c.call('download_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D),
+                       ptr(h['w'], D), ptr(h['awake'], U8), ptr(h['timer'], D), None, None)
         list(self._pool.map(run, zip(self.batches, bufs)))
 
     # -- results ------------------------------------------------------------------
