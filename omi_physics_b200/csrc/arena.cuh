@@ -16,8 +16,6 @@ constexpr int C_PART = 12;
 enum { C_RA = 0, C_RB = 3, C_NM = 6, C_T1M = 7, C_T2M = 8, C_VB = 9, C_DEPTH = 10,
        R_N = 12, R_T1 = 15, R_T2 = 18, R_FRIC = 21, R_IMA = 22, R_IMB = 23, R_IA = 24, R_IB = 33,
        R_AB = 42, R_FLAGS = 43 };
-// most contacts one body pair produces (box-box manifolds are reduced to 4)
-constexpr int RUN_MAX = 4;
 // per-joint prepared row: invIa(9) invIb(9) rA(3) rB(3) K/LU(9) piv(3) bias(3)
 // n(3) mass bias_s
 constexpr int JD = 48;

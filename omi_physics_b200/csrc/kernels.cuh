@@ -879,35 +879,6 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prep(Arena A) {
     }
 }
 
-// bucket constraints by level inside one warp: ls[0..D] = level starts
-__device__ inline void bucket_levels_warp(int n, int D, const int *level, int *ls, int *cursor,
-                                          int *order) {
-    const int lane = threadIdx.x & 31;
-    for (int l = lane; l <= D; l += 32) { ls[l] = 0; cursor[l] = 0; }
-    __syncwarp();
-    for (int k = lane; k < n; k += 32) atomicAdd(&ls[level[k] + 1], 1);
-    __syncwarp();
-    // exclusive scan of ls[1..D] in chunks of 32 with a carry
-    int carry = 0;
-    for (int base = 1; base <= D; base += 32) {
-        const int i = base + lane;
-        int x = i <= D ? ls[i] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
-        }
-        if (i <= D) ls[i] = x + carry;
-        carry += __shfl_sync(FULL, x, 31);
-        __syncwarp();
-    }
-    __syncwarp();
-    for (int k = lane; k < n; k += 32) {
-        const int l = level[k];
-        order[ls[l] + atomicAdd(&cursor[l], 1)] = k;
-    }
-    __syncwarp();
-}
-
 // The sweep sequence. The Gauss-Seidel unit is a run (the consecutive
 // contacts of one body pair) and the sequence is every pass of the
 // reference's solve in order: the warm start (when on), then each velocity

@@ -54,7 +54,6 @@ struct OmiCtx {
     Arena A{};
     bool loaded = false;
     int max_world_n = 0, max_world_j = 0, sort_cap = 0, sort_block = 256;
-    int solve_block = 128;
     int level_ints = 0;            // shared ints of one k_levels block
     int sm_count = 148;            // multiprocessors of the device (persistent sweep grid)
     int fin_cap = 1;               // bodies whose sleep flags / islands k_finalize keeps in shared memory
@@ -718,7 +717,6 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->max_world_j = max_j;
     ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
     ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
-    ctx->solve_block = max_n > 1024 ? 256 : 128;
     // sleep flags and union-find parents of the largest world (two ints per body, <= 64 KB)
     ctx->fin_cap = std::min(std::max(max_n, 1), 8192);
     // body buckets of the largest world: 2 ints per body + 2 per run (~1.5 runs per body)
