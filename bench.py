@@ -11,7 +11,11 @@ per group; one "step" = every world advances one dt). Reported beside it:
     launch + sync per world per step) on a sample of the mix;
   * roofline of the dominant stage from per-stage CUDA events;
   * cpu_baseline: the reference's own CPU step (oracle/_ref, NumPy + its
-    Cython accelerators) on a bounded sample, all host cores.
+    Cython accelerators) on a bounded sample, all host cores;
+  * capsule_triangles: the capsule-against-triangles query (65536 capsules x
+    256 candidate triangles by default) device-resident, through host
+    buffers, against the reference's compiled routine on all host cores, with
+    its own roofline.
 
 ``--impl reference`` times the reference CPU implementation on the same
 workload and prints its JSON line (rank 0 only under torchrun).
@@ -56,6 +60,10 @@ def parse():
     ap.add_argument('--serve-requests', type=int, default=None,
                     help='requests in the serving run (default: --worlds; 0 skips it)')
     ap.add_argument('--serve-slots', type=int, default=96, help='slots per size class')
+    ap.add_argument('--capsule-blocks', type=int, default=64,
+                    help='capsule-triangle workload: blocks of 1024 capsules x 256 triangles (0 skips it)')
+    ap.add_argument('--capsule-only', action='store_true',
+                    help='run only the capsule-triangle measurement (device part) and print it')
     ap.add_argument('--groups', type=int, default=4,
                     help='worlds are stepped as this many concurrent groups (one context + stream each)')
     return ap.parse_args()
@@ -353,6 +361,163 @@ def plain_per_world(worlds, reqs, sample, device, preroll):
 
 
 # ---------------------------------------------------------------------------
+# capsule against triangles (the character controller's query, batched)
+# ---------------------------------------------------------------------------
+CAPS_PER_BLOCK, TRIS_PER_CAPSULE = 1024, 256
+CT_BYTES = 72 + 57          # per triangle: vertices in; hit, point, normal, depth out
+
+
+def capsule_block(seed, b):
+    """Block ``b``: 1024 capsules (random pose, half height [0, 0.9), radius
+    [0.2, 0.8)), each with 256 candidate triangles scattered around it."""
+    rng = np.random.default_rng([seed, b])
+    q, k = CAPS_PER_BLOCK, TRIS_PER_CAPSULE
+    centres = rng.uniform(-50, 50, size=(q, 3))
+    axes = rng.normal(size=(q, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    half = rng.uniform(0.0, 0.9, size=q)
+    caps = np.concatenate([centres - axes * half[:, None], centres + axes * half[:, None],
+                           rng.uniform(0.2, 0.8, size=(q, 1))], axis=1)
+    verts = np.repeat(centres, k, axis=0)[:, None, :] + rng.normal(scale=1.0, size=(q * k, 3, 3))
+    return caps, verts
+
+
+def _capsule_ref_worker(payload):
+    seed, blocks = payload
+    sys.path.insert(0, os.path.join(ROOT, 'oracle', '_ref'))
+    from omi_physics import collide
+    nat = collide._native
+    k = TRIS_PER_CAPSULE
+    hit = np.zeros(k, np.uint8)
+    pts, nrm, dep = np.zeros((k, 3)), np.zeros((k, 3)), np.zeros(k)
+    done, spent = 0, 0.0
+    for b in blocks:
+        caps, verts = capsule_block(seed, b)
+        t = time.perf_counter()
+        for c in range(len(caps)):
+            nat.capsule_triangles(caps[c, :3], caps[c, 3:6], float(caps[c, 6]), verts[c * k:(c + 1) * k],
+                                  hit, pts, nrm, dep)
+        spent += time.perf_counter() - t
+        done += len(verts)
+    return done, spent
+
+
+def capsule_cpu_reference(seed, blocks, cores=None):
+    """The reference's compiled capsule_triangles (oracle/_ref) over the same
+    capsules, one call per capsule with reused output arrays, blocks spread
+    over a process pool."""
+    import multiprocessing as mp
+    if not os.path.isdir(os.path.join(ROOT, 'oracle', '_ref', 'omi_physics')):
+        return None
+    cores = min(cores or os.cpu_count() or 1, blocks)
+    chunks = [list(range(i, blocks, cores)) for i in range(cores)]
+    t = time.perf_counter()
+    with mp.get_context('spawn').Pool(cores) as pool:
+        res = pool.map(_capsule_ref_worker, [(seed, c) for c in chunks])
+    wall = time.perf_counter() - t
+    tris = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    per_core = tris / sum(r[1] for r in res)
+    return {'value': tris / slowest, 'unit': 'triangles/s', 'cores': cores, 'kind': 'reference',
+            'sample': '%d triangles (%d capsules x %d), _native.capsule_triangles per capsule with '
+                      'reused outputs, %d processes, %.1f s wall' % (tris, tris // TRIS_PER_CAPSULE,
+                                                                     TRIS_PER_CAPSULE, cores, wall),
+            'per_core': per_core}
+
+
+def capsule_triangles_run(seed, blocks, local, steps, warmup, device_only=False):
+    """Device-resident throughput of k_capsule_triangles (CUDA events on the
+    launching stream), the same through host buffers (omi_capsule_triangles_batch
+    from pinned memory, copies inside the timed region), and the reference's
+    compiled routine on the host cores."""
+    import torch
+    from omi_physics_b200 import collide as oc
+    parts = [capsule_block(seed, b) for b in range(blocks)]
+    caps = np.concatenate([p[0] for p in parts])
+    verts = np.concatenate([p[1] for p in parts])
+    del parts
+    q, n = len(caps), len(verts)
+    off = np.arange(0, n + 1, TRIS_PER_CAPSULE, dtype=np.int64)
+    dev = torch.device('cuda', local)
+    tc, to = torch.from_numpy(caps).to(dev), torch.from_numpy(off).to(dev)
+    tv = torch.from_numpy(verts).to(dev)
+    th = torch.empty(n, dtype=torch.uint8, device=dev)
+    tp = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    tn = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    td = torch.empty(n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx, lock = oc.context(local)
+    with lock:
+        ctx.call('set_stream', stream.cuda_stream)
+        args = (ctx, q, tc.data_ptr(), to.data_ptr(), tv.data_ptr(), n, th.data_ptr(), tp.data_ptr(),
+                tn.data_ptr(), td.data_ptr())
+        for _ in range(max(3, warmup)):
+            oc.capsule_triangles_device(*args)
+        torch.cuda.synchronize(dev)
+        launches0 = ctx.launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                oc.capsule_triangles_device(*args)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+        launches = ctx.launches() - launches0
+        ms = e0.elapsed_time(e1) / steps
+        ctx.call('set_stream', None)
+    hits = int(th.sum().item())
+    value = n / (ms / 1e3)
+    peaks = json.load(open(MEASURED)) if os.path.exists(MEASURED) else {}
+    peak = float(peaks.get('hbm_gbs', FALLBACK_HBM))
+    achieved = CT_BYTES * n / (ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath)).get('capsule_triangles')
+        if tr is not None:
+            traffic = tr.get('bytes_per_triangle', 0.0) * n
+    del tv, th, tp, tn, td
+    torch.cuda.empty_cache()
+    if device_only:
+        return {'workload': '%d capsules x %d triangles' % (q, TRIS_PER_CAPSULE), 'value': value,
+                'unit': 'triangles/s', 'ms_per_launch': ms, 'achieved_gbs': achieved, 'peak_gbs': peak,
+                'frac': achieved / peak, 'gpu_launches': launches, 'clocks': clk.summary()}
+
+    # host buffers: pinned, copies in the timed region
+    def pinned(shape, dt):
+        return torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+    hv = pinned((n, 3, 3), torch.float64)
+    hv[:] = verts
+    del verts
+    out = (pinned(n, torch.uint8), pinned((n, 3), torch.float64), pinned((n, 3), torch.float64),
+           pinned(n, torch.float64))
+    oc.capsule_triangles_many(caps, off, hv, device=local, out=out)
+    e2e_calls = 3
+    t = time.perf_counter()
+    for _ in range(e2e_calls):
+        oc.capsule_triangles_many(caps, off, hv, device=local, out=out)
+    e2e_s = (time.perf_counter() - t) / e2e_calls
+    cb = capsule_cpu_reference(seed, blocks)
+    line = {'workload': '%d capsules x %d triangles (%d triangles, %.2f GB in + out)'
+                        % (q, TRIS_PER_CAPSULE, n, CT_BYTES * n / 1e9),
+            'metric': 'triangles/s', 'value': value, 'ms_per_launch': ms, 'hit_fraction': hits / n,
+            'gpu_launches': launches, 'dtype': 'f64', 'clocks': clk.summary(),
+            'l2': 'inputs larger than L2 (%.1f GB of vertices)' % (72 * n / 1e9),
+            'roofline': {'bound': 'hbm', 'kernel': 'k_capsule_triangles', 'achieved': round(achieved, 3),
+                         'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': traffic,
+                         'algorithmic_bytes': CT_BYTES * n,
+                         'peak_source': 'measured' if 'hbm_gbs' in peaks else 'fallback'},
+            'e2e': {'value': n / e2e_s, 'unit': 'triangles/s', 'h2d_bytes_per_step': 72 * n + caps.nbytes +
+                    off.nbytes, 'd2h_bytes_per_step': 57 * n,
+                    'path': 'omi_capsule_triangles_batch from pinned host arrays (2 streams, 2M-triangle '
+                            'chunks)'}}
+    if cb is not None:
+        line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        line['e2e_over_cpu'] = line['e2e']['value'] / cb['value']
+    return line
+
+
+# ---------------------------------------------------------------------------
 # CPU reference (oracle/_ref: the reference built from its own sources)
 # ---------------------------------------------------------------------------
 def _ref_worker(payload):
@@ -435,6 +600,11 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+    if args.capsule_only:
+        if rank == 0:
+            print(json.dumps(capsule_triangles_run(args.seed, args.capsule_blocks, local, args.steps,
+                                                   args.warmup, device_only=True)))
+        return
     res = run_ours(args, rank, world, local)
     if rank == 0:
         ticks = sorted(res['ticks'])
@@ -459,6 +629,9 @@ def main():
             cb = cpu_reference(args.worlds, args.seed, args.cpu_sample_s, args.preroll)
             if cb is not None:
                 line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+            if args.capsule_blocks > 0:
+                line['capsule_triangles'] = capsule_triangles_run(args.seed, args.capsule_blocks, local,
+                                                                  args.steps, args.warmup)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -24,14 +24,17 @@ extern "C" {
 #define OMI_OK 0
 #define OMI_E_CUDA (-1)         /* CUDA runtime error (message has details) */
 #define OMI_E_ARG (-2)          /* bad argument / size */
-#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triggers, capsules ...) */
+#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triggers, trimesh ...) */
 #define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
 #define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
 #define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
 
 /* Shape types, combine modes, joint types: same meaning as the reference's
  * model.Shape.type, model.combine modes (model.py:231-243) and joints.py. */
-enum { OMI_SHAPE_SPHERE = 1, OMI_SHAPE_BOX = 2, OMI_SHAPE_CONVEX = 3 };
+/* OMI_SHAPE_CAPSULE also carries the reference's cylinder, which it collides
+ * as a capsule (body.py:224-228): shape_radius = radiusBottom,
+ * shape_size = (0, height, 0). Capsule pairs go through GJK/EPA. */
+enum { OMI_SHAPE_SPHERE = 1, OMI_SHAPE_BOX = 2, OMI_SHAPE_CONVEX = 3, OMI_SHAPE_CAPSULE = 4 };
 enum { OMI_AVERAGE = 0, OMI_MINIMUM = 1, OMI_MAXIMUM = 2, OMI_MULTIPLY = 3 };
 enum { OMI_JOINT_POINT = 0, OMI_JOINT_DISTANCE = 1, OMI_JOINT_MOTOR = 2 };
 /* per-world flag bits */
@@ -207,6 +210,40 @@ int omi_get_contacts(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double 
                      double *normal, double *depth, double *impulse, int32_t cap);
 /* sleep-island label per body of one world (-1 = not in contact) */
 int omi_get_islands(OmiCtx *ctx, int32_t world, int32_t *labels);
+
+/* ---- capsule against triangles (the character controller's query) ----
+ *
+ * The compiled capsule_triangles (_collide_native.pyx:454-574), reached from
+ * collide.capsule_triangle_batch / capsule_triangles / capsule_mesh_pushes
+ * (collide.py:385-462) and the mesh route of collide.collide
+ * (collide.py:272-306). A capsule is the segment p0-p1 with a radius; verts
+ * is (n, 3, 3) (triangle, vertex, axis). For every triangle: hit (1 byte),
+ * point on the triangle (3), normal from the triangle toward the capsule (3)
+ * and depth, bit-identical to the reference's; triangles without contact get
+ * hit 0 and zeros, as the arrays capsule_triangle_batch passes in hold.
+ * These calls need no loaded scene. */
+
+/* One capsule, host buffers: the reference's
+ * _native.capsule_triangles(cp0, cp1, radius, verts, hit, points, normals,
+ * depths) (_collide_native.pyx:454-574). Returns when the outputs are written. */
+int omi_capsule_triangles(OmiCtx *ctx, const double *p0, const double *p1, double radius,
+                          const double *verts, int64_t n, uint8_t *hit, double *points,
+                          double *normals, double *depths);
+/* q capsules at once, host buffers: caps is (q, 7) = p0 (3), p1 (3), radius;
+ * the triangles of capsule c are rows [tri_off[c], tri_off[c+1]) of verts,
+ * with tri_off[0] = 0, tri_off[q] = n and non-decreasing (checked). Copies in,
+ * computes and copies out in chunks on two internal streams, so transfers
+ * overlap the kernel (pinned host buffers let them run asynchronously).
+ * Returns when the outputs are written. */
+int omi_capsule_triangles_batch(OmiCtx *ctx, int32_t q, const double *caps, const int64_t *tri_off,
+                                const double *verts, int64_t n, uint8_t *hit, double *points,
+                                double *normals, double *depths);
+/* The same on DEVICE buffers, enqueued on the context's stream (omi_set_stream);
+ * returns without waiting. tri_off is not checked here: a malformed one gives
+ * wrong answers but every read stays inside caps (q rows) and tri_off (q+1). */
+int omi_capsule_triangles_device(OmiCtx *ctx, int32_t q, const double *caps, const int64_t *tri_off,
+                                 const double *verts, int64_t n, uint8_t *hit, double *points,
+                                 double *normals, double *depths);
 /*
  * Allocation-free sweep-and-prune for one world. (This entry point has no
  * counterpart in the reference.) It is for callers that must not allocate

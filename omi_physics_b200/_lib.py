@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, '_omi_b200.so')
 
 D = C.POINTER(C.c_double)
 I = C.POINTER(C.c_int32)
+I64 = C.POINTER(C.c_int64)
 U8 = C.POINTER(C.c_uint8)
 
 OMI_E_CUDA, OMI_E_ARG, OMI_E_UNSUPPORTED, OMI_E_STATE, OMI_E_TIMEOUT, OMI_E_OOM = -1, -2, -3, -4, -5, -6
@@ -30,7 +31,7 @@ class OmiError(RuntimeError):
 
 
 class UnsupportedFeature(OmiError):
-    """The scene uses something outside the device path (triggers, capsules ...)."""
+    """The scene uses something outside the device path (triggers, trimesh ...)."""
 
 
 class OutOfBudget(OmiError):
@@ -109,6 +110,12 @@ PROTOTYPES = {
     'omi_profile_step': (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, I]),
     'omi_kernel_name': (C.c_char_p, [C.c_int32]),
     'omi_launch_count': (C.c_int64, [C.c_void_p]),
+    'omi_capsule_triangles': (C.c_int, [C.c_void_p, D, D, C.c_double, D, C.c_int64, U8, D, D, D]),
+    'omi_capsule_triangles_batch': (C.c_int, [C.c_void_p, C.c_int32, D, I64, D,
+                                              C.c_int64, U8, D, D, D]),
+    'omi_capsule_triangles_device': (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p]),
     'omi_sweep_pairs_noalloc': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                           C.c_int32, C.c_void_p, C.c_void_p, C.c_char_p,

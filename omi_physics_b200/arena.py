@@ -17,7 +17,8 @@ from ._lib import D, I, U8, OmiScene, UnsupportedFeature, WF_ACTIVE, WF_COLLISIO
 from .joints import joint_kind
 from .model import COMBINE_CODES
 
-SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3}
+# a cylinder is collided as a capsule (make_proxy, body.py:224-228)
+SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4}
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
 
@@ -132,9 +133,14 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
         for sh in world.shapes:
             code = SHAPE_CODES.get(sh.type, 0)
             parts['shape_type'].append([code])
-            parts['shape_radius'].append([float(sh.radius)])
-            size = np.asarray(sh.size, 'd') if np.size(sh.size) == 3 else np.zeros(3)
-            parts['shape_size'].append(size.reshape(1, 3))
+            if code == 4:
+                # capsule proxy: radiusBottom, half height 0.5 * height
+                parts['shape_radius'].append([float(sh.radiusBottom)])
+                parts['shape_size'].append(np.array([[0.0, float(sh.height), 0.0]]))
+            else:
+                parts['shape_radius'].append([float(sh.radius)])
+                size = np.asarray(sh.size, 'd') if np.size(sh.size) == 3 else np.zeros(3)
+                parts['shape_size'].append(size.reshape(1, 3))
             if sh.type == 'convex':
                 pts = np.asarray(sh.points, 'd').reshape(-1, 3)
                 parts['shape_pt_off'].append([npts])

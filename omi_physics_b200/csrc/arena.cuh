@@ -56,7 +56,7 @@ struct Arena {
     double *timer;
     uint8_t *awake;
     const int *mtype, *shape, *material, *material_key, *filter_row, *body_world;
-    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 other (convex)
+    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 convex, 4 capsule
     const double *half;      // refit half extents (world.py:443-469)
     double *aabb_min, *aabb_max, *invIw;
 

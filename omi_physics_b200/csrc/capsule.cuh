@@ -1,0 +1,277 @@
+// Capsule against batches of triangles: the compiled capsule_triangles of
+// _collide_native.pyx:454-574 (the character controller's depenetration
+// query, collide.py:438-462), for many capsules at once.
+//
+// Layout: q capsules as rows of 7 doubles (p0 xyz, p1 xyz, radius), the
+// triangles of capsule c at [tri_off[c], tri_off[c+1]) of one (n, 3, 3)
+// vertex array; outputs line up with the triangles (hit byte, point (3),
+// normal (3), depth), zeros where there is no contact.
+//
+// One thread per triangle. A block takes tiles of CT_THREADS triangles: the
+// tile's 72-byte vertex records are read with coalesced streaming loads into
+// shared memory, each thread answers its triangle, and the point / normal rows
+// are written back through shared memory so every global store is coalesced.
+// Per triangle 72 bytes are read and 57 written; the arithmetic (float64, in
+// the reference's operation order, no contraction) is a few hundred
+// operations, so the kernel sits near the HBM / FP64 ridge.
+#pragma once
+#include "geometry.cuh"
+
+namespace omi {
+
+constexpr int CT_THREADS = 256;   // triangles per tile, one thread each
+constexpr int CT_CAP_DOUBLES = 7; // p0 (3), p1 (3), radius
+
+// _dot3 (_collide_native.pyx:16-17): left to right
+__device__ __forceinline__ double dot3_seq(const double *a, const double *b) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+__device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+// closest point on triangle abc to p: Ericson's Voronoi regions in the order
+// _closest_on_tri tests them (_collide_native.pyx:364-410)
+__device__ inline void tri_closest(const double *p, const double *a, const double *b, const double *c,
+                                   double *out) {
+    double ab[3], ac[3], ap[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) { ab[m] = b[m] - a[m]; ac[m] = c[m] - a[m]; ap[m] = p[m] - a[m]; }
+    const double d1 = dot3_seq(ab, ap), d2 = dot3_seq(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) { out[0] = a[0]; out[1] = a[1]; out[2] = a[2]; return; }
+    double bp[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) bp[m] = p[m] - b[m];
+    const double d3 = dot3_seq(ab, bp), d4 = dot3_seq(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) { out[0] = b[0]; out[1] = b[1]; out[2] = b[2]; return; }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double v = d1 / (d1 - d3);
+#pragma unroll
+        for (int m = 0; m < 3; m++) out[m] = a[m] + v * ab[m];
+        return;
+    }
+    double cp[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) cp[m] = p[m] - c[m];
+    const double d5 = dot3_seq(ab, cp), d6 = dot3_seq(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) { out[0] = c[0]; out[1] = c[1]; out[2] = c[2]; return; }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double w = d2 / (d2 - d6);
+#pragma unroll
+        for (int m = 0; m < 3; m++) out[m] = a[m] + w * ac[m];
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+#pragma unroll
+        for (int m = 0; m < 3; m++) out[m] = b[m] + w * (c[m] - b[m]);
+        return;
+    }
+    const double inv = 1.0 / (va + vb + vc);
+    const double v = vb * inv, w = vc * inv;
+#pragma unroll
+    for (int m = 0; m < 3; m++) out[m] = a[m] + ab[m] * v + ac[m] * w;
+}
+
+// closest points of segments p1q1 and p2q2 (_collide_native.pyx:413-451)
+__device__ inline void seg_closest(const double *p1, const double *q1, const double *p2, const double *q2,
+                                   double *o1, double *o2) {
+    double d1[3], d2[3], r[3], s, t;
+#pragma unroll
+    for (int m = 0; m < 3; m++) { d1[m] = q1[m] - p1[m]; d2[m] = q2[m] - p2[m]; r[m] = p1[m] - p2[m]; }
+    const double aa = dot3_seq(d1, d1), e = dot3_seq(d2, d2), f = dot3_seq(d2, r);
+    if (aa <= EPS_COLLIDE && e <= EPS_COLLIDE) {
+#pragma unroll
+        for (int m = 0; m < 3; m++) { o1[m] = p1[m]; o2[m] = p2[m]; }
+        return;
+    }
+    if (aa <= EPS_COLLIDE) {
+        s = 0.0;
+        t = clamp01(f / e);
+    } else {
+        const double cc = dot3_seq(d1, r);
+        if (e <= EPS_COLLIDE) {
+            t = 0.0;
+            s = clamp01(-cc / aa);
+        } else {
+            const double bb = dot3_seq(d1, d2);
+            const double den = aa * e - bb * bb;
+            s = den > EPS_COLLIDE ? clamp01((bb * f - cc * e) / den) : 0.0;
+            t = (bb * s + f) / e;
+            if (t < 0.0) {
+                t = 0.0;
+                s = clamp01(-cc / aa);
+            } else if (t > 1.0) {
+                t = 1.0;
+                s = clamp01((bb - cc) / aa);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 3; m++) { o1[m] = p1[m] + d1[m] * s; o2[m] = p2[m] + d2[m] * t; }
+}
+
+// One triangle against the capsule (collide.py:309-382 as compiled): over
+// the face, the deepest cap end whose perpendicular foot lies on the triangle
+// is pushed back to the side the capsule's centre is on, depth unbounded;
+// otherwise the nearest of the cap ends to the triangle and of the axis to
+// the three edges (first strict minimum), if nearer than the radius. Returns
+// 1 on contact with the point on the triangle and the normal pointing from
+// the triangle toward the capsule.
+__device__ inline int capsule_triangle(const double *c0, const double *c1, const double *centre, double radius,
+                                       const double *v0, const double *v1, const double *v2, double *point,
+                                       double *normal, double *depth) {
+    double e1[3], e2[3], face[3], tp[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) { e1[m] = v1[m] - v0[m]; e2[m] = v2[m] - v0[m]; }
+    face[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    face[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    face[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    const double face_len = sqrt(dot3_seq(face, face));
+    if (face_len > EPS_COLLIDE) {
+        double fn[3];
+#pragma unroll
+        for (int m = 0; m < 3; m++) fn[m] = face[m] / face_len;
+        double g[3] = {centre[0] - v0[0], centre[1] - v0[1], centre[2] - v0[2]};
+        if (fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2] < 0.0) {
+            fn[0] = -fn[0]; fn[1] = -fn[1]; fn[2] = -fn[2];
+        }
+        bool found = false;
+        double best = -1e300, bp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double *sp = k ? c1 : c0;
+#pragma unroll
+            for (int m = 0; m < 3; m++) g[m] = sp[m] - v0[m];
+            const double h = fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2];
+            double foot[3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) foot[m] = sp[m] - fn[m] * h;
+            tri_closest(sp, v0, v1, v2, tp);
+#pragma unroll
+            for (int m = 0; m < 3; m++) g[m] = foot[m] - tp[m];
+            if (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] > EPS_COLLIDE * EPS_COLLIDE) continue;
+            const double reach = radius - h;
+            if (reach > 0.0 && reach > best) {
+                best = reach;
+                found = true;
+                bp[0] = tp[0]; bp[1] = tp[1]; bp[2] = tp[2];
+            }
+        }
+        if (found) {
+            *depth = best;
+#pragma unroll
+            for (int m = 0; m < 3; m++) { point[m] = bp[m]; normal[m] = fn[m]; }
+            return 1;
+        }
+    }
+    double best_d2 = 1e300, bsp[3] = {0.0, 0.0, 0.0}, btp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const double *sp = k ? c1 : c0;
+        tri_closest(sp, v0, v1, v2, tp);
+        const double gx = sp[0] - tp[0], gy = sp[1] - tp[1], gz = sp[2] - tp[2];
+        const double d2 = gx * gx + gy * gy + gz * gz;
+        if (d2 < best_d2) {
+            best_d2 = d2;
+#pragma unroll
+            for (int m = 0; m < 3; m++) { bsp[m] = sp[m]; btp[m] = tp[m]; }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double *ea = k == 0 ? v0 : (k == 1 ? v1 : v2);
+        const double *eb = k == 0 ? v1 : (k == 1 ? v2 : v0);
+        double ax[3], ed[3];
+        seg_closest(c0, c1, ea, eb, ax, ed);
+        const double gx = ax[0] - ed[0], gy = ax[1] - ed[1], gz = ax[2] - ed[2];
+        const double d2 = gx * gx + gy * gy + gz * gz;
+        if (d2 < best_d2) {
+            best_d2 = d2;
+#pragma unroll
+            for (int m = 0; m < 3; m++) { bsp[m] = ax[m]; btp[m] = ed[m]; }
+        }
+    }
+    if (best_d2 >= radius * radius) return 0;
+    const double dist = sqrt(best_d2);
+    if (dist > EPS_COLLIDE) {
+#pragma unroll
+        for (int m = 0; m < 3; m++) normal[m] = (bsp[m] - btp[m]) / dist;
+    } else if (face_len > EPS_COLLIDE) {
+#pragma unroll
+        for (int m = 0; m < 3; m++) normal[m] = face[m] / face_len;
+    } else {
+        normal[0] = normal[1] = normal[2] = 0.0;
+    }
+    *depth = radius - dist;
+#pragma unroll
+    for (int m = 0; m < 3; m++) point[m] = btp[m];
+    return 1;
+}
+
+// the capsule owning triangle i: the largest c in [lo, hi] with off[c] <= i
+// (reads off[lo + 1 .. hi] only)
+__device__ __forceinline__ int capsule_of(const int64_t *off, int lo, int hi, int64_t i) {
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&off[mid]) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Triangles [0, n) of this launch are global triangles [base, base + n): the
+// vertex and output pointers are the launch's own, the capsule ranges
+// tri_off are global (a host pipeline launches one chunk at a time).
+__global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
+    const double *__restrict__ caps, const int64_t *__restrict__ tri_off, int q,
+    const double *__restrict__ verts, int64_t base, int64_t n, uint8_t *__restrict__ hit,
+    double *__restrict__ points, double *__restrict__ normals, double *__restrict__ depths) {
+    __shared__ double sv[CT_THREADS * 9];
+    __shared__ double sp[CT_THREADS * 3];
+    __shared__ double sn[CT_THREADS * 3];
+    __shared__ int s_range[2];
+    const int tid = threadIdx.x;
+    for (int64_t t0 = (int64_t)blockIdx.x * CT_THREADS; t0 < n; t0 += (int64_t)gridDim.x * CT_THREADS) {
+        const int m = (int)(n - t0 < CT_THREADS ? n - t0 : CT_THREADS);
+        const double *src = verts + t0 * 9;
+        for (int j = tid; j < m * 9; j += CT_THREADS) sv[j] = __ldcs(src + j);
+        if (tid == 0) {
+            const int first = capsule_of(tri_off, 0, q - 1, base + t0);
+            s_range[0] = first;
+            s_range[1] = capsule_of(tri_off, first, q - 1, base + t0 + m - 1);
+        }
+        __syncthreads();
+        if (tid < m) {
+            const int c = capsule_of(tri_off, s_range[0], s_range[1], base + t0 + tid);
+            const double *cp = caps + (size_t)c * CT_CAP_DOUBLES;
+            double c0[3], c1[3], centre[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                c0[k] = __ldg(&cp[k]);
+                c1[k] = __ldg(&cp[3 + k]);
+                centre[k] = (c0[k] + c1[k]) * 0.5;
+            }
+            const double radius = __ldg(&cp[6]);
+            double v[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) v[k] = sv[tid * 9 + k];
+            double pt[3], nr[3], dep;
+            const int h = capsule_triangle(c0, c1, centre, radius, v, v + 3, v + 6, pt, nr, &dep);
+            if (!h) { pt[0] = pt[1] = pt[2] = 0.0; nr[0] = nr[1] = nr[2] = 0.0; dep = 0.0; }
+#pragma unroll
+            for (int k = 0; k < 3; k++) { sp[tid * 3 + k] = pt[k]; sn[tid * 3 + k] = nr[k]; }
+            hit[t0 + tid] = (uint8_t)h;
+            __stcs(&depths[t0 + tid], dep);
+        }
+        __syncthreads();
+        for (int j = tid; j < m * 3; j += CT_THREADS) {
+            __stcs(&points[t0 * 3 + j], sp[j]);
+            __stcs(&normals[t0 * 3 + j], sn[j]);
+        }
+    }
+}
+
+}  // namespace omi

@@ -45,6 +45,18 @@ __device__ __forceinline__ void normalize3(const double *v, double *o) {
     o[0] = v[0] / d; o[1] = v[1] / d; o[2] = v[2] / d;
 }
 
+// CapsuleProxy segment ends (body.py:84-91): axis = R @ (0, 1, 0) as one
+// dgemv row each, p0 = c - axis * hh, p1 = c + axis * hh
+__device__ __forceinline__ void capsule_ends(const double *c, const double *R, double hh, double *p0,
+                                             double *p1) {
+    const double y[3] = {0.0, 1.0, 0.0};
+    for (int k = 0; k < 3; k++) {
+        const double a = gemv_row(&R[k * 3], y) * hh;
+        p0[k] = c[k] - a;
+        p1[k] = c[k] + a;
+    }
+}
+
 // mathutil.quat_to_matrix (mathutil.py:59-76); R row-major, columns = axes
 __device__ __forceinline__ void quat_to_matrix(const double *qi, double *m) {
     double n = sqrt(((qi[0] * qi[0] + qi[1] * qi[1]) + qi[2] * qi[2]) + qi[3] * qi[3]);

@@ -22,24 +22,31 @@ constexpr int WARP_LANES = 1;
 constexpr int WARP_LANES = 32;
 #endif
 
+// Polytope bounds: 64 EPA iterations add at most 64 vertices; faces and
+// horizon edges are bounded as the oracle bounds them. Rounded Minkowski sums
+// (capsules, spheres against hulls) need more than 2V - 4 faces when nearly
+// coplanar faces make the visible set ragged.
 constexpr int EPA_V = 4 + 64 + 1;
-constexpr int EPA_F = 160;
-constexpr int EPA_E = 480;
+constexpr int EPA_F = 512;
+constexpr int EPA_E = 3 * EPA_F;
 
 struct Proxy {
-    int kind;              // 1 sphere, 2 box, 3 convex
+    int kind;              // 1 sphere, 2 box, 3 convex, 4 capsule
     double c[3], R[9], h[3], r;
+    double e0[3], e1[3];   // capsule segment ends
     const double *local;   // convex local points (global memory)
     int m;
 };
 
+// Vertex indices are below EPA_V, so faces and edges are stored as bytes
+// (about 11 KB per warp).
 struct EpaWork {
     double V[EPA_V][9];    // Minkowski point v, witness a, witness b
-    int F[EPA_F][3];
-    int Fk[EPA_F][3];
-    int E[EPA_E][2];
+    unsigned char F[EPA_F][3];
+    unsigned char E[EPA_E][2];
     unsigned char Ealive[EPA_E];
 };
+static_assert(EPA_V <= 256, "face and edge vertex indices are stored as bytes");
 
 __device__ inline unsigned lane_id() { return threadIdx.x % WARP_LANES; }
 
@@ -62,7 +69,7 @@ __device__ inline int warp_min_index(int i) {
 #endif
 }
 
-// Proxy.support(d) (body.py:46-48, 69-73, 125-128)
+// Proxy.support(d) (body.py:46-48, 69-73, 100-104, 125-128)
 __device__ inline void support(const Proxy &p, const double *d, double *out) {
     if (p.kind == 1) {
         double u[3];
@@ -77,6 +84,12 @@ __device__ inline void support(const Proxy &p, const double *d, double *out) {
             s[j] = sg * p.h[j];
         }
         for (int k = 0; k < 3; k++) out[k] = p.c[k] + gemv_row(&p.R[k * 3], s);
+    } else if (p.kind == 4) {
+        // the segment end farther along d (the second on ties), plus radius
+        const double *end = dot_blas(p.e0, d) > dot_blas(p.e1, d) ? p.e0 : p.e1;
+        double u[3];
+        normalize3(d, u);
+        for (int k = 0; k < 3; k++) out[k] = end[k] + p.r * u[k];
     } else {
         // world = local @ R.T + center; argmax(world @ d), first index on ties:
         // warp max of the values, then the lowest index holding that value;
@@ -278,17 +291,16 @@ __device__ inline int rebuild(EpaWork &W, int nf, int ni) {
                     }
                 }
             } else {
-                if (nk >= EPA_F) { bad = true; break; }
-                W.Fk[nk][0] = W.F[f][0]; W.Fk[nk][1] = W.F[f][1]; W.Fk[nk][2] = W.F[f][2]; nk++;
+                // kept faces compact in place: nk <= f, so face f is read before
+                // any later write reaches its slot
+                W.F[nk][0] = W.F[f][0]; W.F[nk][1] = W.F[f][1]; W.F[nk][2] = W.F[f][2]; nk++;
             }
         }
         for (int q = 0; q < ne && !bad; q++) {
             if (!W.Ealive[q]) continue;
             if (nk >= EPA_F) { bad = true; break; }
-            W.Fk[nk][0] = W.E[q][0]; W.Fk[nk][1] = W.E[q][1]; W.Fk[nk][2] = ni; nk++;
+            W.F[nk][0] = W.E[q][0]; W.F[nk][1] = W.E[q][1]; W.F[nk][2] = (unsigned char)ni; nk++;
         }
-        if (!bad)
-            for (int f = 0; f < nk; f++) { W.F[f][0] = W.Fk[f][0]; W.F[f][1] = W.Fk[f][1]; W.F[f][2] = W.Fk[f][2]; }
         out = bad ? -1 : nk;
     }
     __syncwarp();

@@ -65,6 +65,14 @@ __global__ void k_refit(Arena A) {
                 }
             }
             for (int c = 0; c < 3; c++) { lo[c] = mn[c] - 0.05; hi[c] = mx[c] + 0.05; }
+        } else if (kind == 4) {
+            // CapsuleProxy.aabb (body.py:84-98): segment ends min/max -+ radius
+            double e0[3], e1[3];
+            capsule_ends(p, R, h[1], e0, e1);
+            for (int c = 0; c < 3; c++) {
+                lo[c] = ((e0[c] < e1[c] ? e0[c] : e1[c]) - h[0]) - 0.05;
+                hi[c] = ((e0[c] > e1[c] ? e0[c] : e1[c]) + h[0]) + 0.05;
+            }
         }
         for (int r = 0; r < 3; r++) { A.aabb_min[i * 3 + r] = lo[r]; A.aabb_max[i * 3 + r] = hi[r]; }
         const double *ii = &A.inv_inertia[i * 3];
@@ -443,7 +451,7 @@ __global__ void k_narrow(Arena A) {
             const int a = A.pair_a[p], b = A.pair_b[p];
             const int ka = A.kind[a], kb = A.kind[b];
             double *s = &A.slot[(size_t)p * SLOT];
-            if (ka == 3 || kb == 3) {
+            if (ka >= 3 || kb >= 3) {
                 const int idx = atomicAdd(A.gjk_n, 1);
                 A.gjk_list[idx] = p;
             } else {
@@ -518,6 +526,7 @@ __device__ inline void make_proxy(const Arena &A, int i, Proxy &P) {
     for (int c = 0; c < 3; c++) P.h[c] = 0.5 * A.shape_size[s * 3 + c];
     P.local = &A.points[A.pt_off[s] * 3];
     P.m = A.pt_cnt[s];
+    if (P.kind == 4) capsule_ends(P.c, P.R, 0.5 * A.shape_size[s * 3 + 1], P.e0, P.e1);
 }
 
 // gjk.collide_convex (gjk.py:249-264) through collide.collide (collide.py:251-269)

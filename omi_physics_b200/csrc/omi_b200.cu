@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/omi_b200.h"
+#include "capsule.cuh"
 #include "kernels2.cuh"
 
 using namespace omi;
@@ -67,6 +68,17 @@ struct OmiCtx {
     std::vector<int> h_body_off, h_body_n, h_joint_off;
     bool slots = false;
     SlotTable slot;                // capacities and table offsets of each slot
+    // capsule-triangle host pipeline: two buffer sets, one per internal stream
+    std::vector<Buf> capbufs;
+    int64_t cap_chunk = 0;         // triangles one buffer set holds
+    int cap_q = 0;                 // capsule rows the caps / tri_off buffers hold
+    double *cap_caps = nullptr;
+    int64_t *cap_off = nullptr;
+    double *cap_v[2] = {}, *cap_p[2] = {}, *cap_n[2] = {}, *cap_d[2] = {};
+    uint8_t *cap_h[2] = {};
+    cudaStream_t cap_s[2] = {};
+    cudaEvent_t cap_ev = nullptr;
+    int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
 };
 
 namespace {
@@ -490,6 +502,10 @@ int omi_destroy(OmiCtx *ctx) {
     free_pool(ctx, ctx->dyn);
     free_pool(ctx, ctx->cache);
     free_pool(ctx, ctx->statics);
+    for (int k = 0; k < 2; k++)
+        if (ctx->cap_s[k]) { cudaStreamSynchronize(ctx->cap_s[k]); cudaStreamDestroy(ctx->cap_s[k]); }
+    if (ctx->cap_ev) cudaEventDestroy(ctx->cap_ev);
+    free_pool(ctx, ctx->capbufs);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
@@ -573,6 +589,11 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
             if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
                 s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
                 return fail(ctx, OMI_E_ARG, "convex point range out of bounds");
+        } else if (t == OMI_SHAPE_CAPSULE) {
+            kind[i] = 4;
+            half[i * 3] = s->shape_radius[sh];
+            half[i * 3 + 1] = 0.5 * s->shape_size[sh * 3 + 1];
+            half[i * 3 + 2] = 0.0;
         } else {
             return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
         }
@@ -858,6 +879,10 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
         const int t = o->shape_type[sh];
         if (t == OMI_SHAPE_SPHERE) { kind[i] = 1; for (int k = 0; k < 3; k++) half[i * 3 + k] = o->shape_radius[sh]; }
         else if (t == OMI_SHAPE_BOX) { kind[i] = 2; for (int k = 0; k < 3; k++) half[i * 3 + k] = 0.5 * o->shape_size[sh * 3 + k]; }
+        else if (t == OMI_SHAPE_CAPSULE) {
+            kind[i] = 4;
+            half[i * 3] = o->shape_radius[sh]; half[i * 3 + 1] = 0.5 * o->shape_size[sh * 3 + 1]; half[i * 3 + 2] = 0.0;
+        }
         else if (t == OMI_SHAPE_CONVEX) {
             kind[i] = 3;
             if (o->shape_pt_cnt[sh] < 1 || o->shape_pt_off[sh] < 0 || o->shape_pt_off[sh] + o->shape_pt_cnt[sh] > np_)
@@ -1373,6 +1398,134 @@ int omi_profile_step(OmiCtx *ctx, float *ms, int32_t n, int32_t *n_out) {
     const int m = std::min<int>(n, KN_COUNT);
     for (int k = 0; k < m; k++) ms[k] = ctx->prof_ms[k];
     if (n_out) *n_out = KN_COUNT;
+    return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Capsule against triangles (omi_capsule_triangles*)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t CT_CHUNK = int64_t(1) << 21;   // triangles per pipelined chunk (~270 MB a buffer set)
+
+int capsule_grid(OmiCtx *ctx, int64_t n) {
+    if (!ctx->cap_blocks) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_capsule_triangles, CT_THREADS, 0) != cudaSuccess ||
+            b < 1)
+            b = 1;
+        ctx->cap_blocks = b;
+    }
+    const int64_t tiles = (n + CT_THREADS - 1) / CT_THREADS;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)ctx->sm_count * ctx->cap_blocks));
+}
+
+int capsule_check(OmiCtx *ctx, int32_t q, int64_t n, const void *caps, const void *tri_off, const void *verts,
+                  const void *hit, const void *points, const void *normals, const void *depths) {
+    if (!ctx) return OMI_E_ARG;
+    if (n < 0) return fail(ctx, OMI_E_ARG, "negative triangle count");
+    if (n > 0 && q < 1) return fail(ctx, OMI_E_ARG, "triangles without a capsule");
+    if (q < 0) return fail(ctx, OMI_E_ARG, "negative capsule count");
+    if (n > 0 && (!caps || !tri_off || !verts || !hit || !points || !normals || !depths))
+        return fail(ctx, OMI_E_ARG, "null buffer");
+    return 0;
+}
+
+// buffers for q capsules and chunks of `chunk` triangles (regrown, never shrunk)
+int capsule_buffers(OmiCtx *ctx, int32_t q, int64_t chunk) {
+    if (!ctx->cap_s[0]) {
+        for (int k = 0; k < 2; k++) CK(cudaStreamCreateWithFlags(&ctx->cap_s[k], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->cap_ev, cudaEventDisableTiming));
+    }
+    if (q <= ctx->cap_q && chunk <= ctx->cap_chunk) return 0;
+    for (int k = 0; k < 2; k++) CK(cudaStreamSynchronize(ctx->cap_s[k]));
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_pool(ctx, ctx->capbufs);
+    ctx->cap_q = std::max(q, ctx->cap_q);
+    ctx->cap_chunk = std::max(chunk, ctx->cap_chunk);
+    int rc = alloc(ctx, ctx->capbufs, ctx->cap_caps, (size_t)ctx->cap_q * CT_CAP_DOUBLES);
+    rc = rc ? rc : alloc(ctx, ctx->capbufs, ctx->cap_off, (size_t)ctx->cap_q + 1);
+    for (int k = 0; k < 2 && !rc; k++) {
+        const size_t m = (size_t)ctx->cap_chunk;
+        rc = alloc(ctx, ctx->capbufs, ctx->cap_v[k], m * 9);
+        rc = rc ? rc : alloc(ctx, ctx->capbufs, ctx->cap_h[k], m);
+        rc = rc ? rc : alloc(ctx, ctx->capbufs, ctx->cap_p[k], m * 3);
+        rc = rc ? rc : alloc(ctx, ctx->capbufs, ctx->cap_n[k], m * 3);
+        rc = rc ? rc : alloc(ctx, ctx->capbufs, ctx->cap_d[k], m);
+    }
+    if (rc) { free_pool(ctx, ctx->capbufs); ctx->cap_q = 0; ctx->cap_chunk = 0; }
+    return rc;
+}
+
+int capsule_pipeline(OmiCtx *ctx, int32_t q, const double *caps, const int64_t *tri_off, const double *verts,
+                     int64_t n, uint8_t *hit, double *points, double *normals, double *depths) {
+    int rc = capsule_check(ctx, q, n, caps, tri_off, verts, hit, points, normals, depths);
+    if (rc || n == 0) return rc;
+    if (tri_off[0] != 0 || tri_off[q] != n) return fail(ctx, OMI_E_ARG, "tri_off must run from 0 to n");
+    for (int c = 0; c < q; c++)
+        if (tri_off[c + 1] < tri_off[c]) return fail(ctx, OMI_E_ARG, "tri_off must be non-decreasing");
+    const int64_t chunk = std::min<int64_t>(CT_CHUNK, (n + CT_THREADS - 1) / CT_THREADS * CT_THREADS);
+    rc = capsule_buffers(ctx, q, chunk);
+    if (rc) return rc;
+    cudaStream_t s0 = ctx->cap_s[0], s1 = ctx->cap_s[1];
+    // after the caller's earlier work on the context stream
+    CK(cudaEventRecord(ctx->cap_ev, ctx->stream));
+    CK(cudaStreamWaitEvent(s0, ctx->cap_ev, 0));
+    CK(cudaMemcpyAsync(ctx->cap_caps, caps, sizeof(double) * CT_CAP_DOUBLES * q, cudaMemcpyHostToDevice, s0));
+    CK(cudaMemcpyAsync(ctx->cap_off, tri_off, sizeof(int64_t) * (q + 1), cudaMemcpyHostToDevice, s0));
+    CK(cudaEventRecord(ctx->cap_ev, s0));
+    CK(cudaStreamWaitEvent(s1, ctx->cap_ev, 0));
+    int k = 0;
+    for (int64_t t0 = 0; t0 < n; t0 += ctx->cap_chunk, k ^= 1) {
+        const int64_t m = std::min<int64_t>(ctx->cap_chunk, n - t0);
+        cudaStream_t s = ctx->cap_s[k];
+        CK(cudaMemcpyAsync(ctx->cap_v[k], verts + t0 * 9, sizeof(double) * 9 * m, cudaMemcpyHostToDevice, s));
+        k_capsule_triangles<<<capsule_grid(ctx, m), CT_THREADS, 0, s>>>(
+            ctx->cap_caps, ctx->cap_off, q, ctx->cap_v[k], t0, m, ctx->cap_h[k], ctx->cap_p[k], ctx->cap_n[k],
+            ctx->cap_d[k]);
+        CK(cudaGetLastError());
+        ctx->launches++;
+        CK(cudaMemcpyAsync(hit + t0, ctx->cap_h[k], m, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(points + t0 * 3, ctx->cap_p[k], sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(normals + t0 * 3, ctx->cap_n[k], sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(depths + t0, ctx->cap_d[k], sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s0));
+    CK(cudaStreamSynchronize(s1));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int omi_capsule_triangles(OmiCtx *ctx, const double *p0, const double *p1, double radius, const double *verts,
+                          int64_t n, uint8_t *hit, double *points, double *normals, double *depths) {
+    if (!ctx) return OMI_E_ARG;
+    if (!p0 || !p1) return fail(ctx, OMI_E_ARG, "null capsule end");
+    const double cap[CT_CAP_DOUBLES] = {p0[0], p0[1], p0[2], p1[0], p1[1], p1[2], radius};
+    const int64_t off[2] = {0, n};
+    return capsule_pipeline(ctx, 1, cap, off, verts, n, hit, points, normals, depths);
+}
+
+int omi_capsule_triangles_batch(OmiCtx *ctx, int32_t q, const double *caps, const int64_t *tri_off,
+                                const double *verts, int64_t n, uint8_t *hit, double *points, double *normals,
+                                double *depths) {
+    if (ctx && q >= 0 && !tri_off) return fail(ctx, OMI_E_ARG, "null tri_off");
+    return capsule_pipeline(ctx, q, caps, tri_off, verts, n, hit, points, normals, depths);
+}
+
+int omi_capsule_triangles_device(OmiCtx *ctx, int32_t q, const double *caps, const int64_t *tri_off,
+                                 const double *verts, int64_t n, uint8_t *hit, double *points, double *normals,
+                                 double *depths) {
+    int rc = capsule_check(ctx, q, n, caps, tri_off, verts, hit, points, normals, depths);
+    if (rc || n == 0) return rc;
+    k_capsule_triangles<<<capsule_grid(ctx, n), CT_THREADS, 0, ctx->stream>>>(caps, tri_off, q, verts, 0, n, hit,
+                                                                              points, normals, depths);
+    CK(cudaGetLastError());
+    ctx->launches++;
     return 0;
 }
 

@@ -5,8 +5,8 @@ reference defines them in ``src/omi_physics/model.py:33-243``; keeping them
 identical is what lets a scene written against the reference load here
 unchanged. Only the parts the CUDA step consumes are listed (shapes, motion,
 collider, material, collision filter, global gravity) plus the joint/trigger
-records so documents round-trip; triggers, gravity volumes, capsules,
-cylinders and triangle meshes are rejected by the backend
+records so documents round-trip; triggers, gravity volumes and triangle
+meshes are rejected by the backend
 (:class:`omi_physics_b200.backend.UnsupportedFeature`).
 """
 from dataclasses import dataclass, field
@@ -57,8 +57,15 @@ class Shape:
 
     @classmethod
     def capsule(cls, height: float = 1.0, radius: float = 0.5) -> 'Shape':
-        """Capsule (accepted by the schema, rejected by the CUDA backend)."""
+        """Capsule: ``height`` is the cylindrical mid-section length."""
         return cls(type='capsule', height=float(height), radiusBottom=float(radius),
+                   radiusTop=float(radius))
+
+    @classmethod
+    def cylinder(cls, height: float = 2.0, radius: float = 0.5) -> 'Shape':
+        """Cylinder of total length ``height``; collided as a capsule of that
+        mid-section length, as the reference does (body.py:226-228)."""
+        return cls(type='cylinder', height=float(height), radiusBottom=float(radius),
                    radiusTop=float(radius))
 
 

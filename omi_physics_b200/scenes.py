@@ -13,6 +13,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``convex_pile``  50/25/25 box/sphere/convex in a walled 100x100 m arena
   * ``serving_mix``  request stream of debris worlds, N log-uniform in [16, 2048]
   * ``joint_chain``  pinned chain of 0.2x0.2x1 m links plus loose boxes
+  * ``capsule_pile`` capsules / cylinders / boxes / spheres in a walled arena
 """
 import math
 from types import SimpleNamespace
@@ -166,6 +167,64 @@ def convex_pile(api=None, backend=None, n: int = 32768, seed: int = 0, iteration
     return w, dict(dt=1.0 / 120.0, steps=300, name='convex%d' % n)
 
 
+def capsule_pile(api=None, backend=None, n: int = 4096, seed: int = 0, iterations: int = 8,
+                 arena: float = 40.0, height: float = 20.0):
+    """Capsules, cylinders, boxes and spheres (30/20/30/20) in a walled arena.
+
+    Capsule and cylinder pairs go through GJK/EPA (a cylinder is collided as a
+    capsule of its length, as the reference does).
+    """
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    floor = w.add_shape(m.Shape.box((arena, 1.0, arena)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=floor, physicsMaterial=gmat),
+               position=(0.0, -0.5, 0.0))
+    half = arena / 2.0
+    wall_x = w.add_shape(m.Shape.box((1.0, 10.0, arena)))
+    wall_z = w.add_shape(m.Shape.box((arena, 10.0, 1.0)))
+    for sx in (-1.0, 1.0):
+        w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=wall_x, physicsMaterial=gmat),
+                   position=(sx * (half + 0.5), 5.0, 0.0))
+    for sz in (-1.0, 1.0):
+        w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=wall_z, physicsMaterial=gmat),
+                   position=(0.0, 5.0, sz * (half + 0.5)))
+    u = rng.random(n)
+    sizes = rng.uniform(0.5, 1.5, size=(n, 3))
+    radii = rng.uniform(0.2, 0.5, size=n)
+    lengths = rng.uniform(0.4, 1.6, size=n)
+    lim = half - 2.0
+    pos = rng.uniform((-lim, 1.0, -lim), (lim, 1.0 + height, lim), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    mus = rng.uniform(0.3, 0.8, size=n)
+    for i in range(n):
+        mat = w.add_material(m.Material(staticFriction=float(mus[i]),
+                                         dynamicFriction=float(mus[i])))
+        r, h = float(radii[i]), float(lengths[i])
+        if u[i] < 0.3:
+            shape = w.add_shape(m.Shape.capsule(h, r))
+            mass = 1000.0 * (math.pi * r * r * h + (4.0 / 3.0) * math.pi * r ** 3)
+        elif u[i] < 0.5:
+            shape = w.add_shape(m.Shape.cylinder(h, r))
+            mass = 1000.0 * math.pi * r * r * h
+        elif u[i] < 0.8:
+            sz = tuple(float(x) for x in sizes[i])
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        else:
+            shape = w.add_shape(m.Shape.sphere(r + 0.1))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * (r + 0.1) ** 3
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass),
+                   m.Collider(shape=shape, physicsMaterial=mat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='capsules%d' % n)
+
+
 def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
                 motor_frac: float = 0.1, iterations: int = 12):
     """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
@@ -268,6 +327,8 @@ GOLDEN_SCENES = {
                                                          height=6.0),
     'chain': lambda api=None, backend=None: joint_chain(api, backend, links=12, loose=16, seed=2),
     'spheres': lambda api=None, backend=None: feature_mix(api, backend),
+    'capsules': lambda api=None, backend=None: capsule_pile(api, backend, n=96, seed=7, arena=8.0,
+                                                           height=6.0),
 }
 
 

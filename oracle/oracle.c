@@ -161,6 +161,17 @@ static void refit_half(const OrWorld *w, int i, double *half) {
     }
 }
 
+/* CapsuleProxy segment ends (body.py:84-91): axis = R @ (0, 1, 0),
+ * p0 = center - axis * half_height, p1 = center + axis * half_height */
+static void capsule_ends(const double *center, const double *R, double hh, double *p0, double *p1) {
+    static const double y[3] = {0.0, 1.0, 0.0};
+    for (int c = 0; c < 3; c++) {
+        double a = gemv_row(&R[c * 3], y) * hh;
+        p0[c] = center[c] - a;
+        p1[c] = center[c] + a;
+    }
+}
+
 /* ConvexProxy world points (body.py:111-119): local @ R.T + center */
 static void convex_world_points(const OrWorld *w, int si, const double *center,
                                 const double *R, double *out) {
@@ -190,6 +201,19 @@ void or_refit(OrWorld *w) {
         }
         if (kind == 0) {
             for (int c = 0; c < 3; c++) w->aabb_min[i * 3 + c] = w->aabb_max[i * 3 + c] = pos[c];
+        } else if (kind == 3 && w->shape_type[w->collider_shape[i]] == OR_SHAPE_CAPSULE) {
+            /* CapsuleProxy.aabb (body.py:84-98) through world_aabb: segment
+             * ends min/max -+ radius, then the refit margin */
+            int si = w->collider_shape[i];
+            double p0[3], p1[3];
+            capsule_ends(pos, R, 0.5 * w->shape_size[si * 3 + 1], p0, p1);
+            const double r = w->shape_radius[si];
+            for (int c = 0; c < 3; c++) {
+                double lo = p0[c] < p1[c] ? p0[c] : p1[c];
+                double hi = p0[c] > p1[c] ? p0[c] : p1[c];
+                w->aabb_min[i * 3 + c] = (lo - r) - margin;
+                w->aabb_max[i * 3 + c] = (hi + r) + margin;
+            }
         } else if (kind == 3) {
             int si = w->collider_shape[i];
             int cnt = w->shape_pt_cnt[si];
@@ -548,8 +572,9 @@ int or_sphere_box(const double *cs, double rs, const double *cb, const double *R
 /* GJK / EPA on support proxies (gjk.py, body.py:33-132)               */
 /* ------------------------------------------------------------------ */
 typedef struct {
-    int kind;             /* 1 sphere, 2 box, 3 convex */
+    int kind;             /* 1 sphere, 2 box, 3 convex, 4 capsule */
     double center[3], R[9], half[3], radius;
+    double p0[3], p1[3];  /* capsule segment ends */
     const double *world;  /* convex world points */
     int m;
 } Proxy;
@@ -570,6 +595,11 @@ static void proxy_support(const Proxy *p, const double *d, double *out) {
             s[j] = sg * p->half[j];
         }
         for (int c = 0; c < 3; c++) out[c] = p->center[c] + gemv_row(&p->R[c * 3], s);
+    } else if (p->kind == OR_SHAPE_CAPSULE) {   /* body.py:100-104 */
+        const double *end = dot_blas(p->p0, d) > dot_blas(p->p1, d) ? p->p0 : p->p1;
+        double u[3];
+        normalize3(d, u);
+        for (int c = 0; c < 3; c++) out[c] = end[c] + p->radius * u[c];
     } else {                                    /* body.py:125-128 */
         int best = 0;
         double bv = gemv_row(&p->world[0], d);
@@ -859,7 +889,8 @@ static int collide_convex(const Proxy *A, const Proxy *B, double *normal, double
 }
 
 /* Test hook: gjk.collide_convex on two proxies given as plain arrays.
- * kind 1 sphere (r), 2 box (half), 3 convex (m local points). */
+ * kind 1 sphere (r), 2 box (half), 3 convex (m local points),
+ * 4 capsule (r, half[1] = half height). */
 int or_collide_convex(int ka, const double *ca, const double *qa, const double *ha, double ra,
                       const double *pa, int ma, int kb, const double *cb, const double *qb,
                       const double *hb, double rb, const double *pb, int mb, double *normal,
@@ -879,6 +910,7 @@ int or_collide_convex(int ka, const double *ca, const double *qa, const double *
         or_quat_to_matrix(qs[e], p->R);
         for (int c = 0; c < 3; c++) { p->center[c] = cs[e][c]; p->half[c] = hs[e][c]; }
         p->radius = rs[e];
+        if (ks[e] == OR_SHAPE_CAPSULE) capsule_ends(p->center, p->R, p->half[1], p->p0, p->p1);
         p->m = ms[e];
         for (int i = 0; i < ms[e]; i++)
             for (int c = 0; c < 3; c++)
@@ -900,6 +932,9 @@ static void make_proxy(const OrWorld *w, int i, Proxy *p, double *scratch) {
         p->radius = w->shape_radius[si];
     } else if (t == OR_SHAPE_BOX) {
         for (int c = 0; c < 3; c++) p->half[c] = 0.5 * w->shape_size[si * 3 + c];
+    } else if (t == OR_SHAPE_CAPSULE) {         /* make_proxy (body.py:224-228) */
+        p->radius = w->shape_radius[si];
+        capsule_ends(p->center, p->R, 0.5 * w->shape_size[si * 3 + 1], p->p0, p->p1);
     } else {
         p->m = w->shape_pt_cnt[si];
         convex_world_points(w, si, p->center, p->R, scratch);
@@ -1610,4 +1645,179 @@ void or_free(OrWorld *w) {
         pp = &(*pp)->next;
     }
     (void)g_mat_w;
+}
+
+/* ------------------------------------------------------------------ */
+/* capsule against a batch of triangles (_collide_native.pyx:347-574, */
+/* the compiled form of collide.py:309-382)                            */
+/* ------------------------------------------------------------------ */
+static inline double dot3_seq(const double *a, const double *b) {
+    /* _dot3 (_collide_native.pyx:16-17): left to right */
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+/* closest point on triangle abc to p, Ericson's Voronoi regions in the
+ * order _closest_on_tri tests them (_collide_native.pyx:364-410) */
+static void tri_closest(const double *p, const double *a, const double *b, const double *c,
+                        double *out) {
+    double ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int m = 0; m < 3; m++) { ab[m] = b[m] - a[m]; ac[m] = c[m] - a[m]; ap[m] = p[m] - a[m]; }
+    const double d1 = dot3_seq(ab, ap), d2 = dot3_seq(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) { for (int m = 0; m < 3; m++) out[m] = a[m]; return; }
+    for (int m = 0; m < 3; m++) bp[m] = p[m] - b[m];
+    const double d3 = dot3_seq(ab, bp), d4 = dot3_seq(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) { for (int m = 0; m < 3; m++) out[m] = b[m]; return; }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double v = d1 / (d1 - d3);
+        for (int m = 0; m < 3; m++) out[m] = a[m] + v * ab[m];
+        return;
+    }
+    for (int m = 0; m < 3; m++) cp[m] = p[m] - c[m];
+    const double d5 = dot3_seq(ab, cp), d6 = dot3_seq(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) { for (int m = 0; m < 3; m++) out[m] = c[m]; return; }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double w = d2 / (d2 - d6);
+        for (int m = 0; m < 3; m++) out[m] = a[m] + w * ac[m];
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int m = 0; m < 3; m++) out[m] = b[m] + w * (c[m] - b[m]);
+        return;
+    }
+    const double inv = 1.0 / (va + vb + vc);
+    const double v = vb * inv, w = vc * inv;
+    for (int m = 0; m < 3; m++) out[m] = a[m] + ab[m] * v + ac[m] * w;
+}
+
+static inline double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+/* closest points of segments p1q1 and p2q2 (_collide_native.pyx:413-451) */
+static void seg_closest(const double *p1, const double *q1, const double *p2, const double *q2,
+                        double *o1, double *o2) {
+    double d1[3], d2[3], r[3], s, t;
+    for (int m = 0; m < 3; m++) { d1[m] = q1[m] - p1[m]; d2[m] = q2[m] - p2[m]; r[m] = p1[m] - p2[m]; }
+    const double aa = dot3_seq(d1, d1), e = dot3_seq(d2, d2), f = dot3_seq(d2, r);
+    if (aa <= EPS_COLLIDE && e <= EPS_COLLIDE) {
+        for (int m = 0; m < 3; m++) { o1[m] = p1[m]; o2[m] = p2[m]; }
+        return;
+    }
+    if (aa <= EPS_COLLIDE) {
+        s = 0.0;
+        t = clamp01(f / e);
+    } else {
+        const double cc = dot3_seq(d1, r);
+        if (e <= EPS_COLLIDE) {
+            t = 0.0;
+            s = clamp01(-cc / aa);
+        } else {
+            const double bb = dot3_seq(d1, d2);
+            const double den = aa * e - bb * bb;
+            s = den > EPS_COLLIDE ? clamp01((bb * f - cc * e) / den) : 0.0;
+            t = (bb * s + f) / e;
+            if (t < 0.0) {
+                t = 0.0;
+                s = clamp01(-cc / aa);
+            } else if (t > 1.0) {
+                t = 1.0;
+                s = clamp01((bb - cc) / aa);
+            }
+        }
+    }
+    for (int m = 0; m < 3; m++) { o1[m] = p1[m] + d1[m] * s; o2[m] = p2[m] + d2[m] * t; }
+}
+
+/* one triangle; returns 1 on contact (point on the triangle, normal from the
+ * triangle toward the capsule, depth) */
+static int capsule_triangle_one(const double *c0, const double *c1, const double *centre, double radius,
+                                const double *v0, const double *v1, const double *v2,
+                                double *point, double *normal, double *depth) {
+    double e1[3], e2[3], face[3], fn[3], tp[3];
+    const double *ends[2] = {c0, c1};
+    for (int m = 0; m < 3; m++) { e1[m] = v1[m] - v0[m]; e2[m] = v2[m] - v0[m]; }
+    face[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    face[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    face[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    const double face_len = sqrt(dot3_seq(face, face));
+    /* over the face: pushed back to the side the capsule's centre is on,
+     * by the deepest cap end whose foot lies on the triangle */
+    if (face_len > EPS_COLLIDE) {
+        for (int m = 0; m < 3; m++) fn[m] = face[m] / face_len;
+        double g[3] = {centre[0] - v0[0], centre[1] - v0[1], centre[2] - v0[2]};
+        if (fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2] < 0.0)
+            for (int m = 0; m < 3; m++) fn[m] = -fn[m];
+        int found = 0;
+        double best = -1e300, bp[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 2; k++) {
+            const double *sp = ends[k];
+            for (int m = 0; m < 3; m++) g[m] = sp[m] - v0[m];
+            const double h = fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2];
+            double foot[3];
+            for (int m = 0; m < 3; m++) foot[m] = sp[m] - fn[m] * h;
+            tri_closest(sp, v0, v1, v2, tp);
+            for (int m = 0; m < 3; m++) g[m] = foot[m] - tp[m];
+            if (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] > EPS_COLLIDE * EPS_COLLIDE) continue;
+            const double reach = radius - h;
+            if (reach > 0.0 && reach > best) {
+                best = reach;
+                found = 1;
+                for (int m = 0; m < 3; m++) bp[m] = tp[m];
+            }
+        }
+        if (found) {
+            *depth = best;
+            for (int m = 0; m < 3; m++) { point[m] = bp[m]; normal[m] = fn[m]; }
+            return 1;
+        }
+    }
+    /* off the rim: nearest of the cap ends to the triangle and of the axis
+     * to the three edges, first strict minimum */
+    double best_d2 = 1e300, bsp[3] = {0.0, 0.0, 0.0}, btp[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < 2; k++) {
+        const double *sp = ends[k];
+        tri_closest(sp, v0, v1, v2, tp);
+        const double gx = sp[0] - tp[0], gy = sp[1] - tp[1], gz = sp[2] - tp[2];
+        const double d2 = gx * gx + gy * gy + gz * gz;
+        if (d2 < best_d2) {
+            best_d2 = d2;
+            for (int m = 0; m < 3; m++) { bsp[m] = sp[m]; btp[m] = tp[m]; }
+        }
+    }
+    const double *ea[3] = {v0, v1, v2}, *eb[3] = {v1, v2, v0};
+    for (int k = 0; k < 3; k++) {
+        double ax[3], ed[3];
+        seg_closest(c0, c1, ea[k], eb[k], ax, ed);
+        const double gx = ax[0] - ed[0], gy = ax[1] - ed[1], gz = ax[2] - ed[2];
+        const double d2 = gx * gx + gy * gy + gz * gz;
+        if (d2 < best_d2) {
+            best_d2 = d2;
+            for (int m = 0; m < 3; m++) { bsp[m] = ax[m]; btp[m] = ed[m]; }
+        }
+    }
+    if (best_d2 >= radius * radius) return 0;
+    const double dist = sqrt(best_d2);
+    if (dist > EPS_COLLIDE) {
+        for (int m = 0; m < 3; m++) normal[m] = (bsp[m] - btp[m]) / dist;
+    } else if (face_len > EPS_COLLIDE) {
+        for (int m = 0; m < 3; m++) normal[m] = face[m] / face_len;
+    } else {
+        normal[0] = normal[1] = normal[2] = 0.0;
+    }
+    *depth = radius - dist;
+    for (int m = 0; m < 3; m++) point[m] = btp[m];
+    return 1;
+}
+
+void or_capsule_triangles(const double *p0, const double *p1, double radius, const double *verts,
+                          int64_t n, uint8_t *hit, double *points, double *normals, double *depths) {
+    double centre[3];
+    for (int m = 0; m < 3; m++) centre[m] = (p0[m] + p1[m]) * 0.5;
+    for (int64_t i = 0; i < n; i++) {
+        const double *t = &verts[i * 9];
+        hit[i] = (uint8_t)capsule_triangle_one(p0, p1, centre, radius, t, t + 3, t + 6, &points[i * 3],
+                                               &normals[i * 3], &depths[i]);
+    }
 }

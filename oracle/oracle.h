@@ -23,7 +23,9 @@ extern "C" {
 #endif
 
 /* shape types */
-enum { OR_SHAPE_SPHERE = 1, OR_SHAPE_BOX = 2, OR_SHAPE_CONVEX = 3 };
+/* capsule also stands for the reference's cylinder, which it collides as a
+ * capsule (body.py:224-228); shape_radius = radiusBottom, shape_size[1] = height */
+enum { OR_SHAPE_SPHERE = 1, OR_SHAPE_BOX = 2, OR_SHAPE_CONVEX = 3, OR_SHAPE_CAPSULE = 4 };
 /* combine modes (model.py:231-243) */
 enum { OR_AVERAGE = 0, OR_MINIMUM = 1, OR_MAXIMUM = 2, OR_MULTIPLY = 3 };
 /* joint types (joints.py) */
@@ -105,6 +107,13 @@ int or_sphere_sphere(const double *ca, double ra, const double *cb, double rb,
 int or_sphere_box(const double *cs, double rs, const double *cb, const double *Rb,
                   const double *hb, double *normal, double *pts, double *depths);
 void or_quat_to_matrix(const double *q, double *R);   /* mathutil.py:59-76 */
+
+/* capsule_triangles (_collide_native.pyx:454-574): the capsule segment
+ * p0-p1 with radius against n triangles verts (n,3,3). hit[i] is written for
+ * every triangle; points/normals/depths only where hit[i] = 1. */
+void or_capsule_triangles(const double *p0, const double *p1, double radius,
+                          const double *verts, int64_t n, uint8_t *hit,
+                          double *points, double *normals, double *depths);
 
 #ifdef __cplusplus
 }

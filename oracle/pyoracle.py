@@ -91,6 +91,8 @@ def lib():
         L.or_sphere_box.restype = C.c_int
         L.or_quat_to_matrix.argtypes = [D, D]
         L.or_quat_to_matrix.restype = None
+        L.or_capsule_triangles.argtypes = [D, D, C.c_double, D, C.c_int64, U8, D, D, D]
+        L.or_capsule_triangles.restype = None
         _LIB = L
     return _LIB
 
@@ -99,7 +101,8 @@ def _ptr(a, t):
     return a.ctypes.data_as(t)
 
 
-SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3}
+# a cylinder is collided as a capsule by the reference (body.py:224-228)
+SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4}
 COMBINE = {'average': 0, 'minimum': 1, 'maximum': 2, 'multiply': 3}
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
@@ -164,8 +167,12 @@ class OracleWorld:
                 stype[s] = 0
                 continue
             stype[s] = SHAPE_CODES[sh.type]
-            srad[s] = sh.radius
-            ssize[s] = np.asarray(sh.size, dtype='d')
+            if stype[s] == 4:
+                srad[s] = sh.radiusBottom
+                ssize[s] = (0.0, float(sh.height), 0.0)
+            else:
+                srad[s] = sh.radius
+                ssize[s] = np.asarray(sh.size, dtype='d')
             if sh.type == 'convex':
                 p = np.asarray(sh.points, dtype='d').reshape(-1, 3)
                 poff[s] = total
@@ -367,6 +374,24 @@ _SCALARS = ('n', 'n_shapes', 'n_materials', 'n_pair_friction', 'n_filters', 'n_j
 _ARRAYS = {name: t for name, t in OrWorldC._fields_ if t in (D, I, U8)}
 _OUTPUTS = ('pairs', 'solid', 'c_a', 'c_b', 'c_pt', 'c_n', 'c_depth', 'c_imp', 'cache_a',
             'cache_b', 'cache_pt', 'cache_imp')
+
+
+def capsule_triangles(p0, p1, radius, verts):
+    """``or_capsule_triangles`` with the reference's ``capsule_triangle_batch``
+    return convention (collide.py:438-462): ``(hit, points, normals, depths)``,
+    zeros where there is no hit."""
+    verts = np.ascontiguousarray(verts, dtype='d').reshape(-1, 3, 3)
+    n = len(verts)
+    hit = np.zeros(n, np.uint8)
+    points = np.zeros((n, 3))
+    normals = np.zeros((n, 3))
+    depths = np.zeros(n)
+    a = np.ascontiguousarray(p0, dtype='d')
+    b = np.ascontiguousarray(p1, dtype='d')
+    if n:
+        lib().or_capsule_triangles(_ptr(a, D), _ptr(b, D), float(radius), _ptr(verts, D), n,
+                                   _ptr(hit, U8), _ptr(points, D), _ptr(normals, D), _ptr(depths, D))
+    return hit.astype(bool), points, normals, depths
 
 
 def to_arrays(ow):

@@ -7,6 +7,8 @@
   world is larger than every shared-memory stage buffer, so it runs the
   global-memory forms of the sort, the sweep links, the sweep itself and the
   island pass;
+* capsule pile, 4096 bodies (30% capsules, 20% cylinders, the rest boxes and
+  spheres): 120 steps, compared bit for bit every 40 steps;
 * batched joint chains (point joints, motors, loose boxes; 1/240 s, 12 contact
   and 12 joint iterations): 8 worlds of uneven sizes in one batch, each within
   1e-6 m / 1e-6 of the oracle after 60 steps (point joints go through an
@@ -66,6 +68,14 @@ def test_convex_pile_32768_full_size():
     w, meta = scenes.convex_pile(n=32768, seed=0)
     b = _run_exact(w, meta['dt'], 20, 5, 'convex32768')
     assert b.counts()[1][0] > 10000
+
+
+def test_capsule_pile_4096_full_size():
+    """4096 capsules / cylinders / boxes / spheres: every capsule pair through
+    GJK/EPA, 120 steps compared bit for bit every 40."""
+    w, meta = scenes.capsule_pile(n=4096, seed=0)
+    b = _run_exact(w, meta['dt'], 120, 40, 'capsules4096')
+    assert b.counts()[1][0] > 1000
 
 
 def test_batched_joint_chains():

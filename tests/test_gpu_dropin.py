@@ -32,7 +32,8 @@ def _ref_api():
     return SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=model, joints=joints)
 
 
-@pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60)])
+@pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60),
+                                         ('capsules', 30)])
 def test_reference_world_steps_on_cuda_backend(scene, steps):
     from omi_physics_b200.backend import CudaBackend
     api = _ref_api()

@@ -3,7 +3,7 @@
 (1) Golden checkpoints: the reference's own one-step inputs (state, joint
 state, warm-start cache) replayed on the B200 must give the reference's
 pairs, contacts, impulses, poses and sleep flags — bit for bit on the
-box/sphere/convex scenes (the kernels keep the reference's arithmetic order
+box/sphere/convex/capsule scenes (the kernels keep the reference's arithmetic order
 and are built with --fmad=false), within 1e-12 relative on the joint scene
 (the reference solves point joints with LAPACK).
 (2) Trajectories against the oracle, every step, at sizes the oracle runs in
@@ -19,7 +19,7 @@ from util import assert_close, world_at_checkpoint
 
 pytestmark = pytest.mark.gpu
 
-EXACT = {'pyramid', 'debris', 'convex', 'spheres'}
+EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules'}
 
 
 @pytest.mark.parametrize('scene', SCENES)
@@ -75,6 +75,7 @@ def _island_sets(labels):
     ('debris512', lambda: scenes.debris(n=512, seed=1, extent=8.0, height=12.0, ground=30.0), 150),
     ('convex160', lambda: scenes.convex_pile(n=160, seed=2, arena=10.0, height=8.0), 150),
     ('feature_mix', lambda: scenes.feature_mix(), 120),
+    ('capsules256', lambda: scenes.capsule_pile(n=256, seed=3, arena=12.0, height=8.0), 150),
 ])
 def test_trajectory_matches_oracle_every_step(name, builder, steps):
     w, meta = builder()

@@ -50,8 +50,9 @@ def test_pack_two_worlds_offsets_and_remaps():
 def test_unsupported_features_raise():
     from omi_physics_b200 import model
     w, _ = scenes.GOLDEN_SCENES['pyramid']()
-    cap = w.add_shape(model.Shape.capsule(1.0, 0.3))
-    w.add_body(model.Motion(type=model.DYNAMIC), model.Collider(shape=cap), position=(0, 5, 0))
+    pts = np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1]], dtype='d')
+    mesh = w.add_shape(model.Shape(type='trimesh', points=pts, indices=np.array([[0, 1, 2]], 'i')))
+    w.add_body(model.Motion(type=model.STATIC), model.Collider(shape=mesh), position=(0, 5, 0))
     with pytest.raises(UnsupportedFeature):
         check_supported(w)
     with pytest.raises(UnsupportedFeature):

@@ -13,7 +13,7 @@ import pytest
 import pyoracle
 from golden_util import SCENES, checkpoint, checkpoints, load
 
-EXACT = ('pyramid', 'debris', 'convex', 'spheres')
+EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules')
 
 
 def _close(a, b, exact):
@@ -46,7 +46,8 @@ def test_oracle_matches_reference_checkpoints(scene):
 
 
 def test_golden_scenes_exercise_every_narrowphase_route():
-    """The fixtures cover box-box, sphere-sphere, sphere-box and GJK/EPA pairs."""
+    """The fixtures cover box-box, sphere-sphere, sphere-box and GJK/EPA pairs
+    (convex hulls and capsules / cylinders)."""
     seen = set()
     for scene in SCENES:
         data = load(scene)
@@ -58,3 +59,4 @@ def test_golden_scenes_exercise_every_narrowphase_route():
                 seen.add(tuple(sorted((int(kinds[a]), int(kinds[b])))))
     assert {(2, 2), (1, 1), (1, 2)} <= seen
     assert any(3 in k for k in seen)
+    assert {(1, 4), (2, 4), (4, 4)} <= seen
