@@ -5,9 +5,8 @@ reference defines them in ``src/omi_physics/model.py:33-243``; keeping them
 identical is what lets a scene written against the reference load here
 unchanged. Only the parts the CUDA step consumes are listed (shapes, motion,
 collider, material, collision filter, global gravity) plus the joint/trigger
-records so documents round-trip; triggers, gravity volumes and triangle
-meshes are rejected by the backend
-(:class:`omi_physics_b200.backend.UnsupportedFeature`).
+records so documents round-trip; triangle meshes are rejected by the
+backend (:class:`omi_physics_b200.backend.UnsupportedFeature`).
 """
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -95,7 +94,8 @@ class Collider:
 
 @dataclass
 class Trigger:
-    """``OMI_physics_body.trigger`` (model.py:113-117); rejected by the backend."""
+    """``OMI_physics_body.trigger`` (model.py:113-117): a sensor shape that
+    reports overlaps (enter / stay / exit events) and takes no impulse."""
     shape: int = -1
     collisionFilter: int = -1
 
@@ -138,7 +138,7 @@ POINT = 'point'
 
 @dataclass
 class Gravity:
-    """Global uniform gravity (model.py:163-178)."""
+    """Global gravity, or the field of a gravity volume (model.py:163-178)."""
     type: str = DIRECTIONAL
     gravity: float = 9.81
     direction: tuple = (0.0, -1.0, 0.0)

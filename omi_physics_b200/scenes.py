@@ -14,6 +14,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``serving_mix``  request stream of debris worlds, N log-uniform in [16, 2048]
   * ``joint_chain``  pinned chain of 0.2x0.2x1 m links plus loose boxes
   * ``capsule_pile`` capsules / cylinders / boxes / spheres in a walled arena
+  * ``zones``        debris through trigger sensors and gravity volumes
 """
 import math
 from types import SimpleNamespace
@@ -24,9 +25,9 @@ import numpy as np
 
 def default_api():
     """This package as a scene-building namespace."""
-    from . import joints, model
+    from . import gravity, joints, model
     from .world import PhysicsWorld
-    return SimpleNamespace(PhysicsWorld=PhysicsWorld, model=model, joints=joints)
+    return SimpleNamespace(PhysicsWorld=PhysicsWorld, model=model, joints=joints, gravity=gravity)
 
 
 def _quat_axis_angle(axis: np.ndarray, angle: float) -> Tuple[float, float, float, float]:
@@ -225,6 +226,71 @@ def capsule_pile(api=None, backend=None, n: int = 4096, seed: int = 0, iteration
     return w, dict(dt=1.0 / 120.0, steps=300, name='capsules%d' % n)
 
 
+def zones(api=None, backend=None, n: int = 120, seed: int = 0, iterations: int = 8,
+          extent: float = 5.0, height: float = 8.0):
+    """Debris falling through trigger sensors and gravity volumes.
+
+    Sensors: a static box zone on the ground, a static sphere zone in the air,
+    a kinematic platform carrying a collider and a sensor (its pairs are sensor
+    pairs, so it pushes nothing), and a falling dynamic body that is a sensor
+    only. Gravity volumes, in priority order: a weak everywhere wind (adds), a
+    point attractor in a sphere (adds), a sideways box column (replaces) and a
+    zero-gravity box column (stops).
+    """
+    api = api or default_api()
+    m, G = api.model, api.gravity
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    ground = w.add_shape(m.Shape.box((4.0 * extent, 1.0, 4.0 * extent)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=gmat),
+               position=(0.0, -0.5, 0.0))
+    pad = w.add_shape(m.Shape.box((4.0, 2.0, 4.0)))
+    w.add_body(m.Motion(type=m.STATIC), trigger=m.Trigger(shape=pad), position=(3.0, 1.0, 3.0))
+    ball = w.add_shape(m.Shape.sphere(2.0))
+    w.add_body(m.Motion(type=m.STATIC), trigger=m.Trigger(shape=ball), position=(-3.0, 3.0, -2.0))
+    deck = w.add_shape(m.Shape.box((1.5, 0.4, 1.5)))
+    halo = w.add_shape(m.Shape.sphere(1.2))
+    w.add_body(m.Motion(type=m.KINEMATIC, linearVelocity=(0.6, 0.0, 0.0)),
+               m.Collider(shape=deck, physicsMaterial=gmat), trigger=m.Trigger(shape=halo),
+               position=(-4.0, 0.5, 3.0))
+    probe = w.add_shape(m.Shape.capsule(0.6, 0.3))
+    w.add_body(m.Motion(type=m.DYNAMIC, mass=2.0), trigger=m.Trigger(shape=probe),
+               position=(0.5, 9.0, 0.5))
+    kinds = rng.random(n)
+    sizes = rng.uniform(0.4, 1.0, size=(n, 3))
+    radii = rng.uniform(0.2, 0.5, size=n)
+    pos = rng.uniform((-extent, 1.0, -extent), (extent, 1.0 + height, extent), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    for i in range(n):
+        if kinds[i] < 0.5:
+            sz = tuple(float(x) for x in sizes[i])
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        elif kinds[i] < 0.8:
+            r = float(radii[i])
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        else:
+            r, h = float(radii[i]), float(sizes[i, 0])
+            shape = w.add_shape(m.Shape.capsule(h, r))
+            mass = 1000.0 * (math.pi * r * r * h + (4.0 / 3.0) * math.pi * r ** 3)
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass), m.Collider(shape=shape, physicsMaterial=gmat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(gravity=0.5, direction=(0.0, 0.0, 1.0), priority=0)))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(type='point', gravity=6.0, center=(0.0, 4.0, 0.0),
+                                                   priority=1), G.SphereRegion((0.0, 4.0, 0.0), 3.0)))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(gravity=4.0, direction=(1.0, 0.2, 0.0), priority=2,
+                                                   replace=True),
+                                         G.BoxRegion((-3.0, 5.0, 3.0), (1.5, 5.0, 1.5))))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(priority=3, stop=True),
+                                         G.BoxRegion((3.0, 6.0, -3.0), (1.5, 6.0, 1.5))))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='zones%d' % n)
+
+
 def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
                 motor_frac: float = 0.1, iterations: int = 12):
     """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
@@ -329,6 +395,7 @@ GOLDEN_SCENES = {
     'spheres': lambda api=None, backend=None: feature_mix(api, backend),
     'capsules': lambda api=None, backend=None: capsule_pile(api, backend, n=96, seed=7, arena=8.0,
                                                            height=6.0),
+    'zones': lambda api=None, backend=None: zones(api, backend),
 }
 
 

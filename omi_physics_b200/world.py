@@ -348,9 +348,18 @@ class PhysicsWorld:
         return constraint
 
     def add_gravity_volume(self, volume: Any) -> Any:
-        """Register a gravity volume (the CUDA backend rejects worlds with one)."""
+        """Register a gravity zone (an :class:`omi_physics_b200.gravity.GravityVolume`); return it."""
         self.gravity_volumes.append(volume)
         return volume
+
+    def add_trigger_listener(self, fn: Any) -> None:
+        """Register ``fn(event_type, trigger_index, other_index)`` (world.py:580-582)."""
+        self.trigger_listeners.append(fn)
+
+    def dispatch_trigger(self, event_type: str, trigger_index: int, other_index: int) -> None:
+        """Notify every trigger listener of one overlap event (world.py:584-588)."""
+        for fn in self.trigger_listeners:
+            fn(event_type, trigger_index, other_index)
 
 
 class _DeviceCollisionStub:

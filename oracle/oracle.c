@@ -122,7 +122,7 @@ static void *grow(void *p, size_t elem, int32_t need, int32_t *cap) {
 }
 
 typedef struct {
-    int32_t pair_cap, solid_cap, contact_cap, cache_cap;
+    int32_t pair_cap, solid_cap, contact_cap, cache_cap, overlap_cap;
 } Caps;
 static Caps g_caps_dummy;
 
@@ -141,9 +141,22 @@ static Caps *caps_for(const OrWorld *w) {
 /* ------------------------------------------------------------------ */
 /* refit (world.py:443-508)                                            */
 /* ------------------------------------------------------------------ */
-static int refit_kind(const OrWorld *w, int i) {
+static inline int trigger_of(const OrWorld *w, int i) {
+    return w->trigger_shape ? w->trigger_shape[i] : -1;
+}
+
+/* the shape a body's AABB comes from: its collider, else its trigger
+ * (world.py:452-455, 502-505) */
+static int refit_shape(const OrWorld *w, int i) {
     int si = w->collider_shape[i];
-    if (si < 0 || si >= w->n_shapes) return 0;
+    if (si >= 0 && si < w->n_shapes) return si;
+    int ti = trigger_of(w, i);
+    return (ti >= 0 && ti < w->n_shapes) ? ti : -1;
+}
+
+static int refit_kind(const OrWorld *w, int i) {
+    int si = refit_shape(w, i);
+    if (si < 0) return 0;
     int t = w->shape_type[si];
     if (t == OR_SHAPE_SPHERE) return 1;
     if (t == OR_SHAPE_BOX) return 2;
@@ -151,9 +164,9 @@ static int refit_kind(const OrWorld *w, int i) {
 }
 
 static void refit_half(const OrWorld *w, int i, double *half) {
-    int si = w->collider_shape[i];
+    int si = refit_shape(w, i);
     half[0] = half[1] = half[2] = 0.0;
-    if (si < 0 || si >= w->n_shapes) return;
+    if (si < 0) return;
     if (w->shape_type[si] == OR_SHAPE_SPHERE) {
         half[0] = half[1] = half[2] = w->shape_radius[si];
     } else if (w->shape_type[si] == OR_SHAPE_BOX) {
@@ -201,10 +214,10 @@ void or_refit(OrWorld *w) {
         }
         if (kind == 0) {
             for (int c = 0; c < 3; c++) w->aabb_min[i * 3 + c] = w->aabb_max[i * 3 + c] = pos[c];
-        } else if (kind == 3 && w->shape_type[w->collider_shape[i]] == OR_SHAPE_CAPSULE) {
+        } else if (kind == 3 && w->shape_type[refit_shape(w, i)] == OR_SHAPE_CAPSULE) {
             /* CapsuleProxy.aabb (body.py:84-98) through world_aabb: segment
              * ends min/max -+ radius, then the refit margin */
-            int si = w->collider_shape[i];
+            int si = refit_shape(w, i);
             double p0[3], p1[3];
             capsule_ends(pos, R, 0.5 * w->shape_size[si * 3 + 1], p0, p1);
             const double r = w->shape_radius[si];
@@ -215,7 +228,7 @@ void or_refit(OrWorld *w) {
                 w->aabb_max[i * 3 + c] = (hi + r) + margin;
             }
         } else if (kind == 3) {
-            int si = w->collider_shape[i];
+            int si = refit_shape(w, i);
             int cnt = w->shape_pt_cnt[si];
             double *pts = (double *)malloc(sizeof(double) * 3 * (cnt > 0 ? cnt : 1));
             convex_world_points(w, si, pos, R, pts);
@@ -922,8 +935,8 @@ int or_collide_convex(int ka, const double *ca, const double *qa, const double *
     return r;
 }
 
-static void make_proxy(const OrWorld *w, int i, Proxy *p, double *scratch) {
-    int si = w->collider_shape[i];
+/* make_proxy (body.py:214-237) of shape si at body i's pose */
+static void make_proxy_shape(const OrWorld *w, int si, int i, Proxy *p, double *scratch) {
     int t = w->shape_type[si];
     or_quat_to_matrix(&w->q[i * 4], p->R);
     for (int c = 0; c < 3; c++) p->center[c] = w->pos[i * 3 + c];
@@ -940,6 +953,10 @@ static void make_proxy(const OrWorld *w, int i, Proxy *p, double *scratch) {
         convex_world_points(w, si, p->center, p->R, scratch);
         p->world = scratch;
     }
+}
+
+static void make_proxy(const OrWorld *w, int i, Proxy *p, double *scratch) {
+    make_proxy_shape(w, w->collider_shape[i], i, p, scratch);
 }
 
 /* ------------------------------------------------------------------ */
@@ -986,6 +1003,7 @@ static int narrowphase(OrWorld *w) {
     double *sb = (double *)malloc(sizeof(double) * 3 * maxpts);
     for (int p = 0; p < w->n_pairs; p++) {
         int i = w->pairs[p * 2], j = w->pairs[p * 2 + 1];
+        if (trigger_of(w, i) >= 0 || trigger_of(w, j) >= 0) continue;   /* trigger pairs: no contact */
         if (!(w->collider_shape[i] >= 0 && w->collider_shape[j] >= 0)) continue;
         if (!(awake_mover(w, i) || awake_mover(w, j))) continue;
         w->solid = (int32_t *)grow(w->solid, sizeof(int32_t) * 2, w->n_solid + 1, &cp->solid_cap);
@@ -1493,13 +1511,50 @@ static int solve_joints(OrWorld *w) {
 /* ------------------------------------------------------------------ */
 /* integration (backend.py:26-49, mathutil.py:32-41, 108-113)         */
 /* ------------------------------------------------------------------ */
+/* resolve_gravity with apply_volumes (world.py:386-396, gravity.py:82-108):
+ * the world's vector, then every volume containing the body's position in
+ * application order: replace sets, stop zeroes, otherwise the field adds */
+static void body_gravity(const OrWorld *w, int i, double *g) {
+    const double *pos = &w->pos[i * 3];
+    for (int c = 0; c < 3; c++) g[c] = w->g[c];
+    for (int k = 0; k < w->n_volumes; k++) {
+        const int kind = w->vol_kind[k];
+        const double *rc = &w->vol_rc[k * 3], *rr = &w->vol_rr[k * 3];
+        int inside = 1;
+        if (kind & OR_VOL_SPHERE) {                      /* gravity.py:22-25 */
+            double d[3] = {pos[0] - rc[0], pos[1] - rc[1], pos[2] - rc[2]};
+            inside = dot_blas(d, d) <= rr[0];
+        } else if (kind & OR_VOL_BOX) {                  /* gravity.py:34-37 */
+            for (int c = 0; c < 3; c++) inside &= fabs(pos[c] - rc[c]) <= rr[c];
+        }
+        if (!inside) continue;
+        if (kind & OR_VOL_STOP) {
+            g[0] = g[1] = g[2] = 0.0;
+            continue;
+        }
+        double f[3];                                     /* field_at, gravity.py:66-79 */
+        const double *fd = &w->vol_field[k * 3];
+        if (kind & OR_VOL_POINT) {
+            double d[3] = {fd[0] - pos[0], fd[1] - pos[1], fd[2] - pos[2]}, u[3];
+            normalize3(d, u);
+            for (int c = 0; c < 3; c++) f[c] = u[c] * w->vol_g[k];
+        } else {
+            for (int c = 0; c < 3; c++) f[c] = fd[c];
+        }
+        if (kind & OR_VOL_REPLACE) for (int c = 0; c < 3; c++) g[c] = f[c];
+        else for (int c = 0; c < 3; c++) g[c] = g[c] + f[c];
+    }
+}
+
 void or_integrate_forces(OrWorld *w) {
     double dt = w->dt;
     for (int i = 0; i < w->n; i++) {
         if (!(w->motion_type[i] == 2 && w->awake[i])) continue;
         double *v = &w->v[i * 3], *om = &w->w[i * 3];
         double gf = w->gravity_factor[i];
-        for (int c = 0; c < 3; c++) v[c] = v[c] + (w->g[c] * gf) * dt;
+        double g[3];
+        body_gravity(w, i, g);
+        for (int c = 0; c < 3; c++) v[c] = v[c] + (g[c] * gf) * dt;
         double ld = w->lin_damp[i] + w->default_lin_damp;
         double ad = w->ang_damp[i] + w->default_ang_damp;
         double fl = 1.0 - ld * dt;
@@ -1595,6 +1650,86 @@ static void update_sleep(OrWorld *w) {
 /* ------------------------------------------------------------------ */
 /* the step (world.py:410-430)                                         */
 /* ------------------------------------------------------------------ */
+/* ------------------------------------------------------------------ */
+/* trigger overlaps (triggers.py:24-72, world.py:662-676)              */
+/* ------------------------------------------------------------------ */
+/* collide.sphere_sphere is empty iff dist >= ra + rb (collide.py:56-66) */
+static int py_sphere_sphere_hit(const Proxy *A, const Proxy *B) {
+    double d[3] = {B->center[0] - A->center[0], B->center[1] - A->center[1], B->center[2] - A->center[2]};
+    return !(norm_blas3(d) >= A->radius + B->radius);
+}
+
+/* collide.sphere_box is empty iff the clamped distance exceeds the radius
+ * (collide.py:69-88); local = R.T @ (cs - cb), norm over the whole vector */
+static int py_sphere_box_hit(const Proxy *S, const Proxy *B) {
+    double v[3] = {S->center[0] - B->center[0], S->center[1] - B->center[1], S->center[2] - B->center[2]};
+    double delta[3];
+    for (int j = 0; j < 3; j++) {
+        double col[3] = {B->R[j], B->R[3 + j], B->R[6 + j]};
+        double l = dot_blas(col, v);
+        double cl = l > -B->half[j] ? l : -B->half[j];
+        cl = cl < B->half[j] ? cl : B->half[j];
+        delta[j] = l - cl;
+    }
+    return !(norm_blas3(delta) > S->radius);
+}
+
+/* len(collide.collide(trg, other, PA, PB)) > 0 (collide.py:251-269): the
+ * analytic routes for sphere/box pairs, GJK/EPA otherwise. box_box is
+ * non-empty exactly when its separating-axis test finds no gap; that test is
+ * taken from the compiled box_box here. */
+static int shapes_overlap(OrWorld *w, int ts, int trg, int os, int other, double *sa, double *sb) {
+    Proxy A, B;
+    make_proxy_shape(w, ts, trg, &A, sa);
+    make_proxy_shape(w, os, other, &B, sb);
+    const int ka = A.kind, kb = B.kind;
+    if (ka == OR_SHAPE_SPHERE && kb == OR_SHAPE_SPHERE) return py_sphere_sphere_hit(&A, &B);
+    if (ka == OR_SHAPE_SPHERE && kb == OR_SHAPE_BOX) return py_sphere_box_hit(&A, &B);
+    if (ka == OR_SHAPE_BOX && kb == OR_SHAPE_SPHERE) return py_sphere_box_hit(&B, &A);
+    double nrm[3], pts[12], dep[4];
+    if (ka == OR_SHAPE_BOX && kb == OR_SHAPE_BOX)
+        return or_box_box(A.center, A.R, A.half, B.center, B.R, B.half, nrm, pts, dep) > 0;
+    return collide_convex(&A, &B, nrm, pts, dep) > 0;
+}
+
+/* this step's (trigger, other) overlaps in pair order: a pair with a sensor
+ * on either body (the first body's when both have one) against the other
+ * body's collider, else its sensor (triggers.py:46-72) */
+static int trigger_overlaps(OrWorld *w) {
+    Caps *cp = caps_for(w);
+    w->n_overlaps = 0;
+    if (!w->trigger_shape) return 0;
+    int maxpts = 1;
+    for (int s = 0; s < w->n_shapes; s++)
+        if (w->shape_type[s] == OR_SHAPE_CONVEX && w->shape_pt_cnt[s] > maxpts) maxpts = w->shape_pt_cnt[s];
+    double *sa = (double *)malloc(sizeof(double) * 3 * maxpts);
+    double *sb = (double *)malloc(sizeof(double) * 3 * maxpts);
+    int rc = 0;
+    for (int p = 0; p < w->n_pairs; p++) {
+        const int i = w->pairs[p * 2], j = w->pairs[p * 2 + 1];
+        const int ti = trigger_of(w, i), tj = trigger_of(w, j);
+        if (ti < 0 && tj < 0) continue;
+        const int trg = ti >= 0 ? i : j, other = ti >= 0 ? j : i;
+        const int ts = ti >= 0 ? ti : tj;
+        int os = w->collider_shape[other];
+        if (os < 0) os = trigger_of(w, other);
+        if (os < 0) continue;
+        if (!shapes_overlap(w, ts, trg, os, other, sa, sb)) continue;
+        const int k = w->n_overlaps;
+        int32_t cap = cp->overlap_cap;
+        w->ov_trg = (int32_t *)grow(w->ov_trg, sizeof(int32_t), k + 1, &cap);
+        cap = cp->overlap_cap;
+        w->ov_other = (int32_t *)grow(w->ov_other, sizeof(int32_t), k + 1, &cap);
+        cp->overlap_cap = cap;
+        if (!w->ov_trg || !w->ov_other) { rc = -1; break; }
+        w->ov_trg[k] = trg;
+        w->ov_other[k] = other;
+        w->n_overlaps = k + 1;
+    }
+    free(sa); free(sb);
+    return rc;
+}
+
 int or_step(OrWorld *w) {
     int n = w->n;
     memcpy(w->prev_pos, w->pos, sizeof(double) * 3 * n);
@@ -1606,6 +1741,7 @@ int or_step(OrWorld *w) {
         if (or_broadphase(w)) return -1;
         if (narrowphase(w)) return -2;
         if (solve_contacts(w)) return -3;
+        if (trigger_overlaps(w)) return -5;
     }
     if (w->n_joints) { if (solve_joints(w)) return -4; }
     or_integrate_positions(w);
@@ -1635,7 +1771,9 @@ int or_set_cache(OrWorld *w, int32_t n, const int32_t *a, const int32_t *b, cons
 void or_free(OrWorld *w) {
     free(w->pairs); free(w->solid); free(w->c_a); free(w->c_b); free(w->c_pt); free(w->c_n);
     free(w->c_depth); free(w->c_imp); free(w->cache_a); free(w->cache_b); free(w->cache_pt);
-    free(w->cache_imp);
+    free(w->cache_imp); free(w->ov_trg); free(w->ov_other);
+    w->ov_trg = w->ov_other = NULL;
+    w->n_overlaps = 0;
     w->pairs = w->solid = w->c_a = w->c_b = w->cache_a = w->cache_b = NULL;
     w->c_pt = w->c_n = w->c_depth = w->c_imp = w->cache_pt = w->cache_imp = NULL;
     w->n_pairs = w->n_solid = w->n_contacts = w->cache_n = 0;

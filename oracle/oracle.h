@@ -82,7 +82,22 @@ typedef struct OrWorld {
     int32_t *c_a, *c_b;
     double *c_pt, *c_n, *c_depth, *c_imp;                /* *3, *3, 1, *3 */
     int32_t *island;                                     /* n: sleep-island label or -1 */
+    /* ---- triggers (triggers.py:17-72): sensor shape per body, -1 none;
+     *      NULL means no body has one ---- */
+    int32_t *trigger_shape;
+    /* ---- gravity volumes (gravity.py:51-108), in application order (stable
+     *      by priority): kind = OR_VOL_* flags, g = field magnitude, field =
+     *      directional acceleration or point centre (*3), rc = region centre
+     *      (*3), rr = sphere radius**2 in [0] or box half-extents (*3) ---- */
+    int32_t n_volumes;
+    int32_t *vol_kind;
+    double *vol_g, *vol_field, *vol_rc, *vol_rr;
+    /* ---- per-step trigger overlaps (trigger, other) in pair order, oracle-owned ---- */
+    int32_t n_overlaps;
+    int32_t *ov_trg, *ov_other;
 } OrWorld;
+
+enum { OR_VOL_POINT = 1, OR_VOL_SPHERE = 2, OR_VOL_BOX = 4, OR_VOL_REPLACE = 8, OR_VOL_STOP = 16 };
 
 /* One full PhysicsWorld.step(dt) (world.py:410-430). Returns 0 or <0. */
 int or_step(OrWorld *w);

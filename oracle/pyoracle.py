@@ -56,6 +56,10 @@ class OrWorldC(C.Structure):
         ('n_contacts', C.c_int32), ('c_a', I), ('c_b', I), ('c_pt', D), ('c_n', D),
         ('c_depth', D), ('c_imp', D),
         ('island', I),
+        ('trigger_shape', I),
+        ('n_volumes', C.c_int32), ('vol_kind', I), ('vol_g', D), ('vol_field', D), ('vol_rc', D),
+        ('vol_rr', D),
+        ('n_overlaps', C.c_int32), ('ov_trg', I), ('ov_other', I),
     ]
 
 
@@ -107,6 +111,44 @@ COMBINE = {'average': 0, 'minimum': 1, 'maximum': 2, 'multiply': 3}
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
 
+def _pack_volumes(volumes):
+    """The oracle's gravity-volume table (oracle.h): stable priority order
+    (gravity.py:89); a directional field precomputed with numpy exactly as
+    ``GravityVolume.field_at`` computes it (gravity.py:66-79); a sphere region's
+    ``radius ** 2`` as gravity.py:25 evaluates it."""
+    ordered = sorted(volumes, key=lambda v: v.priority)
+    m = len(ordered)
+    kind = np.zeros(max(m, 1), np.int32)
+    g, field = np.zeros(max(m, 1)), np.zeros((max(m, 1), 3))
+    rc, rr = np.zeros((max(m, 1), 3)), np.zeros((max(m, 1), 3))
+    for k, v in enumerate(ordered):
+        f = v.field
+        if f.type == 'point':
+            kind[k] |= 1
+            field[k] = np.asarray(f.center, dtype='d')
+        else:
+            d = np.asarray(f.direction, dtype='d')
+            field[k] = d / np.maximum(np.linalg.norm(d, axis=-1, keepdims=True), 1e-12) * f.gravity
+        g[k] = f.gravity
+        if f.replace:
+            kind[k] |= 8
+        elif f.stop:
+            kind[k] |= 16
+        reg = v.region
+        name = type(reg).__name__
+        if name == 'SphereRegion':
+            kind[k] |= 2
+            rc[k] = reg.center
+            rr[k, 0] = reg.radius ** 2
+        elif name == 'BoxRegion':
+            kind[k] |= 4
+            rc[k] = reg.center
+            rr[k] = reg.half
+        elif name != 'InfiniteRegion':
+            raise ValueError('region %s' % name)
+    return m, dict(vol_kind=kind, vol_g=g, vol_field=field, vol_rc=rc, vol_rr=rr)
+
+
 def _joint_kind(c):
     k = getattr(c, 'kind', None)
     if k in JOINT_CODES:
@@ -152,6 +194,12 @@ class OracleWorld:
         self._set('aabb_min', np.zeros((max(n, 1), 3)), D)
         self._set('aabb_max', np.zeros((max(n, 1), 3)), D)
         self._set('island', np.full(max(n, 1), -1, dtype=np.int32), I)
+        ts = np.ascontiguousarray(getattr(world, '_trigger_shape')[:n], dtype=np.int32).copy()
+        if n and np.any(ts >= 0):
+            self._set('trigger_shape', ts, I)
+        c.n_volumes, vols = _pack_volumes(getattr(world, 'gravity_volumes', None) or [])
+        for name, arr in vols.items():
+            self._set(name, arr, I if name == 'vol_kind' else D)
         # shapes
         shapes = world.shapes
         ns = len(shapes)
@@ -320,6 +368,13 @@ class OracleWorld:
                     depth=self._arr(self.c.c_depth, K, (K,), 'd'),
                     impulse=self._arr(self.c.c_imp, K, (K, 3), 'd'))
 
+    def overlaps(self):
+        """This step's trigger overlaps as a set of (trigger, other) body pairs."""
+        k = self.c.n_overlaps
+        t = self._arr(self.c.ov_trg, k, (k,), np.int32)
+        o = self._arr(self.c.ov_other, k, (k,), np.int32)
+        return {(int(a), int(b)) for a, b in zip(t, o)}
+
     def cache(self):
         n = self.c.cache_n
         return dict(a=self._arr(self.c.cache_a, n, (n,), np.int32),
@@ -370,10 +425,10 @@ class OracleWorld:
 _SCALARS = ('n', 'n_shapes', 'n_materials', 'n_pair_friction', 'n_filters', 'n_joints',
             'default_lin_damp', 'default_ang_damp', 'velocity_iterations', 'joint_iterations',
             'sleep_enabled', 'warm_start', 'has_collision', 'restitution_threshold', 'slop',
-            'correction', 'margin')
+            'correction', 'margin', 'n_volumes')
 _ARRAYS = {name: t for name, t in OrWorldC._fields_ if t in (D, I, U8)}
 _OUTPUTS = ('pairs', 'solid', 'c_a', 'c_b', 'c_pt', 'c_n', 'c_depth', 'c_imp', 'cache_a',
-            'cache_b', 'cache_pt', 'cache_imp')
+            'cache_b', 'cache_pt', 'cache_imp', 'ov_trg', 'ov_other')
 
 
 def capsule_triangles(p0, p1, radius, verts):
@@ -413,7 +468,8 @@ def from_arrays(d):
         if name in d and name not in _OUTPUTS:
             ow._set(name, np.ascontiguousarray(d[name]).copy(), t)
     for s in _SCALARS:
-        setattr(ow.c, s, d['s_' + s].item())
+        if 's_' + s in d:
+            setattr(ow.c, s, d['s_' + s].item())
     ow.c.g = (C.c_double * 3)(*[float(x) for x in d['g']])
     if len(d['cache_a']):
         ow.set_cache(d['cache_a'], d['cache_b'], d['cache_point'], d['cache_impulse'])

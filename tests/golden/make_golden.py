@@ -30,15 +30,21 @@ sys.path.insert(0, os.path.join(ROOT, 'oracle'))
 sys.path.insert(0, ROOT)
 
 import omi_physics as ref                       # noqa: E402  (the reference)
-from omi_physics import joints as rjoints, model as rmodel   # noqa: E402
+from omi_physics import gravity as rgravity, joints as rjoints, model as rmodel   # noqa: E402
 import pyoracle                                  # noqa: E402
 from omi_physics_b200 import scenes              # noqa: E402
 
-API = SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=rmodel, joints=rjoints)
+API = SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=rmodel, joints=rjoints, gravity=rgravity)
+EVENT_CODES = {'enter': 0, 'stay': 1, 'exit': 2}
 
 STEPS = {'pyramid': (50, (0, 3, 12, 30, 44)), 'debris': (240, (0, 90, 150, 239)),
          'convex': (180, (0, 100, 140, 179)), 'chain': (140, (0, 60, 139)),
-         'spheres': (120, (0, 60, 119)), 'capsules': (180, (0, 40, 100, 179))}
+         'spheres': (120, (0, 60, 119)), 'capsules': (180, (0, 40, 100, 179)),
+         'zones': (150, (0, 40, 90, 149))}
+
+
+def _pairs_array(pairs):
+    return np.array(sorted(pairs), dtype=np.int32).reshape(-1, 2)
 
 
 def snapshot_init(w):
@@ -150,13 +156,20 @@ def main(names=()):
             rec['pairs'] = np.array(p, dtype=np.int32).reshape(-1, 2)
             return p
         bp.pairs = recording
+        events = []
+        w.add_trigger_listener(lambda kind, t, o: events.append((EVENT_CODES[kind], t, o)))
         for s in range(steps):
             if s in checkpoints:
                 ow = pyoracle.OracleWorld.from_world(w)
                 for k, v in pyoracle.to_arrays(ow).items():
                     data['ck%d/in/%s' % (s, k)] = v
+                data['ck%d/in/overlaps_prev' % s] = _pairs_array(w._collision.triggers.overlaps)
                 rec.clear()
+            events.clear()
             w.step(dt)
+            if s in checkpoints:
+                data['ck%d/out/overlaps' % s] = _pairs_array(w._collision.triggers.overlaps)
+                data['ck%d/out/events' % s] = np.array(sorted(events), dtype=np.int32).reshape(-1, 3)
             if s in checkpoints:
                 p = 'ck%d/out/' % s
                 cs = w.contacts
