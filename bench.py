@@ -173,7 +173,7 @@ STAGE_GROUPS = {
     'refit+integrate_forces': ('refit', 'integrate_forces'),
     'broadphase': ('sort', 'pair_count', 'pair_scan', 'pair_emit'),
     'narrowphase': ('narrow', 'gjk_epa', 'contact_scan', 'contact_compact'),
-    'solve': ('wake', 'prep', 'levels', 'solve', 'cache_store'),
+    'solve': ('wake', 'prep', 'levels', 'solve', 'triggers', 'cache_store'),
     'integrate_positions_sleep': ('integrate_positions_sleep',),
 }
 

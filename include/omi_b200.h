@@ -24,7 +24,7 @@ extern "C" {
 #define OMI_OK 0
 #define OMI_E_CUDA (-1)         /* CUDA runtime error (message has details) */
 #define OMI_E_ARG (-2)          /* bad argument / size */
-#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triggers, trimesh ...) */
+#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triangle meshes ...) */
 #define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
 #define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
 #define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
@@ -100,7 +100,25 @@ typedef struct OmiScene {
     const double *j_length;
     const uint8_t *j_has_length;
     const double *j_axis, *j_target, *j_max_force, *j_accum;
+
+    /* sensors (triggers.py:17-72): a body's sensor shape (global index) or -1;
+     * NULL when no body has one. A pair with a sensor on either body makes no
+     * contact; its overlap is tested after the contact solve. */
+    const int32_t *trigger_shape;
+    /* gravity volumes (gravity.py:51-108), each world's rows in application
+     * order (stable by priority); w_vol_off NULL when there are none */
+    const int32_t *w_vol_off;       /* n_worlds+1 */
+    int32_t n_volumes;
+    const int32_t *vol_kind;        /* OMI_VOL_* flags */
+    const double *vol_g;            /* field magnitude */
+    const double *vol_field;        /* *3: a directional field's acceleration (normalize(direction) *
+                                       gravity, as field_at forms it), or a point field's centre */
+    const double *vol_rc, *vol_rr;  /* *3: region centre; radius**2 in [0] (sphere) or half-extents (box) */
 } OmiScene;
+
+/* gravity volume kind flags: point field (else directional); region sphere,
+ * box (else everywhere); replace (overrides) or stop (zeroes), else adds */
+enum { OMI_VOL_POINT = 1, OMI_VOL_SPHERE = 2, OMI_VOL_BOX = 4, OMI_VOL_REPLACE = 8, OMI_VOL_STOP = 16 };
 
 typedef struct OmiCtx OmiCtx;
 
@@ -210,6 +228,13 @@ int omi_get_contacts(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double 
                      double *normal, double *depth, double *impulse, int32_t cap);
 /* sleep-island label per body of one world (-1 = not in contact) */
 int omi_get_islands(OmiCtx *ctx, int32_t world, int32_t *labels);
+
+/* This step's sensor overlaps in `world` (TriggerSystem.overlaps after
+ * triggers.update, triggers.py:24-44): (trigger body, other body) pairs with
+ * world-local indices, sorted, at most `cap` written. Returns the count (which
+ * may exceed cap) or a negative OMI_E_*. Enter / stay / exit events are the
+ * difference between consecutive steps' sets, formed by the caller. */
+int omi_get_trigger_overlaps(OmiCtx *ctx, int32_t world, int32_t *trg, int32_t *other, int32_t cap);
 
 /* ---- capsule against triangles (the character controller's query) ----
  *

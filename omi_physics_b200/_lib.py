@@ -62,6 +62,9 @@ class OmiScene(C.Structure):
         ('j_anchor', D), ('j_anchor_b', D), ('j_local_a', D), ('j_local_b', D),
         ('j_has_local_a', U8), ('j_has_local_b', U8), ('j_length', D), ('j_has_length', U8),
         ('j_axis', D), ('j_target', D), ('j_max_force', D), ('j_accum', D),
+        ('trigger_shape', I),
+        ('w_vol_off', I), ('n_volumes', C.c_int32), ('vol_kind', I), ('vol_g', D), ('vol_field', D),
+        ('vol_rc', D), ('vol_rr', D),
     ]
 
 
@@ -110,6 +113,7 @@ PROTOTYPES = {
     'omi_profile_step': (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, I]),
     'omi_kernel_name': (C.c_char_p, [C.c_int32]),
     'omi_launch_count': (C.c_int64, [C.c_void_p]),
+    'omi_get_trigger_overlaps': (C.c_int, [C.c_void_p, C.c_int32, I, I, C.c_int32]),
     'omi_capsule_triangles': (C.c_int, [C.c_void_p, D, D, C.c_double, D, C.c_int64, U8, D, D, D]),
     'omi_capsule_triangles_batch': (C.c_int, [C.c_void_p, C.c_int32, D, I64, D,
                                               C.c_int64, U8, D, D, D]),

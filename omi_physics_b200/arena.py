@@ -14,6 +14,7 @@ import numpy as np
 
 from ._lib import D, I, U8, OmiScene, UnsupportedFeature, WF_ACTIVE, WF_COLLISION, WF_SLEEP, \
     WF_WARM, ptr
+from .gravity import pack_volumes
 from .joints import joint_kind
 from .model import COMBINE_CODES
 
@@ -57,12 +58,14 @@ def world_iterations(world) -> int:
 def check_supported(world) -> None:
     """Raise :class:`UnsupportedFeature` for anything outside the device step."""
     n = world.body_count
-    if getattr(world, 'gravity_volumes', None):
-        raise UnsupportedFeature(-3, 'gravity volumes are not supported on the CUDA path')
-    if n and np.any(np.asarray(world._trigger_shape[:n]) >= 0):
-        raise UnsupportedFeature(-3, 'trigger shapes are not supported on the CUDA path')
-    cs = np.asarray(world._collider_shape[:n])
-    used = set(int(s) for s in cs[(cs >= 0) & (cs < len(world.shapes))])
+    try:
+        pack_volumes(getattr(world, 'gravity_volumes', None) or [])
+    except (ValueError, AttributeError, TypeError) as e:
+        raise UnsupportedFeature(-3, 'gravity volume outside the device path: %s' % e)
+    used = set()
+    for col in ('_collider_shape', '_trigger_shape'):
+        cs = np.asarray(getattr(world, col)[:n])
+        used |= set(int(s) for s in cs[(cs >= 0) & (cs < len(world.shapes))])
     for s in used:
         t = world.shapes[s].type
         if t not in SHAPE_CODES:
@@ -98,8 +101,10 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                              'mat_rcomb', 'pf_a', 'pf_b', 'pf_mu', 'filter_matrix', 'j_type',
                              'j_a', 'j_b', 'j_anchor', 'j_anchor_b', 'j_local_a', 'j_local_b',
                              'j_has_local_a', 'j_has_local_b', 'j_length', 'j_has_length',
-                             'j_axis', 'j_target', 'j_max_force', 'j_accum')}
-    body_off, joint_off = [0], [0]
+                             'j_axis', 'j_target', 'j_max_force', 'j_accum', 'trigger_shape',
+                             'vol_kind', 'vol_g', 'vol_field', 'vol_rc', 'vol_rr')}
+    body_off, joint_off, vol_off = [0], [0], [0]
+    any_sensor = False
     w_g, w_dt, w_iters, w_jiters, w_flags, w_damp, w_solver = [], [], [], [], [], [], []
     w_foff, w_frows, w_pfoff, w_pfn = [], [], [], []
     nb = ns = nm = npts = nf = npf = nj = 0
@@ -122,6 +127,15 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
         cs = np.asarray(world._collider_shape[:n], np.int64)
         valid = (cs >= 0) & (cs < len(world.shapes))
         parts['shape'].append(np.where(valid, cs + ns, -1).astype(np.int32))
+        ts = np.asarray(world._trigger_shape[:n], np.int64)
+        tvalid = (ts >= 0) & (ts < len(world.shapes))
+        any_sensor |= bool(tvalid.any())
+        parts['trigger_shape'].append(np.where(tvalid, ts + ns, -1).astype(np.int32))
+        vols = pack_volumes(getattr(world, 'gravity_volumes', None) or [])
+        for key in ('kind', 'g', 'field', 'rc', 'rr'):
+            if len(vols[key]):
+                parts['vol_' + key].append(vols[key])
+        vol_off.append(vol_off[-1] + len(vols['kind']))
         cm = np.asarray(world._collider_material[:n], np.int64)
         mvalid = (cm >= 0) & (cm < len(world.materials))
         parts['material'].append(np.where(mvalid, cm + nm, -1).astype(np.int32))
@@ -288,6 +302,16 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                               ('j_target', D, 'd', None), ('j_max_force', D, 'd', None),
                               ('j_accum', D, 'd', None)):
         P.set(key, cat(key, dt, width), t)
+    if any_sensor:
+        P.set('trigger_shape', cat('trigger_shape', np.int32), I)
+    if vol_off[-1]:
+        P.set('w_vol_off', np.array(vol_off, np.int32), I)
+        s.n_volumes = vol_off[-1]
+        P.set('vol_kind', cat('vol_kind', np.int32), I)
+        P.set('vol_g', cat('vol_g', 'd'), D)
+        for key in ('vol_field', 'vol_rc', 'vol_rr'):
+            P.set(key, cat(key, 'd', 3), D)
+    P.has_sensors = any_sensor
     P.body_off = body_off
     P.joint_off = joint_off
     P.n_bodies = nb
@@ -305,7 +329,10 @@ def static_signature(world) -> tuple:
                  '_angular_damping', '_quadratic_drag', '_motion_type', '_collider_shape',
                  '_collider_material', '_collider_filter', '_trigger_shape'):
         crc = zlib.crc32(np.ascontiguousarray(getattr(world, name)[:n]).view(np.uint8), crc)
+    vols = pack_volumes(getattr(world, 'gravity_volumes', None) or [])
+    for key in ('kind', 'g', 'field', 'rc', 'rr'):
+        crc = zlib.crc32(np.ascontiguousarray(vols[key]).view(np.uint8), crc)
     return (n, len(world.shapes), len(world.materials), len(world.filters),
             len(world.joint_constraints), tuple(sorted(world.pair_friction.items())),
             tuple(id(c) for c in world.joint_constraints), world.gravity.gravity,
-            tuple(world.gravity.direction), crc)
+            tuple(world.gravity.direction), len(vols['kind']), crc)

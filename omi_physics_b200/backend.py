@@ -60,12 +60,23 @@ class _DevicePairs:
         return [tuple(map(int, p)) for p in b.pairs(0)] if b is not None else []
 
 
+class _SensorState:
+    """``triggers`` stand-in (triggers.py:17-44): the last step's overlaps."""
+
+    def __init__(self, original: Any):
+        self.overlaps = set(getattr(getattr(original, 'triggers', None), 'overlaps', set()))
+
+
 class DeviceCollisionStages:
     """Replaces ``world._collision`` (world.py:642-676) once the backend attaches.
 
     ``solver`` keeps the original solver object so iteration counts and
     solver parameters set on it keep their effect; the contacts and the
-    warm-start cache live on the device.
+    warm-start cache live on the device. Sensor overlaps are tested on the
+    device after the contact solve, as the reference tests them; ``run``
+    dispatches the step's enter / stay / exit events to the world's trigger
+    listeners (world.py:674-676), sorted within each kind, once the step's
+    state is back on the host.
     """
 
     def __init__(self, backend: 'CudaBackend', original: Any):
@@ -73,11 +84,22 @@ class DeviceCollisionStages:
         self.solver = getattr(original, 'solver', original)
         self.broadphase = _DevicePairs(backend)
         self.narrowphase = None
+        self.triggers = _SensorState(original)
         self.contacts: Any = []
 
     def run(self, world, dt: float) -> None:
         """The device already ran this stage inside ``integrate_forces``."""
         self.contacts = world.contacts = self.backend.last_contacts()
+        b = self.backend._batch
+        if b is None or not (b.has_sensors or self.triggers.overlaps):
+            return
+        new = b.trigger_overlaps(0)
+        old = self.triggers.overlaps
+        events = ([('enter',) + p for p in sorted(new - old)] + [('stay',) + p for p in sorted(new & old)] +
+                  [('exit',) + p for p in sorted(old - new)])
+        self.triggers.overlaps = new
+        for ev in events:
+            world.dispatch_trigger(*ev)
 
 
 def _noop(dt: float) -> None:

@@ -42,13 +42,56 @@ class WorldBatch:
         self.ctx.call('load', C.byref(self.packed.scene))
         self.offsets = self.packed.body_off
         self.joint_offsets = self.packed.joint_off
+        # sensor overlaps of the last step per world and the enter / stay /
+        # exit events of every step since the last take_events()
+        self.has_sensors = bool(getattr(self.packed, 'has_sensors', False))
+        self.overlaps = [set() for _ in self.worlds]
+        self.events = [[] for _ in self.worlds]
 
     # -- stepping -----------------------------------------------------------
     def step(self, n: int = 1) -> None:
-        """``n`` steps of every active world (capacity regrowth handled inside)."""
-        self.ctx.call('step', int(n))
+        """``n`` steps of every active world (capacity regrowth handled inside).
+        With sensors present the steps run one at a time, so each step's
+        trigger events are recorded (:meth:`take_events`)."""
+        if self.has_sensors:
+            for _ in range(int(n)):
+                self.ctx.call('step', 1)
+                self._record_events()
+        else:
+            self.ctx.call('step', int(n))
         for w, dt in zip(self.worlds, self.dts):
             w.time += n * dt
+
+    def trigger_overlaps(self, i: int) -> set:
+        """The last step's (trigger, other) overlaps of world ``i`` (world-local
+        indices), as the reference's ``TriggerSystem.overlaps`` holds them."""
+        if not self.has_sensors:
+            return set()
+        cap = 256
+        while True:
+            t = np.zeros(cap, np.int32)
+            o = np.zeros(cap, np.int32)
+            m = self.ctx.call('get_trigger_overlaps', i, ptr(t, I), ptr(o, I), cap)
+            if m <= cap:
+                return {(int(a), int(b)) for a, b in zip(t[:m], o[:m])}
+            cap = m
+
+    def _record_events(self) -> None:
+        """Enter / stay / exit of one step (triggers.py:36-42), sorted within
+        each kind."""
+        for i in range(len(self.worlds)):
+            new = self.trigger_overlaps(i)
+            old = self.overlaps[i]
+            if new or old:
+                self.events[i].extend([('enter',) + p for p in sorted(new - old)] +
+                                      [('stay',) + p for p in sorted(new & old)] +
+                                      [('exit',) + p for p in sorted(old - new)])
+            self.overlaps[i] = new
+
+    def take_events(self, i: int) -> list:
+        """World ``i``'s trigger events since the last call, oldest first."""
+        ev, self.events[i] = self.events[i], []
+        return ev
 
     def step_async(self, n: int = 1) -> None:
         self.ctx.call('step_async', int(n))
@@ -191,15 +234,17 @@ class WorldBatch:
 
         Restoring it (here or into another batch holding the same world) and
         stepping gives exactly what stepping on from here would: pose,
-        velocities, sleep state and the solver's warm-start impulses
-        (solver.py:91, 272-278) are all the step carries over.
+        velocities, sleep state, the solver's warm-start impulses
+        (solver.py:91, 272-278) and the sensor overlaps the next step's
+        events are formed against are all the step carries over.
         """
         w = self.worlds[i]
         n = w.body_count
         self.download_state(i)
-        snap = {name: np.array(getattr(w, '_' + name)[:n], copy=True)
-                for name in ('position', 'orientation', 'linear_velocity', 'angular_velocity',
-                             'awake', 'sleep_timer')}
+        snap = {'overlaps': set(self.overlaps[i])}
+        snap.update({name: np.array(getattr(w, '_' + name)[:n], copy=True)
+                     for name in ('position', 'orientation', 'linear_velocity', 'angular_velocity',
+                                  'awake', 'sleep_timer')})
         snap['cache'] = self.cache(i)
         snap['time'] = w.time
         return snap
@@ -212,6 +257,7 @@ class WorldBatch:
                      'sleep_timer'):
             getattr(w, '_' + name)[:n] = snap[name]
         w.time = snap['time']
+        self.overlaps[i] = set(snap.get('overlaps', ()))
         self.upload_state(i)
         c = snap['cache']
         self.set_cache(i, c['a'], c['b'], c['point'], c['impulse'])

@@ -49,6 +49,11 @@ struct Arena {
     const uint8_t *w_active;
     const double *w_def_damp, *w_solver;
     const int *w_filter_off, *w_filter_rows, *w_pf_off, *w_pf_n, *w_joint_off;
+    // gravity volumes (gravity.py:51-108): rows [w_vol_off[w], w_vol_off[w+1])
+    // in application order; kind flags OMI_VOL_*, field = directional
+    // acceleration or point centre, rc/rr = region centre, radius^2 / half
+    const int *w_vol_off, *vol_kind;
+    const double *vol_g, *vol_field, *vol_rc, *vol_rr;
 
     // bodies
     double *pos, *q, *v, *w, *prev_pos, *prev_q;
@@ -56,8 +61,10 @@ struct Arena {
     double *timer;
     uint8_t *awake;
     const int *mtype, *shape, *material, *material_key, *filter_row, *body_world;
-    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 convex, 4 capsule
+    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 convex, 4 capsule (of rshape)
     const double *half;      // refit half extents (world.py:443-469)
+    const int *tshape;       // sensor shape (triggers.py) or -1
+    const int *rshape;       // the shape a body's AABB comes from: collider, else sensor
     double *aabb_min, *aabb_max, *invIw;
 
     // shapes / materials / filters
@@ -83,18 +90,21 @@ struct Arena {
     int *order;              // sorted global body index per row (per world range)
     double *sorted_x;
     double *srt_box;         // per sorted row: lo/hi x, y, z and 2 pad (8 doubles)
-    int *srt_info;           // per sorted row: motion type | filter row << 2
+    int *srt_info;           // per sorted row: motion type (bits 0-1), solid collider (2), awake (3),
+                             // sensor (4), filter row (5-)
     int *pair_end;           // per sorted row: end of its sweep window
     double *sort_k[2];
     int *sort_v[2];
     int *pair_cnt, *pair_scan;      // NB, NB+1
     int *pair_a, *pair_b;           // pair_cap
-    uint8_t *pair_solid;
+    uint8_t *pair_solid;            // 1 contact pair, 2 sensor pair (no contact), 0 neither
 
     // narrowphase
     int *slot_cnt;                  // pair_cap (+1 scratch)
     double *slot;                   // pair_cap * SLOT
     int *gjk_list, *gjk_n;
+    int *trig_list, *trig_n;        // sensor pairs this step (pair indices)
+    int *trig_out;                  // per sensor pair: trigger, other, overlap (1/0, -1 no shape)
     int *clip_list, *clip_n;        // touching box-box pairs awaiting face clipping
     int *contact_scan;              // pair_cap + 1
 

@@ -7,10 +7,11 @@
 // vertex array; outputs line up with the triangles (hit byte, point (3),
 // normal (3), depth), zeros where there is no contact.
 //
-// One thread per triangle. A block takes tiles of CT_THREADS triangles: the
-// tile's 72-byte vertex records are read with coalesced streaming loads into
-// shared memory, each thread answers its triangle, and the point / normal rows
-// are written back through shared memory so every global store is coalesced.
+// One thread per triangle. Each warp takes tiles of 32 triangles: the tile's
+// 72-byte vertex records are read with coalesced streaming loads into the
+// warp's shared memory, each lane answers its triangle, and the point /
+// normal rows are written back through shared memory so every global store is
+// coalesced.
 // Per triangle 72 bytes are read and 57 written; the arithmetic (float64, in
 // the reference's operation order, no contraction) is a few hundred
 // operations, so the kernel sits near the HBM / FP64 ridge.
@@ -123,13 +124,17 @@ __device__ inline void seg_closest(const double *p1, const double *q1, const dou
 __device__ inline int capsule_triangle(const double *c0, const double *c1, const double *centre, double radius,
                                        const double *v0, const double *v1, const double *v2, double *point,
                                        double *normal, double *depth) {
-    double e1[3], e2[3], face[3], tp[3];
+    double e1[3], e2[3], face[3];
 #pragma unroll
     for (int m = 0; m < 3; m++) { e1[m] = v1[m] - v0[m]; e2[m] = v2[m] - v0[m]; }
     face[0] = e1[1] * e2[2] - e1[2] * e2[1];
     face[1] = e1[2] * e2[0] - e1[0] * e2[2];
     face[2] = e1[0] * e2[1] - e1[1] * e2[0];
     const double face_len = sqrt(dot3_seq(face, face));
+    // closest points on the triangle to the two cap ends: the face test and
+    // the rim test ask for the same two (a pure function), so they are found once
+    double tpk[2][3];
+    bool have_tp = false;
     if (face_len > EPS_COLLIDE) {
         double fn[3];
 #pragma unroll
@@ -149,6 +154,7 @@ __device__ inline int capsule_triangle(const double *c0, const double *c1, const
             double foot[3];
 #pragma unroll
             for (int m = 0; m < 3; m++) foot[m] = sp[m] - fn[m] * h;
+            double *tp = tpk[k];
             tri_closest(sp, v0, v1, v2, tp);
 #pragma unroll
             for (int m = 0; m < 3; m++) g[m] = foot[m] - tp[m];
@@ -166,12 +172,17 @@ __device__ inline int capsule_triangle(const double *c0, const double *c1, const
             for (int m = 0; m < 3; m++) { point[m] = bp[m]; normal[m] = fn[m]; }
             return 1;
         }
+        have_tp = true;
+    }
+    if (!have_tp) {
+        tri_closest(c0, v0, v1, v2, tpk[0]);
+        tri_closest(c1, v0, v1, v2, tpk[1]);
     }
     double best_d2 = 1e300, bsp[3] = {0.0, 0.0, 0.0}, btp[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         const double *sp = k ? c1 : c0;
-        tri_closest(sp, v0, v1, v2, tp);
+        const double *tp = tpk[k];
         const double gx = sp[0] - tp[0], gy = sp[1] - tp[1], gz = sp[2] - tp[2];
         const double d2 = gx * gx + gy * gy + gz * gz;
         if (d2 < best_d2) {
@@ -211,6 +222,10 @@ __device__ inline int capsule_triangle(const double *c0, const double *c1, const
     return 1;
 }
 
+// Host builds of this header (a test-only emulation that checks the per-
+// triangle arithmetic against the oracle on the CPU) stop here.
+#ifndef OMI_HOST_EMULATION
+
 // the capsule owning triangle i: the largest c in [lo, hi] with off[c] <= i
 // (reads off[lo + 1 .. hi] only)
 __device__ __forceinline__ int capsule_of(const int64_t *off, int lo, int hi, int64_t i) {
@@ -222,30 +237,50 @@ __device__ __forceinline__ int capsule_of(const int64_t *off, int lo, int hi, in
     return lo;
 }
 
+// the same by a whole warp, 32 candidates a round (~4 rounds for 65536
+// capsules instead of 16 dependent loads); every lane returns the answer.
+// The range shrinks every round and every read stays in [lo, hi], whatever
+// off holds.
+__device__ __forceinline__ int capsule_of_warp(const int64_t *off, int lo, int hi, int64_t i, int lane) {
+    while (hi > lo) {
+        const int step = (hi - lo + 31) / 32;
+        const int c = min(hi, lo + (lane + 1) * step);
+        const int k = __popc(__ballot_sync(0xffffffffu, __ldg(&off[c]) <= i));
+        const int nlo = k == 0 ? lo : min(hi, lo + k * step);
+        const int nhi = k == 32 ? hi : min(hi, lo + (k + 1) * step - 1);
+        lo = nlo;
+        hi = max(nlo, nhi);
+    }
+    return lo;
+}
+
+constexpr int CT_WARPS = CT_THREADS / 32;
+
 // Triangles [0, n) of this launch are global triangles [base, base + n): the
 // vertex and output pointers are the launch's own, the capsule ranges
-// tri_off are global (a host pipeline launches one chunk at a time).
+// tri_off are global (a host pipeline launches one chunk at a time). Each
+// warp takes tiles of 32 triangles (grid-stride): coalesced streaming loads of
+// the tile's vertex records into the warp's shared memory, one triangle per
+// lane, the point / normal rows written back through shared memory; only
+// __syncwarp orders the warp's tile, no block-wide barrier.
 __global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
     const double *__restrict__ caps, const int64_t *__restrict__ tri_off, int q,
     const double *__restrict__ verts, int64_t base, int64_t n, uint8_t *__restrict__ hit,
     double *__restrict__ points, double *__restrict__ normals, double *__restrict__ depths) {
-    __shared__ double sv[CT_THREADS * 9];
-    __shared__ double sp[CT_THREADS * 3];
-    __shared__ double sn[CT_THREADS * 3];
-    __shared__ int s_range[2];
-    const int tid = threadIdx.x;
-    for (int64_t t0 = (int64_t)blockIdx.x * CT_THREADS; t0 < n; t0 += (int64_t)gridDim.x * CT_THREADS) {
-        const int m = (int)(n - t0 < CT_THREADS ? n - t0 : CT_THREADS);
+    __shared__ double sv[CT_WARPS][32 * 9];
+    __shared__ double so[CT_WARPS][32 * 6];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *wv = sv[wib], *wo = so[wib];
+    const int64_t stride = (int64_t)gridDim.x * CT_THREADS;
+    for (int64_t t0 = ((int64_t)blockIdx.x * CT_WARPS + wib) * 32; t0 < n; t0 += stride) {
+        const int m = (int)(n - t0 < 32 ? n - t0 : 32);
         const double *src = verts + t0 * 9;
-        for (int j = tid; j < m * 9; j += CT_THREADS) sv[j] = __ldcs(src + j);
-        if (tid == 0) {
-            const int first = capsule_of(tri_off, 0, q - 1, base + t0);
-            s_range[0] = first;
-            s_range[1] = capsule_of(tri_off, first, q - 1, base + t0 + m - 1);
-        }
-        __syncthreads();
-        if (tid < m) {
-            const int c = capsule_of(tri_off, s_range[0], s_range[1], base + t0 + tid);
+        for (int j = lane; j < m * 9; j += 32) wv[j] = __ldcs(src + j);
+        const int first = capsule_of_warp(tri_off, 0, q - 1, base + t0, lane);
+        const int last = capsule_of_warp(tri_off, first, q - 1, base + t0 + m - 1, lane);
+        __syncwarp();
+        if (lane < m) {
+            const int c = capsule_of(tri_off, first, last, base + t0 + lane);
             const double *cp = caps + (size_t)c * CT_CAP_DOUBLES;
             double c0[3], c1[3], centre[3];
 #pragma unroll
@@ -257,21 +292,24 @@ __global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
             const double radius = __ldg(&cp[6]);
             double v[9];
 #pragma unroll
-            for (int k = 0; k < 9; k++) v[k] = sv[tid * 9 + k];
+            for (int k = 0; k < 9; k++) v[k] = wv[lane * 9 + k];
             double pt[3], nr[3], dep;
             const int h = capsule_triangle(c0, c1, centre, radius, v, v + 3, v + 6, pt, nr, &dep);
             if (!h) { pt[0] = pt[1] = pt[2] = 0.0; nr[0] = nr[1] = nr[2] = 0.0; dep = 0.0; }
 #pragma unroll
-            for (int k = 0; k < 3; k++) { sp[tid * 3 + k] = pt[k]; sn[tid * 3 + k] = nr[k]; }
-            hit[t0 + tid] = (uint8_t)h;
-            __stcs(&depths[t0 + tid], dep);
+            for (int k = 0; k < 3; k++) { wo[lane * 3 + k] = pt[k]; wo[96 + lane * 3 + k] = nr[k]; }
+            hit[t0 + lane] = (uint8_t)h;
+            __stcs(&depths[t0 + lane], dep);
         }
-        __syncthreads();
-        for (int j = tid; j < m * 3; j += CT_THREADS) {
-            __stcs(&points[t0 * 3 + j], sp[j]);
-            __stcs(&normals[t0 * 3 + j], sn[j]);
+        __syncwarp();
+        for (int j = lane; j < m * 3; j += 32) {
+            __stcs(&points[t0 * 3 + j], wo[j]);
+            __stcs(&normals[t0 * 3 + j], wo[96 + j]);
         }
+        __syncwarp();
     }
 }
+
+#endif  // OMI_HOST_EMULATION
 
 }  // namespace omi

@@ -35,7 +35,7 @@ __device__ __forceinline__ bool dyn(const Arena &A, int i) { return A.mtype[i] =
 // einsum('nij,nkj->nik', R*invI, R) (solver.py:215-220), one thread per body
 // ---------------------------------------------------------------------------
 __global__ void k_refit(Arena A) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) { A.gjk_n[0] = 0; A.clip_n[0] = 0; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.gjk_n[0] = 0; A.clip_n[0] = 0; A.trig_n[0] = 0; }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.NB; i += gridDim.x * blockDim.x) {
         int w = A.body_world[i];
         if (!world_collides(A, w) || i - A.w_body_off[w] >= A.w_body_n[w]) continue;
@@ -53,7 +53,7 @@ __global__ void k_refit(Arena A) {
         if (kind == 0) {
             for (int r = 0; r < 3; r++) lo[r] = hi[r] = p[r];
         } else if (kind == 3) {
-            const int s = A.shape[i];
+            const int s = A.rshape[i];
             const double *pts = &A.points[A.pt_off[s] * 3];
             const int m = A.pt_cnt[s];
             double mn[3], mx[3];
@@ -152,8 +152,9 @@ __global__ void k_sort(Arena A, int smem_cap) {
             const double *lo = &A.aabb_min[body * 3], *hi = &A.aabb_max[body * 3];
             row[0] = make_double4(lo[0], hi[0], lo[1], hi[1]);
             row[1] = make_double4(lo[2], hi[2], 0.0, 0.0);
-            A.srt_info[off + i] = A.mtype[body] | (A.shape[body] >= 0 ? 4 : 0) | (A.awake[body] ? 8 : 0) |
-                                  (A.filter_row[body] << 4);
+            const bool sensor = A.tshape[body] >= 0;
+            A.srt_info[off + i] = A.mtype[body] | (A.shape[body] >= 0 && !sensor ? 4 : 0) |
+                                  (A.awake[body] ? 8 : 0) | (sensor ? 16 : 0) | (A.filter_row[body] << 5);
         }
         __syncthreads();
     }
@@ -234,15 +235,15 @@ __device__ __forceinline__ int window_end_warp(const double *sx, int lo, int hi,
 }
 
 // pair_keep on sorted rows: `ra`/`rb` are the rows' boxes (lo/hi x, y, z),
-// `ia`/`ib` their info words: motion type (bits 0-1), has a shape (2), awake
-// (3), filter row (4-)
+// `ia`/`ib` their info words: motion type (bits 0-1), collider and no sensor
+// (2), awake (3), sensor (4), filter row (5-)
 __device__ __forceinline__ bool row_keep(const Arena &A, int w, const double4 &a0, const double4 &a1, int ia,
                                          const double4 &b0, const double4 &b1, int ib) {
     bool keep = (a0.w >= b0.z) & (b0.w >= a0.z) & (a1.y >= b1.x) & (b1.y >= a1.x);
     keep &= ((ia & 3) == 2) | ((ib & 3) == 2);
     if (keep) {
         const int rows = A.w_filter_rows[w];
-        keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 4) * rows + (ib >> 4)] != 0;
+        keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 5) * rows + (ib >> 5)] != 0;
     }
     return keep;
 }
@@ -302,10 +303,11 @@ __global__ void k_pair_emit(Arena A) {
                 const int slot = out + __popc(m & ((1u << lane) - 1u));
                 A.pair_a[slot] = a < b ? a : b;
                 A.pair_b[slot] = a < b ? b : a;
-                // solid-pair filter (world.py:663-670): both colliders and an awake mover
+                // solid-pair filter (world.py:663-670): a sensor on either body makes
+                // a sensor pair; else both colliders and an awake mover
                 const bool ma = ((ia & 3) == 2 && (ia & 8)) || (ia & 3) == 1;
                 const bool mb = ((ib & 3) == 2 && (ib & 8)) || (ib & 3) == 1;
-                A.pair_solid[slot] = ((ia & 4) && (ib & 4) && (ma || mb)) ? 1 : 0;
+                A.pair_solid[slot] = ((ia | ib) & 16) ? 2 : (((ia & 4) && (ib & 4) && (ma || mb)) ? 1 : 0);
             }
             out += __popc(m);
         }
@@ -411,6 +413,42 @@ __global__ void k_contact_check(Arena A) {
 // ---------------------------------------------------------------------------
 // integrate forces (backend.py:26-40) + prev pose copy (world.py:414-415)
 // ---------------------------------------------------------------------------
+// resolve_gravity with the world's volumes (world.py:386-396,
+// gravity.py:82-108): the world vector, then each volume whose region holds
+// the body's position, in application order: replace sets the field, stop
+// zeroes, otherwise the field adds. A point field is normalize(centre - pos)
+// times its magnitude; a directional field arrives precomputed.
+__device__ __forceinline__ void body_gravity(const Arena &A, int w, int i, double *g) {
+    g[0] = A.w_g[w * 3]; g[1] = A.w_g[w * 3 + 1]; g[2] = A.w_g[w * 3 + 2];
+    const int v1 = A.w_vol_off[w + 1];
+    for (int k = A.w_vol_off[w]; k < v1; k++) {
+        const int kind = A.vol_kind[k];
+        const double *pos = &A.pos[i * 3], *rc = &A.vol_rc[k * 3], *rr = &A.vol_rr[k * 3];
+        bool inside = true;
+        if (kind & 2) {
+            const double d[3] = {pos[0] - rc[0], pos[1] - rc[1], pos[2] - rc[2]};
+            inside = dot_blas(d, d) <= rr[0];
+        } else if (kind & 4) {
+            inside = fabs(pos[0] - rc[0]) <= rr[0] && fabs(pos[1] - rc[1]) <= rr[1] &&
+                     fabs(pos[2] - rc[2]) <= rr[2];
+        }
+        if (!inside) continue;
+        if (kind & 16) { g[0] = g[1] = g[2] = 0.0; continue; }
+        const double *fd = &A.vol_field[k * 3];
+        double f[3];
+        if (kind & 1) {
+            const double d[3] = {fd[0] - pos[0], fd[1] - pos[1], fd[2] - pos[2]};
+            double u[3];
+            normalize3(d, u);
+            f[0] = u[0] * A.vol_g[k]; f[1] = u[1] * A.vol_g[k]; f[2] = u[2] * A.vol_g[k];
+        } else {
+            f[0] = fd[0]; f[1] = fd[1]; f[2] = fd[2];
+        }
+        if (kind & 8) { g[0] = f[0]; g[1] = f[1]; g[2] = f[2]; }
+        else { g[0] = g[0] + f[0]; g[1] = g[1] + f[1]; g[2] = g[2] + f[2]; }
+    }
+}
+
 __global__ void k_integrate_forces(Arena A, int gated) {
     if (gated && overflowed(A)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.NB; i += gridDim.x * blockDim.x) {
@@ -420,7 +458,8 @@ __global__ void k_integrate_forces(Arena A, int gated) {
         for (int c = 0; c < 4; c++) A.prev_q[i * 4 + c] = A.q[i * 4 + c];
         if (!(A.mtype[i] == 2 && A.awake[i])) continue;
         const double dt = A.w_dt[w];
-        const double *g = &A.w_g[w * 3];
+        double g[3];
+        body_gravity(A, w, i, g);
         double *v = &A.v[i * 3], *om = &A.w[i * 3];
         const double gf = A.gf[i];
         double v0 = v[0] + (g[0] * gf) * dt, v1 = v[1] + (g[1] * gf) * dt, v2 = v[2] + (g[2] * gf) * dt;
@@ -447,7 +486,10 @@ __global__ void k_narrow(Arena A) {
     const int P = A.pair_scan[A.NB];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
         int cnt = 0;
-        if (A.pair_solid[p]) {
+        const int kindp = A.pair_solid[p];
+        if (kindp == 2) {
+            A.trig_list[atomicAdd(A.trig_n, 1)] = p;     // overlap tested after the solve
+        } else if (kindp == 1) {
             const int a = A.pair_a[p], b = A.pair_b[p];
             const int ka = A.kind[a], kb = A.kind[b];
             double *s = &A.slot[(size_t)p * SLOT];
@@ -517,8 +559,8 @@ __global__ void k_clip(Arena A) {
     }
 }
 
-__device__ inline void make_proxy(const Arena &A, int i, Proxy &P) {
-    const int s = A.shape[i];
+// make_proxy (body.py:214-237) of shape s at body i's pose
+__device__ inline void make_proxy_shape(const Arena &A, int s, int i, Proxy &P) {
     P.kind = A.shape_type[s];
     quat_to_matrix(&A.q[i * 4], P.R);
     for (int c = 0; c < 3; c++) P.c[c] = A.pos[i * 3 + c];
@@ -528,6 +570,8 @@ __device__ inline void make_proxy(const Arena &A, int i, Proxy &P) {
     P.m = A.pt_cnt[s];
     if (P.kind == 4) capsule_ends(P.c, P.R, 0.5 * A.shape_size[s * 3 + 1], P.e0, P.e1);
 }
+
+__device__ inline void make_proxy(const Arena &A, int i, Proxy &P) { make_proxy_shape(A, A.shape[i], i, P); }
 
 // gjk.collide_convex (gjk.py:249-264) through collide.collide (collide.py:251-269)
 __global__ void k_gjk(Arena A) {
@@ -554,6 +598,77 @@ __global__ void k_gjk(Arena A) {
                 s[3] = pt[0]; s[4] = pt[1]; s[5] = pt[2]; s[6] = dep;
             }
             A.slot_cnt[p] = r > 0 ? 1 : 0;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sensor overlaps (triggers.py:24-72), after the contact solve as the
+// reference's _CollisionStages.run does them (world.py:674-676): one warp per
+// sensor pair, len(collide.collide(trigger, other, ...)) > 0 with the sensor
+// shape at the sensor body's pose against the other body's collider (else
+// its sensor). Sphere routes follow collide.sphere_sphere / sphere_box
+// (collide.py:56-88); box-box is non-empty exactly when no separating axis
+// exists; every other pair goes through GJK/EPA.
+// ---------------------------------------------------------------------------
+__device__ inline bool py_sphere_sphere_hit(const Proxy &A, const Proxy &B) {
+    const double d[3] = {B.c[0] - A.c[0], B.c[1] - A.c[1], B.c[2] - A.c[2]};
+    return !(sqrt(dot_blas(d, d)) >= A.r + B.r);
+}
+
+__device__ inline bool py_sphere_box_hit(const Proxy &S, const Proxy &B) {
+    const double v[3] = {S.c[0] - B.c[0], S.c[1] - B.c[1], S.c[2] - B.c[2]};
+    double delta[3];
+    for (int j = 0; j < 3; j++) {
+        const double col[3] = {B.R[j], B.R[3 + j], B.R[6 + j]};
+        const double l = dot_blas(col, v);
+        double cl = l > -B.h[j] ? l : -B.h[j];
+        cl = cl < B.h[j] ? cl : B.h[j];
+        delta[j] = l - cl;
+    }
+    return !(sqrt(dot_blas(delta, delta)) > S.r);
+}
+
+__global__ void k_triggers(Arena A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (overflowed(A)) return;
+    EpaWork &W = reinterpret_cast<EpaWork *>(smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int nitems = *A.trig_n;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += nwarps) {
+        const int p = A.trig_list[it];
+        const int i = A.pair_a[p], j = A.pair_b[p];
+        const int ti = A.tshape[i], tj = A.tshape[j];
+        const int trg = ti >= 0 ? i : j, other = ti >= 0 ? j : i;
+        const int ts = ti >= 0 ? ti : tj;
+        const int os = A.shape[other] >= 0 ? A.shape[other] : A.tshape[other];
+        int hit = -1;
+        if (os >= 0) {
+            Proxy PA, PB;
+            make_proxy_shape(A, ts, trg, PA);
+            make_proxy_shape(A, os, other, PB);
+            if (PA.kind == 1 && PB.kind == 1) {
+                hit = py_sphere_sphere_hit(PA, PB);
+            } else if (PA.kind == 1 && PB.kind == 2) {
+                hit = py_sphere_box_hit(PA, PB);
+            } else if (PA.kind == 2 && PB.kind == 1) {
+                hit = py_sphere_box_hit(PB, PA);
+            } else if (PA.kind == 2 && PB.kind == 2) {
+                double nrm[3], depth;
+                hit = box_box_sat(PA.c, PA.R, PA.h, PB.c, PB.R, PB.h, nrm, depth) ? 1 : 0;
+            } else {
+                double nrm[3], pt[3], dep = 0.0;
+                const int r = collide_convex(PA, PB, W, nrm, pt, &dep);
+                if (r < 0 && lane == 0) atomicAdd(&A.status[ST_EPA_LIMIT], 1);
+                hit = r > 0 ? 1 : 0;
+            }
+        }
+        if (lane == 0) {
+            A.trig_out[it * 3] = trg;
+            A.trig_out[it * 3 + 1] = other;
+            A.trig_out[it * 3 + 2] = hit;
         }
         __syncwarp();
     }

@@ -23,12 +23,12 @@ namespace {
 enum KernelId {
     KN_REFIT, KN_SORT, KN_PAIR_COUNT, KN_PAIR_SCAN, KN_PAIR_EMIT, KN_NARROW, KN_GJK,
     KN_CONTACT_SCAN, KN_INTEGRATE_FORCES, KN_COMPACT, KN_WAKE, KN_PREP, KN_LEVELS, KN_SOLVE,
-    KN_CACHE, KN_JOINTS, KN_FINALIZE, KN_COUNT
+    KN_TRIGGERS, KN_CACHE, KN_JOINTS, KN_FINALIZE, KN_COUNT
 };
 const char *kKernelNames[KN_COUNT] = {
     "refit", "sort", "pair_count", "pair_scan", "pair_emit", "narrow", "gjk_epa",
     "contact_scan", "integrate_forces", "contact_compact", "wake", "prep", "levels", "solve",
-    "cache_store", "joints", "integrate_positions_sleep"};
+    "triggers", "cache_store", "joints", "integrate_positions_sleep"};
 
 struct Buf {
     void *p = nullptr;
@@ -60,6 +60,7 @@ struct OmiCtx {
     int fin_cap = 1;               // bodies whose sleep flags / islands k_finalize keeps in shared memory
     int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
+    bool has_triggers = false;     // some body carries a sensor shape: k_triggers runs each step
     cudaGraphExec_t graph = nullptr;
     int *h_status = nullptr;       // pinned mirror of the status words
     int64_t launches = 0;
@@ -171,6 +172,8 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.slot, (size_t)pair_cap * SLOT);
     rc |= alloc(ctx, ctx->dyn, A.clip_list, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.gjk_list, pair_cap);
+    rc |= alloc(ctx, ctx->dyn, A.trig_list, ctx->has_triggers ? pair_cap : 1);
+    rc |= alloc(ctx, ctx->dyn, A.trig_out, ctx->has_triggers ? 3 * (size_t)pair_cap : 3);
     rc |= alloc(ctx, ctx->dyn, A.contact_scan, (size_t)pair_cap + 1);
     rc |= alloc(ctx, ctx->dyn, A.c_a, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.c_b, contact_cap);
@@ -322,6 +325,11 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     k_iterate<<<std::min(A.W, ctx->sm_count), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
     ctx->launches += 4;
     mark(ctx, pf, KN_SOLVE);
+    if (ctx->has_triggers) {
+        k_triggers<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
+        ctx->launches++;
+    }
+    mark(ctx, pf, KN_TRIGGERS);
     k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
     k_hash_clear<<<grid_for(ctx->cache_cap, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
     k_cache_copy<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
@@ -406,6 +414,7 @@ int64_t step_launches(OmiCtx *ctx) {
     // kernels per captured step (same sequence as enqueue_step)
     int64_t n = 1 + 1 + 1 + 3 + 1 + 2 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
     if (ctx->A.NJ > 0) n += 1;
+    if (ctx->has_triggers) n += 1;
     return n;
 }
 
@@ -476,6 +485,7 @@ int omi_create(int device, OmiCtx **out) {
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
     const struct { const void *fn; int bytes; const char *name; } smem[] = {
         {(const void *)k_gjk, 4 * (int)sizeof(EpaWork), "k_gjk"},
+        {(const void *)k_triggers, 4 * (int)sizeof(EpaWork), "k_triggers"},
         {(const void *)k_sort<true>, 8192 * 24, "k_sort"},
         {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
@@ -560,6 +570,24 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     std::vector<int> body_world(NB);
     std::vector<int8_t> kind(NB, 0);
     std::vector<double> half((size_t)NB * 3, 0.0);
+    std::vector<int> tshape(NB, -1), rshape(NB, -1);
+    bool sensors = false;
+    if (s->trigger_shape)
+        for (int i = 0; i < NB; i++) {
+            const int t = s->trigger_shape[i];
+            if (t < -1 || t >= s->n_shapes) return fail(ctx, OMI_E_ARG, "trigger shape index out of range");
+            tshape[i] = t;
+            sensors |= t >= 0;
+        }
+    std::vector<int> vol_off(W + 1, 0);
+    if (s->w_vol_off) {
+        for (int w = 0; w <= W; w++) vol_off[w] = s->w_vol_off[w];
+        if (vol_off[0] != 0 || vol_off[W] != s->n_volumes) return fail(ctx, OMI_E_ARG, "inconsistent volume offsets");
+        for (int w = 0; w < W; w++)
+            if (vol_off[w + 1] < vol_off[w]) return fail(ctx, OMI_E_ARG, "volume offsets decrease");
+    } else if (s->n_volumes != 0) {
+        return fail(ctx, OMI_E_ARG, "gravity volumes without w_vol_off");
+    }
     int max_n = 0, max_nc = 0;
     for (int w = 0; w < W; w++) {
         const int n = s->w_body_off[w + 1] - s->w_body_off[w];
@@ -572,11 +600,13 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
         }
     }
     for (int i = 0; i < NB; i++) {
-        const int sh = s->shape[i];
+        if (s->shape[i] >= s->n_shapes) return fail(ctx, OMI_E_ARG, "shape index out of range");
+        // the AABB comes from the collider, else the sensor (world.py:452-455)
+        const int sh = s->shape[i] >= 0 ? s->shape[i] : tshape[i];
+        rshape[i] = sh;
         if (s->motion_type[i] < 0 || s->motion_type[i] > 2) return fail(ctx, OMI_E_ARG, "motion type");
         if (s->material[i] >= s->n_materials || s->material[i] < -1) return fail(ctx, OMI_E_ARG, "material index out of range");
         if (sh < 0) continue;
-        if (sh >= s->n_shapes) return fail(ctx, OMI_E_ARG, "shape index out of range");
         const int t = s->shape_type[sh];
         if (t == OMI_SHAPE_SPHERE) {
             kind[i] = 1;
@@ -665,6 +695,17 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= upload(ctx, const_cast<int *&>(A.body_world), body_world.data(), NB);
     rc |= upload(ctx, const_cast<int8_t *&>(A.kind), kind.data(), NB);
     rc |= upload(ctx, const_cast<double *&>(A.half), half.data(), (size_t)NB * 3);
+    rc |= upload(ctx, const_cast<int *&>(A.tshape), tshape.data(), NB);
+    rc |= upload(ctx, const_cast<int *&>(A.rshape), rshape.data(), NB);
+    ctx->has_triggers = sensors;
+    // gravity volumes
+    const int NV = s->w_vol_off ? s->n_volumes : 0;
+    rc |= upload(ctx, const_cast<int *&>(A.w_vol_off), vol_off.data(), W + 1);
+    rc |= upload(ctx, const_cast<int *&>(A.vol_kind), NV ? s->vol_kind : nullptr, NV);
+    rc |= upload(ctx, const_cast<double *&>(A.vol_g), NV ? s->vol_g : nullptr, NV);
+    rc |= upload(ctx, const_cast<double *&>(A.vol_field), NV ? s->vol_field : nullptr, (size_t)NV * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.vol_rc), NV ? s->vol_rc : nullptr, (size_t)NV * 3);
+    rc |= upload(ctx, const_cast<double *&>(A.vol_rr), NV ? s->vol_rr : nullptr, (size_t)NV * 3);
     rc |= alloc(ctx, ctx->statics, A.aabb_min, (size_t)NB * 3);
     rc |= alloc(ctx, ctx->statics, A.aabb_max, (size_t)NB * 3);
     rc |= alloc(ctx, ctx->statics, A.invIw, (size_t)NB * 9);
@@ -723,6 +764,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.w_levels, W);
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
+    rc |= alloc(ctx, ctx->statics, A.trig_n, 1);
     rc |= alloc(ctx, ctx->statics, A.clip_n, 1);
     rc |= alloc(ctx, ctx->statics, A.sweep_next, 1);
     for (int t = 0; t < 2; t++) {
@@ -889,6 +931,11 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
                 return fail(ctx, OMI_E_ARG, "convex point range");
         } else return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
     }
+    if ((o->w_vol_off && o->n_volumes > 0))
+        return fail(ctx, OMI_E_UNSUPPORTED, "serving slots do not take gravity volumes");
+    if (o->trigger_shape)
+        for (int i = 0; i < n; i++)
+            if (o->trigger_shape[i] >= 0) return fail(ctx, OMI_E_UNSUPPORTED, "serving slots do not take sensors");
     std::vector<int> ptoff(ns);
     for (int k = 0; k < ns; k++) ptoff[k] = o->shape_pt_off[k] + p0;
     std::vector<int> ja(nj), jb(nj);
@@ -916,6 +963,7 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
     rc |= put(ctx, A.awake + b0, o->awake, n);
     rc |= put(ctx, const_cast<int *>(A.mtype) + b0, o->motion_type, n);
     rc |= put(ctx, const_cast<int *>(A.shape) + b0, shape.data(), n);
+    rc |= put(ctx, const_cast<int *>(A.rshape) + b0, shape.data(), n);
     rc |= put(ctx, const_cast<int *>(A.material) + b0, mat.data(), n);
     rc |= put(ctx, const_cast<int *>(A.material_key) + b0, o->material_key, n);
     rc |= put(ctx, const_cast<int *>(A.filter_row) + b0, o->filter_row, n);
@@ -1268,6 +1316,29 @@ int omi_get_contacts(OmiCtx *ctx, int32_t w, int32_t *a, int32_t *b, double *pt,
     CK(cp(imp, A.c_imp + (size_t)c0 * 3, sizeof(double) * 3 * n));
     CK(cudaStreamSynchronize(ctx->stream));
     return n;
+}
+
+int omi_get_trigger_overlaps(OmiCtx *ctx, int32_t w, int32_t *trg, int32_t *other, int32_t cap) {
+    int rc = check_world(ctx, w);
+    if (rc) return rc;
+    if (cap < 0 || (cap > 0 && (!trg || !other))) return fail(ctx, OMI_E_ARG, "null output or negative cap");
+    if (!ctx->has_triggers) return 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    int n = 0;
+    CK(cudaMemcpy(&n, ctx->A.trig_n, sizeof(int), cudaMemcpyDeviceToHost));
+    n = std::min(n, ctx->A.pair_cap);
+    std::vector<int> out((size_t)n * 3);
+    if (n) CK(cudaMemcpy(out.data(), ctx->A.trig_out, sizeof(int) * 3 * n, cudaMemcpyDeviceToHost));
+    const int b0 = ctx->h_body_off[w], b1 = b0 + ctx->h_body_n[w];
+    std::vector<std::pair<int, int>> hits;
+    for (int k = 0; k < n; k++) {
+        const int t = out[k * 3], o = out[k * 3 + 1];
+        if (out[k * 3 + 2] == 1 && t >= b0 && t < b1) hits.emplace_back(t - b0, o - b0);
+    }
+    std::sort(hits.begin(), hits.end());
+    const int m = (int)hits.size();
+    for (int k = 0; k < std::min(m, (int)cap); k++) { trg[k] = hits[k].first; other[k] = hits[k].second; }
+    return m;
 }
 
 int omi_world_levels(OmiCtx *ctx, int32_t *levels) {

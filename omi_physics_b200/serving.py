@@ -27,7 +27,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import D, I, U8, Context, OmiSlotCaps, ptr
+from ._lib import D, I, OMI_E_UNSUPPORTED, U8, Context, OmiSlotCaps, UnsupportedFeature, ptr
 from .arena import pack_worlds
 
 
@@ -171,6 +171,9 @@ class Server:
     def submit(self, world, steps: int, dt: float = None, arrival: float = 0.0) -> Request:
         dt = float(world.fixed_dt if dt is None else dt)
         packed = pack_worlds([world], [dt], active=True)
+        if packed.has_sensors or packed.scene.n_volumes:
+            raise UnsupportedFeature(OMI_E_UNSUPPORTED, 'serving slots do not take sensors or gravity '
+                                     'volumes; step such worlds in a WorldBatch')
         req = Request(self._next_rid, world, int(steps), dt, float(arrival), packed,
                       need_of(packed.scene), int(np.count_nonzero(world.motion_type == 2)))
         if not self.pool.could_ever_fit(req.need):

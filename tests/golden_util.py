@@ -4,7 +4,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
-SCENES = ('pyramid', 'debris', 'convex', 'chain', 'spheres', 'capsules')
+SCENES = ('pyramid', 'debris', 'convex', 'chain', 'spheres', 'capsules', 'zones')
 
 
 def load(name):
@@ -19,6 +19,20 @@ def checkpoint(data, step):
     ins = {k[len(pin):]: v for k, v in data.items() if k.startswith(pin)}
     outs = {k[len(pout):]: v for k, v in data.items() if k.startswith(pout)}
     return ins, outs
+
+
+EVENT_KINDS = ('enter', 'stay', 'exit')
+
+
+def events_from_overlaps(prev, new):
+    """Trigger events of one step as the reference forms them
+    (triggers.py:36-42), as a sorted array of (kind code, trigger, other)."""
+    ev = [(0,) + p for p in new - prev] + [(1,) + p for p in new & prev] + [(2,) + p for p in prev - new]
+    return np.array(sorted(ev), dtype=np.int32).reshape(-1, 3)
+
+
+def pair_set(arr):
+    return {(int(a), int(b)) for a, b in np.asarray(arr).reshape(-1, 2)}
 
 
 def checkpoints(data):

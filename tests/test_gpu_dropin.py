@@ -3,7 +3,8 @@
 The reference (built from its sources into ``oracle/_ref``) takes an object
 backend as fixed (world.py:335-338). One reference world steps with the CUDA
 backend, a twin with the reference's default CPU path (its Cython
-accelerators); pair sets, contact counts and sleep flags must match exactly,
+accelerators); pair sets, contact counts, sleep flags and the trigger
+events dispatched to listeners (as sets per step) must match exactly,
 poses within 1e-6 m over 60 steps and contact normals/depths within 1e-9.
 Skipped when the reference has not been built here.
 """
@@ -28,12 +29,12 @@ def _ref_api():
     if REF not in sys.path:
         sys.path.insert(0, REF)
     import omi_physics as ref
-    from omi_physics import joints, model
-    return SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=model, joints=joints)
+    from omi_physics import gravity, joints, model
+    return SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=model, joints=joints, gravity=gravity)
 
 
 @pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60),
-                                         ('capsules', 30)])
+                                         ('capsules', 30), ('zones', 60)])
 def test_reference_world_steps_on_cuda_backend(scene, steps):
     from omi_physics_b200.backend import CudaBackend
     api = _ref_api()
@@ -42,10 +43,16 @@ def test_reference_world_steps_on_cuda_backend(scene, steps):
     dt = meta['dt']
     assert gpu.backend.name == 'cuda' and gpu._backend_mode == 'fixed'
     n = cpu.body_count
+    gev, cev = [], []
+    gpu.add_trigger_listener(lambda *e: gev.append(e))
+    cpu.add_trigger_listener(lambda *e: cev.append(e))
     for s in range(steps):
+        gev.clear()
+        cev.clear()
         gpu.step(dt)
         cpu.step(dt)
         tag = '%s step %d' % (scene, s)
+        assert sorted(gev) == sorted(cev), tag + ' trigger events'
         gp = gpu._collision.broadphase.pairs(gpu)
         cp = [tuple(map(int, p)) for p in cpu._collision.broadphase.pairs(cpu)]
         assert gp == cp, tag + ' pairs (set and order)'

@@ -1,6 +1,8 @@
 """Host paths on the GPU: buffer regrowth on overflow (synchronous and
-asynchronous steps), the warm-start cache round trip, and snapshot / restore
-of a world (state + warm-start cache) in a batch and in a serving slot."""
+asynchronous steps), the warm-start cache round trip, snapshot / restore of a
+world (state + warm-start cache + sensor overlaps) in a batch and in a
+serving slot, sensor worlds batched with plain ones, and serving slots
+refusing sensor worlds."""
 import numpy as np
 import pytest
 
@@ -144,3 +146,65 @@ def test_world_groups_equal_one_batch():
         n = w1.body_count
         assert np.array_equal(w1._position[:n], w2._position[:n])
     g.close()
+
+
+def _oracle_events(o, prev):
+    new = o.overlaps()
+    ev = ([('enter',) + p for p in sorted(new - prev)] + [('stay',) + p for p in sorted(new & prev)] +
+          [('exit',) + p for p in sorted(prev - new)])
+    return new, ev
+
+
+def test_sensor_worlds_in_a_batch_match_the_oracle():
+    """Three sensor / gravity-volume worlds and a plain one stepped together:
+    every world's per-step trigger events and final state equal the oracle's
+    for that world alone."""
+    def build():
+        return [scenes.zones(n=80 + 20 * k, seed=k) for k in range(3)] + \
+               [scenes.debris(n=100, seed=5, extent=4.0, height=5.0, ground=16.0)]
+    worlds = [w for w, _ in build()]
+    b = WorldBatch(worlds, dts=[1 / 120.0] * 4)
+    assert b.has_sensors
+    refs = [pyoracle.OracleWorld.from_world(w) for w, _ in build()]
+    prev = [set() for _ in refs]
+    want = [[] for _ in refs]
+    for _ in range(80):
+        b.step(1)
+        for k, o in enumerate(refs):
+            o.step(1 / 120.0)
+            prev[k], ev = _oracle_events(o, prev[k])
+            want[k].extend(ev)
+    b.sync_to_host()
+    for k, (w, o) in enumerate(zip(worlds, refs)):
+        assert b.take_events(k) == want[k], k
+        _equal_state(w, o, 'world %d ' % k)
+    assert len(want[0]) > 50 and not want[3]
+
+
+def test_sensor_snapshot_restore_continues_identically():
+    w1, meta = scenes.zones(n=120, seed=8)
+    b1 = WorldBatch([w1], dts=[meta['dt']])
+    b1.step(40)
+    snap = b1.snapshot(0)
+    b1.take_events(0)
+    b1.step(30)
+    ev1 = b1.take_events(0)
+    b1.sync_to_host()
+    w2, _ = scenes.zones(n=120, seed=8)
+    b2 = WorldBatch([w2], dts=[meta['dt']])
+    b2.restore(0, snap)
+    b2.step(30)
+    assert b2.take_events(0) == ev1 and ev1
+    b2.sync_to_host()
+    n = w1.body_count
+    for col in COLS:
+        assert np.array_equal(getattr(w1, col)[:n], getattr(w2, col)[:n]), col
+
+
+def test_serving_slots_refuse_sensor_worlds():
+    from omi_physics_b200._lib import UnsupportedFeature
+    srv = Server(size_classes(256, per_class=1, min_bodies=64))
+    w, meta = scenes.zones(n=60, seed=2)
+    with pytest.raises(UnsupportedFeature):
+        srv.submit(w, steps=5, dt=meta['dt'], arrival=0)
+    srv.close()

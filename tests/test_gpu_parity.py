@@ -2,7 +2,7 @@
 
 (1) Golden checkpoints: the reference's own one-step inputs (state, joint
 state, warm-start cache) replayed on the B200 must give the reference's
-pairs, contacts, impulses, poses and sleep flags — bit for bit on the
+pairs, contacts, impulses, poses, sleep flags and sensor overlaps / events — bit for bit on the
 box/sphere/convex/capsule scenes (the kernels keep the reference's arithmetic order
 and are built with --fmad=false), within 1e-12 relative on the joint scene
 (the reference solves point joints with LAPACK).
@@ -13,13 +13,13 @@ import numpy as np
 import pytest
 
 import pyoracle
-from golden_util import SCENES, checkpoints, load
+from golden_util import SCENES, checkpoints, events_from_overlaps, load, pair_set
 from omi_physics_b200 import WorldBatch, scenes
 from util import assert_close, world_at_checkpoint
 
 pytestmark = pytest.mark.gpu
 
-EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules'}
+EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones'}
 
 
 @pytest.mark.parametrize('scene', SCENES)
@@ -46,6 +46,11 @@ def test_golden_checkpoints_on_gpu(scene):
                          ('aabb_min', 'aabb_min'), ('aabb_max', 'aabb_max')):
             assert_close(getattr(w, col), outs[key], rel, tag + ' ' + col)
         assert np.array_equal(w.awake, outs['awake'].astype(bool)), tag + ' awake'
+        if 'overlaps' in outs:
+            new = b.trigger_overlaps(0)
+            assert new == pair_set(outs['overlaps']), tag + ' trigger overlaps'
+            ev = events_from_overlaps(pair_set(ins['overlaps_prev']), new)
+            assert np.array_equal(ev, outs['events']), tag + ' trigger events'
 
 
 def _compare_step(b, w, o, tag):
@@ -60,6 +65,8 @@ def _compare_step(b, w, o, tag):
         assert np.array_equal(getattr(w, col), st[col]), tag + ' ' + col
     assert np.array_equal(w.awake, st['awake']), tag + ' awake'
     assert o.islands() == _island_sets(b.islands(0)), tag + ' islands'
+    if b.has_sensors:
+        assert b.trigger_overlaps(0) == o.overlaps(), tag + ' trigger overlaps'
 
 
 def _island_sets(labels):
@@ -76,6 +83,7 @@ def _island_sets(labels):
     ('convex160', lambda: scenes.convex_pile(n=160, seed=2, arena=10.0, height=8.0), 150),
     ('feature_mix', lambda: scenes.feature_mix(), 120),
     ('capsules256', lambda: scenes.capsule_pile(n=256, seed=3, arena=12.0, height=8.0), 150),
+    ('zones300', lambda: scenes.zones(n=300, seed=4, extent=6.0, height=10.0), 150),
 ])
 def test_trajectory_matches_oracle_every_step(name, builder, steps):
     w, meta = builder()

@@ -58,14 +58,16 @@ def test_unsupported_features_raise():
     with pytest.raises(UnsupportedFeature):
         CudaBackend().attach(w)
     w2, _ = scenes.GOLDEN_SCENES['pyramid']()
-    s = w2.add_shape(model.Shape.box((1, 1, 1)))
+    s = w2.add_shape(model.Shape(type='trimesh', points=pts, indices=np.array([[0, 1, 2]], 'i')))
     w2.add_body(model.Motion(type=model.STATIC), trigger=model.Trigger(shape=s), position=(0, 9, 0))
     with pytest.raises(UnsupportedFeature):
-        check_supported(w2)
+        check_supported(w2)                       # a triangle-mesh sensor
     w3, _ = scenes.GOLDEN_SCENES['pyramid']()
     w3.add_gravity_volume(object())
     with pytest.raises(UnsupportedFeature):
-        check_supported(w3)
+        check_supported(w3)                       # not a gravity volume
+    w4, _ = scenes.GOLDEN_SCENES['zones']()
+    check_supported(w4)                           # box / sphere / capsule sensors, all four volume kinds
 
 
 def test_select_backend_has_no_fallback():

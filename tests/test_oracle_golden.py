@@ -11,9 +11,9 @@ import numpy as np
 import pytest
 
 import pyoracle
-from golden_util import SCENES, checkpoint, checkpoints, load
+from golden_util import SCENES, checkpoint, checkpoints, events_from_overlaps, load, pair_set
 
-EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules')
+EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones')
 
 
 def _close(a, b, exact):
@@ -43,6 +43,11 @@ def test_oracle_matches_reference_checkpoints(scene):
                     'sleep_timer', 'aabb_min', 'aabb_max'):
             assert _close(st[key], outs[key], exact), (scene, step, key)
         assert np.array_equal(st['awake'], outs['awake']), (scene, step, 'awake')
+        if 'overlaps' in outs:
+            new = ow.overlaps()
+            assert new == pair_set(outs['overlaps']), (scene, step, 'trigger overlaps')
+            ev = events_from_overlaps(pair_set(ins['overlaps_prev']), new)
+            assert np.array_equal(ev, outs['events']), (scene, step, 'trigger events')
 
 
 def test_golden_scenes_exercise_every_narrowphase_route():
@@ -60,3 +65,17 @@ def test_golden_scenes_exercise_every_narrowphase_route():
     assert {(2, 2), (1, 1), (1, 2)} <= seen
     assert any(3 in k for k in seen)
     assert {(1, 4), (2, 4), (4, 4)} <= seen
+
+
+def test_zones_fixture_exercises_triggers_and_volumes():
+    """Sensors enter, stay and exit; all four volume behaviours are present."""
+    data = load('zones')
+    kinds = set()
+    for step in checkpoints(data):
+        ins, outs = checkpoint(data, step)
+        kinds |= set(int(k) for k in outs['events'][:, 0])
+        assert len(outs['overlaps']) > 5
+    assert {0, 1} <= kinds
+    vk = data['ck0/in/vol_kind']
+    assert int(data['ck0/in/s_n_volumes']) == 4
+    assert any(k & 1 for k in vk) and any(k & 8 for k in vk) and any(k & 16 for k in vk)
