@@ -149,10 +149,42 @@ class Gravity:
 
 
 @dataclass
+class JointLimit:
+    """One ``OMI_physics_joint`` limit row over a set of axes (model.py:181-189)."""
+    linearAxes: tuple = ()
+    angularAxes: tuple = ()
+    min: float = -np.inf
+    max: float = np.inf
+    stiffness: float = np.inf
+    damping: float = 0.0
+
+
+@dataclass
+class JointDrive:
+    """One ``OMI_physics_joint`` drive row (model.py:192-202)."""
+    type: str = 'linear'
+    mode: str = 'force'
+    axis: int = 0
+    maxForce: float = np.inf
+    positionTarget: Optional[float] = None
+    velocityTarget: Optional[float] = None
+    stiffness: float = 0.0
+    damping: float = 0.0
+
+
+@dataclass
 class Joint:
     """A ``physicsJoints[]`` entry (model.py:205-209); kept for documents only."""
     limits: List = field(default_factory=list)
     drives: List = field(default_factory=list)
+
+
+@dataclass
+class JointAttach:
+    """Per-body joint attachment (model.py:212-217); kept for documents only."""
+    joint: int = -1
+    connectedNode: int = -1
+    enableCollision: bool = False
 
 
 DEFAULT_MATERIAL = Material()

@@ -185,6 +185,12 @@ class Server:
         self.queue.insert(i, req)
         return req
 
+    def submit_document(self, gltf: dict, steps: int, dt: float = 1.0 / 60.0, arrival: float = 0.0,
+                        **build) -> Request:
+        """Serve an OMI glTF document: its world (``gltf.build_world``) as a request."""
+        from .gltf import build_world
+        return self.submit(build_world(gltf, fixed_dt=dt, **build), steps, dt, arrival)
+
     def _admit(self, now: float) -> int:
         n = 0
         keep = []

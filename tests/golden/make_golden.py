@@ -8,7 +8,8 @@ neither the reference nor its build:
 
 ``capsule_triangles.npz`` holds capsule queries against triangle batches and
 the reference's compiled ``capsule_triangles`` answers (the scene name
-``capsule_triangles`` makes only that file).
+``capsule_triangles`` makes only that file); ``omi_document.json`` an OMI glTF
+physics document with the reference's export of it (name ``omi_document``).
 
 For each scene the fixture holds (i) the reference world's column snapshot
 right after construction (``init/*``, used to check that
@@ -31,6 +32,7 @@ sys.path.insert(0, ROOT)
 
 import omi_physics as ref                       # noqa: E402  (the reference)
 from omi_physics import gravity as rgravity, joints as rjoints, model as rmodel   # noqa: E402
+from omi_physics import omi_gltf as rgltf        # noqa: E402
 import pyoracle                                  # noqa: E402
 from omi_physics_b200 import scenes              # noqa: E402
 
@@ -138,7 +140,108 @@ def make_capsule_triangles():
           int(np.concatenate(hit).sum()), 'hits')
 
 
+def omi_document(seed=3, n=40):
+    """An OMI glTF physics document: every shape kind, materials with combine
+    modes, collision filters, a joint table, global gravity, dynamic / static /
+    kinematic bodies, sensors and gravity-volume nodes (some bounded by their
+    own sensor shape)."""
+    rng = np.random.default_rng(seed)
+    shapes = [{'type': 'box', 'box': {'size': [20.0, 1.0, 20.0]}},
+              {'type': 'sphere', 'sphere': {'radius': 2.5}},
+              {'type': 'box', 'box': {'size': [3.0, 4.0, 3.0]}},
+              {'type': 'cylinder', 'cylinder': {'height': 1.2, 'radiusBottom': 0.3, 'radiusTop': 0.3}},
+              {'type': 'trimesh', 'trimesh': {'mesh': 1}}]
+    for _ in range(6):
+        k = rng.integers(3)
+        if k == 0:
+            shapes.append({'type': 'box', 'box': {'size': [float(x) for x in rng.uniform(0.4, 1.2, 3)]}})
+        elif k == 1:
+            shapes.append({'type': 'sphere', 'sphere': {'radius': float(rng.uniform(0.2, 0.6))}})
+        else:
+            shapes.append({'type': 'capsule', 'capsule': {'height': float(rng.uniform(0.3, 1.0)),
+                                                          'radius': float(rng.uniform(0.2, 0.4))}})
+    mats = [{'staticFriction': 0.6, 'dynamicFriction': 0.5, 'restitution': 0.1, 'frictionCombine': 'average',
+             'restitutionCombine': 'maximum'},
+            {'staticFriction': 0.9, 'dynamicFriction': 0.8, 'restitution': 0.4, 'frictionCombine': 'minimum',
+             'restitutionCombine': 'multiply'}]
+    filters = [{'collisionSystems': ['props'], 'notCollideWithSystems': ['fx']},
+               {'collisionSystems': ['fx'], 'collideWithSystems': ['ground']}]
+    joints = [{'limits': [{'linearAxes': [0, 1, 2], 'min': 0.0, 'max': 0.0}, {'angularAxes': [0, 2]}],
+               'drives': [{'type': 'angular', 'mode': 'force', 'axis': 1, 'velocityTarget': 2.0,
+                           'maxForce': 40.0}]}]
+    motion = lambda t, **kw: dict({'type': t, 'mass': 1.0, 'centerOfMass': [0, 0, 0],
+                                   'inertiaDiagonal': [0, 0, 0], 'inertiaOrientation': [0, 0, 0, 1],
+                                   'linearVelocity': [0, 0, 0], 'angularVelocity': [0, 0, 0],
+                                   'gravityFactor': 1.0}, **kw)
+    nodes = [{'name': 'ground', 'translation': [0.0, -0.5, 0.0],
+              'extensions': {'OMI_physics_body': {'motion': motion('static'),
+                                                  'collider': {'shape': 0, 'physicsMaterial': 0}}}},
+             {'name': 'well', 'translation': [3.0, 4.0, -2.0],
+              'extensions': {'OMI_physics_body': {'trigger': {'shape': 1}},
+                             'OMI_physics_gravity': {'type': 'point', 'gravity': 5.0, 'priority': 2,
+                                                     'replace': False, 'stop': False,
+                                                     'center': [3.0, 4.0, -2.0]}}},
+             {'name': 'column', 'translation': [-3.0, 2.0, 2.0],
+              'extensions': {'OMI_physics_body': {'trigger': {'shape': 2}},
+                             'OMI_physics_gravity': {'type': 'directional', 'gravity': 3.0, 'priority': 3,
+                                                     'replace': True, 'stop': False,
+                                                     'direction': [0.0, 1.0, 0.0]}}},
+             {'name': 'wind', 'extensions': {'OMI_physics_gravity': {
+                 'type': 'directional', 'gravity': 0.4, 'priority': 0, 'replace': False, 'stop': False,
+                 'direction': [1.0, 0.0, 0.0]}}},
+             {'name': 'lift', 'translation': [0.0, 0.3, 4.0], 'rotation': [0.0, 0.38268343, 0.0, 0.92387953],
+              'extensions': {'OMI_physics_body': {
+                  'motion': motion('kinematic', linearVelocity=[0.0, 0.0, -0.5]),
+                  'collider': {'shape': 3}, 'joint': {'joint': 0, 'connectedNode': 0,
+                                                      'enableCollision': True}}}},
+             {'name': 'mesh', 'translation': [0.0, 0.0, 0.0],
+              'extensions': {'OMI_physics_body': {'collider': {'shape': 4}}}}]
+    for i in range(n):
+        axis = rng.normal(size=3)
+        axis /= np.linalg.norm(axis)
+        ang = rng.uniform(0, np.pi)
+        q = [float(x) for x in np.concatenate([axis * np.sin(ang / 2), [np.cos(ang / 2)]])]
+        body = {'motion': motion('dynamic', mass=float(rng.uniform(0.5, 4.0)),
+                                 linearVelocity=[float(x) for x in rng.normal(0, 0.5, 3)],
+                                 gravityFactor=float(rng.uniform(0.5, 1.5))),
+                'collider': {'shape': int(rng.integers(5, len(shapes)))}}
+        if i % 3 == 0:
+            body['collider']['physicsMaterial'] = int(rng.integers(2))
+        if i % 5 == 0:
+            body['collider']['collisionFilter'] = int(rng.integers(2))
+        nodes.append({'name': 'item%d' % i, 'translation': [float(x) for x in rng.uniform((-4, 1, -4), (4, 6, 4))],
+                      'rotation': q, 'extensions': {'OMI_physics_body': body}})
+    return {'asset': {'version': '2.0'}, 'extensionsUsed': list(rgltf.SUPPORTED),
+            'extensions': {'OMI_physics_shape': {'shapes': shapes},
+                           'OMI_physics_body': {'physicsMaterials': mats, 'collisionFilters': filters},
+                           'OMI_physics_joint': {'physicsJoints': joints},
+                           'OMI_physics_gravity': {'gravity': 9.81, 'direction': [0.0, -1.0, 0.0]}},
+            'nodes': nodes}
+
+
+def make_omi_document():
+    """tests/golden/omi_document.json: the document, the reference's own
+    export of it (omi_gltf.load_document + export_extensions) and the column
+    snapshot of the world built from it with the reference's classes (the
+    triangle-mesh node left out)."""
+    import json
+    from omi_physics_b200.gltf import build_world
+    gltf = omi_document()
+    top, nodes = rgltf.export_extensions(rgltf.load_document(gltf))
+    plain = dict(gltf, nodes=[nd for nd in gltf['nodes'] if nd['name'] != 'mesh'])
+    w = build_world(plain, api=API, fixed_dt=1.0 / 120.0)
+    init = {k[len('init/'):]: v.tolist() for k, v in snapshot_init(w).items()}
+    out = {'gltf': gltf, 'export_top': top, 'export_nodes': {str(k): v for k, v in nodes.items()},
+           'world_init': init, 'volumes': len(w.gravity_volumes)}
+    path = os.path.join(HERE, 'omi_document.json')
+    with open(path, 'w') as f:
+        json.dump(out, f, indent=1, allow_nan=True)
+    print('omi_document', len(gltf['nodes']), 'nodes', w.body_count, 'bodies')
+
+
 def main(names=()):
+    if not names or 'omi_document' in names:
+        make_omi_document()
     if not names or 'capsule_triangles' in names:
         make_capsule_triangles()
     for name, (steps, checkpoints) in STEPS.items():

@@ -61,3 +61,26 @@ def test_serving_budget_refuses_oversized_reservation():
     from omi_physics_b200._lib import OutOfBudget
     with pytest.raises(OutOfBudget):
         Server(size_classes(2048, per_class=64), budget_bytes=64 << 20)
+
+
+def test_serving_an_omi_document():
+    """An OMI glTF document (no sensors or volumes) served through a slot ends
+    where the oracle, stepping the world built from the same document, ends."""
+    import json
+    from golden_util import GOLDEN
+    from omi_physics_b200 import gltf
+    doc = json.load(open(GOLDEN + '/omi_document.json'))['gltf']
+    keep = [nd for nd in doc['nodes'] if nd['name'] not in ('mesh', 'well', 'column', 'wind')]
+    plain = dict(doc, nodes=keep)
+    srv = Server(size_classes(64, per_class=2, min_bodies=32))
+    req = srv.submit_document(plain, steps=90, dt=1 / 120.0)
+    srv.run(clock='ticks')
+    o = pyoracle.OracleWorld.from_world(gltf.build_world(plain, fixed_dt=1 / 120.0))
+    for _ in range(90):
+        o.step(1 / 120.0)
+    st = o.state()
+    n = req.world.body_count
+    for col, key in zip(STATE, ('position', 'orientation', 'linear_velocity', 'angular_velocity', 'awake',
+                                'sleep_timer')):
+        assert np.array_equal(getattr(req.world, col)[:n], st[key]), col
+    srv.close()
