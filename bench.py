@@ -456,14 +456,15 @@ def capsule_triangles_run(seed, blocks, local, steps, warmup, device_only=False)
         torch.cuda.synchronize(dev)
         launches0 = ctx.launches()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(steps, 10 * steps)       # long enough for the clock sampler to see it
         with ClockSampler(local) as clk:
             e0.record(stream)
-            for _ in range(steps):
+            for _ in range(reps):
                 oc.capsule_triangles_device(*args)
             e1.record(stream)
             torch.cuda.synchronize(dev)
         launches = ctx.launches() - launches0
-        ms = e0.elapsed_time(e1) / steps
+        ms = e0.elapsed_time(e1) / reps
         ctx.call('set_stream', None)
     hits = int(th.sum().item())
     value = n / (ms / 1e3)
