@@ -24,7 +24,7 @@ extern "C" {
 #define OMI_OK 0
 #define OMI_E_CUDA (-1)         /* CUDA runtime error (message has details) */
 #define OMI_E_ARG (-2)          /* bad argument / size */
-#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (triangle meshes ...) */
+#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (a moving triangle mesh ...) */
 #define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
 #define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
 #define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
@@ -34,7 +34,7 @@ extern "C" {
 /* OMI_SHAPE_CAPSULE also carries the reference's cylinder, which it collides
  * as a capsule (body.py:224-228): shape_radius = radiusBottom,
  * shape_size = (0, height, 0). Capsule pairs go through GJK/EPA. */
-enum { OMI_SHAPE_SPHERE = 1, OMI_SHAPE_BOX = 2, OMI_SHAPE_CONVEX = 3, OMI_SHAPE_CAPSULE = 4 };
+enum { OMI_SHAPE_SPHERE = 1, OMI_SHAPE_BOX = 2, OMI_SHAPE_CONVEX = 3, OMI_SHAPE_CAPSULE = 4, OMI_SHAPE_TRIMESH = 5 };
 enum { OMI_AVERAGE = 0, OMI_MINIMUM = 1, OMI_MAXIMUM = 2, OMI_MULTIPLY = 3 };
 enum { OMI_JOINT_POINT = 0, OMI_JOINT_DISTANCE = 1, OMI_JOINT_MOTOR = 2 };
 /* per-world flag bits */
@@ -114,6 +114,20 @@ typedef struct OmiScene {
     const double *vol_field;        /* *3: a directional field's acceleration (normalize(direction) *
                                        gravity, as field_at forms it), or a point field's centre */
     const double *vol_rc, *vol_rr;  /* *3: region centre; radius**2 in [0] (sphere) or half-extents (box) */
+
+    /* triangle meshes (body.py:155-212, trigrid.py:63-218): static bodies whose
+     * collider is an OMI_SHAPE_TRIMESH shape (its points listed as for a hull),
+     * each with its triangles in world space and the reference's uniform grid
+     * over them, built on the host from the body's pose */
+    int32_t n_meshes;
+    const int32_t *mesh_body;       /* n_meshes: global body index */
+    const int32_t *mesh_tri_off;    /* n_meshes+1: rows of the triangle tables */
+    const int32_t *mesh_grid_i;     /* n_meshes*4: exact (fewer than 256 triangles), grid shape (3) */
+    const double *mesh_grid_d;      /* n_meshes*7: grid low (3), high (3), cell size */
+    const double *tri_verts;        /* n_tris*9: world vertices */
+    const double *tri_box;          /* n_tris*6: bounds lo (3), hi (3) */
+    const int32_t *tri_cells;       /* n_tris*6: first cell (3), last cell (3) */
+    const uint8_t *tri_big;         /* n_tris: spans more than 64 cells (always a candidate) */
 } OmiScene;
 
 /* gravity volume kind flags: point field (else directional); region sphere,

@@ -65,6 +65,8 @@ class OmiScene(C.Structure):
         ('trigger_shape', I),
         ('w_vol_off', I), ('n_volumes', C.c_int32), ('vol_kind', I), ('vol_g', D), ('vol_field', D),
         ('vol_rc', D), ('vol_rr', D),
+        ('n_meshes', C.c_int32), ('mesh_body', I), ('mesh_tri_off', I), ('mesh_grid_i', I),
+        ('mesh_grid_d', D), ('tri_verts', D), ('tri_box', D), ('tri_cells', I), ('tri_big', U8),
     ]
 
 

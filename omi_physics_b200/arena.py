@@ -19,7 +19,50 @@ from .joints import joint_kind
 from .model import COMBINE_CODES
 
 # a cylinder is collided as a capsule (make_proxy, body.py:224-228)
-SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4}
+SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4, 'trimesh': 5}
+
+
+def _quat_matrix(q) -> np.ndarray:
+    """mathutil.quat_to_matrix (mathutil.py:59-76) of one quaternion, in numpy."""
+    q = np.asarray(q, dtype='d')
+    q = q / np.maximum(np.linalg.norm(q, axis=-1, keepdims=True), 1e-12)
+    x, y, z, w = q[0], q[1], q[2], q[3]
+    xx, yy, zz, xy, xz, yz, wx, wy, wz = x * x, y * y, z * z, x * y, x * z, y * z, w * x, w * y, w * z
+    return np.array([[1 - 2 * (yy + zz), 2 * (xy - wz), 2 * (xz + wy)],
+                     [2 * (xy + wz), 1 - 2 * (xx + zz), 2 * (yz - wx)],
+                     [2 * (xz - wy), 2 * (yz + wx), 1 - 2 * (xx + yy)]])
+
+
+def mesh_tables(points, indices, position, orientation) -> dict:
+    """A static mesh body's triangles as the reference collides them: world
+    vertices (``points @ R.T + position``, body.py:164), per-triangle bounds
+    and the uniform grid of trigrid.py:63-97 (64 cells along the longest
+    side, triangles spanning more than 64 cells set aside, no grid below 256
+    triangles), with numpy's arithmetic throughout."""
+    R = _quat_matrix(orientation)
+    wp = np.asarray(points, dtype='d') @ R.T + np.asarray(position, dtype='d')
+    tris = wp[np.asarray(indices, dtype=np.int64).reshape(-1, 3)]
+    lo, hi = tris.min(axis=1), tris.max(axis=1)
+    T = len(tris)
+    gi = np.zeros(4, np.int32)
+    gd = np.zeros(7)
+    cells = np.zeros((T, 6), np.int32)
+    big = np.zeros(T, np.uint8)
+    if T < 256:
+        gi[0] = 1
+    else:
+        low, high = lo.min(axis=0), hi.max(axis=0)
+        extent = np.maximum(high - low, 1e-9)
+        cell = float(extent.max()) / 64
+        top = (1 << 30) - 1
+        first = np.clip(np.floor((lo - low) / cell).astype(int), 0, top)
+        last = np.clip(np.floor((hi - low) / cell).astype(int), 0, top)
+        gi[1:] = last.max(axis=0) + 1
+        gd[:3], gd[3:6], gd[6] = low, high, cell
+        cells[:, :3], cells[:, 3:] = first, last
+        big[:] = np.prod(last - first + 1, axis=1) > 64
+    return dict(verts=tris.reshape(T, 9), box=np.concatenate([lo, hi], axis=1), cells=cells, big=big,
+                grid_i=gi, grid_d=gd)
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
 
@@ -70,6 +113,16 @@ def check_supported(world) -> None:
         t = world.shapes[s].type
         if t not in SHAPE_CODES:
             raise UnsupportedFeature(-3, 'shape type %r is not supported on the CUDA path' % t)
+    ts = np.asarray(world._trigger_shape[:n])
+    cs = np.asarray(world._collider_shape[:n])
+    for i in range(n):
+        if 0 <= ts[i] < len(world.shapes) and world.shapes[int(ts[i])].type == 'trimesh':
+            raise UnsupportedFeature(-3, 'triangle-mesh sensors are not supported on the CUDA path')
+        if 0 <= cs[i] < len(world.shapes) and world.shapes[int(cs[i])].type == 'trimesh':
+            if int(world._motion_type[i]) != 0:
+                raise UnsupportedFeature(-3, 'triangle meshes are taken as static colliders only')
+            if world.shapes[int(cs[i])].points is None or world.shapes[int(cs[i])].indices is None:
+                raise UnsupportedFeature(-3, 'a triangle mesh needs its points and indices')
 
 
 class PackedScene:
@@ -102,8 +155,9 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                              'j_a', 'j_b', 'j_anchor', 'j_anchor_b', 'j_local_a', 'j_local_b',
                              'j_has_local_a', 'j_has_local_b', 'j_length', 'j_has_length',
                              'j_axis', 'j_target', 'j_max_force', 'j_accum', 'trigger_shape',
-                             'vol_kind', 'vol_g', 'vol_field', 'vol_rc', 'vol_rr')}
-    body_off, joint_off, vol_off = [0], [0], [0]
+                             'vol_kind', 'vol_g', 'vol_field', 'vol_rc', 'vol_rr', 'mesh_body',
+                             'mesh_grid_i', 'mesh_grid_d', 'tri_verts', 'tri_box', 'tri_cells', 'tri_big')}
+    body_off, joint_off, vol_off, tri_off = [0], [0], [0], [0]
     any_sensor = False
     w_g, w_dt, w_iters, w_jiters, w_flags, w_damp, w_solver = [], [], [], [], [], [], []
     w_foff, w_frows, w_pfoff, w_pfn = [], [], [], []
@@ -131,6 +185,16 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
         tvalid = (ts >= 0) & (ts < len(world.shapes))
         any_sensor |= bool(tvalid.any())
         parts['trigger_shape'].append(np.where(tvalid, ts + ns, -1).astype(np.int32))
+        for i in range(n):
+            if valid[i] and world.shapes[int(cs[i])].type == 'trimesh':
+                sh = world.shapes[int(cs[i])]
+                mt = mesh_tables(sh.points, sh.indices, world._position[i], world._orientation[i])
+                parts['mesh_body'].append([nb + i])
+                parts['mesh_grid_i'].append(mt['grid_i'])
+                parts['mesh_grid_d'].append(mt['grid_d'])
+                for key in ('verts', 'box', 'cells', 'big'):
+                    parts['tri_' + key].append(mt[key])
+                tri_off.append(tri_off[-1] + len(mt['big']))
         vols = pack_volumes(getattr(world, 'gravity_volumes', None) or [])
         for key in ('kind', 'g', 'field', 'rc', 'rr'):
             if len(vols[key]):
@@ -155,7 +219,7 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                 parts['shape_radius'].append([float(sh.radius)])
                 size = np.asarray(sh.size, 'd') if np.size(sh.size) == 3 else np.zeros(3)
                 parts['shape_size'].append(size.reshape(1, 3))
-            if sh.type == 'convex':
+            if sh.type in ('convex', 'trimesh'):
                 pts = np.asarray(sh.points, 'd').reshape(-1, 3)
                 parts['shape_pt_off'].append([npts])
                 parts['shape_pt_cnt'].append([len(pts)])
@@ -311,6 +375,16 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
         P.set('vol_g', cat('vol_g', 'd'), D)
         for key in ('vol_field', 'vol_rc', 'vol_rr'):
             P.set(key, cat(key, 'd', 3), D)
+    if len(tri_off) > 1:
+        s.n_meshes = len(tri_off) - 1
+        P.set('mesh_body', cat('mesh_body', np.int32), I)
+        P.set('mesh_tri_off', np.array(tri_off, np.int32), I)
+        P.set('mesh_grid_i', cat('mesh_grid_i', np.int32, 4), I)
+        P.set('mesh_grid_d', cat('mesh_grid_d', 'd', 7), D)
+        P.set('tri_verts', cat('tri_verts', 'd', 9), D)
+        P.set('tri_box', cat('tri_box', 'd', 6), D)
+        P.set('tri_cells', cat('tri_cells', np.int32, 6), I)
+        P.set('tri_big', cat('tri_big', np.uint8), U8)
     P.has_sensors = any_sensor
     P.body_off = body_off
     P.joint_off = joint_off

@@ -61,7 +61,7 @@ struct Arena {
     double *timer;
     uint8_t *awake;
     const int *mtype, *shape, *material, *material_key, *filter_row, *body_world;
-    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 convex, 4 capsule (of rshape)
+    const int8_t *kind;      // 0 no shape, 1 sphere, 2 box, 3 convex, 4 capsule, 5 triangle mesh (of rshape)
     const double *half;      // refit half extents (world.py:443-469)
     const int *tshape;       // sensor shape (triggers.py) or -1
     const int *rshape;       // the shape a body's AABB comes from: collider, else sensor
@@ -97,13 +97,24 @@ struct Arena {
     int *sort_v[2];
     int *pair_cnt, *pair_scan;      // NB, NB+1
     int *pair_a, *pair_b;           // pair_cap
-    uint8_t *pair_solid;            // 1 contact pair, 2 sensor pair (no contact), 0 neither
+    uint8_t *pair_solid;            // 1 contact pair, 2 sensor pair (no contact), 3 contact pair with a
+                                    // triangle mesh (contacts written by k_mesh_emit), 0 neither
 
     // narrowphase
     int *slot_cnt;                  // pair_cap (+1 scratch)
     double *slot;                   // pair_cap * SLOT
     int *gjk_list, *gjk_n;
     int *trig_list, *trig_n;        // sensor pairs this step (pair indices)
+    int *mesh_list, *mesh_n;        // pairs with a triangle-mesh body this step
+    // static triangle-mesh bodies (body.py:155-212): per mesh its triangle rows
+    // [mesh_tri_off[m], mesh_tri_off[m+1]), the reference's uniform grid
+    // (trigrid.py: exact flag, grid shape (3); low (3), high (3), cell size)
+    // and per triangle world vertices (9), bounds (6), cell range (6), big flag
+    const int *body_mesh;           // per body: mesh row or -1
+    const int *mesh_tri_off, *mesh_grid_i;
+    const double *mesh_grid_d, *tri_verts, *tri_box;
+    const int *tri_cells;
+    const uint8_t *tri_big;
     int *trig_out;                  // per sensor pair: trigger, other, overlap (1/0, -1 no shape)
     int *clip_list, *clip_n;        // touching box-box pairs awaiting face clipping
     int *contact_scan;              // pair_cap + 1

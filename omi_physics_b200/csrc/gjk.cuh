@@ -31,7 +31,7 @@ constexpr int EPA_F = 512;
 constexpr int EPA_E = 3 * EPA_F;
 
 struct Proxy {
-    int kind;              // 1 sphere, 2 box, 3 convex, 4 capsule
+    int kind;              // 1 sphere, 2 box, 3 convex, 4 capsule, 5 triangle (local = 3 world vertices)
     double c[3], R[9], h[3], r;
     double e0[3], e1[3];   // capsule segment ends
     const double *local;   // convex local points (global memory)
@@ -69,7 +69,7 @@ __device__ inline int warp_min_index(int i) {
 #endif
 }
 
-// Proxy.support(d) (body.py:46-48, 69-73, 100-104, 125-128)
+// Proxy.support(d) (body.py:46-48, 69-73, 100-104, 125-128, 146-148)
 __device__ inline void support(const Proxy &p, const double *d, double *out) {
     if (p.kind == 1) {
         double u[3];
@@ -84,6 +84,16 @@ __device__ inline void support(const Proxy &p, const double *d, double *out) {
             s[j] = sg * p.h[j];
         }
         for (int k = 0; k < 3; k++) out[k] = p.c[k] + gemv_row(&p.R[k * 3], s);
+    } else if (p.kind == 5) {
+        // TriangleProxy.support (body.py:146-148): the first vertex of the
+        // largest verts @ d
+        int best = 0;
+        double bv = gemv_row(&p.local[0], d);
+        for (int i = 1; i < 3; i++) {
+            const double v = gemv_row(&p.local[i * 3], d);
+            if (v > bv) { bv = v; best = i; }
+        }
+        for (int k = 0; k < 3; k++) out[k] = p.local[best * 3 + k];
     } else if (p.kind == 4) {
         // the segment end farther along d (the second on ties), plus radius
         const double *end = dot_blas(p.e0, d) > dot_blas(p.e1, d) ? p.e0 : p.e1;
@@ -113,6 +123,10 @@ __device__ inline void support(const Proxy &p, const double *d, double *out) {
 }
 
 __device__ inline void center_hint(const Proxy &p, double *out) {
+    if (p.kind == 5) {                     // verts.mean(axis=0) (body.py:150-152)
+        for (int k = 0; k < 3; k++) out[k] = ((p.local[k] + p.local[3 + k]) + p.local[6 + k]) / 3.0;
+        return;
+    }
     if (p.kind != 3) { out[0] = p.c[0]; out[1] = p.c[1]; out[2] = p.c[2]; return; }
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;   // mean(axis=0): sequential row sum
     for (int i = 0; i < p.m; i++) {

@@ -11,6 +11,7 @@
 #include "arena.cuh"
 #include "geometry.cuh"
 #include "gjk.cuh"
+#include "capsule.cuh"
 
 namespace omi {
 
@@ -35,7 +36,7 @@ __device__ __forceinline__ bool dyn(const Arena &A, int i) { return A.mtype[i] =
 // einsum('nij,nkj->nik', R*invI, R) (solver.py:215-220), one thread per body
 // ---------------------------------------------------------------------------
 __global__ void k_refit(Arena A) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) { A.gjk_n[0] = 0; A.clip_n[0] = 0; A.trig_n[0] = 0; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.gjk_n[0] = 0; A.clip_n[0] = 0; A.trig_n[0] = 0; A.mesh_n[0] = 0; }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.NB; i += gridDim.x * blockDim.x) {
         int w = A.body_world[i];
         if (!world_collides(A, w) || i - A.w_body_off[w] >= A.w_body_n[w]) continue;
@@ -52,7 +53,7 @@ __global__ void k_refit(Arena A) {
         }
         if (kind == 0) {
             for (int r = 0; r < 3; r++) lo[r] = hi[r] = p[r];
-        } else if (kind == 3) {
+        } else if (kind == 3 || kind == 5) {         // hull or mesh: world points min / max
             const int s = A.rshape[i];
             const double *pts = &A.points[A.pt_off[s] * 3];
             const int m = A.pt_cnt[s];
@@ -493,7 +494,12 @@ __global__ void k_narrow(Arena A) {
             const int a = A.pair_a[p], b = A.pair_b[p];
             const int ka = A.kind[a], kb = A.kind[b];
             double *s = &A.slot[(size_t)p * SLOT];
-            if (ka >= 3 || kb >= 3) {
+            if (ka == 5 || kb == 5) {
+                // the mesh route (collide.py:272-306): counted by k_mesh_count,
+                // written straight into the contact arrays by k_mesh_emit
+                A.pair_solid[p] = 3;
+                A.mesh_list[atomicAdd(A.mesh_n, 1)] = p;
+            } else if (ka >= 3 || kb >= 3) {
                 const int idx = atomicAdd(A.gjk_n, 1);
                 A.gjk_list[idx] = p;
             } else {
@@ -674,12 +680,195 @@ __global__ void k_triggers(Arena A) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// triangle meshes (collide.py:272-306 with trigrid.py): a static mesh body
+// against another body, one warp per pair. The candidates are the triangles
+// the reference's uniform grid hands back for the other proxy's bounds
+// (trigrid.py:99-111): every triangle whose bounds meet the query when the
+// mesh has fewer than 256 triangles, else the oversized ones plus those
+// binned in a cell the query's cell range covers. A capsule is tested
+// against its candidates in one pass (capsule_triangle_batch), any other
+// proxy through GJK/EPA with one candidate triangle at a time. Contacts come
+// in ascending triangle order, normals from a to b. k_mesh_count writes the
+// pair's count for the contact scan; k_mesh_emit repeats the pass and writes
+// the contacts at the pair's place in the contact arrays.
+// ---------------------------------------------------------------------------
+// the proxy's own bounds, no margin (body.py: aabb() of each proxy kind)
+__device__ inline void proxy_bounds(const Proxy &P, double *lo, double *hi) {
+    if (P.kind == 1) {
+        for (int c = 0; c < 3; c++) { lo[c] = P.c[c] - P.r; hi[c] = P.c[c] + P.r; }
+    } else if (P.kind == 2) {              // _box_corners(half) @ R.T + center
+        for (int c = 0; c < 3; c++) { lo[c] = INFINITY; hi[c] = -INFINITY; }
+        for (int k = 0; k < 8; k++) {
+            const double sv[3] = {(k & 4) ? P.h[0] : -P.h[0], (k & 2) ? P.h[1] : -P.h[1], (k & 1) ? P.h[2] : -P.h[2]};
+            for (int c = 0; c < 3; c++) {
+                const double x = dot_blas(sv, &P.R[c * 3]) + P.c[c];
+                lo[c] = x < lo[c] ? x : lo[c];
+                hi[c] = x > hi[c] ? x : hi[c];
+            }
+        }
+    } else if (P.kind == 4) {
+        for (int c = 0; c < 3; c++) {
+            lo[c] = (P.e0[c] < P.e1[c] ? P.e0[c] : P.e1[c]) - P.r;
+            hi[c] = (P.e0[c] > P.e1[c] ? P.e0[c] : P.e1[c]) + P.r;
+        }
+    } else {
+        for (int i = 0; i < P.m; i++)
+            for (int c = 0; c < 3; c++) {
+                const double x = dot_blas(&P.local[i * 3], &P.R[c * 3]) + P.c[c];
+                if (i == 0 || x < lo[c]) lo[c] = x;
+                if (i == 0 || x > hi[c]) hi[c] = x;
+            }
+    }
+}
+
+// numpy's float floor division (npy_divmod): fmod, then snap to the integer
+__device__ inline double py_floordiv(double a, double b) {
+    double mod = fmod(a, b);
+    double div = (a - mod) / b;
+    if (mod != 0.0 && ((b < 0) != (mod < 0))) div -= 1.0;
+    if (div != 0.0) {
+        double fd = floor(div);
+        if (div - fd > 0.5) fd += 1.0;
+        return fd;
+    }
+    return copysign(0.0, a / b);
+}
+
+// TriangleGrid._corner (trigrid.py:113-127) on one axis
+__device__ inline int grid_corner(double p, double low, double cell, int shape) {
+    const double q = py_floordiv(p - low, cell);
+    long long c = (long long)q;
+    c = c < 0 ? 0 : c;
+    return (int)(c > shape - 1 ? shape - 1 : c);
+}
+
+__device__ int mesh_pair(const Arena &A, int p, bool emit, EpaWork &W) {
+    const int lane = threadIdx.x & 31;
+    const int a = A.pair_a[p], b = A.pair_b[p];
+    const bool mesh_is_a = A.kind[a] == 5;
+    const int mb = mesh_is_a ? a : b, ob = mesh_is_a ? b : a;
+    const int m = A.body_mesh[mb];
+    Proxy O;
+    make_proxy(A, ob, O);
+    double lo[3], hi[3];
+    proxy_bounds(O, lo, hi);
+    const int *gi = &A.mesh_grid_i[m * 4];
+    const double *gd = &A.mesh_grid_d[m * 7];
+    const bool exact = gi[0] != 0;
+    bool outside = false;
+    int fq[3] = {0, 0, 0}, lq[3] = {0, 0, 0};
+    if (!exact) {
+        for (int k = 0; k < 3; k++) outside |= lo[k] > gd[3 + k] || hi[k] < gd[k];
+        for (int k = 0; k < 3; k++) {
+            fq[k] = grid_corner(lo[k], gd[k], gd[6], gi[1 + k]);
+            lq[k] = grid_corner(hi[k], gd[k], gd[6], gi[1 + k]);
+        }
+    }
+    const int t0 = A.mesh_tri_off[m], t1 = A.mesh_tri_off[m + 1];
+    const int out0 = emit ? A.contact_scan[p] : 0;
+    int count = 0;
+    for (int base = t0; base < t1; base += 32) {
+        const int t = base + lane;
+        bool cand = false;
+        if (t < t1) {
+            const double *bx = &A.tri_box[(size_t)t * 6];
+            if (exact) {
+                cand = bx[0] <= hi[0] && bx[1] <= hi[1] && bx[2] <= hi[2] && bx[3] >= lo[0] && bx[4] >= lo[1] &&
+                       bx[5] >= lo[2];
+            } else if (A.tri_big[t]) {
+                cand = true;
+            } else if (!outside) {
+                const int *tc = &A.tri_cells[(size_t)t * 6];
+                cand = max(fq[0], tc[0]) <= min(lq[0], tc[3]) && max(fq[1], tc[1]) <= min(lq[1], tc[4]) &&
+                       max(fq[2], tc[2]) <= min(lq[2], tc[5]);
+            }
+        }
+        if (O.kind == 4) {
+            // capsule_triangle_batch: every lane its own candidate
+            bool hit = false;
+            double pt[3], nr[3], dep = 0.0;
+            if (cand) {
+                const double *v = &A.tri_verts[(size_t)t * 9];
+                const double centre[3] = {(O.e0[0] + O.e1[0]) * 0.5, (O.e0[1] + O.e1[1]) * 0.5,
+                                          (O.e0[2] + O.e1[2]) * 0.5};
+                hit = capsule_triangle(O.e0, O.e1, centre, O.r, v, v + 3, v + 6, pt, nr, &dep) != 0;
+                if (hit && !mesh_is_a) { nr[0] = -nr[0]; nr[1] = -nr[1]; nr[2] = -nr[2]; }
+            }
+            const unsigned mk = __ballot_sync(FULL, hit);
+            if (hit && emit) {
+                const int k = out0 + count + __popc(mk & ((1u << lane) - 1u));
+                if (k < A.contact_cap) {
+                    A.c_a[k] = a; A.c_b[k] = b;
+                    for (int c = 0; c < 3; c++) { A.c_n[k * 3 + c] = nr[c]; A.c_pt[k * 3 + c] = pt[c]; }
+                    A.c_depth[k] = dep;
+                    A.c_imp[k * 3] = A.c_imp[k * 3 + 1] = A.c_imp[k * 3 + 2] = 0.0;
+                }
+            }
+            count += __popc(mk);
+        } else {
+            // collide_convex with a TriangleProxy, one candidate at a time,
+            // the whole warp on each
+            unsigned mk = __ballot_sync(FULL, cand);
+            while (mk) {
+                const int l = __ffs(mk) - 1;
+                mk &= mk - 1;
+                Proxy T;
+                T.kind = 5;
+                T.local = &A.tri_verts[(size_t)(base + l) * 9];
+                T.m = 3;
+                double nrm[3], pt[3], dep = 0.0;
+                const int r = mesh_is_a ? collide_convex(T, O, W, nrm, pt, &dep) : collide_convex(O, T, W, nrm, pt, &dep);
+                if (r < 0 && lane == 0 && !emit) atomicAdd(&A.status[ST_EPA_LIMIT], 1);
+                if (r > 0) {
+                    const int k = out0 + count;
+                    if (emit && lane == 0 && k < A.contact_cap) {
+                        A.c_a[k] = a; A.c_b[k] = b;
+                        for (int c = 0; c < 3; c++) { A.c_n[k * 3 + c] = nrm[c]; A.c_pt[k * 3 + c] = pt[c]; }
+                        A.c_depth[k] = dep;
+                        A.c_imp[k * 3] = A.c_imp[k * 3 + 1] = A.c_imp[k * 3 + 2] = 0.0;
+                    }
+                    count++;
+                }
+                __syncwarp();
+            }
+        }
+    }
+    return count;
+}
+
+__global__ void k_mesh_count(Arena A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (pairs_over(A)) return;
+    EpaWork &W = reinterpret_cast<EpaWork *>(smem)[threadIdx.x >> 5];
+    const int n = *A.mesh_n;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < n; it += nwarps) {
+        const int p = A.mesh_list[it];
+        const int cnt = mesh_pair(A, p, false, W);
+        if ((threadIdx.x & 31) == 0) A.slot_cnt[p] = cnt;
+        __syncwarp();
+    }
+}
+
+__global__ void k_mesh_emit(Arena A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (overflowed(A)) return;
+    EpaWork &W = reinterpret_cast<EpaWork *>(smem)[threadIdx.x >> 5];
+    const int n = *A.mesh_n;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < n; it += nwarps) {
+        mesh_pair(A, A.mesh_list[it], true, W);
+        __syncwarp();
+    }
+}
+
 __global__ void k_contact_compact(Arena A) {
     if (overflowed(A)) return;
     const int P = A.pair_scan[A.NB];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
         const int cnt = A.slot_cnt[p];
-        if (!cnt) continue;
+        if (!cnt || A.pair_solid[p] == 3) continue;      // mesh pairs: k_mesh_emit
         const int base = A.contact_scan[p];
         const double *s = &A.slot[(size_t)p * SLOT];
         for (int j = 0; j < cnt; j++) {

@@ -61,6 +61,7 @@ struct OmiCtx {
     int stage_doubles = 0;         // doubles of world state k_iterate stages in shared memory
     int cache_cap = 0;
     bool has_triggers = false;     // some body carries a sensor shape: k_triggers runs each step
+    bool has_meshes = false;       // some body is a triangle mesh: k_mesh_count / k_mesh_emit run
     cudaGraphExec_t graph = nullptr;
     int *h_status = nullptr;       // pinned mirror of the status words
     int64_t launches = 0;
@@ -173,6 +174,7 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.clip_list, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.gjk_list, pair_cap);
     rc |= alloc(ctx, ctx->dyn, A.trig_list, ctx->has_triggers ? pair_cap : 1);
+    rc |= alloc(ctx, ctx->dyn, A.mesh_list, ctx->has_meshes ? pair_cap : 1);
     rc |= alloc(ctx, ctx->dyn, A.trig_out, ctx->has_triggers ? 3 * (size_t)pair_cap : 3);
     rc |= alloc(ctx, ctx->dyn, A.contact_scan, (size_t)pair_cap + 1);
     rc |= alloc(ctx, ctx->dyn, A.c_a, contact_cap);
@@ -298,6 +300,10 @@ void stage_narrow(OmiCtx *ctx, Prof *pf) {
     mark(ctx, pf, KN_NARROW);
     k_gjk<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
     ctx->launches++;
+    if (ctx->has_meshes) {
+        k_mesh_count<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
+        ctx->launches++;
+    }
     mark(ctx, pf, KN_GJK);
     launch_scan(ctx, A.slot_cnt, A.contact_scan, 0, A.pair_scan + A.NB, A.pair_cap, A.pair_scan, A.NB, A.pair_cap);
     k_contact_check<<<1, 1, 0, ctx->stream>>>(A);
@@ -309,6 +315,10 @@ void stage_compact(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
     k_contact_compact<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
     ctx->launches++;
+    if (ctx->has_meshes) {
+        k_mesh_emit<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
+        ctx->launches++;
+    }
     mark(ctx, pf, KN_COMPACT);
 }
 
@@ -415,6 +425,7 @@ int64_t step_launches(OmiCtx *ctx) {
     int64_t n = 1 + 1 + 1 + 3 + 1 + 2 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
     if (ctx->A.NJ > 0) n += 1;
     if (ctx->has_triggers) n += 1;
+    if (ctx->has_meshes) n += 2;
     return n;
 }
 
@@ -486,6 +497,8 @@ int omi_create(int device, OmiCtx **out) {
     const struct { const void *fn; int bytes; const char *name; } smem[] = {
         {(const void *)k_gjk, 4 * (int)sizeof(EpaWork), "k_gjk"},
         {(const void *)k_triggers, 4 * (int)sizeof(EpaWork), "k_triggers"},
+        {(const void *)k_mesh_count, 4 * (int)sizeof(EpaWork), "k_mesh_count"},
+        {(const void *)k_mesh_emit, 4 * (int)sizeof(EpaWork), "k_mesh_emit"},
         {(const void *)k_sort<true>, 8192 * 24, "k_sort"},
         {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
@@ -624,10 +637,35 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
             half[i * 3] = s->shape_radius[sh];
             half[i * 3 + 1] = 0.5 * s->shape_size[sh * 3 + 1];
             half[i * 3 + 2] = 0.0;
+        } else if (t == OMI_SHAPE_TRIMESH) {
+            kind[i] = 5;
+            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
+                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
+                return fail(ctx, OMI_E_ARG, "mesh point range out of bounds");
+            if (s->shape[i] != sh || s->motion_type[i] != 0)
+                return fail(ctx, OMI_E_UNSUPPORTED, "triangle meshes are taken as static colliders only");
         } else {
             return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
         }
     }
+    // triangle meshes: every mesh body listed once, its tables in range
+    std::vector<int> body_mesh(NB, -1);
+    const int NMESH = s->mesh_body ? s->n_meshes : 0;
+    int n_tris = 0;
+    if (NMESH) {
+        if (s->mesh_tri_off[0] != 0) return fail(ctx, OMI_E_ARG, "mesh triangle offsets must start at 0");
+        for (int m = 0; m < NMESH; m++) {
+            const int b = s->mesh_body[m];
+            if (b < 0 || b >= NB || kind[b] != 5 || body_mesh[b] >= 0) return fail(ctx, OMI_E_ARG, "mesh body");
+            if (s->mesh_tri_off[m + 1] < s->mesh_tri_off[m]) return fail(ctx, OMI_E_ARG, "mesh triangle offsets decrease");
+            const int *gi = &s->mesh_grid_i[m * 4];
+            if (!gi[0] && (gi[1] < 1 || gi[2] < 1 || gi[3] < 1)) return fail(ctx, OMI_E_ARG, "mesh grid shape");
+            body_mesh[b] = m;
+        }
+        n_tris = s->mesh_tri_off[NMESH];
+    }
+    for (int i = 0; i < NB; i++)
+        if (kind[i] == 5 && body_mesh[i] < 0) return fail(ctx, OMI_E_ARG, "a mesh body without its triangle tables");
     for (int p = 0; p < s->n_pair_friction; p++)
         if (s->pf_a[p] >= s->n_materials || s->pf_b[p] >= s->n_materials)
             return fail(ctx, OMI_E_ARG, "pair-friction material out of range");
@@ -696,6 +734,15 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= upload(ctx, const_cast<int8_t *&>(A.kind), kind.data(), NB);
     rc |= upload(ctx, const_cast<double *&>(A.half), half.data(), (size_t)NB * 3);
     rc |= upload(ctx, const_cast<int *&>(A.tshape), tshape.data(), NB);
+    rc |= upload(ctx, const_cast<int *&>(A.body_mesh), body_mesh.data(), NB);
+    rc |= upload(ctx, const_cast<int *&>(A.mesh_tri_off), NMESH ? s->mesh_tri_off : nullptr, (size_t)NMESH + 1);
+    rc |= upload(ctx, const_cast<int *&>(A.mesh_grid_i), NMESH ? s->mesh_grid_i : nullptr, (size_t)NMESH * 4);
+    rc |= upload(ctx, const_cast<double *&>(A.mesh_grid_d), NMESH ? s->mesh_grid_d : nullptr, (size_t)NMESH * 7);
+    rc |= upload(ctx, const_cast<double *&>(A.tri_verts), n_tris ? s->tri_verts : nullptr, (size_t)n_tris * 9);
+    rc |= upload(ctx, const_cast<double *&>(A.tri_box), n_tris ? s->tri_box : nullptr, (size_t)n_tris * 6);
+    rc |= upload(ctx, const_cast<int *&>(A.tri_cells), n_tris ? s->tri_cells : nullptr, (size_t)n_tris * 6);
+    rc |= upload(ctx, const_cast<uint8_t *&>(A.tri_big), n_tris ? s->tri_big : nullptr, n_tris);
+    ctx->has_meshes = NMESH > 0;
     rc |= upload(ctx, const_cast<int *&>(A.rshape), rshape.data(), NB);
     ctx->has_triggers = sensors;
     // gravity volumes
@@ -765,6 +812,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.w_runs, W);
     rc |= alloc(ctx, ctx->statics, A.gjk_n, 1);
     rc |= alloc(ctx, ctx->statics, A.trig_n, 1);
+    rc |= alloc(ctx, ctx->statics, A.mesh_n, 1);
     rc |= alloc(ctx, ctx->statics, A.clip_n, 1);
     rc |= alloc(ctx, ctx->statics, A.sweep_next, 1);
     for (int t = 0; t < 2; t++) {
@@ -925,6 +973,7 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
             kind[i] = 4;
             half[i * 3] = o->shape_radius[sh]; half[i * 3 + 1] = 0.5 * o->shape_size[sh * 3 + 1]; half[i * 3 + 2] = 0.0;
         }
+        else if (t == OMI_SHAPE_TRIMESH) return fail(ctx, OMI_E_UNSUPPORTED, "serving slots do not take triangle meshes");
         else if (t == OMI_SHAPE_CONVEX) {
             kind[i] = 3;
             if (o->shape_pt_cnt[sh] < 1 || o->shape_pt_off[sh] < 0 || o->shape_pt_off[sh] + o->shape_pt_cnt[sh] > np_)

@@ -5,8 +5,8 @@ reference defines them in ``src/omi_physics/model.py:33-243``; keeping them
 identical is what lets a scene written against the reference load here
 unchanged. Only the parts the CUDA step consumes are listed (shapes, motion,
 collider, material, collision filter, global gravity) plus the joint/trigger
-records so documents round-trip; triangle meshes are rejected by the
-backend (:class:`omi_physics_b200.backend.UnsupportedFeature`).
+records so documents round-trip; triangle meshes are taken on static
+bodies only (:class:`omi_physics_b200.backend.UnsupportedFeature` otherwise).
 """
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -53,6 +53,13 @@ class Shape:
     def convex(cls, points) -> 'Shape':
         """Convex hull of an ``(M, 3)`` local point cloud (its own hull)."""
         return cls(type='convex', points=np.asarray(points, dtype='d'))
+
+    @classmethod
+    def trimesh(cls, points, indices) -> 'Shape':
+        """Triangle soup: local vertices ``(M, 3)`` and triangles ``(T, 3)``
+        (model.py:78-82); collided triangle by triangle, static bodies only."""
+        return cls(type='trimesh', points=np.asarray(points, dtype='d'),
+                   indices=np.asarray(indices, dtype='i'))
 
     @classmethod
     def capsule(cls, height: float = 1.0, radius: float = 0.5) -> 'Shape':

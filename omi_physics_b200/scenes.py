@@ -15,6 +15,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``joint_chain``  pinned chain of 0.2x0.2x1 m links plus loose boxes
   * ``capsule_pile`` capsules / cylinders / boxes / spheres in a walled arena
   * ``zones``        debris through trigger sensors and gravity volumes
+  * ``terrain``      capsules, boxes, spheres and hulls on static triangle meshes
 """
 import math
 from types import SimpleNamespace
@@ -291,6 +292,68 @@ def zones(api=None, backend=None, n: int = 120, seed: int = 0, iterations: int =
     return w, dict(dt=1.0 / 120.0, steps=300, name='zones%d' % n)
 
 
+def _grid_mesh(cells: int, extent: float, amp: float, phase: float):
+    """A rippled square grid in the xz plane: vertices ``(cells+1)^2``, two
+    triangles per cell."""
+    xs = np.linspace(-extent, extent, cells + 1)
+    pts = np.array([(x, amp * math.sin(0.9 * i + phase) * math.cos(0.7 * j), z)
+                    for i, x in enumerate(xs) for j, z in enumerate(xs)], dtype='d')
+    idx = []
+    for i in range(cells):
+        for j in range(cells):
+            a, b = i * (cells + 1) + j, (i + 1) * (cells + 1) + j
+            idx.append((a, b, a + 1))
+            idx.append((b, b + 1, a + 1))
+    return pts, np.array(idx, dtype=np.int64)
+
+
+def terrain(api=None, backend=None, n: int = 60, seed: int = 0, iterations: int = 8,
+            cells: int = 24, extent: float = 6.0):
+    """Bodies falling onto static triangle meshes: a rippled floor large
+    enough for the reference's triangle grid and a small tilted ramp it scans
+    exactly. 40% capsules (the batched capsule route), the rest boxes,
+    spheres and hulls (GJK/EPA against each candidate triangle)."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    pts, idx = _grid_mesh(cells, extent, 0.15, 0.3)
+    floor = w.add_shape(m.Shape.trimesh(pts, idx))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=floor, physicsMaterial=gmat), position=(0.0, 0.0, 0.0))
+    rp, ri = _grid_mesh(4, 1.5, 0.0, 0.0)
+    ramp = w.add_shape(m.Shape.trimesh(rp, ri))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ramp, physicsMaterial=gmat), position=(2.5, 0.8, -2.0),
+               orientation=_quat_axis_angle(np.array([1.0, 0.0, 0.3]), 0.35))
+    u = rng.random(n)
+    lim = extent - 1.5
+    pos = rng.uniform((-lim, 1.0, -lim), (lim, 5.0, lim), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    for i in range(n):
+        r = float(rng.uniform(0.2, 0.4))
+        if u[i] < 0.4:
+            h = float(rng.uniform(0.3, 0.9))
+            shape = w.add_shape(m.Shape.capsule(h, r))
+            mass = 1000.0 * (math.pi * r * r * h + (4.0 / 3.0) * math.pi * r ** 3)
+        elif u[i] < 0.6:
+            sz = tuple(float(x) for x in rng.uniform(0.3, 0.8, 3))
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        elif u[i] < 0.8:
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        else:
+            semi = rng.uniform(0.2, 0.5, 3)
+            shape = w.add_shape(m.Shape.convex(_ellipsoid_points(rng, 12, semi)))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * float(np.prod(semi))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass), m.Collider(shape=shape, physicsMaterial=gmat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='terrain%d' % n)
+
+
 def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
                 motor_frac: float = 0.1, iterations: int = 12):
     """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
@@ -396,6 +459,7 @@ GOLDEN_SCENES = {
     'capsules': lambda api=None, backend=None: capsule_pile(api, backend, n=96, seed=7, arena=8.0,
                                                            height=6.0),
     'zones': lambda api=None, backend=None: zones(api, backend),
+    'terrain': lambda api=None, backend=None: terrain(api, backend),
 }
 
 

@@ -992,13 +992,16 @@ static int push_contact(OrWorld *w, Caps *cp, int a, int b, const double *pt, co
     return 0;
 }
 
+static int collide_mesh(OrWorld *w, Caps *cp, int a, int b);
+
 static int narrowphase(OrWorld *w) {
     Caps *cp = caps_for(w);
     w->n_solid = 0;
     w->n_contacts = 0;
     int maxpts = 1;
     for (int s = 0; s < w->n_shapes; s++)
-        if (w->shape_type[s] == OR_SHAPE_CONVEX && w->shape_pt_cnt[s] > maxpts) maxpts = w->shape_pt_cnt[s];
+        if ((w->shape_type[s] == OR_SHAPE_CONVEX || w->shape_type[s] == OR_SHAPE_TRIMESH) &&
+            w->shape_pt_cnt[s] > maxpts) maxpts = w->shape_pt_cnt[s];
     double *sa = (double *)malloc(sizeof(double) * 3 * maxpts);
     double *sb = (double *)malloc(sizeof(double) * 3 * maxpts);
     for (int p = 0; p < w->n_pairs; p++) {
@@ -1030,6 +1033,10 @@ static int narrowphase(OrWorld *w) {
         } else if (ka == 2 && kb == 1) {
             cnt = or_sphere_box(pb, hb[0], pa, Ra, ha, nrm, pts, dep);
             nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2];
+        } else if (w->shape_type[w->collider_shape[a]] == OR_SHAPE_TRIMESH ||
+                   w->shape_type[w->collider_shape[b]] == OR_SHAPE_TRIMESH) {
+            if (collide_mesh(w, cp, a, b)) { free(sa); free(sb); return -1; }
+            continue;
         } else {
             Proxy A, B;
             make_proxy(w, a, &A, sa);
@@ -1958,4 +1965,249 @@ void or_capsule_triangles(const double *p0, const double *p1, double radius, con
         hit[i] = (uint8_t)capsule_triangle_one(p0, p1, centre, radius, t, t + 3, t + 6, &points[i * 3],
                                                &normals[i * 3], &depths[i]);
     }
+}
+
+/* ------------------------------------------------------------------ */
+/* triangle meshes: the uniform grid (trigrid.py:63-218) and the mesh  */
+/* route of collide.collide (collide.py:272-306)                       */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    int T, exact;                 /* exact: fewer than 256 triangles, no grid */
+    const double *lo, *hi;        /* T*3 triangle bounds */
+    double glo[3], ghi[3], cell;
+    int shape[3];
+    int *cell_off, *cell_tri;     /* CSR over dense cell ids (i*s1 + j)*s2 + k */
+    int *big, nbig;
+} TriGrid;
+
+/* numpy / CPython float floor division (npy_divmod): fmod, then snap */
+static double py_floordiv(double a, double b) {
+    double mod = fmod(a, b);
+    double div = (a - mod) / b;
+    if (mod != 0.0) {
+        if ((b < 0) != (mod < 0)) { mod += b; div -= 1.0; }
+    }
+    double fd;
+    if (div != 0.0) {
+        fd = floor(div);
+        if (div - fd > 0.5) fd += 1.0;
+    } else {
+        fd = copysign(0.0, a / b);
+    }
+    return fd;
+}
+
+/* np.floor((p - low) / cell).astype(int), clipped to [0, cap] */
+static int64_t grid_cell_of(double p, double low, double cell, int64_t cap) {
+    int64_t r = (int64_t)floor((p - low) / cell);
+    return r < 0 ? 0 : (r > cap ? cap : r);
+}
+
+static void grid_build(TriGrid *g, int T, const double *lo, const double *hi) {
+    memset(g, 0, sizeof(*g));
+    g->T = T; g->lo = lo; g->hi = hi;
+    if (T < 256) { g->exact = 1; return; }              /* SMALLEST_WORTH_BINNING */
+    for (int c = 0; c < 3; c++) {
+        double mn = lo[c], mx = hi[c];
+        for (int t = 1; t < T; t++) {
+            if (lo[t * 3 + c] < mn) mn = lo[t * 3 + c];
+            if (hi[t * 3 + c] > mx) mx = hi[t * 3 + c];
+        }
+        g->glo[c] = mn; g->ghi[c] = mx;
+    }
+    double ext = 0.0;
+    for (int c = 0; c < 3; c++) {
+        double e = g->ghi[c] - g->glo[c];
+        e = e > 1e-9 ? e : 1e-9;
+        if (c == 0 || e > ext) ext = e;
+    }
+    g->cell = ext / 64.0;                                 /* TARGET_CELLS */
+    const int64_t cap = ((int64_t)1 << 30) - 1;
+    int64_t *first = (int64_t *)malloc(sizeof(int64_t) * 3 * T), *last = (int64_t *)malloc(sizeof(int64_t) * 3 * T);
+    int64_t smax[3] = {0, 0, 0};
+    for (int t = 0; t < T; t++)
+        for (int c = 0; c < 3; c++) {
+            first[t * 3 + c] = grid_cell_of(lo[t * 3 + c], g->glo[c], g->cell, cap);
+            last[t * 3 + c] = grid_cell_of(hi[t * 3 + c], g->glo[c], g->cell, cap);
+            if (last[t * 3 + c] > smax[c]) smax[c] = last[t * 3 + c];
+        }
+    for (int c = 0; c < 3; c++) g->shape[c] = (int)(smax[c] + 1);
+    const int64_t ncell = (int64_t)g->shape[0] * g->shape[1] * g->shape[2];
+    g->cell_off = (int *)calloc((size_t)ncell + 1, sizeof(int));
+    g->big = (int *)malloc(sizeof(int) * (T ? T : 1));
+    for (int pass = 0; pass < 2; pass++) {
+        int64_t fill_base = 0;
+        (void)fill_base;
+        for (int t = 0; t < T; t++) {
+            const int64_t *f = &first[t * 3], *l = &last[t * 3];
+            const int64_t span = (l[0] - f[0] + 1) * (l[1] - f[1] + 1) * (l[2] - f[2] + 1);
+            if (span > 64) {                              /* BIG_CELL_LIMIT */
+                if (pass == 0) g->big[g->nbig++] = t;
+                continue;
+            }
+            for (int64_t i = f[0]; i <= l[0]; i++)
+                for (int64_t j = f[1]; j <= l[1]; j++)
+                    for (int64_t k = f[2]; k <= l[2]; k++) {
+                        const int64_t id = (i * g->shape[1] + j) * g->shape[2] + k;
+                        if (pass == 0) g->cell_off[id + 1]++;
+                        else g->cell_tri[g->cell_off[id]++] = t;
+                    }
+        }
+        if (pass == 0) {
+            for (int64_t id = 0; id < ncell; id++) g->cell_off[id + 1] += g->cell_off[id];
+            g->cell_tri = (int *)malloc(sizeof(int) * (g->cell_off[ncell] ? g->cell_off[ncell] : 1));
+        } else {
+            for (int64_t id = ncell; id > 0; id--) g->cell_off[id] = g->cell_off[id - 1];
+            g->cell_off[0] = 0;
+        }
+    }
+    free(first); free(last);
+}
+
+static void grid_free(TriGrid *g) { free(g->cell_off); free(g->cell_tri); free(g->big); }
+
+static int cmp_int(const void *x, const void *y) { int a = *(const int *)x, b = *(const int *)y; return (a > b) - (a < b); }
+
+/* TriangleGrid.box (trigrid.py:99-111, 183-218): candidate triangles of
+ * [low, high], ascending, no repeats; returns the count, *out malloc'd */
+static int grid_box(const TriGrid *g, const double *low, const double *high, int **out) {
+    int n = 0, cap = 64;
+    int *c = (int *)malloc(sizeof(int) * cap);
+    if (g->exact) {
+        for (int t = 0; t < g->T; t++) {
+            int keep = 1;
+            for (int k = 0; k < 3; k++) keep &= g->lo[t * 3 + k] <= high[k] && g->hi[t * 3 + k] >= low[k];
+            if (!keep) continue;
+            if (n == cap) { cap *= 2; c = (int *)realloc(c, sizeof(int) * cap); }
+            c[n++] = t;
+        }
+        *out = c;
+        return n;
+    }
+    int outside = 0;
+    for (int k = 0; k < 3; k++) outside |= low[k] > g->ghi[k] || high[k] < g->glo[k];
+    if (!outside) {
+        int f[3], l[3];
+        for (int k = 0; k < 3; k++) {
+            double a = py_floordiv(low[k] - g->glo[k], g->cell), b = py_floordiv(high[k] - g->glo[k], g->cell);
+            int64_t ia = (int64_t)a, ib = (int64_t)b;
+            ia = ia < 0 ? 0 : ia; ib = ib < 0 ? 0 : ib;
+            f[k] = (int)(ia > g->shape[k] - 1 ? g->shape[k] - 1 : ia);
+            l[k] = (int)(ib > g->shape[k] - 1 ? g->shape[k] - 1 : ib);
+        }
+        for (int i = f[0]; i <= l[0]; i++)
+            for (int j = f[1]; j <= l[1]; j++)
+                for (int k = f[2]; k <= l[2]; k++) {
+                    const int64_t id = ((int64_t)i * g->shape[1] + j) * g->shape[2] + k;
+                    for (int q = g->cell_off[id]; q < g->cell_off[id + 1]; q++) {
+                        if (n == cap) { cap *= 2; c = (int *)realloc(c, sizeof(int) * cap); }
+                        c[n++] = g->cell_tri[q];
+                    }
+                }
+    }
+    for (int q = 0; q < g->nbig; q++) {
+        if (n == cap) { cap *= 2; c = (int *)realloc(c, sizeof(int) * cap); }
+        c[n++] = g->big[q];
+    }
+    qsort(c, n, sizeof(int), cmp_int);
+    int m = 0;
+    for (int q = 0; q < n; q++) if (m == 0 || c[q] != c[m - 1]) c[m++] = c[q];
+    *out = c;
+    return m;
+}
+
+/* world AABB of a support proxy (body.py: aabb of each proxy), no margin */
+static void proxy_aabb(const OrWorld *w, int si, int i, const Proxy *P, double *lo, double *hi) {
+    const double *pos = &w->pos[i * 3];
+    if (P->kind == OR_SHAPE_SPHERE) {
+        for (int c = 0; c < 3; c++) { lo[c] = pos[c] - P->radius; hi[c] = pos[c] + P->radius; }
+    } else if (P->kind == OR_SHAPE_BOX) {                 /* _box_corners(half) @ R.T + center */
+        for (int c = 0; c < 3; c++) { lo[c] = INFINITY; hi[c] = -INFINITY; }
+        for (int k = 0; k < 8; k++) {
+            double s[3] = {(k & 1) ? P->half[0] : -P->half[0], (k & 2) ? P->half[1] : -P->half[1],
+                           (k & 4) ? P->half[2] : -P->half[2]};
+            for (int c = 0; c < 3; c++) {
+                double x = dot_blas(s, &P->R[c * 3]) + P->center[c];   /* numpy's dgemm order, probed */
+                if (x < lo[c]) lo[c] = x;
+                if (x > hi[c]) hi[c] = x;
+            }
+        }
+    } else if (P->kind == OR_SHAPE_CAPSULE) {
+        for (int c = 0; c < 3; c++) {
+            lo[c] = (P->p0[c] < P->p1[c] ? P->p0[c] : P->p1[c]) - P->radius;
+            hi[c] = (P->p0[c] > P->p1[c] ? P->p0[c] : P->p1[c]) + P->radius;
+        }
+    } else {
+        for (int c = 0; c < 3; c++) {
+            double mn = P->world[c], mx = P->world[c];
+            for (int q = 1; q < P->m; q++) {
+                double x = P->world[q * 3 + c];
+                if (x < mn) mn = x;
+                if (x > mx) mx = x;
+            }
+            lo[c] = mn; hi[c] = mx;
+        }
+    }
+    (void)si;
+}
+
+/* the mesh route (collide.py:272-306): a capsule against every candidate
+ * triangle at once (capsule_triangle_batch), any other proxy through GJK/EPA
+ * one candidate triangle at a time; contacts in candidate order, normals
+ * from a to b */
+static int collide_mesh(OrWorld *w, Caps *cp, int a, int b) {
+    const int mesh_is_a = w->shape_type[w->collider_shape[a]] == OR_SHAPE_TRIMESH;
+    const int mb = mesh_is_a ? a : b, ob = mesh_is_a ? b : a;
+    const int ms = w->collider_shape[mb], os = w->collider_shape[ob];
+    double R[9];
+    or_quat_to_matrix(&w->q[mb * 4], R);
+    const int np_ = w->shape_pt_cnt[ms], T = w->shape_tri_cnt[ms];
+    double *wp = (double *)malloc(sizeof(double) * 3 * (np_ ? np_ : 1));
+    convex_world_points(w, ms, &w->pos[mb * 3], R, wp);
+    double *tlo = (double *)malloc(sizeof(double) * 3 * (T ? T : 1)), *thi = (double *)malloc(sizeof(double) * 3 * (T ? T : 1));
+    const int32_t *tri = &w->tris[(size_t)w->shape_tri_off[ms] * 3];
+    for (int t = 0; t < T; t++)
+        for (int c = 0; c < 3; c++) {
+            double x0 = wp[tri[t * 3] * 3 + c], x1 = wp[tri[t * 3 + 1] * 3 + c], x2 = wp[tri[t * 3 + 2] * 3 + c];
+            double mn = x0 < x1 ? x0 : x1, mx = x0 > x1 ? x0 : x1;
+            tlo[t * 3 + c] = mn < x2 ? mn : x2;
+            thi[t * 3 + c] = mx > x2 ? mx : x2;
+        }
+    TriGrid g;
+    grid_build(&g, T, tlo, thi);
+    int omax = w->shape_type[os] == OR_SHAPE_CONVEX ? w->shape_pt_cnt[os] : 1;
+    double *so = (double *)malloc(sizeof(double) * 3 * (omax > 0 ? omax : 1));
+    Proxy O;
+    make_proxy_shape(w, os, ob, &O, so);
+    double lo[3], hi[3];
+    proxy_aabb(w, os, ob, &O, lo, hi);
+    int *cand = NULL;
+    const int nc = grid_box(&g, lo, hi, &cand);
+    int rc = 0;
+    for (int q = 0; q < nc && !rc; q++) {
+        const int t = cand[q];
+        const double *v0 = &wp[tri[t * 3] * 3], *v1 = &wp[tri[t * 3 + 1] * 3], *v2 = &wp[tri[t * 3 + 2] * 3];
+        double pt[3], nrm[3], dep;
+        int hit;
+        if (O.kind == OR_SHAPE_CAPSULE) {
+            double centre[3];
+            for (int c = 0; c < 3; c++) centre[c] = (O.p0[c] + O.p1[c]) * 0.5;
+            hit = capsule_triangle_one(O.p0, O.p1, centre, O.radius, v0, v1, v2, pt, nrm, &dep);
+            if (hit && !mesh_is_a) for (int c = 0; c < 3; c++) nrm[c] = -nrm[c];
+        } else {
+            /* TriangleProxy (body.py:135-152): a three-point convex */
+            double tv[9];
+            for (int c = 0; c < 3; c++) { tv[c] = v0[c]; tv[3 + c] = v1[c]; tv[6 + c] = v2[c]; }
+            Proxy P;
+            memset(&P, 0, sizeof(P));
+            P.kind = OR_SHAPE_CONVEX; P.world = tv; P.m = 3;
+            double pts[12], deps[4];
+            hit = mesh_is_a ? collide_convex(&P, &O, nrm, pts, deps) : collide_convex(&O, &P, nrm, pts, deps);
+            if (hit > 0) { for (int c = 0; c < 3; c++) pt[c] = pts[c]; dep = deps[0]; }
+            hit = hit > 0;
+        }
+        if (hit) rc = push_contact(w, cp, a, b, pt, nrm, dep);
+    }
+    free(cand); grid_free(&g); free(tlo); free(thi); free(wp); free(so);
+    return rc;
 }

@@ -25,7 +25,7 @@ extern "C" {
 /* shape types */
 /* capsule also stands for the reference's cylinder, which it collides as a
  * capsule (body.py:224-228); shape_radius = radiusBottom, shape_size[1] = height */
-enum { OR_SHAPE_SPHERE = 1, OR_SHAPE_BOX = 2, OR_SHAPE_CONVEX = 3, OR_SHAPE_CAPSULE = 4 };
+enum { OR_SHAPE_SPHERE = 1, OR_SHAPE_BOX = 2, OR_SHAPE_CONVEX = 3, OR_SHAPE_CAPSULE = 4, OR_SHAPE_TRIMESH = 5 };
 /* combine modes (model.py:231-243) */
 enum { OR_AVERAGE = 0, OR_MINIMUM = 1, OR_MAXIMUM = 2, OR_MULTIPLY = 3 };
 /* joint types (joints.py) */
@@ -95,6 +95,11 @@ typedef struct OrWorld {
     /* ---- per-step trigger overlaps (trigger, other) in pair order, oracle-owned ---- */
     int32_t n_overlaps;
     int32_t *ov_trg, *ov_other;
+    /* ---- triangle meshes (body.py:155-212): a trimesh shape's triangles are
+     *      rows [shape_tri_off, +shape_tri_cnt) of tris, vertex indices into
+     *      the shape's own points (shape_pt_off / shape_pt_cnt) ---- */
+    int32_t *shape_tri_off, *shape_tri_cnt;
+    int32_t *tris;                                       /* *3 */
 } OrWorld;
 
 enum { OR_VOL_POINT = 1, OR_VOL_SPHERE = 2, OR_VOL_BOX = 4, OR_VOL_REPLACE = 8, OR_VOL_STOP = 16 };

@@ -60,6 +60,7 @@ class OrWorldC(C.Structure):
         ('n_volumes', C.c_int32), ('vol_kind', I), ('vol_g', D), ('vol_field', D), ('vol_rc', D),
         ('vol_rr', D),
         ('n_overlaps', C.c_int32), ('ov_trg', I), ('ov_other', I),
+        ('shape_tri_off', I), ('shape_tri_cnt', I), ('tris', I),
     ]
 
 
@@ -106,7 +107,7 @@ def _ptr(a, t):
 
 
 # a cylinder is collided as a capsule by the reference (body.py:224-228)
-SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4}
+SHAPE_CODES = {'sphere': 1, 'box': 2, 'convex': 3, 'capsule': 4, 'cylinder': 4, 'trimesh': 5}
 COMBINE = {'average': 0, 'minimum': 1, 'maximum': 2, 'multiply': 3}
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
@@ -210,6 +211,10 @@ class OracleWorld:
         pcnt = np.zeros(max(ns, 1), np.int32)
         pts = []
         total = 0
+        toff = np.zeros(max(ns, 1), np.int32)
+        tcnt = np.zeros(max(ns, 1), np.int32)
+        tris = []
+        ntri = 0
         for s, sh in enumerate(shapes):
             if sh.type not in SHAPE_CODES:
                 stype[s] = 0
@@ -221,17 +226,25 @@ class OracleWorld:
             else:
                 srad[s] = sh.radius
                 ssize[s] = np.asarray(sh.size, dtype='d')
-            if sh.type == 'convex':
+            if sh.type in ('convex', 'trimesh'):
                 p = np.asarray(sh.points, dtype='d').reshape(-1, 3)
                 poff[s] = total
                 pcnt[s] = len(p)
                 total += len(p)
                 pts.append(p)
+            if sh.type == 'trimesh':
+                t = np.asarray(sh.indices, dtype=np.int32).reshape(-1, 3)
+                toff[s] = ntri
+                tcnt[s] = len(t)
+                ntri += len(t)
+                tris.append(t)
         points = np.ascontiguousarray(np.concatenate(pts) if pts else np.zeros((1, 3)))
         c.n_shapes = ns
         self._set('shape_type', stype, I); self._set('shape_radius', srad, D)
         self._set('shape_size', ssize, D); self._set('shape_pt_off', poff, I)
         self._set('shape_pt_cnt', pcnt, I); self._set('points', points, D)
+        self._set('shape_tri_off', toff, I); self._set('shape_tri_cnt', tcnt, I)
+        self._set('tris', np.ascontiguousarray(np.concatenate(tris) if tris else np.zeros((1, 3), np.int32)), I)
         # materials
         mats = world.materials
         nm = len(mats)

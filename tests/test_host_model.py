@@ -52,11 +52,13 @@ def test_unsupported_features_raise():
     w, _ = scenes.GOLDEN_SCENES['pyramid']()
     pts = np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1]], dtype='d')
     mesh = w.add_shape(model.Shape(type='trimesh', points=pts, indices=np.array([[0, 1, 2]], 'i')))
-    w.add_body(model.Motion(type=model.STATIC), model.Collider(shape=mesh), position=(0, 5, 0))
+    w.add_body(model.Motion(type=model.DYNAMIC), model.Collider(shape=mesh), position=(0, 5, 0))
     with pytest.raises(UnsupportedFeature):
-        check_supported(w)
+        check_supported(w)                        # a moving triangle mesh
     with pytest.raises(UnsupportedFeature):
         CudaBackend().attach(w)
+    w5, _ = scenes.GOLDEN_SCENES['terrain']()
+    check_supported(w5)                           # static meshes are taken
     w2, _ = scenes.GOLDEN_SCENES['pyramid']()
     s = w2.add_shape(model.Shape(type='trimesh', points=pts, indices=np.array([[0, 1, 2]], 'i')))
     w2.add_body(model.Motion(type=model.STATIC), trigger=model.Trigger(shape=s), position=(0, 9, 0))

@@ -13,7 +13,7 @@ import pytest
 import pyoracle
 from golden_util import SCENES, checkpoint, checkpoints, events_from_overlaps, load, pair_set
 
-EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones')
+EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain')
 
 
 def _close(a, b, exact):
@@ -65,6 +65,7 @@ def test_golden_scenes_exercise_every_narrowphase_route():
     assert {(2, 2), (1, 1), (1, 2)} <= seen
     assert any(3 in k for k in seen)
     assert {(1, 4), (2, 4), (4, 4)} <= seen
+    assert {(4, 5), (2, 5), (1, 5), (3, 5)} <= seen     # every proxy kind against a triangle mesh
 
 
 def test_zones_fixture_exercises_triggers_and_volumes():
