@@ -219,7 +219,7 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                 parts['shape_radius'].append([float(sh.radius)])
                 size = np.asarray(sh.size, 'd') if np.size(sh.size) == 3 else np.zeros(3)
                 parts['shape_size'].append(size.reshape(1, 3))
-            if sh.type in ('convex', 'trimesh'):
+            if sh.type in ('convex', 'trimesh') and sh.points is not None:
                 pts = np.asarray(sh.points, 'd').reshape(-1, 3)
                 parts['shape_pt_off'].append([npts])
                 parts['shape_pt_cnt'].append([len(pts)])

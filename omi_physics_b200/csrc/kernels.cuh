@@ -1280,15 +1280,20 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
             }
             continue;
         }
-        // runs: maximal stretches of consecutive contacts of one pair
+        // runs: maximal stretches of consecutive contacts of one pair with one
+        // normal (a solver row's pair part - normal, tangents, friction, masses
+        // - is then the same for the whole run; a pair's contacts share their
+        // normal except against a triangle mesh, one normal per triangle)
         int R = 0;
         for (int base = 0; base < K; base += T) {
             const int k = base + tid;
             int start = 0, a = -1, b = -1;
             if (k < K) {
-                a = A.c_a[c0 + k];
-                b = A.c_b[c0 + k];
-                start = k == 0 || a != A.c_a[c0 + k - 1] || b != A.c_b[c0 + k - 1];
+                const int g = c0 + k;
+                a = A.c_a[g];
+                b = A.c_b[g];
+                start = k == 0 || a != A.c_a[g - 1] || b != A.c_b[g - 1] || A.c_n[g * 3] != A.c_n[g * 3 - 3] ||
+                        A.c_n[g * 3 + 1] != A.c_n[g * 3 - 2] || A.c_n[g * 3 + 2] != A.c_n[g * 3 - 1];
             }
             int tot;
             const int r = R + block_exclusive_scan(start, scan_sh, &tot);
