@@ -226,13 +226,13 @@ class OracleWorld:
             else:
                 srad[s] = sh.radius
                 ssize[s] = np.asarray(sh.size, dtype='d')
-            if sh.type in ('convex', 'trimesh'):
+            if sh.type in ('convex', 'trimesh') and sh.points is not None:
                 p = np.asarray(sh.points, dtype='d').reshape(-1, 3)
                 poff[s] = total
                 pcnt[s] = len(p)
                 total += len(p)
                 pts.append(p)
-            if sh.type == 'trimesh':
+            if sh.type == 'trimesh' and sh.indices is not None:
                 t = np.asarray(sh.indices, dtype=np.int32).reshape(-1, 3)
                 toff[s] = ntri
                 tcnt[s] = len(t)
