@@ -1283,7 +1283,8 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
         // runs: maximal stretches of consecutive contacts of one pair with one
         // normal (a solver row's pair part - normal, tangents, friction, masses
         // - is then the same for the whole run; a pair's contacts share their
-        // normal except against a triangle mesh, one normal per triangle)
+        // normal except against a triangle mesh, one normal per triangle, so
+        // only mesh pairs compare normals)
         int R = 0;
         for (int base = 0; base < K; base += T) {
             const int k = base + tid;
@@ -1292,8 +1293,10 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
                 const int g = c0 + k;
                 a = A.c_a[g];
                 b = A.c_b[g];
-                start = k == 0 || a != A.c_a[g - 1] || b != A.c_b[g - 1] || A.c_n[g * 3] != A.c_n[g * 3 - 3] ||
-                        A.c_n[g * 3 + 1] != A.c_n[g * 3 - 2] || A.c_n[g * 3 + 2] != A.c_n[g * 3 - 1];
+                start = k == 0 || a != A.c_a[g - 1] || b != A.c_b[g - 1];
+                if (!start && (A.kind[a] == 5 || A.kind[b] == 5))
+                    start = A.c_n[g * 3] != A.c_n[g * 3 - 3] || A.c_n[g * 3 + 1] != A.c_n[g * 3 - 2] ||
+                            A.c_n[g * 3 + 2] != A.c_n[g * 3 - 1];
             }
             int tot;
             const int r = R + block_exclusive_scan(start, scan_sh, &tot);
@@ -1637,7 +1640,7 @@ __device__ __forceinline__ int sweep_want(const Arena &A, int w) {
 
 // One world's sweep by the `gn` threads of a group (gtid = thread index in it,
 // bar = its barrier id; 0 when the group is the whole block).
-__device__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doubles, int gtid, int gn, int bar,
+__device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_d, int smem_doubles, int gtid, int gn, int bar,
                             SweepShared &sh) {
     const int lane = gtid & 31;
     volatile int *abort = &sh.abort;
