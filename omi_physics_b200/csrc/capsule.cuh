@@ -9,9 +9,10 @@
 //
 // One thread per triangle. Each warp takes tiles of 32 triangles: the tile's
 // 72-byte vertex records are read with coalesced streaming loads into the
-// warp's shared memory, each lane answers its triangle, and the point /
-// normal rows are written back through shared memory so every global store is
-// coalesced.
+// warp's shared memory, each lane runs the face test on its triangle, the
+// point / normal rows are written back through shared memory so every global
+// store is coalesced, and the triangles the face test leaves open wait in a
+// per-warp queue until 32 of them can take the rim test together.
 // Per triangle 72 bytes are read and 57 written; the arithmetic (float64, in
 // the reference's operation order, no contraction) is a few hundred
 // operations, so the kernel sits near the HBM / FP64 ridge.
@@ -20,7 +21,7 @@
 
 namespace omi {
 
-constexpr int CT_THREADS = 256;   // triangles per tile, one thread each
+constexpr int CT_THREADS = 128;   // threads of a block: four warps, each with its own tiles
 constexpr int CT_CAP_DOUBLES = 7; // p0 (3), p1 (3), radius
 
 // _dot3 (_collide_native.pyx:16-17): left to right
@@ -118,71 +119,85 @@ __device__ inline void seg_closest(const double *p1, const double *q1, const dou
 // the face, the deepest cap end whose perpendicular foot lies on the triangle
 // is pushed back to the side the capsule's centre is on, depth unbounded;
 // otherwise the nearest of the cap ends to the triangle and of the axis to
-// the three edges (first strict minimum), if nearer than the radius. Returns
-// 1 on contact with the point on the triangle and the normal pointing from
-// the triangle toward the capsule.
-__device__ inline int capsule_triangle(const double *c0, const double *c1, const double *centre, double radius,
-                                       const double *v0, const double *v1, const double *v2, double *point,
-                                       double *normal, double *depth) {
-    double e1[3], e2[3], face[3];
+// the three edges (first strict minimum), if nearer than the radius. In two
+// phases: capsule_face decides the face case and leaves what the rim test
+// reuses (the closest points on the triangle to the two cap ends - the face
+// and rim tests ask for the same two - when it found them); capsule_rim
+// answers the rest. Each returns 1 on contact, with the point on the
+// triangle and the normal pointing from the triangle toward the capsule.
+struct CapRim {
+    double tpk[2][3];
+    bool have_tp;
+};
+
+__device__ __forceinline__ void tri_face(const double *v0, const double *v1, const double *v2, double *face,
+                                         double &face_len) {
+    double e1[3], e2[3];
 #pragma unroll
     for (int m = 0; m < 3; m++) { e1[m] = v1[m] - v0[m]; e2[m] = v2[m] - v0[m]; }
     face[0] = e1[1] * e2[2] - e1[2] * e2[1];
     face[1] = e1[2] * e2[0] - e1[0] * e2[2];
     face[2] = e1[0] * e2[1] - e1[1] * e2[0];
-    const double face_len = sqrt(dot3_seq(face, face));
-    // closest points on the triangle to the two cap ends: the face test and
-    // the rim test ask for the same two (a pure function), so they are found once
-    double tpk[2][3];
-    bool have_tp = false;
-    if (face_len > EPS_COLLIDE) {
-        double fn[3];
+    face_len = sqrt(dot3_seq(face, face));
+}
+
+__device__ inline int capsule_face(const double *c0, const double *c1, const double *centre, double radius,
+                                   const double *v0, const double *v1, const double *v2, CapRim &rim,
+                                   double *point, double *normal, double *depth) {
+    double face[3], face_len;
+    tri_face(v0, v1, v2, face, face_len);
+    rim.have_tp = false;
+    if (!(face_len > EPS_COLLIDE)) return 0;
+    double fn[3];
 #pragma unroll
-        for (int m = 0; m < 3; m++) fn[m] = face[m] / face_len;
-        double g[3] = {centre[0] - v0[0], centre[1] - v0[1], centre[2] - v0[2]};
-        if (fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2] < 0.0) {
-            fn[0] = -fn[0]; fn[1] = -fn[1]; fn[2] = -fn[2];
-        }
-        bool found = false;
-        double best = -1e300, bp[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const double *sp = k ? c1 : c0;
-#pragma unroll
-            for (int m = 0; m < 3; m++) g[m] = sp[m] - v0[m];
-            const double h = fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2];
-            double foot[3];
-#pragma unroll
-            for (int m = 0; m < 3; m++) foot[m] = sp[m] - fn[m] * h;
-            double *tp = tpk[k];
-            tri_closest(sp, v0, v1, v2, tp);
-#pragma unroll
-            for (int m = 0; m < 3; m++) g[m] = foot[m] - tp[m];
-            if (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] > EPS_COLLIDE * EPS_COLLIDE) continue;
-            const double reach = radius - h;
-            if (reach > 0.0 && reach > best) {
-                best = reach;
-                found = true;
-                bp[0] = tp[0]; bp[1] = tp[1]; bp[2] = tp[2];
-            }
-        }
-        if (found) {
-            *depth = best;
-#pragma unroll
-            for (int m = 0; m < 3; m++) { point[m] = bp[m]; normal[m] = fn[m]; }
-            return 1;
-        }
-        have_tp = true;
+    for (int m = 0; m < 3; m++) fn[m] = face[m] / face_len;
+    double g[3] = {centre[0] - v0[0], centre[1] - v0[1], centre[2] - v0[2]};
+    if (fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2] < 0.0) {
+        fn[0] = -fn[0]; fn[1] = -fn[1]; fn[2] = -fn[2];
     }
-    if (!have_tp) {
-        tri_closest(c0, v0, v1, v2, tpk[0]);
-        tri_closest(c1, v0, v1, v2, tpk[1]);
+    bool found = false;
+    double best = -1e300, bp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const double *sp = k ? c1 : c0;
+#pragma unroll
+        for (int m = 0; m < 3; m++) g[m] = sp[m] - v0[m];
+        const double h = fn[0] * g[0] + fn[1] * g[1] + fn[2] * g[2];
+        double foot[3];
+#pragma unroll
+        for (int m = 0; m < 3; m++) foot[m] = sp[m] - fn[m] * h;
+        double *tp = rim.tpk[k];
+        tri_closest(sp, v0, v1, v2, tp);
+#pragma unroll
+        for (int m = 0; m < 3; m++) g[m] = foot[m] - tp[m];
+        if (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] > EPS_COLLIDE * EPS_COLLIDE) continue;
+        const double reach = radius - h;
+        if (reach > 0.0 && reach > best) {
+            best = reach;
+            found = true;
+            bp[0] = tp[0]; bp[1] = tp[1]; bp[2] = tp[2];
+        }
+    }
+    rim.have_tp = true;
+    if (!found) return 0;
+    *depth = best;
+#pragma unroll
+    for (int m = 0; m < 3; m++) { point[m] = bp[m]; normal[m] = fn[m]; }
+    return 1;
+}
+
+__device__ inline int capsule_rim(const double *c0, const double *c1, double radius, const double *v0,
+                                  const double *v1, const double *v2, CapRim &rim, double *point,
+                                  double *normal, double *depth) {
+    if (!rim.have_tp) {
+        tri_closest(c0, v0, v1, v2, rim.tpk[0]);
+        tri_closest(c1, v0, v1, v2, rim.tpk[1]);
     }
     double best_d2 = 1e300, bsp[3] = {0.0, 0.0, 0.0}, btp[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         const double *sp = k ? c1 : c0;
-        const double *tp = tpk[k];
+        const double *tp = rim.tpk[k];
         const double gx = sp[0] - tp[0], gy = sp[1] - tp[1], gz = sp[2] - tp[2];
         const double d2 = gx * gx + gy * gy + gz * gz;
         if (d2 < best_d2) {
@@ -210,16 +225,28 @@ __device__ inline int capsule_triangle(const double *c0, const double *c1, const
     if (dist > EPS_COLLIDE) {
 #pragma unroll
         for (int m = 0; m < 3; m++) normal[m] = (bsp[m] - btp[m]) / dist;
-    } else if (face_len > EPS_COLLIDE) {
-#pragma unroll
-        for (int m = 0; m < 3; m++) normal[m] = face[m] / face_len;
     } else {
-        normal[0] = normal[1] = normal[2] = 0.0;
+        double face[3], face_len;
+        tri_face(v0, v1, v2, face, face_len);
+        if (face_len > EPS_COLLIDE) {
+#pragma unroll
+            for (int m = 0; m < 3; m++) normal[m] = face[m] / face_len;
+        } else {
+            normal[0] = normal[1] = normal[2] = 0.0;
+        }
     }
     *depth = radius - dist;
 #pragma unroll
     for (int m = 0; m < 3; m++) point[m] = btp[m];
     return 1;
+}
+
+__device__ inline int capsule_triangle(const double *c0, const double *c1, const double *centre, double radius,
+                                       const double *v0, const double *v1, const double *v2, double *point,
+                                       double *normal, double *depth) {
+    CapRim rim;
+    if (capsule_face(c0, c1, centre, radius, v0, v1, v2, rim, point, normal, depth)) return 1;
+    return capsule_rim(c0, c1, radius, v0, v1, v2, rim, point, normal, depth);
 }
 
 // Host builds of this header (a test-only emulation that checks the per-
@@ -255,22 +282,65 @@ __device__ __forceinline__ int capsule_of_warp(const int64_t *off, int lo, int h
 }
 
 constexpr int CT_WARPS = CT_THREADS / 32;
+constexpr int CT_QUEUE = 64;          // rim items a warp holds (31 left over + 32 new at most)
+constexpr int CT_QITEM = 15;          // vertices (9) and the two closest points (6)
 
 // Triangles [0, n) of this launch are global triangles [base, base + n): the
 // vertex and output pointers are the launch's own, the capsule ranges
-// tri_off are global (a host pipeline launches one chunk at a time). Each
-// warp takes tiles of 32 triangles (grid-stride): coalesced streaming loads of
-// the tile's vertex records into the warp's shared memory, one triangle per
-// lane, the point / normal rows written back through shared memory; only
-// __syncwarp orders the warp's tile, no block-wide barrier.
+// tri_off are global (a host pipeline launches one chunk at a time).
+//
+// Each warp takes tiles of 32 triangles (grid-stride): coalesced streaming
+// loads of the tile's vertex records into the warp's shared memory, one
+// triangle per lane through the face test, the tile's outputs written back
+// through shared memory so every global store is coalesced. A triangle the
+// face test does not decide goes to the warp's rim queue with what the rim
+// test reuses; whenever the queue holds 32 items the whole warp runs the rim
+// test on them, one per lane, and writes each answer over its triangle's
+// slot. The two tests thus run on full warps instead of diverging lane by
+// lane. Only __syncwarp orders a warp's work; there is no block barrier.
 __global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
     const double *__restrict__ caps, const int64_t *__restrict__ tri_off, int q,
     const double *__restrict__ verts, int64_t base, int64_t n, uint8_t *__restrict__ hit,
     double *__restrict__ points, double *__restrict__ normals, double *__restrict__ depths) {
-    __shared__ double sv[CT_WARPS][32 * 9];
-    __shared__ double so[CT_WARPS][32 * 6];
+    __shared__ double sv[CT_WARPS][32 * 9];      // the tile's vertices, then its point / normal rows
+    __shared__ double qd[CT_WARPS][CT_QUEUE * CT_QITEM];
+    __shared__ int64_t qt[CT_WARPS][CT_QUEUE];
+    __shared__ int qc[CT_WARPS][CT_QUEUE];
+    __shared__ unsigned char qh[CT_WARPS][CT_QUEUE];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *wv = sv[wib], *wo = so[wib];
+    double *wv = sv[wib], *wq = qd[wib];
+    int64_t *wt = qt[wib];
+    int *wc = qc[wib];
+    unsigned char *wh = qh[wib];
+    int queued = 0;
+    // the rim test on queue items [from, from + count), one per lane
+    auto drain = [&](int from, int count) {
+        if (lane < count) {
+            const int e = from + lane;
+            const double *it = &wq[e * CT_QITEM];
+            const double *cp = caps + (size_t)wc[e] * CT_CAP_DOUBLES;
+            double c0[3], c1[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) { c0[k] = __ldg(&cp[k]); c1[k] = __ldg(&cp[3 + k]); }
+            double v[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) v[k] = it[k];
+            CapRim rim;
+            rim.have_tp = wh[e] != 0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) { rim.tpk[0][k] = it[9 + k]; rim.tpk[1][k] = it[12 + k]; }
+            double pt[3], nr[3], dep;
+            const int h = capsule_rim(c0, c1, __ldg(&cp[6]), v, v + 3, v + 6, rim, pt, nr, &dep);
+            if (h) {
+                const int64_t t = wt[e];
+                hit[t] = 1;
+#pragma unroll
+                for (int k = 0; k < 3; k++) { points[t * 3 + k] = pt[k]; normals[t * 3 + k] = nr[k]; }
+                depths[t] = dep;
+            }
+        }
+        __syncwarp();
+    };
     const int64_t stride = (int64_t)gridDim.x * CT_THREADS;
     for (int64_t t0 = ((int64_t)blockIdx.x * CT_WARPS + wib) * 32; t0 < n; t0 += stride) {
         const int m = (int)(n - t0 < 32 ? n - t0 : 32);
@@ -279,8 +349,12 @@ __global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
         const int first = capsule_of_warp(tri_off, 0, q - 1, base + t0, lane);
         const int last = capsule_of_warp(tri_off, first, q - 1, base + t0 + m - 1, lane);
         __syncwarp();
+        bool defer = false;
+        int c = 0;
+        CapRim rim;
+        double pt[3] = {0.0, 0.0, 0.0}, nr[3] = {0.0, 0.0, 0.0}, dep = 0.0;
         if (lane < m) {
-            const int c = capsule_of(tri_off, first, last, base + t0 + lane);
+            c = capsule_of(tri_off, first, last, base + t0 + lane);
             const double *cp = caps + (size_t)c * CT_CAP_DOUBLES;
             double c0[3], c1[3], centre[3];
 #pragma unroll
@@ -289,25 +363,43 @@ __global__ void __launch_bounds__(CT_THREADS) k_capsule_triangles(
                 c1[k] = __ldg(&cp[3 + k]);
                 centre[k] = (c0[k] + c1[k]) * 0.5;
             }
-            const double radius = __ldg(&cp[6]);
-            double v[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) v[k] = wv[lane * 9 + k];
-            double pt[3], nr[3], dep;
-            const int h = capsule_triangle(c0, c1, centre, radius, v, v + 3, v + 6, pt, nr, &dep);
-            if (!h) { pt[0] = pt[1] = pt[2] = 0.0; nr[0] = nr[1] = nr[2] = 0.0; dep = 0.0; }
-#pragma unroll
-            for (int k = 0; k < 3; k++) { wo[lane * 3 + k] = pt[k]; wo[96 + lane * 3 + k] = nr[k]; }
+            const double *v = &wv[lane * 9];
+            const int h = capsule_face(c0, c1, centre, __ldg(&cp[6]), v, v + 3, v + 6, rim, pt, nr, &dep);
+            defer = !h;
             hit[t0 + lane] = (uint8_t)h;
             __stcs(&depths[t0 + lane], dep);
         }
-        __syncwarp();
-        for (int j = lane; j < m * 3; j += 32) {
-            __stcs(&points[t0 * 3 + j], wo[j]);
-            __stcs(&normals[t0 * 3 + j], wo[96 + j]);
+        // queue the undecided triangles, in lane order
+        const unsigned dm = __ballot_sync(0xffffffffu, defer);
+        if (defer) {
+            const int e = queued + __popc(dm & ((1u << lane) - 1u));
+            double *it = &wq[e * CT_QITEM];
+#pragma unroll
+            for (int k = 0; k < 9; k++) it[k] = wv[lane * 9 + k];
+#pragma unroll
+            for (int k = 0; k < 3; k++) { it[9 + k] = rim.tpk[0][k]; it[12 + k] = rim.tpk[1][k]; }
+            wt[e] = t0 + lane;
+            wc[e] = c;
+            wh[e] = rim.have_tp ? 1 : 0;
+        }
+        queued += __popc(dm);
+        __syncwarp();                                   // the queue has copied the vertices
+        if (lane < m) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) { wv[lane * 3 + k] = pt[k]; wv[96 + lane * 3 + k] = nr[k]; }
         }
         __syncwarp();
+        for (int j = lane; j < m * 3; j += 32) {
+            __stcs(&points[t0 * 3 + j], wv[j]);
+            __stcs(&normals[t0 * 3 + j], wv[96 + j]);
+        }
+        __syncwarp();
+        if (queued >= 32) {
+            drain(queued - 32, 32);
+            queued -= 32;
+        }
     }
+    if (queued > 0) drain(0, queued);
 }
 
 #endif  // OMI_HOST_EMULATION
