@@ -171,9 +171,9 @@ class Server:
     def submit(self, world, steps: int, dt: float = None, arrival: float = 0.0) -> Request:
         dt = float(world.fixed_dt if dt is None else dt)
         packed = pack_worlds([world], [dt], active=True)
-        if packed.has_sensors or packed.scene.n_volumes:
-            raise UnsupportedFeature(OMI_E_UNSUPPORTED, 'serving slots do not take sensors or gravity '
-                                     'volumes; step such worlds in a WorldBatch')
+        if packed.has_sensors or packed.scene.n_volumes or packed.scene.n_meshes:
+            raise UnsupportedFeature(OMI_E_UNSUPPORTED, 'serving slots do not take sensors, gravity volumes '
+                                     'or triangle meshes; step such worlds in a WorldBatch')
         req = Request(self._next_rid, world, int(steps), dt, float(arrival), packed,
                       need_of(packed.scene), int(np.count_nonzero(world.motion_type == 2)))
         if not self.pool.could_ever_fit(req.need):

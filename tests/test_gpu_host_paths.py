@@ -201,10 +201,13 @@ def test_sensor_snapshot_restore_continues_identically():
         assert np.array_equal(getattr(w1, col)[:n], getattr(w2, col)[:n]), col
 
 
-def test_serving_slots_refuse_sensor_worlds():
+def test_serving_slots_refuse_sensor_and_mesh_worlds():
     from omi_physics_b200._lib import UnsupportedFeature
     srv = Server(size_classes(256, per_class=1, min_bodies=64))
     w, meta = scenes.zones(n=60, seed=2)
+    with pytest.raises(UnsupportedFeature):
+        srv.submit(w, steps=5, dt=meta['dt'], arrival=0)
+    w, meta = scenes.terrain(n=20, seed=2, cells=8, extent=3.0)
     with pytest.raises(UnsupportedFeature):
         srv.submit(w, steps=5, dt=meta['dt'], arrival=0)
     srv.close()
