@@ -113,15 +113,17 @@ def check_supported(world) -> None:
         t = world.shapes[s].type
         if t not in SHAPE_CODES:
             raise UnsupportedFeature(-3, 'shape type %r is not supported on the CUDA path' % t)
-    ts = np.asarray(world._trigger_shape[:n])
-    cs = np.asarray(world._collider_shape[:n])
-    for i in range(n):
-        if 0 <= ts[i] < len(world.shapes) and world.shapes[int(ts[i])].type == 'trimesh':
+    meshes = [k for k, sh in enumerate(world.shapes) if sh.type == 'trimesh']
+    if meshes:
+        ts = np.asarray(world._trigger_shape[:n])
+        cs = np.asarray(world._collider_shape[:n])
+        if np.isin(ts, meshes).any():
             raise UnsupportedFeature(-3, 'triangle-mesh sensors are not supported on the CUDA path')
-        if 0 <= cs[i] < len(world.shapes) and world.shapes[int(cs[i])].type == 'trimesh':
-            if int(world._motion_type[i]) != 0:
-                raise UnsupportedFeature(-3, 'triangle meshes are taken as static colliders only')
-            if world.shapes[int(cs[i])].points is None or world.shapes[int(cs[i])].indices is None:
+        on = np.isin(cs, meshes)
+        if (np.asarray(world._motion_type[:n])[on] != 0).any():
+            raise UnsupportedFeature(-3, 'triangle meshes are taken as static colliders only')
+        for k in set(int(x) for x in cs[on]):
+            if world.shapes[k].points is None or world.shapes[k].indices is None:
                 raise UnsupportedFeature(-3, 'a triangle mesh needs its points and indices')
 
 
