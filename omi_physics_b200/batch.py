@@ -94,6 +94,9 @@ class WorldBatch:
         return ev
 
     def step_async(self, n: int = 1) -> None:
+        """Enqueue ``n`` steps without waiting (``sync`` reports an overflow).
+        Trigger events are not recorded on this path; ``trigger_overlaps``
+        still gives the last step's overlaps."""
         self.ctx.call('step_async', int(n))
 
     def sync(self) -> None:
