@@ -45,6 +45,8 @@ class WorldBatch:
         # sensor overlaps of the last step per world and the enter / stay /
         # exit events of every step since the last take_events()
         self.has_sensors = bool(getattr(self.packed, 'has_sensors', False))
+        self._sensor_worlds = [i for i, w in enumerate(self.worlds)
+                               if np.any(np.asarray(w._trigger_shape[:w.body_count]) >= 0)]
         self.overlaps = [set() for _ in self.worlds]
         self.events = [[] for _ in self.worlds]
 
@@ -79,7 +81,7 @@ class WorldBatch:
     def _record_events(self) -> None:
         """Enter / stay / exit of one step (triggers.py:36-42), sorted within
         each kind."""
-        for i in range(len(self.worlds)):
+        for i in self._sensor_worlds:
             new = self.trigger_overlaps(i)
             old = self.overlaps[i]
             if new or old:
