@@ -16,6 +16,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``capsule_pile`` capsules / cylinders / boxes / spheres in a walled arena
   * ``zones``        debris through trigger sensors and gravity volumes
   * ``terrain``      capsules, boxes, spheres and hulls on static triangle meshes
+  * ``ridge``        one mesh mixing a fine floor with triangles the grid sets aside
 """
 import math
 from types import SimpleNamespace
@@ -354,6 +355,49 @@ def terrain(api=None, backend=None, n: int = 60, seed: int = 0, iterations: int 
     return w, dict(dt=1.0 / 120.0, steps=300, name='terrain%d' % n)
 
 
+def ridge(api=None, backend=None, n: int = 60, seed: int = 0, iterations: int = 8, cells: int = 32,
+          extent: float = 8.0):
+    """Bodies falling onto one static mesh that holds a fine rippled floor and
+    two large sloped triangles across it: the large ones span more than 64
+    of the triangle grid's cells, so the grid keeps them aside and hands them
+    to every query (trigrid.py:84-97)."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.5))
+    pts, idx = _grid_mesh(cells, extent, 0.1, 1.1)
+    k = len(pts)
+    ramp = np.array([(-extent, 0.2, 1.0), (extent, 0.2, 1.0), (-extent, 2.5, extent), (extent, 2.5, extent)])
+    pts = np.concatenate([pts, ramp])
+    idx = np.concatenate([idx, np.array([(k, k + 2, k + 1), (k + 1, k + 2, k + 3)], dtype=idx.dtype)])
+    mesh = w.add_shape(m.Shape.trimesh(pts, idx))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=mesh, physicsMaterial=gmat), position=(0.0, 0.0, 0.0))
+    lim = extent - 1.5
+    pos = rng.uniform((-lim, 3.0, -lim), (lim, 7.0, lim), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    u = rng.random(n)
+    for i in range(n):
+        r = float(rng.uniform(0.2, 0.4))
+        if u[i] < 0.5:
+            h = float(rng.uniform(0.3, 0.9))
+            shape = w.add_shape(m.Shape.capsule(h, r))
+            mass = 1000.0 * (math.pi * r * r * h + (4.0 / 3.0) * math.pi * r ** 3)
+        elif u[i] < 0.75:
+            sz = tuple(float(x) for x in rng.uniform(0.3, 0.8, 3))
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        else:
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass), m.Collider(shape=shape, physicsMaterial=gmat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='ridge%d' % n)
+
+
 def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
                 motor_frac: float = 0.1, iterations: int = 12):
     """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
@@ -460,6 +504,7 @@ GOLDEN_SCENES = {
                                                            height=6.0),
     'zones': lambda api=None, backend=None: zones(api, backend),
     'terrain': lambda api=None, backend=None: terrain(api, backend),
+    'ridge': lambda api=None, backend=None: ridge(api, backend),
 }
 
 

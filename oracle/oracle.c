@@ -993,8 +993,10 @@ static int push_contact(OrWorld *w, Caps *cp, int a, int b, const double *pt, co
 }
 
 static int collide_mesh(OrWorld *w, Caps *cp, int a, int b);
+static int g_mesh_pass;
 
 static int narrowphase(OrWorld *w) {
+    g_mesh_pass++;                       /* mesh tables are rebuilt once per pass */
     Caps *cp = caps_for(w);
     w->n_solid = 0;
     w->n_contacts = 0;
@@ -2155,26 +2157,50 @@ static void proxy_aabb(const OrWorld *w, int si, int i, const Proxy *P, double *
  * triangle at once (capsule_triangle_batch), any other proxy through GJK/EPA
  * one candidate triangle at a time; contacts in candidate order, normals
  * from a to b */
+/* A mesh body's world points, triangle bounds and grid, built once per
+ * narrowphase pass (the reference caches the proxy per step, narrowphase.py:40-48) */
+typedef struct { const OrWorld *w; int body, pass; double *wp, *tlo, *thi; TriGrid g; } MeshCache;
+#define MESH_CACHE 8
+static MeshCache g_mesh_cache[MESH_CACHE];
+static int g_mesh_next = 0;
+
+static MeshCache *mesh_body_tables(OrWorld *w, int mb) {
+    for (int k = 0; k < MESH_CACHE; k++) {
+        MeshCache *m = &g_mesh_cache[k];
+        if (m->w == w && m->body == mb && m->pass == g_mesh_pass && m->wp) return m;
+    }
+    MeshCache *m = &g_mesh_cache[g_mesh_next];
+    g_mesh_next = (g_mesh_next + 1) % MESH_CACHE;
+    if (m->wp) { free(m->wp); free(m->tlo); free(m->thi); grid_free(&m->g); }
+    const int ms = w->collider_shape[mb];
+    double R[9];
+    or_quat_to_matrix(&w->q[mb * 4], R);
+    const int np_ = w->shape_pt_cnt[ms], T = w->shape_tri_cnt[ms];
+    m->wp = (double *)malloc(sizeof(double) * 3 * (np_ ? np_ : 1));
+    convex_world_points(w, ms, &w->pos[mb * 3], R, m->wp);
+    m->tlo = (double *)malloc(sizeof(double) * 3 * (T ? T : 1));
+    m->thi = (double *)malloc(sizeof(double) * 3 * (T ? T : 1));
+    const int32_t *tri = &w->tris[(size_t)w->shape_tri_off[ms] * 3];
+    for (int t = 0; t < T; t++)
+        for (int c = 0; c < 3; c++) {
+            double x0 = m->wp[tri[t * 3] * 3 + c], x1 = m->wp[tri[t * 3 + 1] * 3 + c], x2 = m->wp[tri[t * 3 + 2] * 3 + c];
+            double mn = x0 < x1 ? x0 : x1, mx = x0 > x1 ? x0 : x1;
+            m->tlo[t * 3 + c] = mn < x2 ? mn : x2;
+            m->thi[t * 3 + c] = mx > x2 ? mx : x2;
+        }
+    grid_build(&m->g, T, m->tlo, m->thi);
+    m->w = w; m->body = mb; m->pass = g_mesh_pass;
+    return m;
+}
+
 static int collide_mesh(OrWorld *w, Caps *cp, int a, int b) {
     const int mesh_is_a = w->shape_type[w->collider_shape[a]] == OR_SHAPE_TRIMESH;
     const int mb = mesh_is_a ? a : b, ob = mesh_is_a ? b : a;
     const int ms = w->collider_shape[mb], os = w->collider_shape[ob];
-    double R[9];
-    or_quat_to_matrix(&w->q[mb * 4], R);
-    const int np_ = w->shape_pt_cnt[ms], T = w->shape_tri_cnt[ms];
-    double *wp = (double *)malloc(sizeof(double) * 3 * (np_ ? np_ : 1));
-    convex_world_points(w, ms, &w->pos[mb * 3], R, wp);
-    double *tlo = (double *)malloc(sizeof(double) * 3 * (T ? T : 1)), *thi = (double *)malloc(sizeof(double) * 3 * (T ? T : 1));
+    MeshCache *mc = mesh_body_tables(w, mb);
+    const double *wp = mc->wp;
     const int32_t *tri = &w->tris[(size_t)w->shape_tri_off[ms] * 3];
-    for (int t = 0; t < T; t++)
-        for (int c = 0; c < 3; c++) {
-            double x0 = wp[tri[t * 3] * 3 + c], x1 = wp[tri[t * 3 + 1] * 3 + c], x2 = wp[tri[t * 3 + 2] * 3 + c];
-            double mn = x0 < x1 ? x0 : x1, mx = x0 > x1 ? x0 : x1;
-            tlo[t * 3 + c] = mn < x2 ? mn : x2;
-            thi[t * 3 + c] = mx > x2 ? mx : x2;
-        }
-    TriGrid g;
-    grid_build(&g, T, tlo, thi);
+    const TriGrid g = mc->g;
     int omax = w->shape_type[os] == OR_SHAPE_CONVEX ? w->shape_pt_cnt[os] : 1;
     double *so = (double *)malloc(sizeof(double) * 3 * (omax > 0 ? omax : 1));
     Proxy O;
@@ -2208,6 +2234,6 @@ static int collide_mesh(OrWorld *w, Caps *cp, int a, int b) {
         }
         if (hit) rc = push_contact(w, cp, a, b, pt, nrm, dep);
     }
-    free(cand); grid_free(&g); free(tlo); free(thi); free(wp); free(so);
+    free(cand); free(so);
     return rc;
 }

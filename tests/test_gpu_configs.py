@@ -9,6 +9,8 @@
   island pass;
 * capsule pile, 4096 bodies (30% capsules, 20% cylinders, the rest boxes and
   spheres): 120 steps, compared bit for bit every 40 steps;
+* terrain, 2000 bodies on an 18,432-triangle static mesh: 120 steps, compared
+  bit for bit every 40 steps;
 * batched joint chains (point joints, motors, loose boxes; 1/240 s, 12 contact
   and 12 joint iterations): 8 worlds of uneven sizes in one batch, each within
   1e-6 m / 1e-6 of the oracle after 60 steps (point joints go through an
@@ -75,6 +77,15 @@ def test_capsule_pile_4096_full_size():
     GJK/EPA, 120 steps compared bit for bit every 40."""
     w, meta = scenes.capsule_pile(n=4096, seed=0)
     b = _run_exact(w, meta['dt'], 120, 40, 'capsules4096')
+    assert b.counts()[1][0] > 1000
+
+
+def test_terrain_2000_on_an_18k_triangle_mesh():
+    """2000 capsules, boxes, spheres and hulls onto a 96x96-cell rippled mesh
+    (18,432 triangles, the triangle grid's full 64-cell resolution) and a
+    small ramp: 120 steps compared bit for bit every 40."""
+    w, meta = scenes.terrain(n=2000, seed=5, cells=96, extent=20.0)
+    b = _run_exact(w, meta['dt'], 120, 40, 'terrain2000')
     assert b.counts()[1][0] > 1000
 
 

@@ -19,7 +19,7 @@ from util import assert_close, world_at_checkpoint
 
 pytestmark = pytest.mark.gpu
 
-EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain'}
+EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge'}
 
 
 @pytest.mark.parametrize('scene', SCENES)

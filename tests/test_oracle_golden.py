@@ -13,7 +13,7 @@ import pytest
 import pyoracle
 from golden_util import SCENES, checkpoint, checkpoints, events_from_overlaps, load, pair_set
 
-EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain')
+EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge')
 
 
 def _close(a, b, exact):
