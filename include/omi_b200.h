@@ -24,7 +24,7 @@ extern "C" {
 #define OMI_OK 0
 #define OMI_E_CUDA (-1)         /* CUDA runtime error (message has details) */
 #define OMI_E_ARG (-2)          /* bad argument / size */
-#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (a moving triangle mesh ...) */
+#define OMI_E_UNSUPPORTED (-3)  /* feature outside the device path (a dynamic triangle mesh ...) */
 #define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
 #define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
 #define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
@@ -115,10 +115,12 @@ typedef struct OmiScene {
                                        gravity, as field_at forms it), or a point field's centre */
     const double *vol_rc, *vol_rr;  /* *3: region centre; radius**2 in [0] (sphere) or half-extents (box) */
 
-    /* triangle meshes (body.py:155-212, trigrid.py:63-218): static bodies whose
-     * collider is an OMI_SHAPE_TRIMESH shape (its points listed as for a hull),
-     * each with its triangles in world space and the reference's uniform grid
-     * over them, built on the host from the body's pose */
+    /* triangle meshes (body.py:155-212, trigrid.py:63-218): static or kinematic
+     * bodies whose collider is an OMI_SHAPE_TRIMESH shape (its points listed as
+     * for a hull), each with its triangles in world space and the reference's
+     * uniform grid over them, built on the host from the body's pose (and on
+     * the device every step for a kinematic mesh, as the reference rebuilds a
+     * mesh proxy every step) */
     int32_t n_meshes;
     const int32_t *mesh_body;       /* n_meshes: global body index */
     const int32_t *mesh_tri_off;    /* n_meshes+1: rows of the triangle tables */
@@ -128,6 +130,8 @@ typedef struct OmiScene {
     const double *tri_box;          /* n_tris*6: bounds lo (3), hi (3) */
     const int32_t *tri_cells;       /* n_tris*6: first cell (3), last cell (3) */
     const uint8_t *tri_big;         /* n_tris: spans more than 64 cells (always a candidate) */
+    const int32_t *tri_idx;         /* n_tris*3: vertex indices into the mesh shape's points; a kinematic
+                                       mesh's tables are rebuilt from them every step */
 } OmiScene;
 
 /* gravity volume kind flags: point field (else directional); region sphere,

@@ -67,6 +67,7 @@ class OmiScene(C.Structure):
         ('vol_rc', D), ('vol_rr', D),
         ('n_meshes', C.c_int32), ('mesh_body', I), ('mesh_tri_off', I), ('mesh_grid_i', I),
         ('mesh_grid_d', D), ('tri_verts', D), ('tri_box', D), ('tri_cells', I), ('tri_big', U8),
+        ('tri_idx', I),
     ]
 
 

@@ -34,7 +34,7 @@ def _quat_matrix(q) -> np.ndarray:
 
 
 def mesh_tables(points, indices, position, orientation) -> dict:
-    """A static mesh body's triangles as the reference collides them: world
+    """A mesh body's triangles as the reference collides them at this pose: world
     vertices (``points @ R.T + position``, body.py:164), per-triangle bounds
     and the uniform grid of trigrid.py:63-97 (64 cells along the longest
     side, triangles spanning more than 64 cells set aside, no grid below 256
@@ -62,7 +62,7 @@ def mesh_tables(points, indices, position, orientation) -> dict:
         cells[:, :3], cells[:, 3:] = first, last
         big[:] = np.prod(last - first + 1, axis=1) > 64
     return dict(verts=tris.reshape(T, 9), box=np.concatenate([lo, hi], axis=1), cells=cells, big=big,
-                grid_i=gi, grid_d=gd)
+                grid_i=gi, grid_d=gd, idx=np.asarray(indices, dtype=np.int32).reshape(-1, 3))
 JOINT_CODES = {'point': 0, 'distance': 1, 'motor': 2}
 
 
@@ -120,8 +120,8 @@ def check_supported(world) -> None:
         if np.isin(ts, meshes).any():
             raise UnsupportedFeature(-3, 'triangle-mesh sensors are not supported on the CUDA path')
         on = np.isin(cs, meshes)
-        if (np.asarray(world._motion_type[:n])[on] != 0).any():
-            raise UnsupportedFeature(-3, 'triangle meshes are taken as static colliders only')
+        if (np.asarray(world._motion_type[:n])[on] == 2).any():
+            raise UnsupportedFeature(-3, 'triangle meshes are taken as static or kinematic colliders only')
         for k in set(int(x) for x in cs[on]):
             if world.shapes[k].points is None or world.shapes[k].indices is None:
                 raise UnsupportedFeature(-3, 'a triangle mesh needs its points and indices')
@@ -158,7 +158,8 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                              'j_has_local_a', 'j_has_local_b', 'j_length', 'j_has_length',
                              'j_axis', 'j_target', 'j_max_force', 'j_accum', 'trigger_shape',
                              'vol_kind', 'vol_g', 'vol_field', 'vol_rc', 'vol_rr', 'mesh_body',
-                             'mesh_grid_i', 'mesh_grid_d', 'tri_verts', 'tri_box', 'tri_cells', 'tri_big')}
+                             'mesh_grid_i', 'mesh_grid_d', 'tri_verts', 'tri_box', 'tri_cells', 'tri_big',
+                             'tri_idx')}
     body_off, joint_off, vol_off, tri_off = [0], [0], [0], [0]
     any_sensor = False
     w_g, w_dt, w_iters, w_jiters, w_flags, w_damp, w_solver = [], [], [], [], [], [], []
@@ -194,7 +195,7 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
                 parts['mesh_body'].append([nb + i])
                 parts['mesh_grid_i'].append(mt['grid_i'])
                 parts['mesh_grid_d'].append(mt['grid_d'])
-                for key in ('verts', 'box', 'cells', 'big'):
+                for key in ('verts', 'box', 'cells', 'big', 'idx'):
                     parts['tri_' + key].append(mt[key])
                 tri_off.append(tri_off[-1] + len(mt['big']))
         vols = pack_volumes(getattr(world, 'gravity_volumes', None) or [])
@@ -387,6 +388,7 @@ def pack_worlds(worlds: Sequence, dts: Sequence[float] = None, active=True) -> P
         P.set('tri_box', cat('tri_box', 'd', 6), D)
         P.set('tri_cells', cat('tri_cells', np.int32, 6), I)
         P.set('tri_big', cat('tri_big', np.uint8), U8)
+        P.set('tri_idx', cat('tri_idx', np.int32, 3), I)
     P.has_sensors = any_sensor
     P.body_off = body_off
     P.joint_off = joint_off

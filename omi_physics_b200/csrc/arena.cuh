@@ -115,6 +115,8 @@ struct Arena {
     const double *mesh_grid_d, *tri_verts, *tri_box;
     const int *tri_cells;
     const uint8_t *tri_big;
+    const int *tri_idx;             // per triangle: vertex indices into the mesh shape's points
+    const int *mesh_body_of;        // per mesh: its body
     int *trig_out;                  // per sensor pair: trigger, other, overlap (1/0, -1 no shape)
     int *clip_list, *clip_n;        // touching box-box pairs awaiting face clipping
     int *contact_scan;              // pair_cap + 1

@@ -693,6 +693,120 @@ __global__ void k_triggers(Arena A) {
 // pair's count for the contact scan; k_mesh_emit repeats the pass and writes
 // the contacts at the pair's place in the contact arrays.
 // ---------------------------------------------------------------------------
+// A kinematic mesh's tables at this step's pose, one block per mesh: world
+// vertices (points @ R.T + position), per-triangle bounds and the uniform
+// grid of trigrid.py:63-97 - the reference rebuilds a moving mesh's proxy and
+// grid every step (narrowphase.py:40-48). Static meshes keep the tables the
+// host built at load.
+constexpr int MESH_REFRESH_THREADS = 256;
+
+__global__ void __launch_bounds__(MESH_REFRESH_THREADS) k_mesh_refresh(Arena A, int n_meshes) {
+    __shared__ double red[MESH_REFRESH_THREADS];
+    __shared__ int redi[MESH_REFRESH_THREADS];
+    __shared__ double glo[3], ghi[3];
+    __shared__ int shape[3];
+    if (pairs_over(A)) return;
+    const int tid = threadIdx.x;
+    for (int m = blockIdx.x; m < n_meshes; m += gridDim.x) {
+        const int mb = A.mesh_body_of[m];
+        const int w = A.body_world[mb];
+        if (A.mtype[mb] == 0 || !world_collides(A, w)) continue;
+        double R[9];
+        quat_to_matrix(&A.q[mb * 4], R);
+        const double *c = &A.pos[mb * 3];
+        const int s = A.rshape[mb];
+        const double *pts = &A.points[A.pt_off[s] * 3];
+        const int t0 = A.mesh_tri_off[m], t1 = A.mesh_tri_off[m + 1], T = t1 - t0;
+        double *tv = const_cast<double *>(A.tri_verts), *tb = const_cast<double *>(A.tri_box);
+        double lmin[3] = {INFINITY, INFINITY, INFINITY}, lmax[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int t = t0 + tid; t < t1; t += blockDim.x) {
+            double v[9];
+            for (int j = 0; j < 3; j++) {
+                const double *l = &pts[A.tri_idx[t * 3 + j] * 3];
+                for (int k = 0; k < 3; k++) v[j * 3 + k] = dot_blas(l, &R[k * 3]) + c[k];
+            }
+            for (int k = 0; k < 9; k++) tv[(size_t)t * 9 + k] = v[k];
+            for (int k = 0; k < 3; k++) {
+                const double a = v[k], b = v[3 + k], d = v[6 + k];
+                double mn = a < b ? a : b, mx = a > b ? a : b;
+                mn = mn < d ? mn : d;
+                mx = mx > d ? mx : d;
+                tb[(size_t)t * 6 + k] = mn;
+                tb[(size_t)t * 6 + 3 + k] = mx;
+                lmin[k] = mn < lmin[k] ? mn : lmin[k];
+                lmax[k] = mx > lmax[k] ? mx : lmax[k];
+            }
+        }
+        int *gi = const_cast<int *>(&A.mesh_grid_i[m * 4]);
+        double *gd = const_cast<double *>(&A.mesh_grid_d[m * 7]);
+        if (T < 256) {                                   // no grid: every query scans exactly
+            if (tid == 0) gi[0] = 1;
+            __syncthreads();
+            continue;
+        }
+        // lows.min(axis=0), highs.max(axis=0)
+        for (int k = 0; k < 3; k++) {
+            red[tid] = lmin[k];
+            __syncthreads();
+            for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+                if (tid < h) red[tid] = red[tid + h] < red[tid] ? red[tid + h] : red[tid];
+                __syncthreads();
+            }
+            if (tid == 0) glo[k] = red[0];
+            __syncthreads();
+            red[tid] = lmax[k];
+            __syncthreads();
+            for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+                if (tid < h) red[tid] = red[tid + h] > red[tid] ? red[tid + h] : red[tid];
+                __syncthreads();
+            }
+            if (tid == 0) ghi[k] = red[0];
+            __syncthreads();
+        }
+        // cell = max(maximum(high - low, 1e-9)) / 64
+        double ext = 0.0;
+        for (int k = 0; k < 3; k++) {
+            double e = ghi[k] - glo[k];
+            e = e > 1e-9 ? e : 1e-9;
+            ext = k == 0 || e > ext ? e : ext;
+        }
+        const double cell = ext / 64.0;
+        const long long top = (1LL << 30) - 1;
+        int lmaxc[3] = {0, 0, 0};
+        int *tc = const_cast<int *>(A.tri_cells);
+        uint8_t *big = const_cast<uint8_t *>(A.tri_big);
+        for (int t = t0 + tid; t < t1; t += blockDim.x) {
+            long long f[3], l[3];
+            for (int k = 0; k < 3; k++) {
+                long long a = (long long)floor((tb[(size_t)t * 6 + k] - glo[k]) / cell);
+                long long b = (long long)floor((tb[(size_t)t * 6 + 3 + k] - glo[k]) / cell);
+                f[k] = a < 0 ? 0 : (a > top ? top : a);
+                l[k] = b < 0 ? 0 : (b > top ? top : b);
+                tc[(size_t)t * 6 + k] = (int)f[k];
+                tc[(size_t)t * 6 + 3 + k] = (int)l[k];
+                lmaxc[k] = (int)l[k] > lmaxc[k] ? (int)l[k] : lmaxc[k];
+            }
+            big[t] = (l[0] - f[0] + 1) * (l[1] - f[1] + 1) * (l[2] - f[2] + 1) > 64 ? 1 : 0;
+        }
+        for (int k = 0; k < 3; k++) {
+            redi[tid] = lmaxc[k];
+            __syncthreads();
+            for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+                if (tid < h) redi[tid] = redi[tid + h] > redi[tid] ? redi[tid + h] : redi[tid];
+                __syncthreads();
+            }
+            if (tid == 0) shape[k] = redi[0] + 1;
+            __syncthreads();
+        }
+        if (tid == 0) {
+            gi[0] = 0; gi[1] = shape[0]; gi[2] = shape[1]; gi[3] = shape[2];
+            gd[0] = glo[0]; gd[1] = glo[1]; gd[2] = glo[2];
+            gd[3] = ghi[0]; gd[4] = ghi[1]; gd[5] = ghi[2]; gd[6] = cell;
+        }
+        __syncthreads();
+    }
+}
+
 // the proxy's own bounds, no margin (body.py: aabb() of each proxy kind)
 __device__ inline void proxy_bounds(const Proxy &P, double *lo, double *hi) {
     if (P.kind == 1) {

@@ -62,6 +62,7 @@ struct OmiCtx {
     int cache_cap = 0;
     bool has_triggers = false;     // some body carries a sensor shape: k_triggers runs each step
     bool has_meshes = false;       // some body is a triangle mesh: k_mesh_count / k_mesh_emit run
+    int moving_meshes = 0;         // meshes (rows of the mesh tables) when one of them is kinematic, else 0
     cudaGraphExec_t graph = nullptr;
     int *h_status = nullptr;       // pinned mirror of the status words
     int64_t launches = 0;
@@ -294,6 +295,10 @@ void stage_broadphase(OmiCtx *ctx, Prof *pf) {
 
 void stage_narrow(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
+    if (ctx->moving_meshes) {
+        k_mesh_refresh<<<std::min(ctx->moving_meshes, 148), MESH_REFRESH_THREADS, 0, ctx->stream>>>(A, ctx->moving_meshes);
+        ctx->launches++;
+    }
     k_narrow<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
     k_clip<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
     ctx->launches += 2;
@@ -426,6 +431,7 @@ int64_t step_launches(OmiCtx *ctx) {
     if (ctx->A.NJ > 0) n += 1;
     if (ctx->has_triggers) n += 1;
     if (ctx->has_meshes) n += 2;
+    if (ctx->moving_meshes) n += 1;
     return n;
 }
 
@@ -642,8 +648,8 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
             if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
                 s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
                 return fail(ctx, OMI_E_ARG, "mesh point range out of bounds");
-            if (s->shape[i] != sh || s->motion_type[i] != 0)
-                return fail(ctx, OMI_E_UNSUPPORTED, "triangle meshes are taken as static colliders only");
+            if (s->shape[i] != sh || s->motion_type[i] == 2)
+                return fail(ctx, OMI_E_UNSUPPORTED, "triangle meshes are taken as static or kinematic colliders only");
         } else {
             return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
         }
@@ -663,6 +669,14 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
             body_mesh[b] = m;
         }
         n_tris = s->mesh_tri_off[NMESH];
+        if (!s->tri_idx) return fail(ctx, OMI_E_ARG, "mesh tables without tri_idx");
+        for (int m = 0; m < NMESH; m++) {
+            const int b = s->mesh_body[m], sh = s->shape[b];
+            for (int t = s->mesh_tri_off[m]; t < s->mesh_tri_off[m + 1]; t++)
+                for (int j = 0; j < 3; j++)
+                    if (s->tri_idx[t * 3 + j] < 0 || s->tri_idx[t * 3 + j] >= s->shape_pt_cnt[sh])
+                        return fail(ctx, OMI_E_ARG, "mesh triangle vertex index out of range");
+        }
     }
     for (int i = 0; i < NB; i++)
         if (kind[i] == 5 && body_mesh[i] < 0) return fail(ctx, OMI_E_ARG, "a mesh body without its triangle tables");
@@ -742,7 +756,12 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= upload(ctx, const_cast<double *&>(A.tri_box), n_tris ? s->tri_box : nullptr, (size_t)n_tris * 6);
     rc |= upload(ctx, const_cast<int *&>(A.tri_cells), n_tris ? s->tri_cells : nullptr, (size_t)n_tris * 6);
     rc |= upload(ctx, const_cast<uint8_t *&>(A.tri_big), n_tris ? s->tri_big : nullptr, n_tris);
+    rc |= upload(ctx, const_cast<int *&>(A.tri_idx), n_tris ? s->tri_idx : nullptr, (size_t)n_tris * 3);
+    rc |= upload(ctx, const_cast<int *&>(A.mesh_body_of), NMESH ? s->mesh_body : nullptr, NMESH);
     ctx->has_meshes = NMESH > 0;
+    ctx->moving_meshes = 0;
+    for (int m = 0; m < NMESH; m++)
+        if (s->motion_type[s->mesh_body[m]] != 0) ctx->moving_meshes = NMESH;
     rc |= upload(ctx, const_cast<int *&>(A.rshape), rshape.data(), NB);
     ctx->has_triggers = sensors;
     // gravity volumes

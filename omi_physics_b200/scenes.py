@@ -17,6 +17,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``zones``        debris through trigger sensors and gravity volumes
   * ``terrain``      capsules, boxes, spheres and hulls on static triangle meshes
   * ``ridge``        one mesh mixing a fine floor with triangles the grid sets aside
+  * ``conveyor``     bodies riding a kinematic (sliding, turning) triangle-mesh platform
 """
 import math
 from types import SimpleNamespace
@@ -398,6 +399,51 @@ def ridge(api=None, backend=None, n: int = 60, seed: int = 0, iterations: int = 
     return w, dict(dt=1.0 / 120.0, steps=300, name='ridge%d' % n)
 
 
+def conveyor(api=None, backend=None, n: int = 50, seed: int = 0, iterations: int = 8, cells: int = 16,
+             extent: float = 5.0):
+    """Bodies falling onto a kinematic triangle-mesh platform that slides and
+    turns (its mesh proxy and grid rebuilt every step, as the reference does)
+    above a static ground box."""
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    gmat = w.add_material(m.Material(staticFriction=0.6, dynamicFriction=0.6))
+    ground = w.add_shape(m.Shape.box((8.0 * extent, 1.0, 8.0 * extent)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=gmat), position=(0.0, -3.5, 0.0))
+    pts, idx = _grid_mesh(cells, extent, 0.12, 0.7)
+    deck = w.add_shape(m.Shape.trimesh(pts, idx))
+    w.add_body(m.Motion(type=m.KINEMATIC, linearVelocity=(0.4, 0.0, 0.1), angularVelocity=(0.0, 0.25, 0.0)),
+               m.Collider(shape=deck, physicsMaterial=gmat), position=(0.0, 0.0, 0.0))
+    lim = extent - 1.0
+    pos = rng.uniform((-lim, 1.0, -lim), (lim, 4.0, lim), size=(n, 3))
+    axes = rng.normal(size=(n, 3))
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    u = rng.random(n)
+    for i in range(n):
+        r = float(rng.uniform(0.2, 0.4))
+        if u[i] < 0.4:
+            h = float(rng.uniform(0.3, 0.8))
+            shape = w.add_shape(m.Shape.capsule(h, r))
+            mass = 1000.0 * (math.pi * r * r * h + (4.0 / 3.0) * math.pi * r ** 3)
+        elif u[i] < 0.7:
+            sz = tuple(float(x) for x in rng.uniform(0.3, 0.7, 3))
+            shape = w.add_shape(m.Shape.box(sz))
+            mass = 1000.0 * sz[0] * sz[1] * sz[2]
+        elif u[i] < 0.85:
+            shape = w.add_shape(m.Shape.sphere(r))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * r ** 3
+        else:
+            semi = rng.uniform(0.2, 0.45, 3)
+            shape = w.add_shape(m.Shape.convex(_ellipsoid_points(rng, 12, semi)))
+            mass = 1000.0 * (4.0 / 3.0) * math.pi * float(np.prod(semi))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=mass), m.Collider(shape=shape, physicsMaterial=gmat),
+                   position=tuple(float(x) for x in pos[i]),
+                   orientation=_quat_axis_angle(axes[i], float(angles[i])))
+    _set_iterations(w, iterations)
+    return w, dict(dt=1.0 / 120.0, steps=300, name='conveyor%d' % n)
+
+
 def joint_chain(api=None, backend=None, links: int = 32, loose: int = 128, seed: int = 0,
                 motor_frac: float = 0.1, iterations: int = 12):
     """Chain of 0.2x0.2x1 m links pinned to the world at both ends, loose boxes above.
@@ -505,6 +551,7 @@ GOLDEN_SCENES = {
     'zones': lambda api=None, backend=None: zones(api, backend),
     'terrain': lambda api=None, backend=None: terrain(api, backend),
     'ridge': lambda api=None, backend=None: ridge(api, backend),
+    'conveyor': lambda api=None, backend=None: conveyor(api, backend),
 }
 
 
