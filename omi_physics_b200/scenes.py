@@ -18,6 +18,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``terrain``      capsules, boxes, spheres and hulls on static triangle meshes
   * ``ridge``        one mesh mixing a fine floor with triangles the grid sets aside
   * ``conveyor``     bodies riding a kinematic (sliding, turning) triangle-mesh platform
+  * ``degenerate``   coincident centres, zero-depth contacts, sleep and wake-up by a pusher
 """
 import math
 from types import SimpleNamespace
@@ -537,6 +538,59 @@ def feature_mix(api=None, backend=None, n: int = 70, seed: int = 11):
     return w, dict(dt=1.0 / 120.0, steps=120, name='feature_mix')
 
 
+def degenerate(api=None, backend=None):
+    """Edge cases of the contact routes and the sleep logic in one world.
+
+    Coincident centres (box-box, sphere-sphere, a sphere inside a box), contacts
+    of exactly zero depth (a sphere on a box top, a box stack face to face, a
+    capsule lying on the ground), an off-centre mass with an explicit rotated
+    inertia, a body far from everything else, and a row of boxes at rest that
+    falls asleep before a kinematic pusher reaches and wakes it.
+    """
+    api = api or default_api()
+    m = api.model
+    w = _new_world(api, backend, fixed_dt=1.0 / 60.0)
+    mat = w.add_material(m.Material(staticFriction=0.6, dynamicFriction=0.5, restitution=0.0))
+    ground = w.add_shape(m.Shape.box((40.0, 1.0, 40.0)))
+    unit = w.add_shape(m.Shape.box((1.0, 1.0, 1.0)))
+    ball = w.add_shape(m.Shape.sphere(0.5))
+    small = w.add_shape(m.Shape.sphere(0.3))
+    wide = w.add_shape(m.Shape.box((1.5, 1.5, 1.5)))
+    pill = w.add_shape(m.Shape.capsule(1.0, 0.25))
+    tetra = w.add_shape(m.Shape.convex(np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0],
+                                                 [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])))
+    pusher = w.add_shape(m.Shape.box((0.5, 1.0, 3.0)))
+
+    def body(shape, pos, q=(0.0, 0.0, 0.0, 1.0), **motion):
+        kind = motion.pop('type', m.DYNAMIC)
+        return w.add_body(m.Motion(type=kind, **motion),
+                          m.Collider(shape=shape, physicsMaterial=mat),
+                          position=pos, orientation=q)
+
+    body(ground, (0.0, -0.5, 0.0), type=m.STATIC)
+    body(unit, (0.0, 1.5, 0.0))                       # two boxes, one centre
+    body(unit, (0.0, 1.5, 0.0))
+    body(ball, (3.0, 1.5, 0.0))                       # two spheres, one centre
+    body(ball, (3.0, 1.5, 0.0))
+    body(wide, (6.0, 1.2, 0.0))                       # a sphere inside a box, same centre
+    body(small, (6.0, 1.2, 0.0))
+    body(unit, (-3.0, 0.5, 0.0))                      # zero-depth: box on ground, sphere on box
+    body(small, (-3.0, 1.3, 0.0))
+    body(unit, (-6.0, 0.5, 0.0))                      # face-to-face stack at rest
+    body(unit, (-6.0, 1.5, 0.0))
+    body(pill, (-9.0, 0.25, 0.0), _quat_axis_angle(np.array([0.0, 0.0, 1.0]), 0.5 * math.pi))
+    body(tetra, (-12.0, 0.0, 0.0))                    # hull resting on a face, zero depth
+    body(unit, (0.0, 1.0, 4.0), _quat_axis_angle(np.array([0.0, 1.0, 0.0]), 0.25 * math.pi),
+         mass=2.0, centerOfMass=(0.2, 0.0, 0.1), inertiaDiagonal=(0.3, 0.5, 0.4),
+         inertiaOrientation=_quat_axis_angle(np.array([0.0, 0.0, 1.0]), math.pi / 6.0))
+    body(ball, (5000.0, 10.0, -5000.0))               # far from everything
+    for k in range(4):                                # a resting row, asleep before the pusher
+        body(unit, (8.0 + k, 0.5, 4.0))
+    body(pusher, (13.5, 0.5, 4.0), type=m.KINEMATIC, linearVelocity=(-1.0, 0.0, 0.0))
+    _set_iterations(w, 8)
+    return w, dict(dt=1.0 / 60.0, steps=300, name='degenerate')
+
+
 #: the golden-fixture scenes (tests/golden/make_golden.py), by fixture name
 GOLDEN_SCENES = {
     'pyramid': lambda api=None, backend=None: pyramid(api, backend),
@@ -552,6 +606,7 @@ GOLDEN_SCENES = {
     'terrain': lambda api=None, backend=None: terrain(api, backend),
     'ridge': lambda api=None, backend=None: ridge(api, backend),
     'conveyor': lambda api=None, backend=None: conveyor(api, backend),
+    'degenerate': lambda api=None, backend=None: degenerate(api, backend),
 }
 
 

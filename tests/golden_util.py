@@ -4,7 +4,8 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
-SCENES = ('pyramid', 'debris', 'convex', 'chain', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor')
+SCENES = ('pyramid', 'debris', 'convex', 'chain', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
+          'degenerate')
 
 
 def load(name):

@@ -35,7 +35,7 @@ def _ref_api():
 
 @pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60),
                                          ('capsules', 30), ('zones', 60), ('terrain', 40),
-                                         ('conveyor', 40)])
+                                         ('conveyor', 40), ('degenerate', 140)])
 def test_reference_world_steps_on_cuda_backend(scene, steps):
     from omi_physics_b200.backend import CudaBackend
     api = _ref_api()
@@ -68,3 +68,16 @@ def test_reference_world_steps_on_cuda_backend(scene, steps):
             assert np.allclose(gd, cd, rtol=1e-9, atol=1e-12), tag + ' depths'
         assert np.max(np.abs(gpu._position[:n] - cpu._position[:n]), initial=0.0) <= 1e-6, tag + ' pos'
         assert np.max(np.abs(gpu._orientation[:n] - cpu._orientation[:n]), initial=0.0) <= 1e-6, tag
+
+
+def test_reference_empty_world_on_cuda_backend():
+    from omi_physics_b200.backend import CudaBackend
+    api = _ref_api()
+    gpu = api.PhysicsWorld(fixed_dt=1.0 / 60.0, backend=CudaBackend())
+    cpu = api.PhysicsWorld(fixed_dt=1.0 / 60.0)
+    for _ in range(3):
+        gpu.step(1.0 / 60.0)
+        cpu.step(1.0 / 60.0)
+    assert gpu.body_count == cpu.body_count == 0
+    assert len(gpu.contacts) == len(cpu.contacts) == 0
+    assert gpu.time == cpu.time

@@ -19,7 +19,8 @@ from util import assert_close, world_at_checkpoint
 
 pytestmark = pytest.mark.gpu
 
-EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor'}
+EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
+         'degenerate'}
 
 
 @pytest.mark.parametrize('scene', SCENES)
@@ -86,6 +87,7 @@ def _island_sets(labels):
     ('zones300', lambda: scenes.zones(n=300, seed=4, extent=6.0, height=10.0), 150),
     ('terrain150', lambda: scenes.terrain(n=150, seed=2, cells=30, extent=8.0), 150),
     ('conveyor120', lambda: scenes.conveyor(n=120, seed=3, cells=20, extent=6.0), 150),
+    ('degenerate', lambda: scenes.degenerate(), 300),
 ])
 def test_trajectory_matches_oracle_every_step(name, builder, steps):
     w, meta = builder()

@@ -76,3 +76,19 @@ def test_select_backend_has_no_fallback():
     assert isinstance(select_backend('cuda'), CudaBackend)
     with pytest.raises(ValueError):
         select_backend('numpy')
+
+
+def test_pack_with_empty_and_static_only_worlds():
+    api = scenes.default_api()
+    m = api.model
+    empty = api.PhysicsWorld(fixed_dt=1 / 60)
+    statics = api.PhysicsWorld(fixed_dt=1 / 60)
+    slab = statics.add_shape(m.Shape.box((4.0, 1.0, 4.0)))
+    statics.add_body(m.Motion(type=m.STATIC), m.Collider(shape=slab), position=(0.0, -0.5, 0.0))
+    deg, _ = scenes.degenerate()
+    p = pack_worlds([empty, statics, deg, empty])
+    off = p.arrays['w_body_off']
+    assert list(off) == [0, 0, 1, 1 + deg.body_count, 1 + deg.body_count]
+    assert p.scene.n_worlds == 4 and p.scene.n_bodies == 1 + deg.body_count
+    p0 = pack_worlds([empty])
+    assert p0.scene.n_bodies == 0 and list(p0.arrays['w_body_off']) == [0, 0]

@@ -13,7 +13,8 @@ import pytest
 import pyoracle
 from golden_util import SCENES, checkpoint, checkpoints, events_from_overlaps, load, pair_set
 
-EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor')
+EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
+         'degenerate')
 
 
 def _close(a, b, exact):
