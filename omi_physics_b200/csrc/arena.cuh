@@ -106,7 +106,7 @@ struct Arena {
     int *gjk_list, *gjk_n;
     int *trig_list, *trig_n;        // sensor pairs this step (pair indices)
     int *mesh_list, *mesh_n;        // pairs with a triangle-mesh body this step
-    // static triangle-mesh bodies (body.py:155-212): per mesh its triangle rows
+    // static and kinematic triangle-mesh bodies (body.py:155-212): per mesh its triangle rows
     // [mesh_tri_off[m], mesh_tri_off[m+1]), the reference's uniform grid
     // (trigrid.py: exact flag, grid shape (3); low (3), high (3), cell size)
     // and per triangle world vertices (9), bounds (6), cell range (6), big flag

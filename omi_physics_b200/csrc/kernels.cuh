@@ -681,7 +681,7 @@ __global__ void k_triggers(Arena A) {
 }
 
 // ---------------------------------------------------------------------------
-// triangle meshes (collide.py:272-306 with trigrid.py): a static mesh body
+// triangle meshes (collide.py:272-306 with trigrid.py): a static or kinematic mesh body
 // against another body, one warp per pair. The candidates are the triangles
 // the reference's uniform grid hands back for the other proxy's bounds
 // (trigrid.py:99-111): every triangle whose bounds meet the query when the
