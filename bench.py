@@ -90,16 +90,59 @@ def dist_init(n):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock, its maximum and the slowdown reasons, sampled during the timed
+    region: NVML read in-process every 5 ms (the first sample is taken before
+    the region opens), else ``nvidia-smi -lms 100``. Read-only queries."""
     FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
               'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
               'clocks_event_reasons.sw_power_cap')
+    PERIOD_S = 0.005
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self._stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.device)
+            bus = '%08X:%02X:%02X.0' % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        flags = ['Active' if r & b else 'Not Active' for b in bits]
+        self.lines.append(', '.join([str(sm), str(mx), ''] + flags))
+
+    def _poll(self):
+        while not self._stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            self._stop.wait(self.PERIOD_S)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._nvml_sample()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
@@ -116,6 +159,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.nvml is not None:
+            self._stop.set()
+            self.t.join(timeout=5)
+            try:
+                self._nvml_sample()
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:

@@ -28,3 +28,30 @@ def test_reference_arm_json_line():
     cb = d['cpu_baseline']
     assert cb['kind'] == 'reference' and cb['cores'] >= 1 and cb['value'] == d['value']
     assert set(d['e2e']) >= {'value', 'unit', 'h2d_bytes_per_step', 'd2h_bytes_per_step'}
+
+
+def test_clock_sampler_reads_nvml_and_summarises(monkeypatch):
+    """The sampler against a fake NVML module: median SM clock, max clock and
+    the slowdown reasons seen while it ran (only read-only queries are made)."""
+    import types
+    sys.path.insert(0, ROOT)
+    import bench
+    calls = []
+    clocks = iter([1965, 1965, 1800, 1965] + [1965] * 1000)
+    fake = types.SimpleNamespace(
+        NVML_CLOCK_SM=1, nvmlClocksEventReasonHwSlowdown=0x8, nvmlClocksEventReasonHwThermalSlowdown=0x40,
+        nvmlClocksEventReasonSwThermalSlowdown=0x20, nvmlClocksEventReasonSwPowerCap=0x4,
+        nvmlInit=lambda: calls.append('init'), nvmlShutdown=lambda: calls.append('shutdown'),
+        nvmlDeviceGetHandleByPciBusId=lambda bus: 'h',
+        nvmlDeviceGetHandleByIndex=lambda i: 'h',
+        nvmlDeviceGetClockInfo=lambda h, c: next(clocks),
+        nvmlDeviceGetMaxClockInfo=lambda h, c: 1965,
+        nvmlDeviceGetCurrentClocksEventReasons=lambda h: 0x4)
+    monkeypatch.setitem(sys.modules, 'pynvml', fake)
+    with bench.ClockSampler(0) as clk:
+        import time
+        time.sleep(0.03)
+    s = clk.summary()
+    assert calls[0] == 'init' and calls[-1] == 'shutdown'
+    assert s['samples'] >= 3 and s['sm_max_mhz'] == 1965 and s['sm_mhz'] == 1965
+    assert s['reasons'] == ['sw_power_cap']
