@@ -564,7 +564,7 @@ def capsule_triangles_run(seed, blocks, local, steps, warmup, device_only=False)
                     'path': 'omi_capsule_triangles_batch from pinned host arrays (2 streams, 2M-triangle '
                             'chunks)'}}
     if cb is not None:
-        line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'per_core')}
         line['e2e_over_cpu'] = line['e2e']['value'] / cb['value']
     return line
 
@@ -644,7 +644,7 @@ def main():
                         'unit': 'body-steps/s', 'n_gpus': args.gpus, 'steps': args.steps,
                         'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
                         'dtype': 'f64', 'data': 'synthetic', 'config': config,
-                        'cpu_baseline': {k: r[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')},
+                        'cpu_baseline': {k: r[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'per_core')},
                         'e2e': {'value': r['value'], 'unit': 'body-steps/s',
                                 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
                 print(json.dumps(line))
@@ -680,7 +680,7 @@ def main():
         if not args.no_extras:
             cb = cpu_reference(args.worlds, args.seed, args.cpu_sample_s, args.preroll)
             if cb is not None:
-                line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+                line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'per_core')}
             if args.capsule_blocks > 0:
                 line['capsule_triangles'] = capsule_triangles_run(args.seed, args.capsule_blocks, local,
                                                                   args.steps, args.warmup)
