@@ -11,6 +11,8 @@
   spheres): 120 steps, compared bit for bit every 40 steps;
 * terrain, 2000 bodies on an 18,432-triangle static mesh: 120 steps, compared
   bit for bit every 40 steps;
+* the serving mix, 1024 worlds (417K bodies) as 4 concurrent groups: 240
+  steps, 40 sampled worlds bit for bit, size-independent checks on all;
 * batched joint chains (point joints, motors, loose boxes; 1/240 s, 12 contact
   and 12 joint iterations): 8 worlds of uneven sizes in one batch, each within
   1e-6 m / 1e-6 of the oracle after 60 steps (point joints go through an
@@ -109,3 +111,48 @@ def test_batched_joint_chains():
         assert float(np.max(np.abs(w._position[:n] - st['position']))) < 1e-6, k
         assert float(np.max(np.abs(w._orientation[:n] - st['orientation']))) < 1e-6, k
         assert np.array_equal(w._awake[:n], st['awake']), k
+
+
+def test_serving_mix_1024_worlds_full_size():
+    """The measured workload itself: the 1024-world serving mix (417K bodies)
+    stepped as 4 concurrent groups for 240 steps (the bench's pre-roll, into the
+    contact-heavy regime). A seeded sample of 40 worlds, the 8 largest among
+    them, equals the oracle bit for bit (pairs, contacts, impulses, state,
+    islands); every world passes size-independent checks (finite state,
+    unit quaternions, sleeping dynamic bodies at rest, every pair (a < b)
+    unique and within the world)."""
+    from omi_physics_b200.groups import WorldGroups
+    reqs = scenes.serving_requests(1024, seed=0)
+    worlds, dts = [], []
+    for r in reqs:
+        w, meta = scenes.serving_world(r)
+        worlds.append(w)
+        dts.append(meta['dt'])
+    sizes = np.array([w.body_count for w in worlds])
+    rng = np.random.default_rng(17)
+    largest = list(np.argsort(-sizes, kind='stable')[:8])
+    rest = [i for i in range(len(worlds)) if i not in set(largest)]
+    sample = sorted(largest + list(rng.choice(rest, size=32, replace=False)))
+    oracles = {int(i): pyoracle.OracleWorld.from_world(worlds[i]) for i in sample}
+    g = WorldGroups(worlds, dts=dts, groups=4)
+    try:
+        g.step(240)
+        g.sync_to_host()
+        for i, o in oracles.items():
+            for _ in range(240):
+                o.step(dts[i])
+            b, j = g.batch_of(i)
+            _check_exact(b, j, worlds[i], o, 'mix world %d (%d bodies)' % (i, sizes[i]))
+        for i, w in enumerate(worlds):
+            n = w.body_count
+            assert np.isfinite(w._position[:n]).all() and np.isfinite(w._linear_velocity[:n]).all(), i
+            qn = np.linalg.norm(w._orientation[:n], axis=1)
+            assert np.all(np.abs(qn - 1.0) < 1e-9), i
+            asleep = (~w._awake[:n]) & (w._motion_type[:n] == 2)
+            assert not np.any(w._linear_velocity[:n][asleep]) and not np.any(w._angular_velocity[:n][asleep]), i
+            p = g.pairs(i)
+            if len(p):
+                assert (p[:, 0] < p[:, 1]).all() and p.min() >= 0 and p.max() < n, i
+                assert len({tuple(x) for x in p.tolist()}) == len(p), i
+    finally:
+        g.close()
