@@ -16,7 +16,9 @@
 * batched joint chains (point joints, motors, loose boxes; 1/240 s, 12 contact
   and 12 joint iterations): 8 worlds of uneven sizes in one batch, each within
   1e-6 m / 1e-6 of the oracle after 60 steps (point joints go through an
-  explicit 3x3 solve that matches the reference's LAPACK call to ~1e-12).
+  explicit 3x3 solve that matches the reference's LAPACK call to ~1e-12);
+  and at full size, 512 such worlds for 480 steps (16 compared at step 120,
+  size-independent checks on all at 480).
 """
 import numpy as np
 import pytest
@@ -156,3 +158,44 @@ def test_serving_mix_1024_worlds_full_size():
                 assert len({tuple(x) for x in p.tolist()}) == len(p), i
     finally:
         g.close()
+
+
+def test_joint_chains_512_worlds_full_size():
+    """The joints configuration at full size: 512 worlds, each a chain of
+    16-128 links pinned at both ends (point joints, 10% with an angular motor)
+    under 64-512 loose boxes, 1/240 s, 12 contact and 12 joint iterations,
+    480 steps in one batch. The chains are chaotic: on the oracle alone a
+    1e-12 m nudge of the initial poses grows past 1e-9 m by step 240 and to
+    about 1 m by step 480, so 16 seeded worlds are compared with the oracle
+    at step 120 (within 1e-6, point joints matching LAPACK to ~1e-12 per
+    solve) and all 512 pass size-independent checks at step 480 (finite
+    state, unit quaternions, sleeping dynamic bodies at rest)."""
+    rng = np.random.default_rng(21)
+    worlds, dts = [], []
+    for k in range(512):
+        w, meta = scenes.joint_chain(links=int(rng.integers(16, 129)), loose=int(rng.integers(64, 513)),
+                                     seed=1000 + k)
+        worlds.append(w)
+        dts.append(meta['dt'])
+    sample = sorted(int(i) for i in rng.choice(512, size=16, replace=False))
+    oracles = {i: pyoracle.OracleWorld.from_world(worlds[i]) for i in sample}
+    b = WorldBatch(worlds, dts=dts)
+    b.step(120)
+    b.sync_to_host()
+    for i, o in oracles.items():
+        for _ in range(120):
+            o.step(dts[i])
+        st = o.state()
+        w = worlds[i]
+        n = w.body_count
+        assert float(np.max(np.abs(w._position[:n] - st['position']))) < 1e-6, i
+        assert float(np.max(np.abs(w._orientation[:n] - st['orientation']))) < 1e-6, i
+        assert np.array_equal(w._awake[:n], st['awake']), i
+    b.step(360)
+    b.sync_to_host()
+    for i, w in enumerate(worlds):
+        n = w.body_count
+        assert np.isfinite(w._position[:n]).all() and np.isfinite(w._angular_velocity[:n]).all(), i
+        assert np.all(np.abs(np.linalg.norm(w._orientation[:n], axis=1) - 1.0) < 1e-9), i
+        asleep = (~w._awake[:n]) & (w._motion_type[:n] == 2)
+        assert not np.any(w._linear_velocity[:n][asleep]) and not np.any(w._angular_velocity[:n][asleep]), i
