@@ -210,7 +210,7 @@ def dynamic_bodies(worlds):
 
 
 def algorithmic_bytes(stage, N, P, K):
-    """Compulsory fp64 bytes per step of each stage (roofline)."""
+    """Compulsory fp64 bytes per step of each stage (N bodies, P candidate pairs, K contacts)."""
     return {
         'refit+integrate_forces': 269 * N,
         'broadphase': 48 * N + 256 * N + 8 * P,
