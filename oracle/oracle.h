@@ -3,7 +3,7 @@
  * omi_physics' PhysicsWorld.step (reference v0.3.1) in plain C, float64.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may
- * load this library, and only as the checker or the CPU baseline. The
+ * load this library, and only as the parity reference or the CPU baseline. The
  * product (omi_physics_b200) never links or calls it.
  *
  * Parity pin: tests/golden/ holds fixtures produced by running the reference

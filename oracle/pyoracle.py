@@ -7,7 +7,7 @@ reference's ``PhysicsWorld`` attribute layout (the reference's own class or
 exposes the per-step pairs, contacts, impulses and sleep islands.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
-this module, always as the checker or the timed CPU baseline.
+this module, always as the parity reference or the timed CPU baseline.
 """
 import ctypes as C
 import os
