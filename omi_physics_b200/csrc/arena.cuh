@@ -93,6 +93,7 @@ struct Arena {
     int *srt_info;           // per sorted row: motion type (bits 0-1), solid collider (2), awake (3),
                              // sensor (4), filter row (5-)
     int *pair_end;           // per sorted row: end of its sweep window
+    unsigned long long *pair_mask;  // per sorted row: kept bits of its first 64 window rows
     double *sort_k[2];
     int *sort_v[2];
     int *pair_cnt, *pair_scan;      // NB, NB+1

@@ -167,9 +167,10 @@ __global__ void k_sort(Arena A, int smem_cap) {
 // y/z overlap (>=), at least one dynamic body and interacting filters. One
 // warp per sorted row; lanes test 32 candidates at a time and a ballot keeps
 // the reference's k-major, then kj, order. The step's kernels read the rows'
-// boxes in sorted order (written by k_sort) and the count pass records each
-// window's end for the emit pass; the helpers below serve the
-// allocation-free entry point, which reads the caller's boxes in place.
+// boxes in sorted order (written by k_sort); the count pass records each
+// window's end and which of its first 64 rows it kept, so the emit pass
+// tests only rows past those 64. The helpers below serve the allocation-free
+// entry point, which reads the caller's boxes in place.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool pair_keep(const Arena &A, int w, int a, int b) {
     const double *la = &A.aabb_min[a * 3], *ha = &A.aabb_max[a * 3];
@@ -255,23 +256,26 @@ __global__ void k_pair_count(Arena A) {
     for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < A.NB; e += nwarps) {
         const int w = A.body_world[e];
         int cnt = 0, endk = e + 1;
+        unsigned long long kept = 0;
         if (world_collides(A, w) && e - A.w_body_off[w] < A.w_body_n[w]) {
             const int off = A.w_body_off[w], end_w = off + A.w_body_n[w];
             const double4 *ra = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)e * 8]);
             const double4 a0 = ra[0], a1 = ra[1];
             const int ia = A.srt_info[e];
             endk = window_end_warp(A.sorted_x, off, end_w, a0.y);
-            for (int base = e + 1; base < endk; base += 32) {
+            for (int base = e + 1, c = 0; base < endk; base += 32, c++) {
                 const int kj = base + lane;
                 bool keep = false;
                 if (kj < endk) {
                     const double4 *rb = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)kj * 8]);
                     keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], A.srt_info[kj]);
                 }
-                cnt += __popc(__ballot_sync(FULL, keep));
+                const unsigned m = __ballot_sync(FULL, keep);
+                if (c < 2) kept |= (unsigned long long)m << (32 * c);
+                cnt += __popc(m);
             }
         }
-        if (lane == 0) { A.pair_cnt[e] = cnt; A.pair_end[e] = endk; }
+        if (lane == 0) { A.pair_cnt[e] = cnt; A.pair_end[e] = endk; A.pair_mask[e] = kept; }
     }
 }
 
@@ -288,12 +292,16 @@ __global__ void k_pair_emit(Arena A) {
         const double4 *ra = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)e * 8]);
         const double4 a0 = ra[0], a1 = ra[1];
         const int ia = A.srt_info[e];
+        const unsigned long long kept = A.pair_mask[e];
         int out = A.pair_scan[e];
-        for (int base = e + 1; base < endk; base += 32) {
+        for (int base = e + 1, c = 0; base < endk; base += 32, c++) {
             const int kj = base + lane;
             int b = -1, ib = 0;
             bool keep = false;
-            if (kj < endk) {
+            if (c < 2) {                             // decided by the count pass
+                keep = (kept >> (32 * c + lane)) & 1ull;
+                if (keep) { ib = A.srt_info[kj]; b = A.order[kj]; }
+            } else if (kj < endk) {
                 const double4 *rb = reinterpret_cast<const double4 *>(&A.srt_box[(size_t)kj * 8]);
                 ib = A.srt_info[kj];
                 keep = row_keep(A, w, a0, a1, ia, rb[0], rb[1], ib);

@@ -817,6 +817,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.srt_box, (size_t)NB * 8);
     rc |= alloc(ctx, ctx->statics, A.srt_info, NB);
     rc |= alloc(ctx, ctx->statics, A.pair_end, NB);
+    rc |= alloc(ctx, ctx->statics, A.pair_mask, NB);
     for (int t = 0; t < 2; t++) {
         rc |= alloc(ctx, ctx->statics, A.sort_k[t], NB);
         rc |= alloc(ctx, ctx->statics, A.sort_v[t], NB);
