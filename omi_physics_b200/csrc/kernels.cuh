@@ -1222,39 +1222,36 @@ __device__ inline void prep_contact(const Arena &A, int w, int k, bool warm, int
 }
 
 // ---- the solver as four launches -------------------------------------------
-// k_wake     one warp per world: _wake_sleepers (solver.py:321-337)
+// k_wake     one block per world, largest first: _wake_sleepers (solver.py:321-337)
 // k_prep     one thread per contact, every world at once: material combine,
 //            warm-start seed, arms, tangent basis, effective masses, bias
 // k_levels   one block per world: runs and their predecessor / successor links
 // k_iterate  persistent blocks, 1, 2 or 4 worlds each: every pass of every
 //            run (warm start fused with the split-impulse position pass,
 //            then the velocity iterations) as a dataflow
-constexpr int SOLVE_WARPS = 4;   // warps (worlds) per block of the per-world kernels
+constexpr int WAKE_THREADS = 128;
 
-__device__ __forceinline__ int warp_global_id() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
-__device__ __forceinline__ int warp_count() { return (gridDim.x * blockDim.x) >> 5; }
-
-__global__ void k_wake(Arena A) {
+__global__ void __launch_bounds__(WAKE_THREADS) k_wake(Arena A) {
     if (overflowed(A)) return;
-    const int lane = threadIdx.x & 31;
     const double thr = 0.15 * 0.15;
-    for (int w = warp_global_id(); w < A.W; w += warp_count()) {
+    for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
+        const int w = A.w_sched[wi];
         if (!world_collides(A, w)) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
         if (c1 == c0) continue;
         bool cascade = false;
-        for (int k = c0 + lane; k < c1; k += 32) {
+        for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
             const int e[2] = {A.c_a[k], A.c_b[k]};
             for (int j = 0; j < 2; j++) {
                 const int x = e[j];
                 cascade |= A.mtype[x] == 2 && !A.awake[x] && speed2(&A.v[x * 3]) > thr;
             }
         }
-        if (__any_sync(FULL, cascade)) {
+        if (__syncthreads_or(cascade)) {
             // a body asleep at the start could wake and then wake others:
             // resolve in the reference's sequential contact order
-            if (lane == 0) {
+            if (threadIdx.x == 0) {
                 atomicAdd(&A.status[ST_CASCADE], 1);
                 for (int k = c0; k < c1; k++) {
                     const int a = A.c_a[k], b = A.c_b[k];
@@ -1269,8 +1266,9 @@ __global__ void k_wake(Arena A) {
                 }
             }
         } else {
-            // no woken body can wake another: order does not matter
-            for (int k = c0 + lane; k < c1; k += 32) {
+            // no woken body can wake another (every sleeper is at rest): order
+            // does not matter
+            for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
                 const int a = A.c_a[k], b = A.c_b[k];
                 const int ta = A.mtype[a], tb = A.mtype[b];
                 if (!A.awake[b] && (ta == 1 || (ta == 2 && A.awake[a] && speed2(&A.v[a * 3]) > thr)))
@@ -1279,7 +1277,7 @@ __global__ void k_wake(Arena A) {
                     wake_body(A, a);
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 

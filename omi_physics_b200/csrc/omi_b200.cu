@@ -329,9 +329,7 @@ void stage_compact(OmiCtx *ctx, Prof *pf) {
 
 void stage_solve(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
-    const int wb = 32 * SOLVE_WARPS;
-    const int wg = std::max(1, (A.W + SOLVE_WARPS - 1) / SOLVE_WARPS);
-    k_wake<<<wg, wb, 0, ctx->stream>>>(A);
+    k_wake<<<std::min(A.W, 65535), WAKE_THREADS, 0, ctx->stream>>>(A);
     mark(ctx, pf, KN_WAKE);
     k_prep<<<grid_for(A.contact_cap, PREP_THREADS, SM_CAP), PREP_THREADS, (size_t)PREP_THREADS * CD * sizeof(double), ctx->stream>>>(A);
     mark(ctx, pf, KN_PREP);
