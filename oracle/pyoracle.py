@@ -419,6 +419,11 @@ class OracleWorld:
         return dict(local_a=k['j_local_a'][:J].copy(), local_b=k['j_local_b'][:J].copy(),
                     length=k['j_length'][:J].copy(), accum=k['j_accum'][:J].copy())
 
+    def set_linear_velocity(self, i, v):
+        """Overwrite body ``i``'s linear velocity in place (as a host write to
+        ``world.linear_velocity`` between steps does), awake or asleep."""
+        self._keep['v'][i] = np.asarray(v, 'd')
+
     def write_back(self, world):
         """Copy the oracle's body state into ``world``'s columns."""
         n = self.c.n

@@ -4,7 +4,9 @@ Worlds without bodies and worlds of static bodies only, batched with the
 degenerate-contact scene (coincident centres, zero-depth contacts, sleep and
 wake-up) and a pyramid; a batch of empty worlds alone; and an empty world
 stepped through the drop-in backend, which must behave as the reference's
-step on an empty world does (nothing but the clock moves).
+step on an empty world does (nothing but the clock moves); and the wake
+pass's sequential path, taken when a sleeper moving faster than the wake
+threshold is among a world's contacts.
 """
 import numpy as np
 import pytest
@@ -77,3 +79,44 @@ def test_empty_world_through_the_drop_in_backend():
         w.step(1.0 / 60.0)
     assert w.body_count == 0 and len(w.contacts) == 0
     assert w.time == pytest.approx(4.0 / 60.0)
+
+
+def test_wake_cascade_from_a_moving_sleeper():
+    """A sleeping body that carries velocity (written by the host while it
+    sleeps) meets the kinematic pusher: the wake pass finds a sleeper faster
+    than the wake threshold among the contacts and resolves that world in the
+    reference's sequential contact order (solver.py:321-337). The velocity is
+    set on the resting row of the degenerate scene just before the pusher's
+    first contact; every following step equals the oracle bit for bit."""
+    row = [15, 16, 17, 18]
+    probe, meta = scenes.degenerate()
+    dt = meta['dt']
+    po = pyoracle.OracleWorld.from_world(probe)
+    first = None
+    for s in range(200):
+        po.step(dt)
+        c = po.contacts()
+        if any((int(a), int(b)) == (18, 19) for a, b in zip(c['a'], c['b'])):
+            first = s
+            break
+    assert first is not None
+    w, _ = scenes.degenerate()
+    o = pyoracle.OracleWorld.from_world(w)
+    b = WorldBatch([w], dts=[dt])
+    b.step(first)
+    for _ in range(first):
+        o.step(dt)
+    b.sync_to_host()
+    _check(b, 0, w, o, 'before the pusher')
+    assert not w._awake[row].any()
+    for i in row:
+        w._linear_velocity[i] = (-0.3, 0.0, 0.0)
+        o.set_linear_velocity(i, (-0.3, 0.0, 0.0))
+    b.upload_state(0)
+    for s in range(40):
+        b.step(1)
+        b.sync_to_host()
+        o.step(dt)
+        _check(b, 0, w, o, 'cascade step %d' % s)
+        if s == 0:
+            assert w._awake[row].all()          # the pusher woke the whole moving row
