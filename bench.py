@@ -25,7 +25,6 @@ the barrier and the max-over-ranks time use torch.distributed.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess

@@ -8,8 +8,6 @@ usable — there is no CPU fallback anywhere in the package.
 import ctypes as C
 import os
 
-import numpy as np
-
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, '_omi_b200.so')
 

@@ -8,7 +8,7 @@ What the device path does not implement is refused here with
 :class:`UnsupportedFeature`, never approximated.
 """
 import ctypes as C
-from typing import List, Sequence
+from typing import Sequence
 
 import numpy as np
 

@@ -19,10 +19,8 @@ first step raises.
 """
 from typing import Any, Optional
 
-import numpy as np
-
 from ._lib import OmiError, UnsupportedFeature
-from .arena import check_supported, static_signature, world_flags, world_iterations
+from .arena import check_supported, static_signature
 
 
 class _LazyContacts:

@@ -3,7 +3,6 @@ capacities a packed world needs."""
 import pytest
 
 from omi_physics_b200 import scenes
-from omi_physics_b200._lib import OmiSlotCaps
 from omi_physics_b200.arena import pack_worlds
 from omi_physics_b200.serving import SlotClass, SlotPool, fits, need_of, size_classes
 
