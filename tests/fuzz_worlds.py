@@ -1,0 +1,76 @@
+"""Seeded random worlds for the fuzz tests: every shape kind, motion type,
+friction and restitution combine mode, a pair-friction override, collision
+filters, damping / drag / gravity factors, sensors on every motion type, a
+resting stack that falls asleep, and gravity volumes of every kind. ``api``
+is a namespace with ``PhysicsWorld``, ``model`` and ``gravity`` of either the
+reference or this package, which build identical worlds."""
+import numpy as np
+
+
+def _quat(rng):
+    q = rng.normal(size=4)
+    return tuple(float(x) for x in q / np.linalg.norm(q))
+
+
+def random_world(api, seed, n=40):
+    m, G = api.model, api.gravity
+    rng = np.random.default_rng(seed)
+    w = api.PhysicsWorld(fixed_dt=1.0 / 120.0, default_linear_damping=float(rng.choice([0.0, 0.02])))
+    modes = (m.AVERAGE, m.MINIMUM, m.MAXIMUM, m.MULTIPLY)
+    mats = [w.add_material(m.Material(staticFriction=float(rng.uniform(0.1, 1.0)),
+                                      dynamicFriction=float(rng.uniform(0.05, 0.9)),
+                                      restitution=float(rng.choice([0.0, 0.2, 0.7])),
+                                      frictionCombine=modes[k % 4], restitutionCombine=modes[(k + 1) % 4]))
+            for k in range(5)]
+    w.set_pair_friction(mats[0], mats[1], 0.8, 0.7)
+    filters = [-1,
+               w.add_filter(m.CollisionFilter(collisionSystems=('a',), notCollideWithSystems=('b',))),
+               w.add_filter(m.CollisionFilter(collisionSystems=('b',))),
+               w.add_filter(m.CollisionFilter(collisionSystems=('c',), collideWithSystems=('c', 'a')))]
+    ground = w.add_shape(m.Shape.box((14.0, 1.0, 14.0)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=mats[0]),
+               position=(0.0, -0.5, 0.0))
+
+    def shape():
+        k = rng.integers(0, 5)
+        if k == 0:
+            return w.add_shape(m.Shape.box(tuple(float(x) for x in rng.uniform(0.3, 1.4, 3))))
+        if k == 1:
+            return w.add_shape(m.Shape.sphere(float(rng.uniform(0.2, 0.7))))
+        if k == 2:
+            return w.add_shape(m.Shape.capsule(float(rng.uniform(0.3, 1.2)), float(rng.uniform(0.15, 0.4))))
+        if k == 3:
+            return w.add_shape(m.Shape.cylinder(float(rng.uniform(0.4, 1.2)), float(rng.uniform(0.2, 0.5))))
+        pts = rng.normal(size=(int(rng.integers(8, 20)), 3))
+        pts *= rng.uniform(0.3, 0.8, 3) / np.linalg.norm(pts, axis=1, keepdims=True)
+        return w.add_shape(m.Shape.convex(pts))
+
+    for i in range(n):
+        u = rng.random()
+        kind = m.STATIC if u < 0.08 else (m.KINEMATIC if u < 0.16 else m.DYNAMIC)
+        pos = tuple(float(x) for x in rng.uniform((-2.5, 0.3, -2.5), (2.5, 3.0, 2.5)))
+        motion = m.Motion(type=kind, mass=float(rng.uniform(0.5, 4.0)),
+                          linearVelocity=tuple(float(x) for x in rng.normal(0.0, 0.6, 3)) if kind != m.STATIC
+                          else (0.0, 0.0, 0.0),
+                          angularVelocity=tuple(float(x) for x in rng.normal(0.0, 0.4, 3)) if kind != m.STATIC
+                          else (0.0, 0.0, 0.0),
+                          linearDamping=float(rng.choice([0.0, 0.1])), angularDamping=float(rng.choice([0.0, 0.2])),
+                          quadraticDrag=float(rng.choice([0.0, 0.03])), gravityFactor=float(rng.choice([1.0, 0.5, 1.5])))
+        collider = None if rng.random() < 0.05 else m.Collider(shape=shape(), physicsMaterial=mats[i % 5],
+                                                              collisionFilter=filters[i % 4])
+        trigger = m.Trigger(shape=shape()) if rng.random() < 0.12 else None
+        if collider is None and trigger is None and kind == m.STATIC:
+            continue
+        w.add_body(motion, collider, trigger=trigger, position=pos, orientation=_quat(rng))
+    unit = w.add_shape(m.Shape.box((1.0, 1.0, 1.0)))
+    for k in range(4):                  # a resting stack that falls asleep unless something hits it
+        w.add_body(m.Motion(type=m.DYNAMIC), m.Collider(shape=unit, physicsMaterial=mats[0]),
+                   position=(5.5, 0.5 + k, 5.5))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(type='point', gravity=5.0, center=(2.0, 2.0, 0.0), priority=1),
+                                         G.SphereRegion((2.0, 2.0, 0.0), 2.5)))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(gravity=3.0, direction=(0.3, 1.0, 0.0), priority=2,
+                                                   replace=True), G.BoxRegion((-2.5, 2.0, 2.5), (1.5, 2.0, 1.5))))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(priority=3, stop=True), G.BoxRegion((2.5, 1.5, -2.5), (1.0, 1.5, 1.0))))
+    w.add_gravity_volume(G.GravityVolume(m.Gravity(gravity=0.4, direction=(0.0, 0.0, 1.0))))
+    w._collision.solver.velocity_iterations = int(rng.integers(4, 11))
+    return w
