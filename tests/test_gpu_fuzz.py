@@ -1,4 +1,4 @@
-"""The seeded random worlds of the fuzz tests on the GPU: four of them in one
+"""The seeded random worlds of the fuzz tests on the GPU: eight of them in one
 batch (uneven sizes, sensors, gravity volumes, every shape kind and motion
 type), 120 steps, each world's pairs, contacts, impulses, state, sleep flags
 and sensor overlaps equal to the oracle's for that world alone, bit for bit,
@@ -20,7 +20,7 @@ STATE = (('_position', 'position'), ('_orientation', 'orientation'),
 
 def test_random_worlds_batched_match_the_oracle():
     api = scenes.default_api()
-    worlds = [random_world(api, seed) for seed in range(4)]
+    worlds = [random_world(api, seed) for seed in range(8)]
     oracles = [pyoracle.OracleWorld.from_world(w) for w in worlds]
     b = WorldBatch(worlds, dts=[w.fixed_dt for w in worlds])
     for s in range(120):
