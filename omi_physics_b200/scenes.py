@@ -19,6 +19,7 @@ Workloads (sizes and distributions as the benchmark describes them):
   * ``ridge``        one mesh mixing a fine floor with triangles the grid sets aside
   * ``conveyor``     bodies riding a kinematic (sliding, turning) triangle-mesh platform
   * ``degenerate``   coincident centres, zero-depth contacts, sleep and wake-up by a pusher
+  * ``rods``         distance joints (world-anchored and body to body) and motors, no point joints
 """
 import math
 from types import SimpleNamespace
@@ -591,6 +592,49 @@ def degenerate(api=None, backend=None):
     return w, dict(dt=1.0 / 60.0, steps=300, name='degenerate')
 
 
+def rods(api=None, backend=None, seed: int = 6):
+    """Distance joints and motors without point joints (every joint a scalar
+    solve): pendulums hung from world anchors, ropes of spheres linked body to
+    body with off-centre anchors, one rod given an explicit length, motors on
+    some links, and boxes dropping through."""
+    api = api or default_api()
+    m, J = api.model, api.joints
+    w = _new_world(api, backend, fixed_dt=1.0 / 120.0)
+    rng = np.random.default_rng(seed)
+    mat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.4, restitution=0.1))
+    ground = w.add_shape(m.Shape.box((24.0, 1.0, 24.0)))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=ground, physicsMaterial=mat), position=(0.0, -0.5, 0.0))
+    bob = w.add_shape(m.Shape.sphere(0.3))
+    link = w.add_shape(m.Shape.box((0.3, 0.8, 0.3)))
+    for p in range(4):                                  # pendulums from world anchors
+        x = -6.0 + 4.0 * p
+        i = w.add_body(m.Motion(type=m.DYNAMIC, mass=1.5), m.Collider(shape=link, physicsMaterial=mat),
+                       position=(x + 1.5, 6.0, 0.0), orientation=_quat_axis_angle(np.array([0.0, 0.0, 1.0]), 0.6))
+        length = 1.8 if p == 3 else None                # an explicit rest length, else the separation
+        w.add_joint_constraint(J.DistanceConstraint(-1, i, (x, 7.0, 0.0), (0.0, 0.4, 0.0), length))
+        if p % 2 == 0:
+            w.add_joint_constraint(J.AngularMotor(i, tuple(float(v) for v in rng.normal(size=3)), 2.0,
+                                                  max_force=20.0))
+    for r in range(3):                                  # ropes of spheres, body to body
+        z = -4.0 + 4.0 * r
+        prev = -1
+        for k in range(6):
+            i = w.add_body(m.Motion(type=m.DYNAMIC, mass=0.7), m.Collider(shape=bob, physicsMaterial=mat),
+                           position=(0.8 * k, 8.0, z))
+            anchor_prev = (0.8 * k - 0.8, 8.0, z) if prev < 0 else (0.3, 0.0, 0.0)
+            w.add_joint_constraint(J.DistanceConstraint(prev, i, anchor_prev, (-0.3, 0.0, 0.0)))
+            prev = i
+    for k in range(12):                                 # boxes dropping through
+        sz = tuple(float(v) for v in rng.uniform(0.3, 0.7, 3))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=float(rng.uniform(0.5, 2.0))),
+                   m.Collider(shape=w.add_shape(m.Shape.box(sz)), physicsMaterial=mat),
+                   position=tuple(float(v) for v in rng.uniform((-6.0, 9.0, -5.0), (6.0, 12.0, 5.0))),
+                   orientation=_quat_axis_angle(rng.normal(size=3), float(rng.uniform(0, 2 * math.pi))))
+    _set_iterations(w, 8)
+    w.joint_iterations = 10
+    return w, dict(dt=1.0 / 120.0, steps=240, name='rods')
+
+
 #: the golden-fixture scenes (tests/golden/make_golden.py), by fixture name
 GOLDEN_SCENES = {
     'pyramid': lambda api=None, backend=None: pyramid(api, backend),
@@ -607,6 +651,7 @@ GOLDEN_SCENES = {
     'ridge': lambda api=None, backend=None: ridge(api, backend),
     'conveyor': lambda api=None, backend=None: conveyor(api, backend),
     'degenerate': lambda api=None, backend=None: degenerate(api, backend),
+    'rods': lambda api=None, backend=None: rods(api, backend),
 }
 
 

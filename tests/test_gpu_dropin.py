@@ -35,7 +35,8 @@ def _ref_api():
 
 @pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60),
                                          ('capsules', 30), ('zones', 60), ('terrain', 40),
-                                         ('conveyor', 40), ('degenerate', 140)])
+                                         ('conveyor', 40), ('degenerate', 140),
+                                         ('rods', 60)])
 def test_reference_world_steps_on_cuda_backend(scene, steps):
     from omi_physics_b200.backend import CudaBackend
     api = _ref_api()

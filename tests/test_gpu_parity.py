@@ -20,7 +20,7 @@ from util import assert_close, world_at_checkpoint
 pytestmark = pytest.mark.gpu
 
 EXACT = {'pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
-         'degenerate'}
+         'degenerate', 'rods'}
 
 
 @pytest.mark.parametrize('scene', SCENES)
@@ -88,6 +88,7 @@ def _island_sets(labels):
     ('terrain150', lambda: scenes.terrain(n=150, seed=2, cells=30, extent=8.0), 150),
     ('conveyor120', lambda: scenes.conveyor(n=120, seed=3, cells=20, extent=6.0), 150),
     ('degenerate', lambda: scenes.degenerate(), 300),
+    ('rods', lambda: scenes.rods(), 240),
 ])
 def test_trajectory_matches_oracle_every_step(name, builder, steps):
     w, meta = builder()

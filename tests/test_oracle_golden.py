@@ -14,7 +14,7 @@ import pyoracle
 from golden_util import SCENES, checkpoint, checkpoints, events_from_overlaps, load, pair_set
 
 EXACT = ('pyramid', 'debris', 'convex', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
-         'degenerate')
+         'degenerate', 'rods')
 
 
 def _close(a, b, exact):
