@@ -241,7 +241,9 @@ int omi_counts(OmiCtx *ctx, int32_t *pairs, int32_t *contacts);
 /* broadphase pairs of one world as global body indices (2*cap int32) */
 int omi_get_pairs(OmiCtx *ctx, int32_t world, int32_t *out, int32_t cap);
 /* contacts of one world (Contact records, collide.py:37-53) with the solver's
- * accumulated impulses (normal, tangent0, tangent1) */
+ * accumulated impulses (normal, tangent0, tangent1); the impulses are zero when
+ * the world's warm start is off, as the reference leaves its contacts then
+ * (solver.py:271-278) */
 int omi_get_contacts(OmiCtx *ctx, int32_t world, int32_t *a, int32_t *b, double *point,
                      double *normal, double *depth, double *impulse, int32_t cap);
 /* sleep-island label per body of one world (-1 = not in contact) */

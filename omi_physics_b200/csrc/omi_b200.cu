@@ -1381,7 +1381,12 @@ int omi_get_contacts(OmiCtx *ctx, int32_t w, int32_t *a, int32_t *b, double *pt,
     CK(cp(nrm, A.c_n + (size_t)c0 * 3, sizeof(double) * 3 * n));
     CK(cp(depth, A.c_depth + c0, sizeof(double) * n));
     CK(cp(imp, A.c_imp + (size_t)c0 * 3, sizeof(double) * 3 * n));
+    int flags = 0;
+    CK(cudaMemcpyAsync(&flags, A.w_flags + w, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    // the reference writes the solved impulses back to its contacts only with
+    // warm start on (solver.py:271-278); otherwise they stay zero
+    if (imp && !(flags & OMI_WF_WARM)) std::fill(imp, imp + (size_t)3 * n, 0.0);
     return n;
 }
 

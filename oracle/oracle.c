@@ -1276,12 +1276,14 @@ static int solve_contacts(OrWorld *w) {
             pos[b * 3 + c] += imbk * dL * normal[k * 3 + c];
         }
     }
-    for (int k = 0; k < K; k++) {
-        w->c_imp[k * 3] = nImp[k];
-        w->c_imp[k * 3 + 1] = tImp[k * 2];
-        w->c_imp[k * 3 + 2] = tImp[k * 2 + 1];
-    }
     if (w->warm_start) {                           /* solver.py:271-278 */
+        /* the impulses reach the contacts and the cache only with warm start on;
+         * otherwise the contacts keep zeros and the cache its last contents */
+        for (int k = 0; k < K; k++) {
+            w->c_imp[k * 3] = nImp[k];
+            w->c_imp[k * 3 + 1] = tImp[k * 2];
+            w->c_imp[k * 3 + 2] = tImp[k * 2 + 1];
+        }
         if (or_set_cache(w, K, w->c_a, w->c_b, w->c_pt, w->c_imp)) return -1;
     }
     free(invIw); free(rest); free(fric); free(nImp); free(tImp); free(rA); free(rB);

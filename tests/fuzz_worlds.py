@@ -74,3 +74,37 @@ def random_world(api, seed, n=40):
     w.add_gravity_volume(G.GravityVolume(m.Gravity(gravity=0.4, direction=(0.0, 0.0, 1.0))))
     w._collision.solver.velocity_iterations = int(rng.integers(4, 11))
     return w
+
+
+def switch_worlds(api):
+    """Small debris worlds, one per world-level switch the step branches on:
+    sleeping disabled, warm start off, default damping, no velocity
+    iterations, a tilted weaker world gravity, and bodies with no collider at
+    all (the world then has no collision stage). ``[(name, world), ...]``."""
+    from omi_physics_b200 import scenes
+    m = api.model
+    out = []
+    for k, name in enumerate(('no_sleep', 'no_warm_start', 'default_damping', 'no_iterations', 'tilted_gravity')):
+        w, _ = scenes.debris(api, n=60, seed=40 + k, extent=2.5, height=3.0, ground=12.0)
+        if name == 'no_sleep':
+            w.sleep_enabled = False
+        elif name == 'no_warm_start':
+            w._collision.solver.warm_start = False
+        elif name == 'default_damping':
+            w.default_linear_damping = 0.05
+            w.default_angular_damping = 0.1
+        elif name == 'no_iterations':
+            w._collision.solver.velocity_iterations = 0
+        else:
+            w.gravity = m.Gravity(gravity=5.0, direction=(0.3, -1.0, 0.2))
+        out.append((name, w))
+    w = api.PhysicsWorld(fixed_dt=1.0 / 120.0, default_linear_damping=0.02)
+    rng = np.random.default_rng(47)
+    for i in range(20):
+        w.add_body(m.Motion(type=m.DYNAMIC if i % 4 else m.KINEMATIC, mass=1.0,
+                            linearVelocity=tuple(float(v) for v in rng.normal(0.0, 1.0, 3)),
+                            angularVelocity=tuple(float(v) for v in rng.normal(0.0, 1.0, 3)),
+                            quadraticDrag=0.05 * (i % 3)),
+                   None, position=tuple(float(v) for v in rng.uniform(-3.0, 3.0, 3)))
+    out.append(('no_colliders', w))
+    return out

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from fuzz_worlds import random_world
+from fuzz_worlds import random_world, switch_worlds
 from omi_physics_b200 import WorldBatch, scenes
 
 pytestmark = pytest.mark.gpu
@@ -18,12 +18,10 @@ STATE = (('_position', 'position'), ('_orientation', 'orientation'),
          ('_awake', 'awake'), ('_sleep_timer', 'sleep_timer'))
 
 
-def test_random_worlds_batched_match_the_oracle():
-    api = scenes.default_api()
-    worlds = [random_world(api, seed) for seed in range(8)]
+def _batched_against_oracles(worlds, steps):
     oracles = [pyoracle.OracleWorld.from_world(w) for w in worlds]
     b = WorldBatch(worlds, dts=[w.fixed_dt for w in worlds])
-    for s in range(120):
+    for s in range(steps):
         b.step(1)
         b.sync_to_host()
         for i, (w, o) in enumerate(zip(worlds, oracles)):
@@ -38,3 +36,15 @@ def test_random_worlds_batched_match_the_oracle():
             for col, key in STATE:
                 assert np.array_equal(getattr(w, col)[:n], st[key]), tag + ' ' + key
             assert b.trigger_overlaps(i) == o.overlaps(), tag + ' overlaps'
+
+
+def test_random_worlds_batched_match_the_oracle():
+    api = scenes.default_api()
+    _batched_against_oracles([random_world(api, seed) for seed in range(8)], 120)
+
+
+def test_world_switches_batched_match_the_oracle():
+    """Sleeping disabled, warm start off (contacts report zero impulses, as the
+    reference leaves them), default damping, no velocity iterations, a tilted
+    weaker world gravity and a world without colliders, in one batch."""
+    _batched_against_oracles([w for _, w in switch_worlds(scenes.default_api())], 150)

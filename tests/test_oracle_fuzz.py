@@ -22,7 +22,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from fuzz_worlds import random_world
+from fuzz_worlds import random_world, switch_worlds
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, 'oracle', '_ref')
@@ -41,17 +41,20 @@ def _ref_api():
     return SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=model, gravity=gravity)
 
 
-@pytest.mark.parametrize('seed', range(4))
-def test_random_world_matches_the_reference(seed):
-    api = _ref_api()
-    w = random_world(api, seed)
+def _step_and_compare(w, steps, name):
     o = pyoracle.OracleWorld.from_world(w)
     dt = w.fixed_dt
     n = w.body_count
-    for s in range(120):
+    for s in range(steps):
         w.step(dt)
         o.step(dt)
-        tag = 'seed %d step %d' % (seed, s)
+        tag = '%s step %d' % (name, s)
+        if w._collision is None:
+            assert len(o.pairs()) == 0 and len(o.contacts()['a']) == 0, tag
+            st = o.state()
+            for col, key in STATE:
+                assert np.array_equal(getattr(w, col)[:n], st[key]), tag + ' ' + key
+            continue
         ref_pairs = sorted(tuple(map(int, p)) for p in w._collision.broadphase.pairs(w))
         assert ref_pairs == sorted(map(tuple, o.pairs().tolist())), tag + ' pairs'
         c = o.contacts()
@@ -67,3 +70,15 @@ def test_random_world_matches_the_reference(seed):
         for col, key in STATE:
             assert np.array_equal(getattr(w, col)[:n], st[key]), tag + ' ' + key
         assert set(w._collision.triggers.overlaps) == o.overlaps(), tag + ' overlaps'
+
+
+@pytest.mark.parametrize('seed', range(4))
+def test_random_world_matches_the_reference(seed):
+    _step_and_compare(random_world(_ref_api(), seed), 120, 'seed %d' % seed)
+
+
+def test_world_switches_match_the_reference():
+    """Sleeping disabled, warm start off, default damping, no velocity
+    iterations, a tilted weaker world gravity, and a world without colliders."""
+    for name, w in switch_worlds(_ref_api()):
+        _step_and_compare(w, 150, name)
