@@ -133,9 +133,15 @@ class CudaBackend:
         from .batch import WorldBatch
         sig = static_signature(world)
         if self._batch is None or sig != self._sig:
+            # a topology change (a body or table added) reloads the arena; the
+            # reference's solver keeps its warm-start cache across it, keyed by
+            # body pairs whose indices do not change (solver.py:91, 272-278)
+            carry = self._batch.cache(0) if self._batch is not None else None
             ctx = self._batch.ctx if self._batch is not None else None
             self._batch = WorldBatch([world], device=self.device, dts=[dt], ctx=ctx)
             self._sig = sig
+            if carry is not None and len(carry['a']):
+                self._batch.set_cache(0, carry['a'], carry['b'], carry['point'], carry['impulse'])
         else:
             self._batch.upload_state(0)
         self._batch.dts = [dt]

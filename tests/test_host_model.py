@@ -92,3 +92,46 @@ def test_pack_with_empty_and_static_only_worlds():
     assert p.scene.n_worlds == 4 and p.scene.n_bodies == 1 + deg.body_count
     p0 = pack_worlds([empty])
     assert p0.scene.n_bodies == 0 and list(p0.arrays['w_body_off']) == [0, 0]
+
+
+def test_reload_after_a_topology_change_keeps_the_warm_start_cache(monkeypatch):
+    """Adding a body changes the world's static signature and reloads the
+    arena; the warm-start cache of the last step must carry over, as the
+    reference's solver keeps it (solver.py:91, 272-278). Host logic only: a
+    stand-in batch records the calls."""
+    import omi_physics_b200.batch as batch_mod
+    made = []
+
+    class FakeBatch:
+        def __init__(self, worlds, device=0, dts=None, ctx=None):
+            self.ctx, self.dts, self.set = ctx or object(), dts, None
+            self.entries = dict(a=np.array([1], np.int32), b=np.array([2], np.int32),
+                                point=np.zeros((1, 3)), impulse=np.array([[3.0, 0.5, -0.5]]))
+            made.append(self)
+
+        def cache(self, i):
+            return self.entries
+
+        def set_cache(self, i, a, b, point, impulse):
+            self.set = (a, b, point, impulse)
+
+        def upload_state(self, i):
+            pass
+
+        def refresh_params(self):
+            pass
+
+    monkeypatch.setattr(batch_mod, 'WorldBatch', FakeBatch)
+    w, meta = scenes.pyramid(levels=3)
+    be = CudaBackend()
+    be.attach(w)
+    be._ensure_loaded(w, meta['dt'])
+    assert len(made) == 1 and made[0].set is None        # a first load has nothing to carry
+    be._ensure_loaded(w, meta['dt'])
+    assert len(made) == 1                                # same topology: no reload
+    m = scenes.default_api().model
+    w.add_body(m.Motion(type=m.DYNAMIC), m.Collider(shape=1), position=(0.0, 9.0, 0.0))
+    be._ensure_loaded(w, meta['dt'])
+    assert len(made) == 2 and made[1].ctx is made[0].ctx  # reloaded into the same context
+    a, b, point, impulse = made[1].set
+    assert list(a) == [1] and list(b) == [2] and np.array_equal(impulse, [[3.0, 0.5, -0.5]])
