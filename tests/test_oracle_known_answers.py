@@ -1,0 +1,203 @@
+"""The reference's own known-answer tests for this path, restated against the
+oracle: the same inputs and the same expectations and tolerances as
+tests/test_physics_integrate.py (closed-form free fall, gravity factor,
+constant velocity, static bodies, damping and drag terminal velocities),
+tests/test_collide_primitives.py (sphere and box contacts) and
+tests/test_solver.py (rest, bounce, a resting stack, friction on an incline,
+determinism) of the reference. Worlds are built with this package's world
+mirror, whose columns equal the reference's; the oracle steps them.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import pyoracle
+from omi_physics_b200 import scenes
+
+API = scenes.default_api()
+M = API.model
+
+
+def _run(world, dt, steps):
+    o = pyoracle.OracleWorld.from_world(world)
+    for _ in range(steps):
+        o.step(dt)
+    return o.state()
+
+
+# -- integration (test_physics_integrate.py) ------------------------------------
+def test_freefall_matches_symplectic_closed_form():
+    g, dt, n = 9.81, 1.0 / 240.0, 240
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=g, direction=(0, -1, 0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC), position=(0, 0, 0))
+    st = _run(w, dt, n)
+    assert st['position'][i][1] == pytest.approx(-0.5 * g * dt * dt * n * (n + 1), rel=1e-9)
+
+
+def test_freefall_approaches_analytic_as_dt_shrinks():
+    g, dt = 9.81, 1.0 / 2000.0
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=g, direction=(0, -1, 0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC), position=(0, 0, 0))
+    st = _run(w, dt, int(1.0 / dt))
+    assert st['position'][i][1] == pytest.approx(-0.5 * g, rel=2e-3)
+
+
+def test_gravity_factor_scales_fall():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=10.0, direction=(0, -1, 0)))
+    full = w.add_body(M.Motion(type=M.DYNAMIC, gravityFactor=1.0), position=(0, 0, 0))
+    half = w.add_body(M.Motion(type=M.DYNAMIC, gravityFactor=0.5), position=(0, 0, 0))
+    st = _run(w, 1.0 / 240.0, 240)
+    assert st['position'][half][1] == pytest.approx(0.5 * st['position'][full][1], rel=1e-9)
+
+
+def test_zero_net_force_keeps_constant_velocity():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=0.0))
+    i = w.add_body(M.Motion(type=M.DYNAMIC, linearVelocity=(2.0, 0.0, -3.0)), position=(0, 0, 0))
+    st = _run(w, 1.0 / 120.0, 120)
+    assert np.allclose(st['linear_velocity'][i], (2.0, 0.0, -3.0))
+    assert np.allclose(st['position'][i], (2.0, 0.0, -3.0), atol=1e-9)
+
+
+def test_static_body_never_moves():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81))
+    i = w.add_body(M.Motion(type=M.STATIC), position=(1, 2, 3))
+    assert np.allclose(_run(w, 1 / 60, 100)['position'][i], (1, 2, 3))
+
+
+def test_linear_damping_terminal_velocity():
+    g, c = 9.81, 2.0
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=g, direction=(0, -1, 0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC, linearDamping=c), position=(0, 0, 0))
+    st = _run(w, 1.0 / 240.0, 4000)
+    assert abs(st['linear_velocity'][i][1]) == pytest.approx(g / c, rel=1e-2)
+
+
+def test_quadratic_drag_terminal_velocity():
+    g, k = 9.81, 0.5
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=g, direction=(0, -1, 0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC, quadraticDrag=k), position=(0, 0, 0))
+    st = _run(w, 1.0 / 240.0, 6000)
+    assert abs(st['linear_velocity'][i][1]) == pytest.approx(math.sqrt(g / k), rel=1e-2)
+
+
+# -- narrowphase primitives (test_collide_primitives.py) -------------------------
+def _call(fn, *args, n=4):
+    import ctypes as C
+    ptr = C.POINTER(C.c_double)
+    nrm, pts, dep = np.zeros(3), np.zeros(3 * n), np.zeros(n)
+    conv = [C.c_double(a) if isinstance(a, float) else np.ascontiguousarray(a, 'd').ctypes.data_as(ptr)
+            for a in args]
+    k = fn(*conv, nrm.ctypes.data_as(ptr), pts.ctypes.data_as(ptr), dep.ctypes.data_as(ptr))
+    return k, nrm, pts[:3 * k].reshape(-1, 3), dep[:k]
+
+
+def _quat_matrix(q):
+    R = np.zeros(9)
+    import ctypes as C
+    ptr = C.POINTER(C.c_double)
+    q = np.ascontiguousarray(q, 'd')
+    pyoracle.lib().or_quat_to_matrix(q.ctypes.data_as(ptr), R.ctypes.data_as(ptr))
+    return R
+
+
+def test_sphere_sphere_hit_and_miss():
+    L = pyoracle.lib()
+    k, n, p, d = _call(L.or_sphere_sphere, (0, 0, 0), 1.0, (1.5, 0, 0), 1.0)
+    assert k == 1 and d[0] == pytest.approx(0.5) and np.allclose(n, (1, 0, 0)) and p[0][0] == pytest.approx(0.75)
+    assert _call(L.or_sphere_sphere, (0, 0, 0), 1.0, (3, 0, 0), 1.0)[0] == 0
+
+
+def test_sphere_box_face_miss_and_inside():
+    L = pyoracle.lib()
+    I3 = np.eye(3).reshape(9)
+    k, n, _, d = _call(L.or_sphere_box, (0, 1.3, 0), 0.5, (0, 0, 0), I3, (1, 1, 1))
+    assert k == 1 and d[0] == pytest.approx(0.2, abs=1e-9) and np.allclose(n, (0, -1, 0), atol=1e-9)
+    assert _call(L.or_sphere_box, (0, 2.0, 0), 0.5, (0, 0, 0), I3, (1, 1, 1))[0] == 0
+    k, n, _, _ = _call(L.or_sphere_box, (0.1, 0.0, 0.0), 0.2, (0, 0, 0), I3, (1, 0.3, 1))
+    assert k == 1 and abs(n[1]) == pytest.approx(1.0)
+
+
+def test_box_box_cases():
+    L = pyoracle.lib()
+    I3 = np.eye(3).reshape(9)
+    k, n, _, d = _call(L.or_box_box, (0, 0, 0), I3, (1, 1, 1), (1.5, 0, 0), I3, (1, 1, 1))
+    assert k > 0 and np.allclose(np.abs(n), (1, 0, 0), atol=1e-6) and max(d) == pytest.approx(0.5, abs=1e-6)
+    k, n, _, _ = _call(L.or_box_box, (0, 0, 0), I3, (5, 0.5, 5), (0, 0.99, 0), I3, (0.5, 0.5, 0.5))
+    assert k >= 3 and np.allclose(np.abs(n), (0, 1, 0), atol=1e-6)
+    assert _call(L.or_box_box, (0, 0, 0), I3, (1, 1, 1), (3, 0, 0), I3, (1, 1, 1))[0] == 0
+    s = math.sin(math.pi / 8)
+    R = _quat_matrix((0.0, s, 0.0, math.cos(math.pi / 8)))
+    assert _call(L.or_box_box, (0, 0, 0), I3, (1, 1, 1), (2.2, 0, 0), R, (1, 1, 1))[0] > 0
+
+
+# -- solver (test_solver.py) ----------------------------------------------------------
+DT = 1.0 / 120.0
+
+
+def _ground(gravity_dir=(0, -1, 0), g=9.81, restitution=0.0, friction=0.6):
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=g, direction=gravity_dir), sleep_enabled=False)
+    mat = w.add_material(M.Material(staticFriction=friction, dynamicFriction=friction, restitution=restitution))
+    w.add_body(M.Motion(type=M.STATIC), M.Collider(shape=w.add_shape(M.Shape.box((40, 1, 40))), physicsMaterial=mat),
+               position=(0, -0.5, 0))
+    return w, mat
+
+
+def _sphere(w, mat, height, radius=0.5):
+    return w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0),
+                      M.Collider(shape=w.add_shape(M.Shape.sphere(radius)), physicsMaterial=mat),
+                      position=(0, height, 0))
+
+
+def test_no_restitution_comes_to_rest():
+    w, mat = _ground(restitution=0.0)
+    i = _sphere(w, mat, 3.0)
+    st = _run(w, DT, 600)
+    assert st['position'][i][1] == pytest.approx(0.5, abs=0.05) and abs(st['linear_velocity'][i][1]) < 0.2
+
+
+def test_full_restitution_bounces_back_high():
+    w, mat = _ground(restitution=1.0)
+    i = _sphere(w, mat, 3.0)
+    o = pyoracle.OracleWorld.from_world(w)
+    bounced, peak = False, 0.0
+    for _ in range(400):
+        o.step(DT)
+        y = o.state()['position'][i][1]
+        if y < 0.6:
+            bounced = True
+        elif bounced:
+            peak = max(peak, y)
+    assert bounced and peak > 0.75 * 3.0
+
+
+def test_resting_stack_is_stable():
+    w, mat = _ground(restitution=0.0)
+    shape = w.add_shape(M.Shape.box((1, 1, 1)))
+    bodies = [w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), M.Collider(shape=shape, physicsMaterial=mat),
+                         position=(0, 0.5 + k * 1.001, 0)) for k in range(5)]
+    p = _run(w, DT, 600)['position']
+    assert list(np.argsort([p[b][1] for b in bodies])) == [0, 1, 2, 3, 4]
+    for k, b in enumerate(bodies):
+        assert p[b][1] == pytest.approx(0.5 + k, abs=0.2) and abs(p[b][0]) < 0.5 and abs(p[b][2]) < 0.5
+
+
+@pytest.mark.parametrize('angle_deg,friction,should_slide', [(40, 0.5, True), (10, 0.5, False)])
+def test_incline_slides_iff_tan_exceeds_friction(angle_deg, friction, should_slide):
+    t = math.radians(angle_deg)
+    w, mat = _ground(gravity_dir=(math.sin(t), -math.cos(t), 0.0), friction=friction)
+    i = w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0),
+                   M.Collider(shape=w.add_shape(M.Shape.box((1, 1, 1))), physicsMaterial=mat), position=(0, 0.5, 0))
+    slid = _run(w, DT, 400)['position'][i][0]
+    assert (slid > 0.5) if should_slide else (slid < 0.05)
+
+
+def test_determinism_bit_identical_runs():
+    def run():
+        w, mat = _ground(restitution=0.3)
+        shape = w.add_shape(M.Shape.box((1, 1, 1)))
+        for k in range(6):
+            w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), M.Collider(shape=shape, physicsMaterial=mat),
+                       position=(0.3 * k, 1.0 + 1.2 * k, 0.1 * k))
+        return _run(w, DT, 200)['position']
+    assert np.array_equal(run(), run())
