@@ -108,3 +108,41 @@ def switch_worlds(api):
                    None, position=tuple(float(v) for v in rng.uniform(-3.0, 3.0, 3)))
     out.append(('no_colliders', w))
     return out
+
+
+def joint_world(api, seed):
+    """Boxes and spheres tied by random joints: point joints between two bodies
+    and to the world, distance joints, angular motors (``api`` also needs
+    ``joints``)."""
+    m, J = api.model, api.joints
+    rng = np.random.default_rng(seed)
+    w = api.PhysicsWorld(fixed_dt=1.0 / 240.0)
+    mat = w.add_material(m.Material(staticFriction=0.5, dynamicFriction=0.4))
+    w.add_body(m.Motion(type=m.STATIC), m.Collider(shape=w.add_shape(m.Shape.box((20.0, 1.0, 20.0))),
+                                                   physicsMaterial=mat), position=(0.0, -0.5, 0.0))
+    first = w.body_count
+    n = 16
+    pos = rng.uniform((-3.0, 1.0, -3.0), (3.0, 5.0, 3.0), size=(n, 3))
+    for i in range(n):
+        shape = (m.Shape.box(tuple(float(v) for v in rng.uniform(0.3, 0.8, 3))) if i % 2 else
+                 m.Shape.sphere(float(rng.uniform(0.2, 0.4))))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=float(rng.uniform(0.5, 3.0))),
+                   m.Collider(shape=w.add_shape(shape), physicsMaterial=mat),
+                   position=tuple(float(v) for v in pos[i]), orientation=_quat(rng))
+    for k in range(10):
+        a, b = (int(x) + first for x in rng.choice(n, size=2, replace=False))
+        if k < 6:
+            mid = tuple(float(v) for v in 0.5 * (pos[a - first] + pos[b - first]))
+            w.add_joint_constraint(J.PointConstraint(a, b, mid))
+        else:
+            w.add_joint_constraint(J.DistanceConstraint(a, b, tuple(float(v) for v in rng.uniform(-0.2, 0.2, 3)),
+                                                        tuple(float(v) for v in rng.uniform(-0.2, 0.2, 3))))
+    for k in range(3):
+        i = first + k
+        anchor = tuple(float(v) for v in pos[k] + (0.0, 0.6, 0.0))
+        w.add_joint_constraint(J.PointConstraint(-1, i, anchor) if k % 2 == 0 else J.PointConstraint(i, -1, anchor))
+    for k in range(3):
+        w.add_joint_constraint(J.AngularMotor(first + 5 + k, tuple(float(v) for v in rng.normal(size=3)), 1.5,
+                                              max_force=float(rng.choice([5.0, 50.0]))))
+    w.joint_iterations = int(rng.integers(6, 13))
+    return w
