@@ -2,9 +2,11 @@
 oracle: the same inputs and the same expectations and tolerances as
 tests/test_physics_integrate.py (closed-form free fall, gravity factor,
 constant velocity, static bodies, damping and drag terminal velocities),
-tests/test_collide_primitives.py (sphere and box contacts) and
+tests/test_collide_primitives.py (sphere and box contacts),
 tests/test_solver.py (rest, bounce, a resting stack, friction on an incline,
-determinism) of the reference. Worlds are built with this package's world
+determinism), tests/test_gravity.py (point pull, priority replace, stop,
+region bounds) and tests/test_triggers.py (enter / stay / exit, no impulse)
+of the reference. Worlds are built with this package's world
 mirror, whose columns equal the reference's; the oracle steps them.
 """
 import math
@@ -201,3 +203,83 @@ def test_determinism_bit_identical_runs():
                        position=(0.3 * k, 1.0 + 1.2 * k, 0.1 * k))
         return _run(w, DT, 200)['position']
     assert np.array_equal(run(), run())
+
+
+# -- gravity volumes (test_gravity.py) ------------------------------------------------
+G = API.gravity
+
+
+def test_point_gravity_pulls_body_toward_center():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=0.0))
+    w.add_gravity_volume(G.GravityVolume(M.Gravity(type=M.POINT, gravity=9.81, center=(0, 0, 0)),
+                                         G.SphereRegion((0, 0, 0), 100.0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC), position=(10, 0, 0))
+    st = _run(w, DT, 120)
+    assert st['position'][i][0] < 10.0 and st['linear_velocity'][i][0] < 0
+
+
+def test_higher_priority_replace_overrides_global():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81, direction=(0, -1, 0)))
+    w.add_gravity_volume(G.GravityVolume(M.Gravity(type=M.DIRECTIONAL, gravity=9.81, direction=(0, 1, 0),
+                                                   priority=5, replace=True), G.SphereRegion((0, 0, 0), 100.0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC), position=(0, 0, 0))
+    assert _run(w, DT, 120)['linear_velocity'][i][1] > 0
+
+
+def test_stop_zone_halts_gravity_accumulation():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81, direction=(0, -1, 0)))
+    w.add_gravity_volume(G.GravityVolume(M.Gravity(gravity=0.0, priority=5, stop=True), G.SphereRegion((0, 0, 0), 100.0)))
+    i = w.add_body(M.Motion(type=M.DYNAMIC), position=(0, 0, 0))
+    assert np.allclose(_run(w, DT, 120)['linear_velocity'][i], 0.0)
+
+
+def test_region_bounds_limit_effect():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=0.0))
+    w.add_gravity_volume(G.GravityVolume(M.Gravity(type=M.DIRECTIONAL, gravity=9.81, direction=(0, -1, 0)),
+                                         G.SphereRegion((0, 0, 0), 1.0)))
+    inside = w.add_body(M.Motion(type=M.DYNAMIC), position=(0, 0, 0))
+    outside = w.add_body(M.Motion(type=M.DYNAMIC), position=(50, 0, 0))
+    st = _run(w, DT, 120)
+    assert st['linear_velocity'][inside][1] < -1.0 and np.allclose(st['linear_velocity'][outside], 0.0)
+
+
+# -- sensors (test_triggers.py) -------------------------------------------------------
+def _zone_world(zone_size, ball_radius, velocity, position):
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=0.0))
+    w.add_body(M.Motion(type=M.STATIC), trigger=M.Trigger(shape=w.add_shape(M.Shape.box(zone_size))),
+               position=(0, 0, 0))
+    ball = w.add_body(M.Motion(type=M.DYNAMIC, linearVelocity=velocity),
+                      M.Collider(shape=w.add_shape(M.Shape.sphere(ball_radius))), position=position)
+    return w, ball
+
+
+def _events(w, steps, dt=1.0 / 60.0):
+    """Enter / stay / exit kinds per step, formed from the oracle's overlaps
+    as the reference forms them (triggers.py:36-42)."""
+    o = pyoracle.OracleWorld.from_world(w)
+    prev, kinds = set(), []
+    for _ in range(steps):
+        o.step(dt)
+        new = o.overlaps()
+        kinds += ['enter'] * len(new - prev) + ['stay'] * len(new & prev) + ['exit'] * len(prev - new)
+        prev = new
+    return kinds, o.state()
+
+
+def test_body_passing_through_trigger_fires_enter_and_exit():
+    w, _ = _zone_world((1, 1, 1), 0.2, (2.0, 0, 0), (-3.0, 0, 0))
+    kinds, _ = _events(w, 120)
+    assert 'enter' in kinds and 'exit' in kinds and kinds.index('enter') < kinds.index('exit')
+
+
+def test_trigger_does_not_perturb_trajectory():
+    w, ball = _zone_world((1, 1, 1), 0.3, (2.0, 0, 0), (-3.0, 0, 0))
+    _, st = _events(w, 120)
+    assert np.allclose(st['linear_velocity'][ball], (2.0, 0, 0))
+    assert st['position'][ball][1] == pytest.approx(0.0, abs=1e-9) and st['position'][ball][2] == pytest.approx(0.0, abs=1e-9)
+
+
+def test_stay_events_while_inside():
+    w, _ = _zone_world((2, 2, 2), 0.2, (0.0, 0.0, 0.0), (0, 0, 0))
+    kinds, _ = _events(w, 5)
+    assert kinds[0] == 'enter' and kinds.count('stay') >= 3
