@@ -5,8 +5,9 @@ constant velocity, static bodies, damping and drag terminal velocities),
 tests/test_collide_primitives.py (sphere and box contacts),
 tests/test_solver.py (rest, bounce, a resting stack, friction on an incline,
 determinism), tests/test_gravity.py (point pull, priority replace, stop,
-region bounds) and tests/test_triggers.py (enter / stay / exit, no impulse)
-of the reference. Worlds are built with this package's world
+region bounds), tests/test_triggers.py (enter / stay / exit, no impulse)
+and tests/test_joints.py (rods, pins, motors and their force limit) of the
+reference. Worlds are built with this package's world
 mirror, whose columns equal the reference's; the oracle steps them.
 """
 import math
@@ -283,3 +284,59 @@ def test_stay_events_while_inside():
     w, _ = _zone_world((2, 2, 2), 0.2, (0.0, 0.0, 0.0), (0, 0, 0))
     kinds, _ = _events(w, 5)
     assert kinds[0] == 'enter' and kinds.count('stay') >= 3
+
+
+# -- joints (test_joints.py) ----------------------------------------------------------
+JN = API.joints
+
+
+def test_distance_constraint_keeps_pendulum_arm_length():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81, direction=(0, -1, 0)), sleep_enabled=False)
+    pivot = np.array([0.0, 5.0, 0.0])
+    bob = w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), position=(2.0, 5.0, 0.0))
+    w.add_joint_constraint(JN.DistanceConstraint(-1, bob, tuple(pivot), (0, 0, 0), 2.0))
+    o = pyoracle.OracleWorld.from_world(w)
+    lengths, lowest = [], 5.0
+    for _ in range(600):
+        o.step(DT)
+        p = o.state()['position'][bob]
+        lengths.append(np.linalg.norm(p - pivot))
+        lowest = min(lowest, p[1])
+    assert max(lengths) == pytest.approx(2.0, abs=0.05) and min(lengths) == pytest.approx(2.0, abs=0.05)
+    assert lowest < 3.3
+
+
+def test_point_constraint_pins_extended_body_at_offset():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81, direction=(0, -1, 0)), sleep_enabled=False)
+    bar = w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), M.Collider(shape=w.add_shape(M.Shape.box((2, 0.4, 0.4)))),
+                     position=(1.0, 5.0, 0.0))
+    w.add_joint_constraint(JN.PointConstraint(-1, bar, (0.0, 5.0, 0.0)))
+    st = _run(w, DT, 400)
+    R = _quat_matrix(st['orientation'][bar]).reshape(3, 3)
+    assert np.allclose(st['position'][bar] + R @ np.array([-1.0, 0.0, 0.0]), (0.0, 5.0, 0.0), atol=0.05)
+    assert st['position'][bar][1] < 4.9
+
+
+def test_distance_constraint_holds_between_two_bodies():
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=9.81, direction=(0, -1, 0)), sleep_enabled=False)
+    anchor = w.add_body(M.Motion(type=M.STATIC), position=(0, 5, 0))
+    hanging = w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), position=(0, 2, 0))
+    w.add_joint_constraint(JN.DistanceConstraint(anchor, hanging, (0, 0, 0), (0, 0, 0), 3.0))
+    p = _run(w, DT, 600)['position']
+    assert np.linalg.norm(p[hanging] - p[anchor]) == pytest.approx(3.0, abs=0.05)
+
+
+def _spinner(target, max_force, steps):
+    w = API.PhysicsWorld(gravity=M.Gravity(gravity=0.0), sleep_enabled=False)
+    i = w.add_body(M.Motion(type=M.DYNAMIC, mass=1.0), M.Collider(shape=w.add_shape(M.Shape.box((1, 1, 1)))),
+                   position=(0, 0, 0))
+    w.add_joint_constraint(JN.AngularMotor(i, (0, 1, 0), target, max_force=max_force))
+    return _run(w, DT, steps)['angular_velocity'][i]
+
+
+def test_angular_motor_reaches_velocity_target():
+    assert _spinner(3.0, 50.0, 240)[1] == pytest.approx(3.0, abs=0.1)
+
+
+def test_motor_force_limit_caps_spin_up():
+    assert _spinner(100.0, 0.5, 1)[1] < 5.0
