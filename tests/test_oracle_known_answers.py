@@ -6,8 +6,8 @@ tests/test_collide_primitives.py (sphere and box contacts),
 tests/test_solver.py (rest, bounce, a resting stack, friction on an incline,
 determinism), tests/test_gravity.py (point pull, priority replace, stop,
 region bounds), tests/test_triggers.py (enter / stay / exit, no impulse)
-and tests/test_joints.py (rods, pins, motors and their force limit) of the
-reference. Worlds are built with this package's world
+tests/test_joints.py (rods, pins, motors and their force limit) and
+tests/test_broadphase.py (pairs equal to brute force) of the reference. Worlds are built with this package's world
 mirror, whose columns equal the reference's; the oracle steps them.
 """
 import math
@@ -340,3 +340,43 @@ def test_angular_motor_reaches_velocity_target():
 
 def test_motor_force_limit_caps_spin_up():
     assert _spinner(100.0, 0.5, 1)[1] < 5.0
+
+
+# -- broadphase (test_broadphase.py) ----------------------------------------------------
+@pytest.mark.parametrize('seed,spread', [(1, 3.0), (2, 6.0), (3, 1.5)])
+def test_sweep_pairs_match_brute_force(seed, spread):
+    """The oracle's sweep-and-prune pairs equal the O(N^2) overlap set over the
+    same AABBs: boxes (>=, closed intervals) overlapping on all three axes, at
+    least one dynamic body, interacting filters (broadphase.py:300-316)."""
+    rng = np.random.default_rng(seed)
+    w = API.PhysicsWorld()
+    f_a = w.add_filter(M.CollisionFilter(collisionSystems=('a',), notCollideWithSystems=('b',)))
+    f_b = w.add_filter(M.CollisionFilter(collisionSystems=('b',)))
+    filters = (-1, f_a, f_b)
+    for k in range(150):
+        kind = (M.STATIC, M.KINEMATIC, M.DYNAMIC, M.DYNAMIC)[k % 4]
+        shape = w.add_shape(M.Shape.sphere(0.5) if k % 3 else M.Shape.box(tuple(float(v) for v in rng.uniform(0.4, 1.2, 3))))
+        w.add_body(M.Motion(type=kind), M.Collider(shape=shape, collisionFilter=filters[k % 3]),
+                   position=tuple(float(v) for v in rng.uniform(-spread, spread, 3)), orientation=_quat_any(rng))
+    o = pyoracle.OracleWorld.from_world(w)
+    o.refit()
+    got = {tuple(map(int, p)) for p in o.broadphase()}
+    st = o.state()
+    lo, hi = st['aabb_min'], st['aabb_max']
+    mt = np.asarray(w._motion_type[:w.body_count])
+    fl = np.asarray(w._collider_filter[:w.body_count])
+    brute = set()
+    for i in range(w.body_count):
+        for j in range(i + 1, w.body_count):
+            if mt[i] != 2 and mt[j] != 2:
+                continue
+            if not (np.all(hi[i] >= lo[j]) and np.all(hi[j] >= lo[i])):
+                continue
+            if w.filter_for(fl[i]).collides_with(w.filter_for(fl[j])):
+                brute.add((i, j))
+    assert got == brute and len(brute) > 0
+
+
+def _quat_any(rng):
+    q = rng.normal(size=4)
+    return tuple(float(v) for v in q / np.linalg.norm(q))
