@@ -1,14 +1,15 @@
 """The reference's own known-answer tests for this path, restated against the
-oracle: the same inputs and the same expectations and tolerances as
-tests/test_physics_integrate.py (closed-form free fall, gravity factor,
-constant velocity, static bodies, damping and drag terminal velocities),
-tests/test_collide_primitives.py (sphere and box contacts),
+oracle with the same inputs, expectations and tolerances: from the
+reference's tests/test_physics_integrate.py (closed-form free fall, gravity
+factor, constant velocity, static bodies, damping and drag terminal
+velocities), tests/test_collide_primitives.py (sphere and box contacts),
 tests/test_solver.py (rest, bounce, a resting stack, friction on an incline,
 determinism), tests/test_gravity.py (point pull, priority replace, stop,
-region bounds), tests/test_triggers.py (enter / stay / exit, no impulse)
+region bounds), tests/test_triggers.py (enter / stay / exit, no impulse),
 tests/test_joints.py (rods, pins, motors and their force limit) and
-tests/test_broadphase.py (pairs equal to brute force) of the reference. Worlds are built with this package's world
-mirror, whose columns equal the reference's; the oracle steps them.
+tests/test_broadphase.py (pairs equal to brute force). Worlds are built with
+this package's world mirror, whose columns equal the reference's; the oracle
+steps them.
 """
 import math
 
