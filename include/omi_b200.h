@@ -28,6 +28,9 @@ extern "C" {
 #define OMI_E_STATE (-4)        /* call out of order (e.g. step before load) */
 #define OMI_E_TIMEOUT (-5)      /* a bounded device wait gave up */
 #define OMI_E_OOM (-6)          /* arena would exceed the context's HBM budget */
+#define OMI_E_LIMIT (-7)        /* the step completed, but some convex pairs outgrew the bounded EPA
+                                   polytope and their contacts were dropped (the reference's EPA,
+                                   gjk.py:120-217, keeps an unbounded face list) */
 
 /* Shape types, combine modes, joint types: same meaning as the reference's
  * model.Shape.type, model.combine modes (model.py:231-243) and joints.py. */
@@ -149,6 +152,21 @@ int omi_set_stream(OmiCtx *ctx, void *stream);
 /* Refuse arenas whose device footprint exceeds this many bytes (0 = none). */
 int omi_set_budget(OmiCtx *ctx, int64_t bytes);
 int64_t omi_device_bytes(OmiCtx *ctx);
+/* Lower the device's safety bounds, for tests and diagnostics (no counterpart
+ * in the reference, whose sweep never waits and whose EPA is unbounded):
+ * spin_limit = polls before a contact-sweep wait gives up (the step then
+ * fails with OMI_E_TIMEOUT), epa_faces = EPA polytope faces (4..512; a pair
+ * past it is dropped and the step reports OMI_E_LIMIT), stall_run = a
+ * world-local run index whose sweep entries are made to wait forever in
+ * every world (-1 = none), so a test can make a wait run out. 0 restores a
+ * default. Applies to the next step (the step graph is re-captured). */
+int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t stall_run);
+/* Check a scene the way omi_load does, on the host only (no device, no
+ * context): every index a kernel would follow is range-checked. Returns 0 or
+ * the status omi_load would return, with the message in err (err_cap bytes,
+ * may be NULL). omi_load refuses a scene that fails this check and keeps the
+ * arena it had loaded before. */
+int omi_validate_scene(const OmiScene *scene, char *err, int32_t err_cap);
 
 /* ---- scene ------------------------------------------------------------ */
 /* Upload a whole arena (replaces any previous one). Builds what the reference
@@ -294,14 +312,20 @@ int omi_capsule_triangles_device(OmiCtx *ctx, int32_t q, const double *caps, con
  * counterpart in the reference.) It is for callers that must not allocate
  * device memory: an engine whose memory is fully reserved up front by its own
  * pool, a real-time loop where cudaMalloc/cudaFree would synchronise the
- * device mid-frame, or code running where the allocator is unavailable. It
- * computes the same pair list, in the same order, as omi_broadphase
- * (broadphase.py:243-294) for AABBs the caller already holds on the device.
+ * device mid-frame, or code running where the allocator is unavailable.
+ * Contract: bodies are sorted by aabb_min.x (stable: ties by index, NaN
+ * last); for each body in that order, every later body whose min.x is at
+ * most its max.x and whose y and z ranges overlap (>=) forms a pair, kept
+ * when at least one of the two is dynamic (motion_type 2) and the filter
+ * matrix lets their rows collide. Pairs are written as (min, max) body
+ * indices, ordered by the first body's sorted position, then the second's.
+ * This is the same list, in the same order, as omi_broadphase gives.
  *
  * All array arguments are DEVICE pointers owned by the caller: aabb_min and
  * aabb_max (n*3 doubles), motion_type (n ints), optionally filter_row (n ints,
- * rows of the filter_rows x filter_rows collides_with matrix filter_matrix;
- * both NULL when every pair collides), the output pairs (2*pair_cap ints,
+ * rows of the filter_rows x filter_rows collides_with matrix filter_matrix,
+ * each entry in [0, filter_rows): the kernel does not check them; both NULL
+ * when every pair collides), the output pairs (2*pair_cap ints,
  * (min, max) body indices) and n_pairs (1 int: the full pair count, which may
  * exceed pair_cap; pairs past pair_cap are not written). Work is enqueued on
  * `stream` (a cudaStream_t, NULL = default) and the call returns without

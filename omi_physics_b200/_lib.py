@@ -16,7 +16,8 @@ I = C.POINTER(C.c_int32)
 I64 = C.POINTER(C.c_int64)
 U8 = C.POINTER(C.c_uint8)
 
-OMI_E_CUDA, OMI_E_ARG, OMI_E_UNSUPPORTED, OMI_E_STATE, OMI_E_TIMEOUT, OMI_E_OOM = -1, -2, -3, -4, -5, -6
+OMI_E_CUDA, OMI_E_ARG, OMI_E_UNSUPPORTED, OMI_E_STATE, OMI_E_TIMEOUT, OMI_E_OOM, OMI_E_LIMIT = (
+    -1, -2, -3, -4, -5, -6, -7)
 WF_SLEEP, WF_WARM, WF_COLLISION, WF_ACTIVE = 1, 2, 4, 8
 
 
@@ -34,6 +35,16 @@ class UnsupportedFeature(OmiError):
 
 class OutOfBudget(OmiError):
     """The arena would exceed the context's device-memory budget."""
+
+
+class SweepTimeout(OmiError):
+    """A bounded wait of the contact sweep ran out: the step did not complete
+    (the worlds' state is partly advanced; restore it before stepping on)."""
+
+
+class EpaLimit(OmiError):
+    """The step completed, but some convex pairs outgrew the bounded EPA
+    polytope and their contacts were dropped (the reference's EPA is unbounded)."""
 
 
 class OmiScene(C.Structure):
@@ -83,6 +94,8 @@ PROTOTYPES = {
     'omi_set_stream': (C.c_int, [C.c_void_p, C.c_void_p]),
     'omi_set_budget': (C.c_int, [C.c_void_p, C.c_int64]),
     'omi_device_bytes': (C.c_int64, [C.c_void_p]),
+    'omi_set_limits': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    'omi_validate_scene': (C.c_int, [C.POINTER(OmiScene), C.c_char_p, C.c_int32]),
     'omi_load': (C.c_int, [C.c_void_p, C.POINTER(OmiScene)]),
     'omi_set_active': (C.c_int, [C.c_void_p, U8]),
     'omi_set_world_params': (C.c_int, [C.c_void_p, D, I, I, I]),
@@ -149,6 +162,17 @@ def load_library():
     return _LIB
 
 
+def validate_scene(scene) -> None:
+    """Check an :class:`OmiScene` as ``omi_load`` does, on the host only (no
+    device needed); raise the matching :class:`OmiError` if it is refused."""
+    lib = load_library()
+    err = C.create_string_buffer(512)
+    rc = lib.omi_validate_scene(C.byref(scene), err, len(err))
+    if rc < 0:
+        cls = {OMI_E_UNSUPPORTED: UnsupportedFeature}.get(rc, OmiError)
+        raise cls(rc, 'omi_validate_scene: ' + err.value.decode())
+
+
 def ptr(a, t):
     """ctypes pointer to a contiguous numpy array (None passes NULL)."""
     if a is None:
@@ -176,7 +200,8 @@ class Context:
         """Raise the matching exception for a negative status; return rc."""
         if rc < 0:
             msg = self.lib.omi_last_error(self.h).decode() or what
-            cls = {OMI_E_UNSUPPORTED: UnsupportedFeature, OMI_E_OOM: OutOfBudget}.get(rc, OmiError)
+            cls = {OMI_E_UNSUPPORTED: UnsupportedFeature, OMI_E_OOM: OutOfBudget, OMI_E_TIMEOUT: SweepTimeout,
+                   OMI_E_LIMIT: EpaLimit}.get(rc, OmiError)
             raise cls(rc, '%s: %s' % (what, msg) if what else msg)
         return rc
 
@@ -200,6 +225,11 @@ class Context:
 
     def device_bytes(self) -> int:
         return int(self.lib.omi_device_bytes(self.h))
+
+    def set_limits(self, spin_limit: int = 0, epa_faces: int = 0, stall_run: int = -1) -> None:
+        """Lower the sweep's wait bound or the EPA face bound, or stall one run
+        (tests of the failure paths); zeros restore the defaults."""
+        self.call('set_limits', int(spin_limit), int(epa_faces), int(stall_run))
 
     def profile_step(self):
         """Per-kernel-group device time (ms) of one eagerly launched step."""

@@ -35,9 +35,17 @@ enum {
     ST_WORDS = 8
 };
 
+// default bounds of the device's waits and of the EPA polytope; a context may
+// lower them (omi_set_limits) so that a test can make them run out
+constexpr int SPIN_LIMIT_DEFAULT = 1 << 22;
+
+
 struct Arena {
     int W, NB, NS, NM, NJ, NPTS;
     int pair_cap, contact_cap, hash_mask;
+    int spin_limit;                 // polls before a sweep wait gives up (ST_SWEEP_TIMEOUT)
+    int epa_faces;                  // EPA polytope face bound (<= EPA_F; ST_EPA_LIMIT past it)
+    int stall_run;                  // test hook: world-local run whose sweep entries never become ready (-1: none)
 
     // worlds
     const int *w_body_off;          // row range of each world (its capacity)

@@ -276,8 +276,8 @@ __device__ inline int closest_face(const EpaWork &W, int nf, double *bn, double 
 
 // _rebuild (gjk.py:197-217): visible faces found by all lanes, the ordered
 // horizon-edge dictionary kept by lane 0. Returns the new face count or -1
-// when the bounded storage would overflow.
-__device__ inline int rebuild(EpaWork &W, int nf, int ni) {
+// when the bounded storage (at most `face_cap` <= EPA_F faces) would overflow.
+__device__ inline int rebuild(EpaWork &W, int nf, int ni, int face_cap = EPA_F) {
     int out = 0;
     if (lane_id() == 0) {
         const double *w = W.V[ni];
@@ -312,7 +312,7 @@ __device__ inline int rebuild(EpaWork &W, int nf, int ni) {
         }
         for (int q = 0; q < ne && !bad; q++) {
             if (!W.Ealive[q]) continue;
-            if (nk >= EPA_F) { bad = true; break; }
+            if (nk >= face_cap) { bad = true; break; }
             W.F[nk][0] = W.E[q][0]; W.F[nk][1] = W.E[q][1]; W.F[nk][2] = (unsigned char)ni; nk++;
         }
         out = bad ? -1 : nk;
@@ -347,7 +347,7 @@ __device__ inline void face_contact(const EpaWork &W, int f, const double *nrm, 
 // epa (gjk.py:120-173). Returns 1 with normal/depth/point, 0 for None,
 // -1 when bounded storage overflowed (reported, treated as None).
 __device__ inline int epa(const Proxy &A, const Proxy &B, EpaWork &W, const Vt *s, int nv,
-                          double *nrm, double *depth, double *point) {
+                          double *nrm, double *depth, double *point, int face_cap = EPA_F) {
     for (int i = 0; i < nv; i++) put_vertex(W, i, s[i]);
     if (nv < 4) {                                   // _expand_to_tetra
         Vt pts[4];
@@ -394,7 +394,7 @@ __device__ inline int epa(const Proxy &A, const Proxy &B, EpaWork &W, const Vt *
         if (nv >= EPA_V) return -1;
         put_vertex(W, nv, wv);
         nv++;
-        nf = rebuild(W, nf, nv - 1);
+        nf = rebuild(W, nf, nv - 1, face_cap);
         if (nf < 0) return -1;
         if (nf == 0) return 0;
     }
@@ -407,12 +407,12 @@ __device__ inline int epa(const Proxy &A, const Proxy &B, EpaWork &W, const Vt *
 
 // collide_convex (gjk.py:249-264). Returns contacts (0/1), or -1 on overflow.
 __device__ inline int collide_convex(const Proxy &A, const Proxy &B, EpaWork &W, double *normal,
-                                     double *point, double *depth) {
+                                     double *point, double *depth, int face_cap = EPA_F) {
     Vt s[4];
     int n = 0;
     if (!gjk(A, B, s, n)) return 0;
     double nr[3], dep, pt[3];
-    int r = epa(A, B, W, s, n, nr, &dep, pt);
+    int r = epa(A, B, W, s, n, nr, &dep, pt, face_cap);
     if (r <= 0) return r;
     double ha[3], hb[3], dc[3];
     center_hint(A, ha); center_hint(B, hb);

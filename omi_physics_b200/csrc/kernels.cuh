@@ -21,10 +21,13 @@ constexpr unsigned FULL = 0xffffffffu;
 __device__ __forceinline__ bool pairs_over(const Arena &A) {
     return A.pair_scan[A.NB] > A.pair_cap;
 }
-// pair or contact overflow; valid once the contact scan of this step ran
+// pair or contact overflow, or a sweep wait that ran out earlier in this
+// launch of steps: the rest of the step (and every later step of the launch)
+// does nothing; valid once the contact scan of this step ran
 __device__ __forceinline__ bool overflowed(const Arena &A) {
     if (A.pair_scan[A.NB] > A.pair_cap) return true;
-    return A.contact_scan[A.pair_scan[A.NB]] > A.contact_cap;
+    if (A.contact_scan[A.pair_scan[A.NB]] > A.contact_cap) return true;
+    return *(volatile const int *)&A.status[ST_SWEEP_TIMEOUT] != 0;
 }
 __device__ __forceinline__ bool world_collides(const Arena &A, int w) {
     return A.w_active[w] && (A.w_flags[w] & WF_COLLISION);
@@ -93,7 +96,11 @@ __global__ void k_refit(Arena A) {
 // the index breaking ties, so the result is the stable order. Each pass
 // places every element by one binary search (its rank in the other run).
 // ---------------------------------------------------------------------------
+// numpy's sort order: NaN after every number (+inf included), NaNs among
+// themselves (and equal keys) by index
 __device__ __forceinline__ bool key_less(double ka, int va, double kb, int vb) {
+    const bool na = ka != ka, nb = kb != kb;
+    if (na | nb) return na == nb ? va < vb : nb;
     return ka < kb || (!(kb < ka) && va < vb);
 }
 
@@ -116,8 +123,7 @@ __global__ void k_sort(Arena A, int smem_cap) {
             v0 = A.sort_v[0] + off; v1 = A.sort_v[1] + off;
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double x = A.aabb_min[(off + i) * 3];
-            k0[i] = (x != x) ? INFINITY : x + 0.0;   // NaN sorts last; -0.0 == 0.0
+            k0[i] = A.aabb_min[(off + i) * 3] + 0.0;    // -0.0 == 0.0; NaN stays NaN (sorts last)
             v0[i] = i;
         }
         __syncthreads();
@@ -184,7 +190,10 @@ __device__ __forceinline__ bool pair_keep(const Arena &A, int w, int a, int b) {
     return keep;
 }
 
+// (numpy's searchsorted order: a NaN row is past every finite bound, and a
+// NaN bound is past every row)
 __device__ __forceinline__ int window_end(const Arena &A, int off, int end_w, double hx) {
+    if (hx != hx) return end_w;
     int lo = off, hi = end_w;
     while (lo < hi) {
         int m = (lo + hi) >> 1;
@@ -220,6 +229,7 @@ __global__ void k_pair_count_boxes(Arena A) {
 // search above done 32-ary by a warp (one load per lane per step, ~3 steps)
 __device__ __forceinline__ int window_end_warp(const double *sx, int lo, int hi, double hx) {
     const int lane = threadIdx.x & 31;
+    if (hx != hx) return hi;                         // warp-uniform: one row's bound
     while (hi - lo > 32) {
         const int step = (hi - lo + 31) >> 5;
         const int k = lo + lane * step;
@@ -603,7 +613,7 @@ __global__ void k_gjk(Arena A) {
         make_proxy(A, a, PA);
         make_proxy(A, b, PB);
         double nrm[3], pt[3], dep = 0.0;
-        const int r = collide_convex(PA, PB, W, nrm, pt, &dep);
+        const int r = collide_convex(PA, PB, W, nrm, pt, &dep, A.epa_faces);
         if (lane == 0) {
             if (r < 0) atomicAdd(&A.status[ST_EPA_LIMIT], 1);
             double *s = &A.slot[(size_t)p * SLOT];
@@ -674,7 +684,7 @@ __global__ void k_triggers(Arena A) {
                 hit = box_box_sat(PA.c, PA.R, PA.h, PB.c, PB.R, PB.h, nrm, depth) ? 1 : 0;
             } else {
                 double nrm[3], pt[3], dep = 0.0;
-                const int r = collide_convex(PA, PB, W, nrm, pt, &dep);
+                const int r = collide_convex(PA, PB, W, nrm, pt, &dep, A.epa_faces);
                 if (r < 0 && lane == 0) atomicAdd(&A.status[ST_EPA_LIMIT], 1);
                 hit = r > 0 ? 1 : 0;
             }
@@ -940,7 +950,8 @@ __device__ int mesh_pair(const Arena &A, int p, bool emit, EpaWork &W) {
                 T.local = &A.tri_verts[(size_t)(base + l) * 9];
                 T.m = 3;
                 double nrm[3], pt[3], dep = 0.0;
-                const int r = mesh_is_a ? collide_convex(T, O, W, nrm, pt, &dep) : collide_convex(O, T, W, nrm, pt, &dep);
+                const int r = mesh_is_a ? collide_convex(T, O, W, nrm, pt, &dep, A.epa_faces)
+                                         : collide_convex(O, T, W, nrm, pt, &dep, A.epa_faces);
                 if (r < 0 && lane == 0 && !emit) atomicAdd(&A.status[ST_EPA_LIMIT], 1);
                 if (r > 0) {
                     const int k = out0 + count;
@@ -1464,7 +1475,9 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
             // packed for the sweep: first contact | count << 24, and the
             // same-pass / all-pass predecessor counts
             A.run_kn[c0 + r] = A.run_k[c0 + r] | (A.run_n[c0 + r] << 24);
-            A.run_need[c0 + r] = ((pa >= 0) + (pb >= 0)) | (((pa != LEVEL_NONE) + (pb != LEVEL_NONE)) << 2);
+            // (the test hook's run asks for 3 same-pass arrivals of at most 2: it never becomes ready)
+            A.run_need[c0 + r] = ((pa >= 0) + (pb >= 0)) | (((pa != LEVEL_NONE) + (pb != LEVEL_NONE)) << 2) |
+                                 (r == A.stall_run ? 3 : 0);
         }
         if (tid == 0) A.w_runs[w] = R;
         __syncthreads();
@@ -1685,10 +1698,10 @@ __device__ __forceinline__ void st_release_cta(int *p, int v) {
 }
 __device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
 
-// polls before a wait gives up: far beyond any legitimate wait (a whole
-// world's sweep); one timeout sets the block's abort flag and ends every
-// other wait at once
-constexpr int SPIN_LIMIT = 1 << 22;
+// Polls before a wait gives up (Arena::spin_limit, SPIN_LIMIT_DEFAULT unless
+// a context lowers it): far beyond any legitimate wait (a whole world's
+// sweep); one timeout sets the group's abort flag and ends every other wait
+// at once.
 
 // predecessors entry (p, r) waits for: on each side, a same-pass predecessor
 // always counts, a previous-pass one only after pass 0. Runs count their
@@ -1868,7 +1881,7 @@ __device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_
                     }
                 }
                 if (got) break;
-                if (it >= SPIN_LIMIT) { *abort = 1; cnt = -1; break; }
+                if (it >= A.spin_limit) { *abort = 1; cnt = -1; break; }
                 __nanosleep(32);
             }
         }
@@ -1877,7 +1890,7 @@ __device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_
         if (cnt < 0) break;
         if (lane < cnt) {
             int e1 = 0;
-            for (int it = 0; it < SPIN_LIMIT; it++) {     // the pusher is between its two steps
+            for (int it = 0; it < A.spin_limit; it++) {   // the pusher is between its two steps
                 e1 = ld_acquire_cta(&ring[lo + lane]);
                 if (e1 || *abort) break;
             }

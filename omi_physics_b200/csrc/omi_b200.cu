@@ -82,6 +82,8 @@ struct OmiCtx {
     cudaStream_t cap_s[2] = {};
     cudaEvent_t cap_ev = nullptr;
     int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
+    // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
+    int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
 };
 
 namespace {
@@ -433,6 +435,22 @@ int64_t step_launches(OmiCtx *ctx) {
     return n;
 }
 
+// errors the status words of completed steps carry: a sweep wait that ran
+// out (the step did not complete), or pairs whose EPA polytope outgrew its
+// bound (the step completed, but those pairs' contacts were dropped where the
+// reference's unbounded EPA would have made one)
+int status_errors(OmiCtx *ctx) {
+    const int *st = ctx->h_status;
+    if (st[ST_SWEEP_TIMEOUT])
+        return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out (the step did not complete; "
+                                        "restore the worlds' state before stepping on)");
+    if (st[ST_EPA_LIMIT])
+        return fail(ctx, OMI_E_LIMIT, std::to_string(st[ST_EPA_LIMIT]) +
+                                          " convex pair test(s) outgrew the bounded EPA polytope; their "
+                                          "contacts were dropped (the step completed)");
+    return 0;
+}
+
 int run_steps(OmiCtx *ctx, int n, bool sync) {
     if (!ctx->loaded) return fail(ctx, OMI_E_STATE, "omi_step before omi_load");
     int remaining = n;
@@ -451,7 +469,7 @@ int run_steps(OmiCtx *ctx, int n, bool sync) {
         if (!sync) return 0;
         int rc = read_status(ctx);
         if (rc) return rc;
-        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out");
+        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return status_errors(ctx);
         const int done = ctx->h_status[ST_STEPS_DONE];
         remaining -= done;
         if (remaining > 0) {
@@ -461,7 +479,7 @@ int run_steps(OmiCtx *ctx, int n, bool sync) {
             if (rc) return rc;
         }
     }
-    return 0;
+    return status_errors(ctx);
 }
 
 template <class T>
@@ -559,8 +577,164 @@ int64_t omi_device_bytes(OmiCtx *ctx) { return ctx ? ctx->bytes : 0; }
 int64_t omi_launch_count(OmiCtx *ctx) { return ctx ? ctx->launches : 0; }
 const char *omi_kernel_name(int32_t i) { return (i >= 0 && i < KN_COUNT) ? kKernelNames[i] : ""; }
 
+// Host-side check of a whole-arena scene and the per-body tables derived from
+// it (refit kind and half extents, sensor and AABB shapes, mesh rows). Every
+// index a kernel follows is range-checked here, so no kernel reads out of
+// bounds; nothing touches the device.
+struct SceneDerived {
+    std::vector<int> body_world, tshape, rshape, vol_off, body_mesh;
+    std::vector<int8_t> kind;
+    std::vector<double> half;
+    bool sensors = false;
+    int max_n = 0, max_nc = 0, max_j = 0, n_meshes = 0, n_tris = 0;
+};
+
+#define BAD(code, msg) do { err = (msg); return (code); } while (0)
+
+static int derive_scene(const OmiScene *s, SceneDerived &D, std::string &err) {
+    if (!s) BAD(OMI_E_ARG, "null scene");
+    const int W = s->n_worlds, NB = s->n_bodies;
+    if (W <= 0 || NB < 0 || !s->w_body_off || !s->w_joint_off || s->w_body_off[0] != 0 || s->w_body_off[W] != NB)
+        BAD(OMI_E_ARG, "inconsistent world/body offsets");
+    if (s->n_shapes < 0 || s->n_materials < 0 || s->n_points < 0 || s->n_joints < 0 || s->n_pair_friction < 0 ||
+        s->n_filter_bytes < 0 || s->n_volumes < 0 || s->n_meshes < 0)
+        BAD(OMI_E_ARG, "negative table size");
+    for (int w = 0; w < W; w++) {
+        if (s->w_body_off[w + 1] < s->w_body_off[w]) BAD(OMI_E_ARG, "world offsets decrease");
+        if (s->w_joint_off[w + 1] < s->w_joint_off[w]) BAD(OMI_E_ARG, "joint offsets decrease");
+        const int rows = s->w_filter_rows[w];
+        if (rows < 1 || rows > 4096 || s->w_filter_off[w] < 0 ||
+            (int64_t)s->w_filter_off[w] + (int64_t)rows * rows > s->n_filter_bytes)
+            BAD(OMI_E_ARG, "filter matrix range out of bounds");
+        if (s->w_pf_off[w] < 0 || s->w_pf_n[w] < 0 || s->w_pf_off[w] + s->w_pf_n[w] > s->n_pair_friction)
+            BAD(OMI_E_ARG, "pair-friction range out of bounds");
+        if (s->w_iters[w] < 0 || s->w_joint_iters[w] < 0) BAD(OMI_E_ARG, "negative iteration count");
+    }
+    if (s->w_joint_off[0] != 0 || s->w_joint_off[W] != s->n_joints) BAD(OMI_E_ARG, "inconsistent joint offsets");
+    D = SceneDerived{};
+    D.body_world.assign(NB, 0);
+    D.kind.assign(NB, 0);
+    D.half.assign((size_t)NB * 3, 0.0);
+    D.tshape.assign(NB, -1);
+    D.rshape.assign(NB, -1);
+    if (s->trigger_shape)
+        for (int i = 0; i < NB; i++) {
+            const int t = s->trigger_shape[i];
+            if (t < -1 || t >= s->n_shapes) BAD(OMI_E_ARG, "trigger shape index out of range");
+            D.tshape[i] = t;
+            D.sensors |= t >= 0;
+        }
+    D.vol_off.assign(W + 1, 0);
+    if (s->w_vol_off) {
+        for (int w = 0; w <= W; w++) D.vol_off[w] = s->w_vol_off[w];
+        if (D.vol_off[0] != 0 || D.vol_off[W] != s->n_volumes) BAD(OMI_E_ARG, "inconsistent volume offsets");
+        for (int w = 0; w < W; w++)
+            if (D.vol_off[w + 1] < D.vol_off[w]) BAD(OMI_E_ARG, "volume offsets decrease");
+    } else if (s->n_volumes != 0) {
+        BAD(OMI_E_ARG, "gravity volumes without w_vol_off");
+    }
+    for (int w = 0; w < W; w++) {
+        const int n = s->w_body_off[w + 1] - s->w_body_off[w];
+        D.max_n = std::max(D.max_n, n);
+        if (s->w_flags[w] & OMI_WF_COLLISION) D.max_nc = std::max(D.max_nc, n);
+        for (int i = s->w_body_off[w]; i < s->w_body_off[w + 1]; i++) {
+            D.body_world[i] = w;
+            if (s->filter_row[i] < 0 || s->filter_row[i] >= s->w_filter_rows[w])
+                BAD(OMI_E_ARG, "filter row out of range");
+        }
+    }
+    for (int i = 0; i < NB; i++) {
+        if (s->shape[i] >= s->n_shapes || s->shape[i] < -1) BAD(OMI_E_ARG, "shape index out of range");
+        // the AABB comes from the collider, else the sensor (world.py:452-455)
+        const int sh = s->shape[i] >= 0 ? s->shape[i] : D.tshape[i];
+        D.rshape[i] = sh;
+        if (s->motion_type[i] < 0 || s->motion_type[i] > 2) BAD(OMI_E_ARG, "motion type");
+        if (s->material[i] >= s->n_materials || s->material[i] < -1) BAD(OMI_E_ARG, "material index out of range");
+        if (sh < 0) continue;
+        const int t = s->shape_type[sh];
+        double *half = D.half.data();
+        if (t == OMI_SHAPE_SPHERE) {
+            D.kind[i] = 1;
+            for (int c = 0; c < 3; c++) half[i * 3 + c] = s->shape_radius[sh];
+        } else if (t == OMI_SHAPE_BOX) {
+            D.kind[i] = 2;
+            for (int c = 0; c < 3; c++) half[i * 3 + c] = 0.5 * s->shape_size[sh * 3 + c];
+        } else if (t == OMI_SHAPE_CONVEX) {
+            D.kind[i] = 3;
+            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
+                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
+                BAD(OMI_E_ARG, "convex point range out of bounds");
+        } else if (t == OMI_SHAPE_CAPSULE) {
+            D.kind[i] = 4;
+            half[i * 3] = s->shape_radius[sh];
+            half[i * 3 + 1] = 0.5 * s->shape_size[sh * 3 + 1];
+            half[i * 3 + 2] = 0.0;
+        } else if (t == OMI_SHAPE_TRIMESH) {
+            D.kind[i] = 5;
+            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
+                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
+                BAD(OMI_E_ARG, "mesh point range out of bounds");
+            if (s->shape[i] != sh || s->motion_type[i] == 2)
+                BAD(OMI_E_UNSUPPORTED, "triangle meshes are taken as static or kinematic colliders only");
+        } else {
+            BAD(OMI_E_UNSUPPORTED, "shape type not supported on the device path");
+        }
+    }
+    // triangle meshes: every mesh body listed once, its tables in range
+    D.body_mesh.assign(NB, -1);
+    const int NMESH = s->mesh_body ? s->n_meshes : 0;
+    D.n_meshes = NMESH;
+    if (NMESH) {
+        if (!s->mesh_tri_off || !s->mesh_grid_i) BAD(OMI_E_ARG, "mesh tables missing");
+        if (s->mesh_tri_off[0] != 0) BAD(OMI_E_ARG, "mesh triangle offsets must start at 0");
+        for (int m = 0; m < NMESH; m++) {
+            const int b = s->mesh_body[m];
+            if (b < 0 || b >= NB || D.kind[b] != 5 || D.body_mesh[b] >= 0) BAD(OMI_E_ARG, "mesh body");
+            if (s->mesh_tri_off[m + 1] < s->mesh_tri_off[m]) BAD(OMI_E_ARG, "mesh triangle offsets decrease");
+            const int *gi = &s->mesh_grid_i[m * 4];
+            if (!gi[0] && (gi[1] < 1 || gi[2] < 1 || gi[3] < 1)) BAD(OMI_E_ARG, "mesh grid shape");
+            D.body_mesh[b] = m;
+        }
+        D.n_tris = s->mesh_tri_off[NMESH];
+        if (!s->tri_idx) BAD(OMI_E_ARG, "mesh tables without tri_idx");
+        for (int m = 0; m < NMESH; m++) {
+            const int b = s->mesh_body[m], sh = s->shape[b];
+            for (int t = s->mesh_tri_off[m]; t < s->mesh_tri_off[m + 1]; t++)
+                for (int j = 0; j < 3; j++)
+                    if (s->tri_idx[t * 3 + j] < 0 || s->tri_idx[t * 3 + j] >= s->shape_pt_cnt[sh])
+                        BAD(OMI_E_ARG, "mesh triangle vertex index out of range");
+        }
+    }
+    for (int i = 0; i < NB; i++)
+        if (D.kind[i] == 5 && D.body_mesh[i] < 0) BAD(OMI_E_ARG, "a mesh body without its triangle tables");
+    for (int p = 0; p < s->n_pair_friction; p++)
+        if (s->pf_a[p] >= s->n_materials || s->pf_b[p] >= s->n_materials)
+            BAD(OMI_E_ARG, "pair-friction material out of range");
+    for (int w = 0; w < W; w++) {
+        for (int j = s->w_joint_off[w]; j < s->w_joint_off[w + 1]; j++) {
+            if (s->j_type[j] < 0 || s->j_type[j] > 2) BAD(OMI_E_ARG, "joint type");
+            if (s->j_a[j] >= NB || s->j_b[j] >= NB || s->j_a[j] < -1 || s->j_b[j] < -1)
+                BAD(OMI_E_ARG, "joint body out of range");
+            if (s->j_type[j] == OMI_JOINT_MOTOR && s->j_a[j] < 0) BAD(OMI_E_ARG, "motor without a body");
+            // a joint's bodies belong to its own world (each world's joints are solved by one block)
+            if ((s->j_a[j] >= 0 && D.body_world[s->j_a[j]] != w) || (s->j_b[j] >= 0 && D.body_world[s->j_b[j]] != w))
+                BAD(OMI_E_ARG, "joint body outside the joint's world");
+        }
+        D.max_j = std::max(D.max_j, s->w_joint_off[w + 1] - s->w_joint_off[w]);
+    }
+    return 0;
+}
+#undef BAD
+
 static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const int *joint_n) {
     if (!ctx || !s) return OMI_E_ARG;
+    // check everything before the previous arena is released: a refused scene leaves it loaded
+    SceneDerived D;
+    {
+        std::string msg;
+        const int vrc = derive_scene(s, D, msg);
+        if (vrc) return fail(ctx, vrc, msg);
+    }
     CK(cudaSetDevice(ctx->device));
     cudaStreamSynchronize(ctx->stream);
     drop_graph(ctx);
@@ -570,129 +744,19 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     ctx->cache_cap = 0;
     ctx->loaded = false;
     const int W = s->n_worlds, NB = s->n_bodies;
-    if (W <= 0 || NB < 0 || s->w_body_off[0] != 0 || s->w_body_off[W] != NB)
-        return fail(ctx, OMI_E_ARG, "inconsistent world/body offsets");
-    // validate indices on the host so no kernel can read out of bounds
-    for (int w = 0; w < W; w++) {
-        if (s->w_body_off[w + 1] < s->w_body_off[w]) return fail(ctx, OMI_E_ARG, "world offsets decrease");
-        if (s->w_joint_off[w + 1] < s->w_joint_off[w]) return fail(ctx, OMI_E_ARG, "joint offsets decrease");
-        const int rows = s->w_filter_rows[w];
-        if (rows < 1 || s->w_filter_off[w] < 0 || s->w_filter_off[w] + rows * rows > s->n_filter_bytes)
-            return fail(ctx, OMI_E_ARG, "filter matrix range out of bounds");
-        if (s->w_pf_off[w] < 0 || s->w_pf_n[w] < 0 || s->w_pf_off[w] + s->w_pf_n[w] > s->n_pair_friction)
-            return fail(ctx, OMI_E_ARG, "pair-friction range out of bounds");
-    }
-    if (s->w_joint_off[0] != 0 || s->w_joint_off[W] != s->n_joints)
-        return fail(ctx, OMI_E_ARG, "inconsistent joint offsets");
-    std::vector<int> body_world(NB);
-    std::vector<int8_t> kind(NB, 0);
-    std::vector<double> half((size_t)NB * 3, 0.0);
-    std::vector<int> tshape(NB, -1), rshape(NB, -1);
-    bool sensors = false;
-    if (s->trigger_shape)
-        for (int i = 0; i < NB; i++) {
-            const int t = s->trigger_shape[i];
-            if (t < -1 || t >= s->n_shapes) return fail(ctx, OMI_E_ARG, "trigger shape index out of range");
-            tshape[i] = t;
-            sensors |= t >= 0;
-        }
-    std::vector<int> vol_off(W + 1, 0);
-    if (s->w_vol_off) {
-        for (int w = 0; w <= W; w++) vol_off[w] = s->w_vol_off[w];
-        if (vol_off[0] != 0 || vol_off[W] != s->n_volumes) return fail(ctx, OMI_E_ARG, "inconsistent volume offsets");
-        for (int w = 0; w < W; w++)
-            if (vol_off[w + 1] < vol_off[w]) return fail(ctx, OMI_E_ARG, "volume offsets decrease");
-    } else if (s->n_volumes != 0) {
-        return fail(ctx, OMI_E_ARG, "gravity volumes without w_vol_off");
-    }
-    int max_n = 0, max_nc = 0;
-    for (int w = 0; w < W; w++) {
-        const int n = s->w_body_off[w + 1] - s->w_body_off[w];
-        max_n = std::max(max_n, n);
-        if (s->w_flags[w] & OMI_WF_COLLISION) max_nc = std::max(max_nc, n);
-        for (int i = s->w_body_off[w]; i < s->w_body_off[w + 1]; i++) {
-            body_world[i] = w;
-            if (s->filter_row[i] < 0 || s->filter_row[i] >= s->w_filter_rows[w])
-                return fail(ctx, OMI_E_ARG, "filter row out of range");
-        }
-    }
-    for (int i = 0; i < NB; i++) {
-        if (s->shape[i] >= s->n_shapes) return fail(ctx, OMI_E_ARG, "shape index out of range");
-        // the AABB comes from the collider, else the sensor (world.py:452-455)
-        const int sh = s->shape[i] >= 0 ? s->shape[i] : tshape[i];
-        rshape[i] = sh;
-        if (s->motion_type[i] < 0 || s->motion_type[i] > 2) return fail(ctx, OMI_E_ARG, "motion type");
-        if (s->material[i] >= s->n_materials || s->material[i] < -1) return fail(ctx, OMI_E_ARG, "material index out of range");
-        if (sh < 0) continue;
-        const int t = s->shape_type[sh];
-        if (t == OMI_SHAPE_SPHERE) {
-            kind[i] = 1;
-            for (int c = 0; c < 3; c++) half[i * 3 + c] = s->shape_radius[sh];
-        } else if (t == OMI_SHAPE_BOX) {
-            kind[i] = 2;
-            for (int c = 0; c < 3; c++) half[i * 3 + c] = 0.5 * s->shape_size[sh * 3 + c];
-        } else if (t == OMI_SHAPE_CONVEX) {
-            kind[i] = 3;
-            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
-                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
-                return fail(ctx, OMI_E_ARG, "convex point range out of bounds");
-        } else if (t == OMI_SHAPE_CAPSULE) {
-            kind[i] = 4;
-            half[i * 3] = s->shape_radius[sh];
-            half[i * 3 + 1] = 0.5 * s->shape_size[sh * 3 + 1];
-            half[i * 3 + 2] = 0.0;
-        } else if (t == OMI_SHAPE_TRIMESH) {
-            kind[i] = 5;
-            if (s->shape_pt_cnt[sh] < 1 || s->shape_pt_off[sh] < 0 ||
-                s->shape_pt_off[sh] + s->shape_pt_cnt[sh] > s->n_points)
-                return fail(ctx, OMI_E_ARG, "mesh point range out of bounds");
-            if (s->shape[i] != sh || s->motion_type[i] == 2)
-                return fail(ctx, OMI_E_UNSUPPORTED, "triangle meshes are taken as static or kinematic colliders only");
-        } else {
-            return fail(ctx, OMI_E_UNSUPPORTED, "shape type not supported on the device path");
-        }
-    }
-    // triangle meshes: every mesh body listed once, its tables in range
-    std::vector<int> body_mesh(NB, -1);
-    const int NMESH = s->mesh_body ? s->n_meshes : 0;
-    int n_tris = 0;
-    if (NMESH) {
-        if (s->mesh_tri_off[0] != 0) return fail(ctx, OMI_E_ARG, "mesh triangle offsets must start at 0");
-        for (int m = 0; m < NMESH; m++) {
-            const int b = s->mesh_body[m];
-            if (b < 0 || b >= NB || kind[b] != 5 || body_mesh[b] >= 0) return fail(ctx, OMI_E_ARG, "mesh body");
-            if (s->mesh_tri_off[m + 1] < s->mesh_tri_off[m]) return fail(ctx, OMI_E_ARG, "mesh triangle offsets decrease");
-            const int *gi = &s->mesh_grid_i[m * 4];
-            if (!gi[0] && (gi[1] < 1 || gi[2] < 1 || gi[3] < 1)) return fail(ctx, OMI_E_ARG, "mesh grid shape");
-            body_mesh[b] = m;
-        }
-        n_tris = s->mesh_tri_off[NMESH];
-        if (!s->tri_idx) return fail(ctx, OMI_E_ARG, "mesh tables without tri_idx");
-        for (int m = 0; m < NMESH; m++) {
-            const int b = s->mesh_body[m], sh = s->shape[b];
-            for (int t = s->mesh_tri_off[m]; t < s->mesh_tri_off[m + 1]; t++)
-                for (int j = 0; j < 3; j++)
-                    if (s->tri_idx[t * 3 + j] < 0 || s->tri_idx[t * 3 + j] >= s->shape_pt_cnt[sh])
-                        return fail(ctx, OMI_E_ARG, "mesh triangle vertex index out of range");
-        }
-    }
-    for (int i = 0; i < NB; i++)
-        if (kind[i] == 5 && body_mesh[i] < 0) return fail(ctx, OMI_E_ARG, "a mesh body without its triangle tables");
-    for (int p = 0; p < s->n_pair_friction; p++)
-        if (s->pf_a[p] >= s->n_materials || s->pf_b[p] >= s->n_materials)
-            return fail(ctx, OMI_E_ARG, "pair-friction material out of range");
-    for (int j = 0; j < s->n_joints; j++) {
-        if (s->j_type[j] < 0 || s->j_type[j] > 2) return fail(ctx, OMI_E_ARG, "joint type");
-        if (s->j_a[j] >= NB || s->j_b[j] >= NB) return fail(ctx, OMI_E_ARG, "joint body out of range");
-        if (s->j_type[j] == OMI_JOINT_MOTOR && s->j_a[j] < 0) return fail(ctx, OMI_E_ARG, "motor without a body");
-    }
-    int max_j = 0;
-    for (int w = 0; w < W; w++) max_j = std::max(max_j, s->w_joint_off[w + 1] - s->w_joint_off[w]);
-
+    const std::vector<int> &body_world = D.body_world, &tshape = D.tshape, &rshape = D.rshape;
+    const std::vector<int> &vol_off = D.vol_off, &body_mesh = D.body_mesh;
+    const std::vector<int8_t> &kind = D.kind;
+    const std::vector<double> &half = D.half;
+    const bool sensors = D.sensors;
+    const int max_n = D.max_n, max_nc = D.max_nc, max_j = D.max_j, NMESH = D.n_meshes, n_tris = D.n_tris;
     Arena &A = ctx->A;
     A = Arena{};
     A.W = W; A.NB = NB; A.NS = s->n_shapes; A.NM = s->n_materials; A.NJ = s->n_joints;
     A.NPTS = s->n_points;
+    A.spin_limit = ctx->spin_limit;
+    A.epa_faces = ctx->epa_faces;
+    A.stall_run = ctx->stall_run;
     int rc = 0;
     // worlds
     rc |= upload(ctx, const_cast<int *&>(A.w_body_off), s->w_body_off, W + 1);
@@ -1215,10 +1279,39 @@ int omi_sync(OmiCtx *ctx) {
     if (!ctx) return OMI_E_ARG;
     int rc = read_status(ctx);
     if (rc) return rc;
+    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return status_errors(ctx);
     if (ctx->h_status[ST_OVERFLOW])
         return fail(ctx, OMI_E_STATE, "an asynchronous step overflowed its buffers; re-run with omi_step");
-    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out");
+    return status_errors(ctx);
+}
+
+int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t stall_run) {
+    if (!ctx) return OMI_E_ARG;
+    if (epa_faces > EPA_F || (epa_faces > 0 && epa_faces < 4) || stall_run < -1)
+        return fail(ctx, OMI_E_ARG, "limits out of range (epa_faces 4.." + std::to_string(EPA_F) + ", stall_run >= -1)");
+    ctx->spin_limit = spin_limit > 0 ? spin_limit : SPIN_LIMIT_DEFAULT;
+    ctx->epa_faces = epa_faces > 0 ? epa_faces : EPA_F;
+    ctx->stall_run = stall_run;
+    if (ctx->loaded) {
+        cudaStreamSynchronize(ctx->stream);
+        drop_graph(ctx);                 // the captured launches hold the arena by value
+        ctx->A.spin_limit = ctx->spin_limit;
+        ctx->A.epa_faces = ctx->epa_faces;
+        ctx->A.stall_run = ctx->stall_run;
+    }
     return 0;
+}
+
+int omi_validate_scene(const OmiScene *scene, char *err, int32_t err_cap) {
+    SceneDerived D;
+    std::string msg;
+    const int rc = derive_scene(scene, D, msg);
+    if (rc && err && err_cap > 0) {
+        const size_t k = std::min<size_t>(msg.size(), (size_t)err_cap - 1);
+        std::memcpy(err, msg.data(), k);
+        err[k] = 0;
+    }
+    return rc;
 }
 
 // ---- stage entry points -------------------------------------------------

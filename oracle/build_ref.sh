@@ -4,9 +4,10 @@
 # CPU reference arm of bench.py. pip writes build files into the source tree,
 # so it installs from a scratch copy; outputs land only in oracle/_ref.
 #   usage: sh oracle/build_ref.sh [/path/to/reference]
+# Without an argument: $OMI_REFERENCE_SRC, else a 'reference' folder beside the repository.
 set -e
-SRC=${1:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+SRC=${1:-${OMI_REFERENCE_SRC:-$(cd "$HERE/../.." && pwd)/reference}}
 TMP=$(mktemp -d /tmp/omi_ref_src.XXXXXX)
 cp -r "$SRC"/. "$TMP"/
 chmod -R u+w "$TMP"

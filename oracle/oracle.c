@@ -250,12 +250,18 @@ void or_refit(OrWorld *w) {
 /* ------------------------------------------------------------------ */
 /* broadphase (broadphase.py:243-301)                                  */
 /* ------------------------------------------------------------------ */
+/* np.argsort(kind='stable') order: NaN after every number (+inf included),
+ * -0.0 equal to 0.0, ties (NaNs among themselves too) by original index */
 static const double *g_sort_keys;
 static int cmp_stable(const void *pa, const void *pb) {
     int a = *(const int *)pa, b = *(const int *)pb;
     double ka = g_sort_keys[a * 3], kb = g_sort_keys[b * 3];
-    if (ka < kb) return -1;
-    if (ka > kb) return 1;
+    int na = ka != ka, nb = kb != kb;
+    if (na != nb) return na - nb;
+    if (!na) {
+        if (ka < kb) return -1;
+        if (ka > kb) return 1;
+    }
     return (a > b) - (a < b);   /* stable: original index breaks ties */
 }
 
@@ -279,8 +285,11 @@ int or_broadphase(OrWorld *w) {
     for (int k = 0; k < n; k++) {
         int a = order[k];
         double hx = w->aabb_max[a * 3];
-        /* searchsorted(lo_sx, hi_sx[k], 'right'): first index with lo > hi */
+        /* searchsorted(lo_sx, hi_sx[k], 'right'): first index with lo > hi in
+         * numpy's order, where NaN is above every number and equal to NaN: a NaN
+         * row is past every finite hi, and a NaN hi is past every row */
         int lo = 0, hi = n;
+        if (hx != hx) lo = n;
         while (lo < hi) {
             int mid = (lo + hi) >> 1;
             if (w->aabb_min[order[mid] * 3] <= hx) lo = mid + 1; else hi = mid;
