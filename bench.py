@@ -37,7 +37,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from omi_physics_b200.shard import barrier, max_over_ranks, sum_over_ranks  # noqa: E402
+from omi_physics_b200.shard import (ShardedWorlds, barrier, max_over_ranks, merge_ticks,  # noqa: E402
+                                    shard_requests, sum_over_ranks)
 
 MEASURED = os.path.join(ROOT, 'MEASURED_PEAKS.json')
 FALLBACK_HBM = 6650.0
@@ -65,6 +66,15 @@ def parse():
                     help='run only the capsule-triangle measurement (device part) and print it')
     ap.add_argument('--groups', type=int, default=4,
                     help='worlds are stepped as this many concurrent groups (one context + stream each)')
+    ap.add_argument('--workload', default='serving-mix',
+                    choices=['serving-mix', 'pyramid', 'debris4096', 'convex32768', 'joints512'],
+                    help='serving-mix (default): the batched headline; the others time one benchmark '
+                         'configuration over its whole run from its initial state')
+    ap.add_argument('--scaling', default='weak', choices=['weak', 'strong'],
+                    help='serving mix under torchrun: weak = every rank steps its own seeded mix; '
+                         'strong = one mix split across the ranks by body-count bin-packing')
+    ap.add_argument('--config-steps', type=int, default=None,
+                    help='steps of a configuration run (default: the configuration\'s own count)')
     return ap.parse_args()
 
 
@@ -234,8 +244,18 @@ def run_ours(args, rank, world, local):
     from omi_physics_b200._lib import D, U8, OmiError, ptr
     torch.cuda.set_device(local)
     t0 = time.time()
-    reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
-    grp = WorldGroups(worlds, groups=args.groups, device=local)
+    if args.scaling == 'strong':
+        # one mix for the whole job, split across ranks (each builds only its worlds)
+        from omi_physics_b200 import scenes
+        reqs = scenes.serving_requests(args.worlds, seed=args.seed)
+        sw = ShardedWorlds([r['bodies'] + 1 for r in reqs],
+                           lambda i: (lambda r: (r[0], r[1]['dt']))(scenes.serving_world(reqs[i])),
+                           rank, world, groups=args.groups, device=local)
+        worlds, grp = sw.worlds, sw.groups
+        reqs = [reqs[i] for i in sw.indices]
+    else:
+        reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
+        grp = WorldGroups(worlds, groups=args.groups, device=local)
     grp.step(args.preroll)
     setup_s = time.time() - t0
     N = dynamic_bodies(worlds)
@@ -291,10 +311,12 @@ def run_ours(args, rank, world, local):
     # per-step tick latency distribution (every world one step, synchronised per tick)
     ticks = []
     for _ in range(max(10, min(args.steps, 50))):
+        barrier(world)
         a, b = timed_steps(1)
         b.synchronize()
         ticks.append(a.elapsed_time(b))
     grp.sync()
+    ticks = merge_ticks(ticks, world)          # a tick ends when its slowest rank's does
 
     # ---- roofline: per-stage device time of eagerly launched steps (groups one
     # after another, so the sums are the stage times of the whole mix) ----
@@ -351,7 +373,11 @@ def run_ours(args, rank, world, local):
     extras = {}
     n_serve = args.worlds if args.serve_requests is None else args.serve_requests
     if not args.no_extras and n_serve > 0:
-        extras['serving'] = serving_run(n_serve, args.seed + 1000 * rank, args.serve_slots, stream)
+        if args.scaling == 'strong':
+            extras['serving'] = serving_run(n_serve, args.seed, args.serve_slots, stream,
+                                            shard=(rank, world))
+        else:
+            extras['serving'] = serving_run(n_serve, args.seed + 1000 * rank, args.serve_slots, stream)
         barrier(world)
     if not args.no_extras and rank == 0:
         extras['plain'] = plain_per_world(worlds, reqs, args.plain_sample, local, args.preroll)
@@ -364,13 +390,16 @@ def run_ours(args, rank, world, local):
 SERVE_BUDGET = 120 * 10 ** 9
 
 
-def serving_run(n_requests, seed, per_class, stream):
+def serving_run(n_requests, seed, per_class, stream, shard=None):
     """The request loop: Poisson arrivals (200/s), each world admitted into a
     free slot of its size class under the HBM budget, stepped with every other
-    resident world once per tick until its 60-600 steps are done."""
+    resident world once per tick until its 60-600 steps are done. ``shard``
+    (rank, ranks): this rank serves only its share of one request stream."""
     from omi_physics_b200 import scenes
     from omi_physics_b200.serving import Server, size_classes
     reqs = scenes.serving_requests(n_requests, seed=seed)
+    if shard is not None:
+        reqs = [reqs[i] for i in shard_requests(reqs, shard[0], shard[1])]
     srv = Server(size_classes(2048, per_class=per_class), budget_bytes=SERVE_BUDGET,
                  stream=stream.cuda_stream)
     for r in reqs:
@@ -622,14 +651,263 @@ def cpu_reference(n_worlds, seed, budget_s, preroll, cores=None):
             'per_core': per_core}
 
 
+# ---------------------------------------------------------------------------
+# the other benchmark configurations, each timed over its whole run
+# ---------------------------------------------------------------------------
+CONFIG_META = {
+    'pyramid': dict(desc='10-level pyramid of 55 unit boxes on a 20x1x20 m ground box', dt='1/60 s',
+                    iterations=10, cpu_budget_s=20.0),
+    'debris4096': dict(desc='4096 bodies, 70% boxes [0.5,1.5] m / 30% spheres r [0.25,0.75] m, '
+                            'density 1000, above a 60x1x60 m ground box', dt='1/120 s', iterations=8,
+                       cpu_budget_s=40.0),
+    'convex32768': dict(desc='32768 bodies, 50% boxes / 25% spheres / 25% convex hulls (12-32 points on '
+                             'ellipsoids, GJK/EPA) in a walled 100x100 m arena, sleeping on',
+                        dt='1/120 s', iterations=8, cpu_budget_s=60.0),
+    'joints512': dict(desc='512 worlds: chains of 16-128 links (point joints, 10% motored) under 64-512 '
+                           'loose boxes', dt='1/240 s', iterations=12, cpu_budget_s=40.0),
+}
+
+
+def _cfg_ref_worker(payload):
+    """Reference CPU step (oracle/_ref) on worlds ``idx`` of a configuration:
+    each world from its initial state for up to ``max_steps`` steps, within
+    ``budget_s``. Returns (body-steps, seconds stepping, per-step seconds of
+    the first world, steps done)."""
+    name, idx, max_steps, budget_s = payload
+    sys.path.insert(0, os.path.join(ROOT, 'oracle', '_ref'))
+    from types import SimpleNamespace
+    import omi_physics as ref
+    from omi_physics import gravity as rg, joints as rj, model as rm
+    from omi_physics_b200 import scenes
+    api = SimpleNamespace(PhysicsWorld=ref.PhysicsWorld, model=rm, joints=rj, gravity=rg)
+    builder, _ = scenes.CONFIGS[name]
+    if name == 'joints512':
+        worlds, dts = scenes.joint_chains(512, 21, api, which=idx)
+    else:
+        worlds, dts = builder(api)
+    start = time.perf_counter()
+    done = spent = 0.0
+    per_step = []
+    steps_done = 0
+    for s in range(max_steps):
+        for w, dt in zip(worlds, dts):
+            n = int(np.count_nonzero(w.motion_type == 2))
+            t = time.perf_counter()
+            w.step(dt)
+            el = time.perf_counter() - t
+            spent += el
+            done += n
+            if w is worlds[0]:
+                per_step.append(el)
+        steps_done = s + 1
+        if time.perf_counter() - start > budget_s:
+            break
+    return done, spent, per_step, steps_done
+
+
+def config_cpu_reference(name, max_steps, budget_s, cores=None):
+    """The reference's CPU step on a bounded sample of a configuration run
+    (its first steps from the initial state): one process for a one-world
+    configuration (the reference is single-threaded), all host cores through
+    a spawn pool for the multi-world one."""
+    import multiprocessing as mp
+    if not os.path.isdir(os.path.join(ROOT, 'oracle', '_ref', 'omi_physics')):
+        return None
+    ctx = mp.get_context('spawn')
+    t = time.perf_counter()
+    if name == 'joints512':
+        cores = cores or os.cpu_count() or 1
+        chunks = [list(range(i, 512, cores)) for i in range(cores)]
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cfg_ref_worker, [(name, c, max_steps, budget_s) for c in chunks])
+        wall = time.perf_counter() - t
+        body_steps = sum(r[0] for r in res)
+        slowest = max(r[1] for r in res)
+        steps = min(r[3] for r in res)
+        return {'value': body_steps / slowest, 'unit': 'body-steps/s', 'cores': cores, 'kind': 'reference',
+                'per_core': body_steps / sum(r[1] for r in res), 'steps': steps,
+                'sample': '%d body-steps: every world from its initial state for its first %d+ steps, '
+                          '%d processes, %.1f s wall' % (body_steps, steps, cores, wall)}
+    with ctx.Pool(1) as pool:
+        done, spent, per_step, steps = pool.map(_cfg_ref_worker, [(name, [0], max_steps, budget_s)])[0]
+    wall = time.perf_counter() - t
+    return {'value': done / spent, 'unit': 'body-steps/s', 'cores': 1, 'kind': 'reference',
+            'per_core': done / spent, 'steps': steps, 'ms_per_step': [1e3 * x for x in per_step],
+            'sample': 'the first %d steps of the run from the initial state, one process (%.1f s wall '
+                      'with the world build)' % (steps, wall)}
+
+
+def run_config(args, rank, world_size, local):
+    """One benchmark configuration over its whole run: the initial state, every
+    step of the run timed on the device (CUDA events around each step, L2
+    flushed between steps), after an untimed warm-up run of the same steps
+    that sizes the pair and contact buffers."""
+    import torch
+    from omi_physics_b200 import scenes
+    from omi_physics_b200._lib import D, U8, ptr
+    from omi_physics_b200.groups import WorldGroups
+    torch.cuda.set_device(local)
+    builder, cfg_steps = scenes.CONFIGS[args.workload]
+    steps = args.config_steps or cfg_steps
+    t0 = time.time()
+    worlds, dts = builder()
+    N = dynamic_bodies(worlds)
+    grp = WorldGroups(worlds, dts=dts, groups=args.groups if len(worlds) > 1 else 1, device=local)
+    snaps = [[b.snapshot(j) for j in range(len(b.worlds))] for b in grp.batches]
+
+    def restore():
+        for b, ss in zip(grp.batches, snaps):
+            for j, sn in enumerate(ss):
+                b.restore(j, sn)
+        torch.cuda.synchronize()
+
+    streams = [torch.cuda.Stream(device=local) for _ in range(len(grp))]
+    grp.set_streams([s.cuda_stream for s in streams])
+    grp.step(steps)                       # warm-up: the whole run once (buffers grow to what it needs)
+    restore()
+    setup_s = time.time() - t0
+    main = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(main)
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device='cuda:%d' % local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = grp.launches()
+    barrier(world_size)
+    with ClockSampler(local) as clk:
+        for e0, e1 in evs:
+            flush.zero_()                 # L2 flushed between timed steps (outside the events)
+            e0.record(main)
+            for s in streams:
+                s.wait_event(e0)
+            grp.step_async(1)
+            for s in streams:
+                ev = torch.cuda.Event()
+                ev.record(s)
+                main.wait_event(ev)
+            e1.record(main)
+        torch.cuda.synchronize()
+    grp.sync()                            # raises if a step overflowed (it cannot: same run as the warm-up)
+    launches = grp.launches() - launches0
+    step_ms = np.array([a.elapsed_time(b) for a, b in evs])
+    total_ms = max_over_ranks(float(step_ms.sum()), world_size)
+    value = sum_over_ranks(N, world_size) * steps / (total_ms / 1e3)
+    pairs, contacts = grp.counts()
+    P, K = int(pairs.sum()), int(contacts.sum())
+    NB = sum(b.packed.n_bodies for b in grp.batches)
+    # roofline of the dominant stage at the end of the run (eager per-stage events, one group after another)
+    prof = {}
+    for _ in range(3):
+        for bt in grp.batches:
+            for k, v in bt.profile().items():
+                prof[k] = prof.get(k, 0.0) + v / 3
+    stage = {g: sum(prof.get(k, 0.0) for k in ks) for g, ks in STAGE_GROUPS.items()}
+    dominant = max(stage, key=stage.get)
+    peaks = json.load(open(MEASURED)) if os.path.exists(MEASURED) else {}
+    peak = float(peaks.get('hbm_gbs', FALLBACK_HBM))
+    alg = algorithmic_bytes(dominant, NB, P, K)
+    achieved = alg / (stage[dominant] / 1e3) / 1e9 if stage[dominant] > 0 else 0.0
+    step_bytes = sum(algorithmic_bytes(g, NB, P, K) for g in STAGE_GROUPS)
+    roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': round(achieved, 3), 'peak': peak,
+                'unit': 'GB/s', 'frac': achieved / peak, 'traffic': None, 'algorithmic_bytes': alg,
+                'kernel_ms': stage[dominant], 'peak_source': 'measured' if 'hbm_gbs' in peaks else 'fallback',
+                'basis': 'per-stage CUDA events of 3 eagerly launched steps at the end of the run',
+                'stage_ms': {k: round(v, 4) for k, v in stage.items()},
+                'kernel_group_ms': {k: round(v, 4) for k, v in prof.items()},
+                'step_algorithmic_bytes': step_bytes,
+                'step_frac': step_bytes / (float(np.mean(step_ms[-20:])) / 1e3) / 1e9 / peak}
+    # e2e: the same run through the C ABI with host buffers every step
+    restore()
+
+    def pinned(shape, dtype=np.float64):
+        return torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.uint8,
+                           pin_memory=True).numpy()
+    bufs = grp.host_buffers(alloc=pinned)
+    for bt, h in zip(grp.batches, bufs):
+        nb = bt.packed.n_bodies
+        bt.ctx.call('download_state', 0, nb, ptr(h['pos'], D), ptr(h['q'], D), ptr(h['v'], D),
+                    ptr(h['w'], D), ptr(h['awake'], U8), ptr(h['timer'], D), None, None)
+    h2d = sum(a.nbytes for h in bufs for a in h.values())
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    grp.step_from_host(bufs, 1, rounds=steps)
+    e2e_s = max_over_ranks(time.perf_counter() - t, world_size)
+    e2e = {'value': sum_over_ranks(N, world_size) * steps / e2e_s, 'unit': 'body-steps/s',
+           'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': h2d,
+           'path': 'the whole run from the initial state, every step: omi_upload_state + omi_step + '
+                   'omi_download_state from pinned memory (per group, groups concurrent)'}
+    grp.close()
+    return dict(value=value, steps=steps, step_ms=step_ms, N=N, NB=NB, P=P, K=K, launches=launches,
+                roofline=roofline, e2e=e2e, clocks=clk.summary(), setup_s=setup_s,
+                worlds=len(worlds))
+
+
+def main_config(args, rank, world_size, local):
+    name = args.workload
+    meta = CONFIG_META[name]
+    metric = 'body-steps/s (%s configuration, whole run)' % name
+    config = {'workload': name, 'scene': meta['desc'], 'dt': meta['dt'], 'iterations': meta['iterations'],
+              'steps': args.config_steps or None, 'l2': 'flushed between timed steps (256 MB write)',
+              'parallelism': 'one GPU' if world_size == 1 else 'replicas x%d' % world_size}
+    from omi_physics_b200 import scenes
+    cfg_steps = args.config_steps or scenes.CONFIGS[name][1]
+    config['steps'] = cfg_steps
+    if args.impl == 'reference':
+        if rank == 0:
+            r = config_cpu_reference(name, cfg_steps, max(5.0, meta['cpu_budget_s']))
+            if r is None:
+                print(json.dumps({'impl': 'reference', 'unavailable':
+                                  'oracle/_ref (the reference built from its sources) is missing'}))
+            else:
+                print(json.dumps({'impl': 'reference', 'metric': metric, 'value': r['value'],
+                                  'unit': 'body-steps/s', 'n_gpus': args.gpus, 'steps': r['steps'],
+                                  'warmup': 0, 'higher_is_better': True, 'scaling': 'weak', 'dtype': 'f64',
+                                  'data': 'synthetic', 'config': config,
+                                  'cpu_baseline': {k: r[k] for k in ('value', 'unit', 'cores', 'kind',
+                                                                     'sample', 'per_core')},
+                                  'e2e': {'value': r['value'], 'unit': 'body-steps/s',
+                                          'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}))
+        return
+    res = run_config(args, rank, world_size, local)
+    if rank != 0:
+        return
+    sm = res['step_ms']
+    line = {'metric': metric, 'value': res['value'], 'unit': 'body-steps/s', 'n_gpus': world_size,
+            'steps': res['steps'], 'warmup': res['steps'], 'ms_per_step': float(sm.mean()),
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic (seeded %s scene)' % name, 'config': config, 'e2e': res['e2e'],
+            'roofline': res['roofline'], 'clocks': res['clocks'], 'gpu_launches': res['launches'],
+            'step_latency_ms': {'p50': float(np.percentile(sm, 50)), 'p99': float(np.percentile(sm, 99)),
+                                'max': float(sm.max()), 'first': float(sm[0])},
+            'dynamic_bodies': res['N'], 'worlds': res['worlds'], 'final_pairs': res['P'],
+            'final_contacts': res['K']}
+    if not args.no_extras:
+        cb = config_cpu_reference(name, res['steps'], CONFIG_META[name]['cpu_budget_s'])
+        if cb is not None:
+            line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'per_core')}
+            k = cb['steps']
+            win = float(sm[:k].sum())
+            line['gpu_same_window'] = {'steps': k, 'value': res['N'] * k / (win / 1e3), 'unit': 'body-steps/s',
+                                       'note': 'device time of the same first steps the CPU sample ran'}
+            line['same_window_over_cpu'] = line['gpu_same_window']['value'] / cb['value']
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local = dist_init(args.gpus)
+    if args.workload != 'serving-mix':
+        main_config(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     metric = 'body-steps/s (batched serving mix, 1 B200 per rank)'
-    config = {'workload': 'serving-mix', 'worlds_per_gpu': args.worlds,
+    config = {'workload': 'serving-mix',
+              ('worlds' if args.scaling == 'strong' else 'worlds_per_gpu'): args.worlds,
               'bodies': 'log-uniform [16,2048] per world, debris contents', 'dt': '1/120 s',
               'iterations': 8, 'l2': 'inputs larger than L2 (arena state > 126 MB)',
-              'parallelism': 'world-sharded x%d (no data-path collective)' % world,
+              'parallelism': ('one mix split across %d GPUs by body-count bin-packing' % world
+                              if args.scaling == 'strong' else
+                              'world-sharded x%d (no data-path collective)' % world),
               'groups_per_gpu': args.groups}
     if args.impl == 'reference':
         if rank == 0:
@@ -641,7 +919,7 @@ def main():
             else:
                 line = {'impl': 'reference', 'metric': metric, 'value': r['value'],
                         'unit': 'body-steps/s', 'n_gpus': args.gpus, 'steps': args.steps,
-                        'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+                        'warmup': args.warmup, 'higher_is_better': True, 'scaling': args.scaling,
                         'dtype': 'f64', 'data': 'synthetic', 'config': config,
                         'cpu_baseline': {k: r[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'per_core')},
                         'e2e': {'value': r['value'], 'unit': 'body-steps/s',
@@ -662,7 +940,7 @@ def main():
         line = {
             'metric': metric, 'value': res['value'], 'unit': 'body-steps/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms'] / args.steps,
-            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'higher_is_better': True, 'scaling': args.scaling, 'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic (seeded serving-mix scenes)', 'config': config,
             'e2e': res['e2e'], 'roofline': res['roofline'], 'clocks': res['clocks'],
             'gpu_launches': res['launches'],

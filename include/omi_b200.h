@@ -336,7 +336,9 @@ int omi_capsule_triangles_device(OmiCtx *ctx, int32_t q, const double *caps, con
  * n_bodies may not exceed OMI_NOALLOC_MAX_BODIES: larger worlds are refused
  * with OMI_E_ARG and a message in err (err_cap bytes, may be NULL). The first
  * call on each device looks that array's device address up (once per device,
- * with the device current); make that first call before any stream capture.
+ * with the device current, serialised between host threads); make that first
+ * call before any stream capture, and do not call it on a device after a
+ * cudaDeviceReset there (the looked-up address belonged to the old context).
  * Every call shares the one array, so calls whose work overlaps on the GPU
  * (other streams, other host threads) race and must be serialised by the
  * caller. No call allocates or frees memory.

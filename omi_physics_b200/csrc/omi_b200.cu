@@ -7,7 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1799,11 +1801,17 @@ constexpr size_t NA_BYTES = NA_OFF_WORLD + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
+// Per-device address of the array, looked up on the first call on that
+// device. Host threads calling at once are serialised by the mutex during
+// that set-up only; afterwards the ready flag (acquire) guards the address.
+// cudaDeviceReset on a device ends the context the address belongs to: call
+// omi_sweep_pairs_noalloc on that device only in the context it was set up in.
 struct NaDevice {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     unsigned char *base = nullptr;
 };
 NaDevice g_na_dev[64];
+std::mutex g_na_setup;
 
 void na_err(char *err, int cap, const std::string &msg) {
     if (err && cap > 0) {
@@ -1885,22 +1893,25 @@ extern "C" int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aab
         return OMI_E_CUDA;
     }
     NaDevice &nd = g_na_dev[dev];
-    if (!nd.ready) {   // set-up, once per device, with that device current
-        void *addr = nullptr;
-        e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-        if (e != cudaSuccess || !addr) {
-            na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaGetSymbolAddress: ") +
-                                     cudaGetErrorString(e));
-            return OMI_E_CUDA;
+    if (!nd.ready.load(std::memory_order_acquire)) {   // set-up, once per device, with that device current
+        std::lock_guard<std::mutex> lock(g_na_setup);
+        if (!nd.ready.load(std::memory_order_relaxed)) {
+            void *addr = nullptr;
+            e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (e != cudaSuccess || !addr) {
+                na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaGetSymbolAddress: ") +
+                                         cudaGetErrorString(e));
+                return OMI_E_CUDA;
+            }
+            e = cudaFuncSetAttribute(k_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
+            if (e != cudaSuccess) {
+                na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaFuncSetAttribute: ") +
+                                         cudaGetErrorString(e));
+                return OMI_E_CUDA;
+            }
+            nd.base = static_cast<unsigned char *>(addr);
+            nd.ready.store(true, std::memory_order_release);
         }
-        e = cudaFuncSetAttribute(k_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 24);
-        if (e != cudaSuccess) {
-            na_err(err, err_cap, std::string("omi_sweep_pairs_noalloc: cudaFuncSetAttribute: ") +
-                                     cudaGetErrorString(e));
-            return OMI_E_CUDA;
-        }
-        nd.base = static_cast<unsigned char *>(addr);
-        nd.ready = true;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream_v);
     unsigned char *base = nd.base;

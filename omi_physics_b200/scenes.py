@@ -677,3 +677,28 @@ def serving_world(req: dict, api=None, backend=None):
     ext = max(2.0, 20.0 * (n / 4096.0) ** (1.0 / 3.0))
     return debris(api, backend, n=n, seed=req['seed'], extent=ext, height=1.5 * ext,
                   ground=3.0 * ext)
+
+
+def joint_chains(n_worlds: int = 512, seed: int = 21, api=None, backend=None, which=None):
+    """The batched joints configuration: ``n_worlds`` chains of 16-128 links
+    (point joints, 10% with an angular motor) under 64-512 loose boxes,
+    1/240 s, 12 contact and 12 joint iterations. Returns ``(worlds, dts)``;
+    ``which`` (indices) builds only those worlds of the configuration."""
+    rng = np.random.default_rng(seed)
+    sizes = [(int(rng.integers(16, 129)), int(rng.integers(64, 513))) for _ in range(n_worlds)]
+    worlds, dts = [], []
+    for k in (range(n_worlds) if which is None else which):
+        w, meta = joint_chain(api, backend, links=sizes[k][0], loose=sizes[k][1], seed=1000 + k)
+        worlds.append(w)
+        dts.append(meta['dt'])
+    return worlds, dts
+
+
+#: the benchmark configurations other than the serving mix: builder of
+#: ``(worlds, dts)``, the configuration's step count, and whether it is one world
+CONFIGS = {
+    'pyramid': (lambda api=None: (lambda r: ([r[0]], [r[1]['dt']]))(pyramid(api)), 120),
+    'debris4096': (lambda api=None: (lambda r: ([r[0]], [r[1]['dt']]))(debris(api, n=4096, seed=0)), 600),
+    'convex32768': (lambda api=None: (lambda r: ([r[0]], [r[1]['dt']]))(convex_pile(api, n=32768, seed=0)), 300),
+    'joints512': (lambda api=None: joint_chains(512, 21, api), 480),
+}

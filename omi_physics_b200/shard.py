@@ -38,6 +38,61 @@ def local_shard(body_counts: Sequence[int], rank: int, world_size: int) -> List[
     return plan_shards(body_counts, world_size)[rank]
 
 
+def shard_requests(requests: Sequence[dict], rank: int, world_size: int) -> List[int]:
+    """Indices of the serving requests this rank admits: the same LPT plan
+    over the requests' body counts, so one request stream is split across
+    GPUs without any rank seeing another's worlds."""
+    return local_shard([int(r['bodies']) for r in requests], rank, world_size)
+
+
+class ShardedWorlds:
+    """One fixed list of worlds split across ranks: this rank's shard stepped
+    as :class:`~omi_physics_b200.groups.WorldGroups` on its own GPU.
+
+    ``body_counts`` are every world's body counts and ``build(i)`` returns
+    world ``i`` and its dt; each rank builds only its own worlds. ``indices``
+    are the global indices of the local worlds (ascending). Every rank
+    computes the same plan from the body counts, so nothing is exchanged to
+    build it, and stepping involves no collective: only the host-side
+    bookkeeping (the job's step time, totals, merged tick latencies) crosses
+    ranks.
+    """
+
+    def __init__(self, body_counts: Sequence[int], build, rank: int, world_size: int,
+                 groups: int = 4, device: int = 0, load: bool = True):
+        self.rank, self.world_size = rank, world_size
+        self.plan = plan_shards(body_counts, world_size)
+        self.indices = self.plan[rank]
+        built = [build(i) for i in self.indices]
+        self.worlds = [w for w, _ in built]
+        self.dts = [dt for _, dt in built]
+        self.local_bodies = int(sum(int(np.count_nonzero(w.motion_type == 2)) for w in self.worlds))
+        self.groups = None
+        if load and self.worlds:
+            from .groups import WorldGroups
+            self.groups = WorldGroups(self.worlds, dts=self.dts, groups=groups, device=device)
+
+    def step(self, n: int = 1) -> None:
+        if self.groups is not None:
+            self.groups.step(n)
+
+    def close(self) -> None:
+        if self.groups is not None:
+            self.groups.close()
+
+
+def merge_ticks(ticks: Sequence[float], world_size: int) -> List[float]:
+    """Per-tick latency of the job from each rank's per-tick latencies: a
+    tick ends when its slowest rank's does (element-wise max over ranks)."""
+    if world_size == 1:
+        return [float(t) for t in ticks]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x) for x in ticks], dtype=torch.float64, device=_device())
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().tolist()
+
+
 def _device():
     import torch
     import torch.distributed as dist

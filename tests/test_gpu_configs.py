@@ -170,13 +170,8 @@ def test_joint_chains_512_worlds_full_size():
     at step 120 (within 1e-6, point joints matching LAPACK to ~1e-12 per
     solve) and all 512 pass size-independent checks at step 480 (finite
     state, unit quaternions, sleeping dynamic bodies at rest)."""
-    rng = np.random.default_rng(21)
-    worlds, dts = [], []
-    for k in range(512):
-        w, meta = scenes.joint_chain(links=int(rng.integers(16, 129)), loose=int(rng.integers(64, 513)),
-                                     seed=1000 + k)
-        worlds.append(w)
-        dts.append(meta['dt'])
+    worlds, dts = scenes.joint_chains(512, seed=21)
+    rng = np.random.default_rng(22)
     sample = sorted(int(i) for i in rng.choice(512, size=16, replace=False))
     oracles = {i: pyoracle.OracleWorld.from_world(worlds[i]) for i in sample}
     b = WorldBatch(worlds, dts=dts)

@@ -36,19 +36,22 @@ def _ref_api():
 @pytest.mark.parametrize('scene,steps', [('pyramid', 60), ('debris', 60), ('spheres', 60),
                                          ('capsules', 30), ('zones', 60), ('terrain', 40),
                                          ('conveyor', 40), ('degenerate', 140),
-                                         ('rods', 60)])
+                                         ('rods', 60), ('convex', 60), ('chain', 60)])
 def test_reference_world_steps_on_cuda_backend(scene, steps):
     from omi_physics_b200.backend import CudaBackend
     api = _ref_api()
     gpu, meta = scenes.GOLDEN_SCENES[scene](api, CudaBackend())
     cpu, _ = scenes.GOLDEN_SCENES[scene](api)
-    dt = meta['dt']
+    _step_twins(gpu, cpu, meta['dt'], steps, scene)
+
+
+def _step_twins(gpu, cpu, dt, steps, scene, first=0):
     assert gpu.backend.name == 'cuda' and gpu._backend_mode == 'fixed'
     n = cpu.body_count
     gev, cev = [], []
     gpu.add_trigger_listener(lambda *e: gev.append(e))
     cpu.add_trigger_listener(lambda *e: cev.append(e))
-    for s in range(steps):
+    for s in range(first, first + steps):
         gev.clear()
         cev.clear()
         gpu.step(dt)
@@ -82,3 +85,27 @@ def test_reference_empty_world_on_cuda_backend():
     assert gpu.body_count == cpu.body_count == 0
     assert len(gpu.contacts) == len(cpu.contacts) == 0
     assert gpu.time == cpu.time
+
+
+def test_body_added_mid_run_through_the_drop_in():
+    """A topology change between steps: both twins get the same new bodies
+    after 25 steps (a box dropped onto the pile and a sphere resting on the
+    ground), the CUDA backend reloads its arena and carries the warm-start
+    cache over as the reference's solver keeps it (indices do not move,
+    solver.py:91, 272-278), and the twins keep agreeing for 45 more steps."""
+    from omi_physics_b200.backend import CudaBackend
+    api = _ref_api()
+    m = api.model
+    gpu, meta = scenes.GOLDEN_SCENES['debris'](api, CudaBackend())
+    cpu, _ = scenes.GOLDEN_SCENES['debris'](api)
+    dt = meta['dt']
+    _step_twins(gpu, cpu, dt, 25, 'debris before add')
+    for w in (gpu, cpu):
+        box = w.add_shape(m.Shape.box((0.8, 0.6, 1.1)))
+        ball = w.add_shape(m.Shape.sphere(0.4))
+        mat = w.add_material(m.Material(staticFriction=0.6, dynamicFriction=0.6))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=400.0), m.Collider(shape=box, physicsMaterial=mat),
+                   position=(0.3, 4.0, -0.2))
+        w.add_body(m.Motion(type=m.DYNAMIC, mass=250.0), m.Collider(shape=ball, physicsMaterial=mat),
+                   position=(2.0, 0.45, 1.5))
+    _step_twins(gpu, cpu, dt, 45, 'debris after add', first=25)
