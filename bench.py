@@ -64,8 +64,11 @@ def parse():
                     help='capsule-triangle workload: blocks of 1024 capsules x 256 triangles (0 skips it)')
     ap.add_argument('--capsule-only', action='store_true',
                     help='run only the capsule-triangle measurement (device part) and print it')
-    ap.add_argument('--groups', type=int, default=4,
-                    help='worlds are stepped as this many concurrent groups (one context + stream each)')
+    ap.add_argument('--groups', type=int, default=None,
+                    help='worlds are stepped as this many concurrent groups (one context + stream each); '
+                         'default: the autotuner\'s cached choice for this GPU and workload, else 4')
+    ap.add_argument('--tune', action='store_true',
+                    help='run the autotuner on the workload first (and cache its choice)')
     ap.add_argument('--workload', default='serving-mix',
                     choices=['serving-mix', 'pyramid', 'debris4096', 'convex32768', 'joints512'],
                     help='serving-mix (default): the batched headline; the others time one benchmark '
@@ -255,6 +258,9 @@ def run_ours(args, rank, world, local):
         reqs = [reqs[i] for i in sw.indices]
     else:
         reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
+        if args.tune:
+            from omi_physics_b200 import tune
+            tune.autotune(worlds, device=local)
         grp = WorldGroups(worlds, groups=args.groups, device=local)
     grp.step(args.preroll)
     setup_s = time.time() - t0
@@ -384,7 +390,14 @@ def run_ours(args, rank, world, local):
     grp.close()
     return dict(value=value, ms=ms_max, N=total_N, P=P, K=K, launches=launches, setup_s=setup_s,
                 ticks=ticks, roofline=roofline, e2e=e2e, clocks=clk.summary(), extras=extras,
-                NB=NB)
+                NB=NB, tuning=_tuning_note(grp))
+
+
+def _tuning_note(grp):
+    """Which launch configuration and group count ran, and where they came from."""
+    launch = grp.batches[0].ctx.tuning() if grp.batches else {}
+    return {'groups': len(grp.batches), 'launch': launch,
+            'source': 'autotuner cache' if grp.tuned is not None else 'library defaults'}
 
 
 SERVE_BUDGET = 120 * 10 ** 9
@@ -752,6 +765,9 @@ def run_config(args, rank, world_size, local):
     t0 = time.time()
     worlds, dts = builder()
     N = dynamic_bodies(worlds)
+    if args.tune:
+        from omi_physics_b200 import tune
+        tune.autotune(worlds, dts, device=local)
     grp = WorldGroups(worlds, dts=dts, groups=args.groups if len(worlds) > 1 else 1, device=local)
     snaps = [[b.snapshot(j) for j in range(len(b.worlds))] for b in grp.batches]
 
@@ -834,10 +850,11 @@ def run_config(args, rank, world_size, local):
            'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': h2d,
            'path': 'the whole run from the initial state, every step: omi_upload_state + omi_step + '
                    'omi_download_state from pinned memory (per group, groups concurrent)'}
+    note = _tuning_note(grp)
     grp.close()
     return dict(value=value, steps=steps, step_ms=step_ms, N=N, NB=NB, P=P, K=K, launches=launches,
                 roofline=roofline, e2e=e2e, clocks=clk.summary(), setup_s=setup_s,
-                worlds=len(worlds))
+                worlds=len(worlds), tuning=note)
 
 
 def main_config(args, rank, world_size, local):
@@ -878,7 +895,7 @@ def main_config(args, rank, world_size, local):
             'step_latency_ms': {'p50': float(np.percentile(sm, 50)), 'p99': float(np.percentile(sm, 99)),
                                 'max': float(sm.max()), 'first': float(sm[0])},
             'dynamic_bodies': res['N'], 'worlds': res['worlds'], 'final_pairs': res['P'],
-            'final_contacts': res['K']}
+            'final_contacts': res['K'], 'tuning': res['tuning']}
     if not args.no_extras:
         cb = config_cpu_reference(name, res['steps'], CONFIG_META[name]['cpu_budget_s'])
         if cb is not None:
@@ -908,7 +925,7 @@ def main():
               'parallelism': ('one mix split across %d GPUs by body-count bin-packing' % world
                               if args.scaling == 'strong' else
                               'world-sharded x%d (no data-path collective)' % world),
-              'groups_per_gpu': args.groups}
+              'groups_per_gpu': args.groups or 'autotuned (else 4)'}
     if args.impl == 'reference':
         if rank == 0:
             budget = max(5.0, args.cpu_sample_s)
@@ -947,6 +964,7 @@ def main():
             'tick_latency_ms': {'p50': float(np.percentile(ticks, 50)),
                                 'p99': float(np.percentile(ticks, 99))},
             'dynamic_bodies': res['N'], 'rows': res['NB'], 'pairs': res['P'], 'contacts': res['K'],
+            'tuning': res['tuning'],
         }
         ex = res['extras']
         if 'serving' in ex:

@@ -161,6 +161,20 @@ int64_t omi_device_bytes(OmiCtx *ctx);
  * every world (-1 = none), so a test can make a wait run out. 0 restores a
  * default. Applies to the next step (the step graph is re-captured). */
 int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t stall_run);
+/* Launch configuration of the step's kernels (no counterpart in the
+ * reference): results do not depend on it, only speed, so an autotuner may
+ * pick it per GPU and workload. sweep_warps = warps per contact-sweep block
+ * (4 or 8), sweep_max_split = sweep groups a block may split into once its
+ * worlds are small (1, 2, 4), pair_block / pair_blocks_per_sm = block size
+ * (128/256/512) and blocks per SM (1-32) of the pair count and emit passes,
+ * narrow_block = block size of the analytic narrowphase and clipping (64,
+ * 128, 256), gjk_warps = warps (one pair each) per GJK/EPA block (2, 4, 8).
+ * Defaults: 8, 4, 256, 16, 128, 4. A change re-captures the step graph. */
+typedef struct OmiTuning {
+    int32_t sweep_warps, sweep_max_split, pair_block, pair_blocks_per_sm, narrow_block, gjk_warps;
+} OmiTuning;
+int omi_set_tuning(OmiCtx *ctx, const OmiTuning *tuning);
+int omi_get_tuning(OmiCtx *ctx, OmiTuning *tuning);
 /* Check a scene the way omi_load does, on the host only (no device, no
  * context): every index a kernel would follow is range-checked. Returns 0 or
  * the status omi_load would return, with the message in err (err_cap bytes,

@@ -86,6 +86,19 @@ class OmiSlotCaps(C.Structure):
                                           'filter_rows', 'pair_friction')]
 
 
+class OmiTuning(C.Structure):
+    """Mirror of ``struct OmiTuning`` (the step's launch configuration)."""
+    _fields_ = [(n, C.c_int32) for n in ('sweep_warps', 'sweep_max_split', 'pair_block',
+                                          'pair_blocks_per_sm', 'narrow_block', 'gjk_warps')]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+#: the library's default launch configuration
+DEFAULT_TUNING = dict(sweep_warps=8, sweep_max_split=4, pair_block=256, pair_blocks_per_sm=16,
+                      narrow_block=128, gjk_warps=4)
+
 #: every symbol include/omi_b200.h declares, with (restype, argtypes)
 PROTOTYPES = {
     'omi_create': (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -96,6 +109,8 @@ PROTOTYPES = {
     'omi_device_bytes': (C.c_int64, [C.c_void_p]),
     'omi_set_limits': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     'omi_validate_scene': (C.c_int, [C.POINTER(OmiScene), C.c_char_p, C.c_int32]),
+    'omi_set_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
+    'omi_get_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
     'omi_load': (C.c_int, [C.c_void_p, C.POINTER(OmiScene)]),
     'omi_set_active': (C.c_int, [C.c_void_p, U8]),
     'omi_set_world_params': (C.c_int, [C.c_void_p, D, I, I, I]),
@@ -230,6 +245,19 @@ class Context:
         """Lower the sweep's wait bound or the EPA face bound, or stall one run
         (tests of the failure paths); zeros restore the defaults."""
         self.call('set_limits', int(spin_limit), int(epa_faces), int(stall_run))
+
+    def set_tuning(self, **cfg) -> None:
+        """Set the launch configuration (keys of :data:`DEFAULT_TUNING`; missing
+        keys keep their current values)."""
+        cur = self.tuning()
+        cur.update(cfg)
+        t = OmiTuning(**{k: int(cur[k]) for k in DEFAULT_TUNING})
+        self.call('set_tuning', C.byref(t))
+
+    def tuning(self) -> dict:
+        t = OmiTuning()
+        self.call('get_tuning', C.byref(t))
+        return t.as_dict()
 
     def profile_step(self):
         """Per-kernel-group device time (ms) of one eagerly launched step."""

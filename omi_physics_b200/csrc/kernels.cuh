@@ -1752,7 +1752,7 @@ __device__ __forceinline__ void sweep_push(int *ring, SweepShared &sh, int e, in
 // world's velocities, its contacts' impulses, then the work ring (else the
 // global arrays).
 // ---------------------------------------------------------------------------
-constexpr int SWEEP_WARPS = 8;
+constexpr int SWEEP_WARPS = 8;                  // default warps per sweep block (4 is the other choice)
 constexpr int SWEEP_THREADS = 32 * SWEEP_WARPS;
 
 // barrier over the `n` threads of barrier `id` (0 = the whole block)
@@ -1970,11 +1970,15 @@ __device__ __forceinline__ int sweep_take(const Arena &A) {
     }
 }
 
-__global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_doubles) {
+// WARPS warps per block (a launch-configuration choice); max_split caps the
+// groups a block splits into (1, 2 or 4)
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_iterate(Arena A, int smem_doubles, int max_split) {
     extern __shared__ __align__(16) double smem_d[];
     __shared__ SweepShared sh[SWEEP_MAX_GROUPS];
     __shared__ int pick[1 + SWEEP_MAX_GROUPS];    // split (0: done), world per group
     if (overflowed(A)) return;
+    constexpr int THREADS = 32 * WARPS;
     const int tid = threadIdx.x;
     int G;
     for (;;) {
@@ -1983,7 +1987,9 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_dou
             int g = 0;
             if (w >= 0) {
                 const int want = sweep_want(A, w);
-                g = want <= ((smem_doubles / 4) & ~1) ? 4 : (want <= ((smem_doubles / 2) & ~1) ? 2 : 1);
+                g = (max_split >= 4 && want <= ((smem_doubles / 4) & ~1)) ? 4
+                    : ((max_split >= 2 && want <= ((smem_doubles / 2) & ~1)) ? 2 : 1);
+                g = min(g, WARPS);                  // at least one warp per group
             }
             pick[0] = g;
             pick[1] = w;
@@ -1992,11 +1998,11 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_iterate(Arena A, int smem_dou
         G = pick[0];
         if (G == 0) return;
         if (G > 1) break;
-        sweep_world(A, pick[1], smem_d, smem_doubles, tid, SWEEP_THREADS, 0, sh[0]);
+        sweep_world(A, pick[1], smem_d, smem_doubles, tid, THREADS, 0, sh[0]);
         __syncthreads();
     }
     // split for good: group g sweeps its own worlds on named barrier 1 + g
-    const int gn = SWEEP_THREADS / G, g = tid / gn, gtid = tid - g * gn;
+    const int gn = THREADS / G, g = tid / gn, gtid = tid - g * gn;
     const int share = (smem_doubles / G) & ~1;
     int w = g == 0 ? pick[1] : -1;
     for (;;) {

@@ -86,6 +86,7 @@ struct OmiCtx {
     int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
     // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
     int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
+    OmiTuning tune = {8, 4, 256, 16, 128, 4};   // launch configuration (omi_set_tuning)
 };
 
 namespace {
@@ -285,14 +286,16 @@ void stage_broadphase(OmiCtx *ctx, Prof *pf) {
     k_sort<true><<<std::min(A.W, 65535), ctx->sort_block, smem, ctx->stream>>>(A, ctx->sort_cap);
     ctx->launches++;
     mark(ctx, pf, KN_SORT);
-    k_pair_count<<<grid_for(A.NB * 32, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    const OmiTuning &t = ctx->tune;
+    const int pgrid = grid_for(A.NB * 32, t.pair_block, ctx->sm_count * t.pair_blocks_per_sm);
+    k_pair_count<<<pgrid, t.pair_block, 0, ctx->stream>>>(A);
     ctx->launches++;
     mark(ctx, pf, KN_PAIR_COUNT);
     launch_scan(ctx, A.pair_cnt, A.pair_scan, A.NB, nullptr, A.NB, nullptr, 0, 0);
     k_pair_check<<<1, 1, 0, ctx->stream>>>(A);
     ctx->launches++;
     mark(ctx, pf, KN_PAIR_SCAN);
-    k_pair_emit<<<grid_for(A.NB * 32, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
+    k_pair_emit<<<pgrid, t.pair_block, 0, ctx->stream>>>(A);
     ctx->launches++;
     mark(ctx, pf, KN_PAIR_EMIT);
 }
@@ -303,11 +306,12 @@ void stage_narrow(OmiCtx *ctx, Prof *pf) {
         k_mesh_refresh<<<std::min(ctx->moving_meshes, 148), MESH_REFRESH_THREADS, 0, ctx->stream>>>(A, ctx->moving_meshes);
         ctx->launches++;
     }
-    k_narrow<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
-    k_clip<<<grid_for(A.pair_cap, 128, SM_CAP), 128, 0, ctx->stream>>>(A);
+    const int nb = ctx->tune.narrow_block, gw = ctx->tune.gjk_warps;
+    k_narrow<<<grid_for(A.pair_cap, nb, SM_CAP), nb, 0, ctx->stream>>>(A);
+    k_clip<<<grid_for(A.pair_cap, nb, SM_CAP), nb, 0, ctx->stream>>>(A);
     ctx->launches += 2;
     mark(ctx, pf, KN_NARROW);
-    k_gjk<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
+    k_gjk<<<ctx->sm_count * (16 / gw), 32 * gw, gw * sizeof(EpaWork), ctx->stream>>>(A);
     ctx->launches++;
     if (ctx->has_meshes) {
         k_mesh_count<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
@@ -339,7 +343,13 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     mark(ctx, pf, KN_PREP);
     k_levels<<<std::min(A.W, 65535), LEVEL_THREADS, (size_t)ctx->level_ints * sizeof(int), ctx->stream>>>(A, ctx->level_ints);
     mark(ctx, pf, KN_LEVELS);
-    k_iterate<<<std::min(A.W, ctx->sm_count), SWEEP_THREADS, (size_t)ctx->stage_doubles * sizeof(double), ctx->stream>>>(A, ctx->stage_doubles);
+    const size_t sweep_smem = (size_t)ctx->stage_doubles * sizeof(double);
+    if (ctx->tune.sweep_warps == 4)
+        k_iterate<4><<<std::min(A.W, ctx->sm_count), 128, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles,
+                                                                                     ctx->tune.sweep_max_split);
+    else
+        k_iterate<8><<<std::min(A.W, ctx->sm_count), 256, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles,
+                                                                                     ctx->tune.sweep_max_split);
     ctx->launches += 4;
     mark(ctx, pf, KN_SOLVE);
     if (ctx->has_triggers) {
@@ -519,12 +529,13 @@ int omi_create(int device, OmiCtx **out) {
     e = cudaMallocHost(&ctx->h_status, sizeof(int) * ST_WORDS);
     if (e != cudaSuccess) { int rc = cuda_fail(ctx, e, "cudaMallocHost"); *out = ctx; return rc; }
     const struct { const void *fn; int bytes; const char *name; } smem[] = {
-        {(const void *)k_gjk, 4 * (int)sizeof(EpaWork), "k_gjk"},
+        {(const void *)k_gjk, 8 * (int)sizeof(EpaWork), "k_gjk"},
         {(const void *)k_triggers, 4 * (int)sizeof(EpaWork), "k_triggers"},
         {(const void *)k_mesh_count, 4 * (int)sizeof(EpaWork), "k_mesh_count"},
         {(const void *)k_mesh_emit, 4 * (int)sizeof(EpaWork), "k_mesh_emit"},
         {(const void *)k_sort<true>, 8192 * 24, "k_sort"},
-        {(const void *)k_iterate, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate"},
+        {(const void *)k_iterate<8>, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate<8>"},
+        {(const void *)k_iterate<4>, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_iterate<4>"},
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
         {(const void *)k_finalize, 2 * 8192 * (int)sizeof(int), "k_finalize"},
         {(const void *)k_prep, PREP_THREADS * CD * (int)sizeof(double), "k_prep"},
@@ -1301,6 +1312,27 @@ int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t s
         ctx->A.epa_faces = ctx->epa_faces;
         ctx->A.stall_run = ctx->stall_run;
     }
+    return 0;
+}
+
+int omi_set_tuning(OmiCtx *ctx, const OmiTuning *t) {
+    if (!ctx || !t) return OMI_E_ARG;
+    const bool ok = (t->sweep_warps == 4 || t->sweep_warps == 8) &&
+                    (t->sweep_max_split == 1 || t->sweep_max_split == 2 || t->sweep_max_split == 4) &&
+                    (t->pair_block == 128 || t->pair_block == 256 || t->pair_block == 512) &&
+                    t->pair_blocks_per_sm >= 1 && t->pair_blocks_per_sm <= 32 &&
+                    (t->narrow_block == 64 || t->narrow_block == 128 || t->narrow_block == 256) &&
+                    (t->gjk_warps == 2 || t->gjk_warps == 4 || t->gjk_warps == 8);
+    if (!ok) return fail(ctx, OMI_E_ARG, "launch configuration out of range");
+    cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);                     // re-captured with the new launches on the next step
+    ctx->tune = *t;
+    return 0;
+}
+
+int omi_get_tuning(OmiCtx *ctx, OmiTuning *t) {
+    if (!ctx || !t) return OMI_E_ARG;
+    *t = ctx->tune;
     return 0;
 }
 

@@ -13,7 +13,7 @@ releases the GIL and each context belongs to one thread); ``step_async`` +
 ``sync`` enqueue on all groups' streams from the calling thread.
 """
 from concurrent.futures import ThreadPoolExecutor
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -32,15 +32,43 @@ def plan_groups(body_counts: Sequence[int], groups: int) -> List[List[int]]:
 
 
 class WorldGroups:
-    """``worlds`` split into ``groups`` batches stepped concurrently on one GPU."""
+    """``worlds`` split into ``groups`` batches stepped concurrently on one GPU.
 
-    def __init__(self, worlds: Sequence, dts: Sequence[float] = None, groups: int = 4, device: int = 0):
+    ``tuning='auto'`` (the default) applies the autotuner's cached entry for
+    this GPU and workload (:func:`omi_physics_b200.tune.tuned_for`): its
+    launch configuration, and its group count when ``groups`` is None; with
+    no entry the defaults stand (4 groups). ``tuning`` may also be a dict of
+    launch parameters, or None for the library defaults. ``own_streams``
+    gives every group a torch stream of its own (``stream_handles``)."""
+
+    def __init__(self, worlds: Sequence, dts: Sequence[float] = None, groups: Optional[int] = None,
+                 device: int = 0, tuning='auto', own_streams: bool = False):
         self.worlds = list(worlds)
         dts = list(dts) if dts is not None else [w.fixed_dt for w in self.worlds]
+        launch = None
+        self.tuned = None
+        if tuning == 'auto':
+            from .tune import tuned_for
+            self.tuned = tuned_for(self.worlds, device)
+            if self.tuned is not None:
+                launch = self.tuned.get('launch')
+                if groups is None:
+                    groups = int(self.tuned.get('groups', 4))
+        elif isinstance(tuning, dict):
+            launch = tuning
+        if groups is None:
+            groups = 4
         self.plan = plan_groups([w.body_count for w in self.worlds], max(1, groups))
         self.batches = [WorldBatch([self.worlds[i] for i in g], device=device, dts=[dts[i] for i in g])
                         for g in self.plan]
-        self._pool = ThreadPoolExecutor(max_workers=len(self.batches))
+        self._pool = ThreadPoolExecutor(max_workers=max(1, len(self.batches)))
+        self.stream_handles = []
+        if own_streams:
+            import torch
+            self._streams = [torch.cuda.Stream(device=device) for _ in self.batches]
+            self.set_streams([s.cuda_stream for s in self._streams])
+        if launch:
+            self.set_tuning(launch)
         # world index -> (group, index in group)
         self.where = {}
         for gi, g in enumerate(self.plan):
@@ -52,8 +80,14 @@ class WorldGroups:
 
     def set_streams(self, streams: Sequence[int]) -> None:
         """Put each group's launches on the given cudaStream_t handles."""
+        self.stream_handles = [int(s) for s in streams]
         for b, s in zip(self.batches, streams):
             b.ctx.call('set_stream', int(s))
+
+    def set_tuning(self, launch: dict) -> None:
+        """The same launch configuration for every group (keys of DEFAULT_TUNING)."""
+        for b in self.batches:
+            b.ctx.set_tuning(**launch)
 
     # -- stepping ---------------------------------------------------------------
     def _each(self, fn):
@@ -127,4 +161,7 @@ class WorldGroups:
         return sum(b.ctx.launches() for b in self.batches)
 
     def close(self):
+        """Stop the host threads and release every group's context."""
         self._pool.shutdown(wait=True)
+        for b in self.batches:
+            b.ctx.close()

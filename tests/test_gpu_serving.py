@@ -84,3 +84,37 @@ def test_serving_an_omi_document():
                                 'sleep_timer')):
         assert np.array_equal(getattr(req.world, col)[:n], st[key]), col
     srv.close()
+
+
+def test_full_class_spills_into_new_chunks_under_budget_and_waits_over_it():
+    """One 2-slot class and a budget of about two and a half such arenas: the
+    first chunk fills, the third request spills into a second chunk reserved
+    on demand, the next reservation would pass the budget so the fifth and
+    sixth requests wait for a slot to free up. Every result still equals the
+    world stepped alone."""
+    from omi_physics_b200.serving import SlotClass
+    probe = Server([SlotClass(bodies=65, count=2)])
+    one = probe.device_bytes()
+    probe.close()
+    srv = Server([SlotClass(bodies=65, count=2)], budget_bytes=int(2.5 * one))
+    assert srv.grow
+    reqs = scenes.serving_requests(6, seed=11, n_min=20, n_max=60)
+    subs = []
+    for i, r in enumerate(reqs):
+        w, meta = scenes.serving_world(r)
+        subs.append((r, srv.submit(w, 12 + i, dt=meta['dt'], arrival=0)))
+    stats = srv.run(clock='ticks')
+    assert stats.completed == 6
+    assert stats.chunks_added == 1 and len(srv.chunks) == 2 and srv.W == 4
+    assert stats.peak_active == 4                       # capacity grew past the first class
+    assert sum(1 for wt in stats.wait_ms if wt > 0) == 2   # over budget: two requests waited
+    assert srv.device_bytes() <= 2.5 * one
+    for r, q in subs:
+        w, meta = scenes.serving_world(r)
+        b = WorldBatch([w], dts=[meta['dt']])
+        b.step(q.steps)
+        b.sync_to_host()
+        for col in STATE:
+            assert np.array_equal(getattr(q.world, col)[:w.body_count], getattr(w, col)[:w.body_count]), \
+                (q.rid, col)
+    srv.close()

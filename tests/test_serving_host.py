@@ -52,3 +52,18 @@ def test_need_of_packed_serving_world():
     assert any(fits(c.caps(), need) for c in cl)
     smallest = min((c for c in cl if fits(c.caps(), need)), key=lambda c: c.bodies)
     assert smallest.bodies >= need[0] and smallest.bodies < 2 * need[0] + 2
+
+
+def test_pool_grows_by_appended_slots():
+    pool = SlotPool([caps(33)])
+    need = (20, 20, 20, 0, 0, 2, 0)
+    assert pool.take(need) == 0
+    assert pool.take(need) is None           # the class is full
+    ids = pool.add([caps(33), caps(65)])     # a new chunk of slots
+    assert ids == [1, 2]
+    assert pool.take(need) == 1              # the new 33-body slot first
+    assert pool.take(need) == 2
+    pool.give_back(0)
+    assert pool.take(need) == 0
+    with pytest.raises(ValueError):
+        pool.add([caps(33)], first=7)        # ids stay contiguous
