@@ -260,7 +260,7 @@ def run_ours(args, rank, world, local):
         reqs, worlds = build_mix(args.worlds, args.seed + 1000 * rank)
         if args.tune:
             from omi_physics_b200 import tune
-            tune.autotune(worlds, device=local)
+            tune.autotune(worlds, device=local, preroll=args.preroll)
         grp = WorldGroups(worlds, groups=args.groups, device=local)
     grp.step(args.preroll)
     setup_s = time.time() - t0

@@ -175,6 +175,12 @@ typedef struct OmiTuning {
 } OmiTuning;
 int omi_set_tuning(OmiCtx *ctx, const OmiTuning *tuning);
 int omi_get_tuning(OmiCtx *ctx, OmiTuning *tuning);
+/* Colliding worlds with more bodies than this are "wide": their sort, sweep
+ * links, wake, contact sweep, warm-start cache store, positions and sleep
+ * run on many blocks instead of one block per world (the same results, bit
+ * for bit). Default 3072; 0 makes every colliding world wide. Applies from
+ * the next omi_load / omi_reserve_slots. (No counterpart in the reference.) */
+int omi_set_wide_threshold(OmiCtx *ctx, int32_t bodies);
 /* Check a scene the way omi_load does, on the host only (no device, no
  * context): every index a kernel would follow is range-checked. Returns 0 or
  * the status omi_load would return, with the message in err (err_cap bytes,

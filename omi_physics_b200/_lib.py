@@ -111,6 +111,7 @@ PROTOTYPES = {
     'omi_validate_scene': (C.c_int, [C.POINTER(OmiScene), C.c_char_p, C.c_int32]),
     'omi_set_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
     'omi_get_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
+    'omi_set_wide_threshold': (C.c_int, [C.c_void_p, C.c_int32]),
     'omi_load': (C.c_int, [C.c_void_p, C.POINTER(OmiScene)]),
     'omi_set_active': (C.c_int, [C.c_void_p, U8]),
     'omi_set_world_params': (C.c_int, [C.c_void_p, D, I, I, I]),
@@ -196,7 +197,11 @@ def ptr(a, t):
 
 
 class Context:
-    """One library context: a CUDA stream and a device arena."""
+    """One library context: a CUDA stream and a device arena.
+
+    ``OMI_WIDE_THRESHOLD`` in the environment sets the body count above which
+    a world's per-world stages run on many blocks (``omi_set_wide_threshold``)
+    for every new context."""
 
     def __init__(self, device: int = 0):
         self.lib = load_library()
@@ -210,6 +215,9 @@ class Context:
                 self.h = C.c_void_p()
             raise OmiError(rc, msg)
         self._keep = []
+        wide = os.environ.get('OMI_WIDE_THRESHOLD')
+        if wide:
+            self.call('set_wide_threshold', int(wide))
 
     def check(self, rc: int, what: str = '') -> int:
         """Raise the matching exception for a negative status; return rc."""

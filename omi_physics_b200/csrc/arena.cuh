@@ -46,6 +46,16 @@ struct Arena {
     int spin_limit;                 // polls before a sweep wait gives up (ST_SWEEP_TIMEOUT)
     int epa_faces;                  // EPA polytope face bound (<= EPA_F; ST_EPA_LIMIT past it)
     int stall_run;                  // test hook: world-local run whose sweep entries never become ready (-1: none)
+    // wide worlds: large worlds whose stages run on many blocks (wide.cuh) instead of one
+    // block per world; the per-world kernels skip them
+    int n_wide;
+    const int *wide_w;              // the wide worlds
+    const uint8_t *w_wide;          // per world: 1 when wide
+    int *wide_state;                // per wide world: WIDE_STATE_INTS ints of sweep counters
+    int *wl_flag, *wl_scan;         // per contact: run-start flag and its scan (contact_cap + 1)
+    int *wl_cnt, *wl_bstart;        // per body: run-bucket counts and their scan (NB + 1)
+    int *wl_list;                   // run buckets of the wide worlds (2 * contact_cap)
+    int *k_total;                   // contacts of the step (all worlds), the length of the run-start scan
 
     // worlds
     const int *w_body_off;          // row range of each world (its capacity)

@@ -32,6 +32,9 @@ __device__ __forceinline__ bool overflowed(const Arena &A) {
 __device__ __forceinline__ bool world_collides(const Arena &A, int w) {
     return A.w_active[w] && (A.w_flags[w] & WF_COLLISION);
 }
+// a world whose sort, levels, wake, sweep, cache store and sleep pass run on
+// many blocks (wide.cuh); the one-block-per-world kernels skip it
+__device__ __forceinline__ bool world_wide(const Arena &A, int w) { return A.w_wide[w] != 0; }
 __device__ __forceinline__ bool dyn(const Arena &A, int i) { return A.mtype[i] == 2; }
 
 // ---------------------------------------------------------------------------
@@ -109,7 +112,7 @@ template <bool ROWS>
 __global__ void k_sort(Arena A, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem[];
     for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
-        if (!world_collides(A, w)) continue;
+        if (!world_collides(A, w) || (ROWS && world_wide(A, w))) continue;
         const int off = A.w_body_off[w], n = A.w_body_n[w];
         double *k0, *k1;
         int *v0, *v1;
@@ -1247,7 +1250,7 @@ __global__ void __launch_bounds__(WAKE_THREADS) k_wake(Arena A) {
     const double thr = 0.15 * 0.15;
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
-        if (!world_collides(A, w)) continue;
+        if (!world_collides(A, w) || world_wide(A, w)) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
         if (c1 == c0) continue;
@@ -1400,7 +1403,7 @@ __global__ void __launch_bounds__(LEVEL_THREADS) k_levels(Arena A, int smem_ints
     const int tid = threadIdx.x, T = blockDim.x;
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
-        if (!world_collides(A, w)) continue;
+        if (!world_collides(A, w) || world_wide(A, w)) continue;
         int c0, c1;
         world_contacts(A, w, c0, c1);
         const int K = c1 - c0;
@@ -1966,7 +1969,7 @@ __device__ __forceinline__ int sweep_take(const Arena &A) {
         const int wi = atomicAdd(A.sweep_next, 1);
         if (wi >= A.W) return -1;
         const int w = A.w_sched[wi];
-        if (world_collides(A, w)) return w;
+        if (world_collides(A, w) && !world_wide(A, w)) return w;
     }
 }
 

@@ -49,43 +49,51 @@ __global__ void k_hash_clear(Arena A) {
         A.hkey[nxt][A.hused[nxt][i]] = ~0ull;
 }
 
-__global__ void k_cache_copy(Arena A) {   // CTA per world
-    if (overflowed(A)) return;
-    const int cur = *A.parity, nxt = 1 - cur;
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
-        const int dst = A.w_cache_off[nxt][w], n = A.w_cache_n[nxt][w];
-        if (A.w_cache_new[w]) {
-            int c0, c1;
-            world_contacts(A, w, c0, c1);
-            for (int e = threadIdx.x; e < n; e += blockDim.x) {
-                const int k = c0 + e, d = dst + e;
-                A.cache_a[nxt][d] = A.c_a[k];
-                A.cache_b[nxt][d] = A.c_b[k];
-                for (int c = 0; c < 3; c++) {
-                    A.cache_pt[nxt][d * 3 + c] = A.c_pt[k * 3 + c];
-                    A.cache_imp[nxt][d * 3 + c] = A.c_imp[k * 3 + c];
-                }
+// world w's entries first, first + stride, ... of the next cache buffer: a
+// CTA per world (threadIdx.x, blockDim.x), or a whole grid for a wide world
+__device__ __forceinline__ void cache_copy_world(const Arena &A, int w, int cur, int first, int stride) {
+    const int nxt = 1 - cur;
+    const int dst = A.w_cache_off[nxt][w], n = A.w_cache_n[nxt][w];
+    if (A.w_cache_new[w]) {
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        for (int e = first; e < n; e += stride) {
+            const int k = c0 + e, d = dst + e;
+            A.cache_a[nxt][d] = A.c_a[k];
+            A.cache_b[nxt][d] = A.c_b[k];
+            for (int c = 0; c < 3; c++) {
+                A.cache_pt[nxt][d * 3 + c] = A.c_pt[k * 3 + c];
+                A.cache_imp[nxt][d * 3 + c] = A.c_imp[k * 3 + c];
             }
-        } else {
-            const int src = A.w_cache_off[cur][w];
-            for (int e = threadIdx.x; e < n; e += blockDim.x) {
-                const int s = src + e, d = dst + e;
-                A.cache_a[nxt][d] = A.cache_a[cur][s];
-                A.cache_b[nxt][d] = A.cache_b[cur][s];
-                for (int c = 0; c < 3; c++) {
-                    A.cache_pt[nxt][d * 3 + c] = A.cache_pt[cur][s * 3 + c];
-                    A.cache_imp[nxt][d * 3 + c] = A.cache_imp[cur][s * 3 + c];
-                }
+        }
+    } else {
+        const int src = A.w_cache_off[cur][w];
+        for (int e = first; e < n; e += stride) {
+            const int s = src + e, d = dst + e;
+            A.cache_a[nxt][d] = A.cache_a[cur][s];
+            A.cache_b[nxt][d] = A.cache_b[cur][s];
+            for (int c = 0; c < 3; c++) {
+                A.cache_pt[nxt][d * 3 + c] = A.cache_pt[cur][s * 3 + c];
+                A.cache_imp[nxt][d * 3 + c] = A.cache_imp[cur][s * 3 + c];
             }
         }
     }
 }
 
-// insert one key per run of equal (a, b) entries into table t
-__device__ inline void hash_runs(const Arena &A, int t, int w) {
+__global__ void k_cache_copy(Arena A) {   // CTA per world
+    if (overflowed(A)) return;
+    const int cur = *A.parity;
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x)
+        if (!world_wide(A, w)) cache_copy_world(A, w, cur, threadIdx.x, blockDim.x);
+}
+
+// insert one key per run of equal (a, b) entries into table t; entries
+// first, first + stride, ... of the world's range (a CTA per world, or a
+// whole grid for a wide world)
+__device__ inline void hash_runs(const Arena &A, int t, int w, int first, int stride) {
     const int off = A.w_cache_off[t][w], n = A.w_cache_n[t][w];
     const int *ca = A.cache_a[t], *cb = A.cache_b[t];
-    for (int e = off + threadIdx.x; e < off + n; e += blockDim.x) {
+    for (int e = off + first; e < off + n; e += stride) {
         if (e > off && ca[e] == ca[e - 1] && cb[e] == cb[e - 1]) continue;
         int len = 1;
         while (e + len < off + n && ca[e + len] == ca[e] && cb[e + len] == cb[e]) len++;
@@ -107,7 +115,8 @@ __device__ inline void hash_runs(const Arena &A, int t, int w) {
 __global__ void k_hash_build(Arena A) {   // CTA per world, table = next buffer
     if (overflowed(A)) return;
     const int nxt = 1 - *A.parity;
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x) hash_runs(A, nxt, w);
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x)
+        if (!world_wide(A, w)) hash_runs(A, nxt, w, threadIdx.x, blockDim.x);
 }
 
 __global__ void k_flip(Arena A) {
@@ -117,7 +126,7 @@ __global__ void k_flip(Arena A) {
 
 // rebuild table t from cache buffer t (after the host regrows the tables)
 __global__ void k_hash_rebuild(Arena A, int t) {
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x) hash_runs(A, t, w);
+    for (int w = blockIdx.x; w < A.W; w += gridDim.x) hash_runs(A, t, w, threadIdx.x, blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -405,7 +414,7 @@ __global__ void k_finalize(Arena A, int mode, int cap) {
     if ((mode & FIN_COUNT) && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.status[ST_STEPS_DONE], 1);
     for (int wi = blockIdx.x; wi < A.W; wi += gridDim.x) {
         const int w = A.w_sched[wi];
-        if (!A.w_active[w]) continue;
+        if (!A.w_active[w] || world_wide(A, w)) continue;
         const double dt = A.w_dt[w];
         const int b0 = A.w_body_off[w], nb = A.w_body_n[w], b1 = b0 + nb;
         if (mode & FIN_POSITIONS) {

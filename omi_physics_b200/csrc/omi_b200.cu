@@ -16,7 +16,7 @@
 
 #include "../../include/omi_b200.h"
 #include "capsule.cuh"
-#include "kernels2.cuh"
+#include "wide.cuh"
 
 using namespace omi;
 
@@ -87,6 +87,11 @@ struct OmiCtx {
     // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
     int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
     OmiTuning tune = {8, 4, 256, 16, 128, 4};   // launch configuration (omi_set_tuning)
+    // wide worlds (their stages on many blocks): the worlds, bodies of the largest, sort merge passes
+    std::vector<int> h_wide;
+    int wide_max_n = 0, wide_merge_passes = 0;
+    int wide_min_bodies = 3072;                 // a colliding world with more bodies runs wide
+    int64_t graph_launches = 0;                 // kernels one captured step launches
 };
 
 namespace {
@@ -157,6 +162,11 @@ int grid_for(int n, int block, int cap) {
     return std::max(1, std::min(g, cap));
 }
 
+// blocks of `block` threads for n items of a wide world, at most 8 per SM
+int wide_grid(const OmiCtx *ctx, int n, int block) {
+    return std::max(1, std::min((n + block - 1) / block, ctx->sm_count * 8));
+}
+
 int hash_bits_for(int runs) {
     int bits = 10;
     while ((1 << bits) < 2 * runs) bits++;
@@ -202,11 +212,15 @@ int alloc_dynamic(OmiCtx *ctx, int pair_cap, int contact_cap) {
     rc |= alloc(ctx, ctx->dyn, A.run_done, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_tend, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.lv_scratch, 3 * (size_t)contact_cap + 2 * (size_t)A.NB + 2 * (size_t)A.W + 64);
+    const bool wide = !ctx->h_wide.empty();
+    rc |= alloc(ctx, ctx->dyn, A.wl_flag, wide ? contact_cap : 1);
+    rc |= alloc(ctx, ctx->dyn, A.wl_scan, wide ? (size_t)contact_cap + 1 : 1);
+    rc |= alloc(ctx, ctx->dyn, A.wl_list, wide ? 2 * (size_t)contact_cap + 1 : 1);
     rc |= alloc(ctx, ctx->dyn, A.run_k, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_n, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_a, contact_cap);
     rc |= alloc(ctx, ctx->dyn, A.run_b, contact_cap);
-    size_t scan_n = std::max<size_t>((size_t)pair_cap, (size_t)A.NB) / SCAN_TILE + 2;
+    size_t scan_n = std::max({(size_t)pair_cap, (size_t)contact_cap, (size_t)A.NB}) / SCAN_TILE + 2;
     rc |= alloc(ctx, ctx->dyn, A.scan_blocks, scan_n + 1);
     if (rc) return rc;
     // warm-start cache: up to one step's contacts plus worlds keeping old ones
@@ -285,6 +299,15 @@ void stage_broadphase(OmiCtx *ctx, Prof *pf) {
     const size_t smem = (size_t)ctx->sort_cap * (2 * sizeof(double) + 2 * sizeof(int));
     k_sort<true><<<std::min(A.W, 65535), ctx->sort_block, smem, ctx->stream>>>(A, ctx->sort_cap);
     ctx->launches++;
+    if (A.n_wide) {
+        const int tiles = (ctx->wide_max_n + WSORT_TILE - 1) / WSORT_TILE;
+        k_wsort_tiles<<<dim3(tiles, A.n_wide), WSORT_THREADS, (size_t)WSORT_TILE * 24, ctx->stream>>>(A);
+        int src = 0;
+        for (int j = 0, width = WSORT_TILE; j < ctx->wide_merge_passes; j++, width *= 2, src ^= 1)
+            k_wsort_merge<<<dim3(wide_grid(ctx, ctx->wide_max_n, 256), A.n_wide), 256, 0, ctx->stream>>>(A, width, src);
+        k_wsort_rows<<<dim3(wide_grid(ctx, ctx->wide_max_n, 256), A.n_wide), 256, 0, ctx->stream>>>(A, src);
+        ctx->launches += 2 + ctx->wide_merge_passes;
+    }
     mark(ctx, pf, KN_SORT);
     const OmiTuning &t = ctx->tune;
     const int pgrid = grid_for(A.NB * 32, t.pair_block, ctx->sm_count * t.pair_blocks_per_sm);
@@ -337,11 +360,30 @@ void stage_compact(OmiCtx *ctx, Prof *pf) {
 
 void stage_solve(OmiCtx *ctx, Prof *pf) {
     Arena &A = ctx->A;
+    const int nw = A.n_wide;
+    const int cgrid = wide_grid(ctx, A.contact_cap, 256);     // contacts of wide worlds
+    if (nw) cudaMemsetAsync(A.wide_state, 0, sizeof(int) * WIDE_STATE_INTS * nw, ctx->stream);
     k_wake<<<std::min(A.W, 65535), WAKE_THREADS, 0, ctx->stream>>>(A);
+    if (nw) {
+        k_wwake<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A, 0);
+        k_wwake<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A, 1);
+        ctx->launches += 2;
+    }
     mark(ctx, pf, KN_WAKE);
     k_prep<<<grid_for(A.contact_cap, PREP_THREADS, SM_CAP), PREP_THREADS, (size_t)PREP_THREADS * CD * sizeof(double), ctx->stream>>>(A);
     mark(ctx, pf, KN_PREP);
     k_levels<<<std::min(A.W, 65535), LEVEL_THREADS, (size_t)ctx->level_ints * sizeof(int), ctx->stream>>>(A, ctx->level_ints);
+    if (nw) {
+        const int kgrid = wide_grid(ctx, A.contact_cap, 256);
+        k_wl_flags<<<kgrid, 256, 0, ctx->stream>>>(A);
+        launch_scan(ctx, A.wl_flag, A.wl_scan, 0, A.k_total, A.contact_cap, A.pair_scan, A.NB, A.pair_cap);
+        k_wl_runs<<<kgrid, 256, 0, ctx->stream>>>(A);
+        k_wl_count<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A);
+        launch_scan(ctx, A.wl_cnt, A.wl_bstart, A.NB, nullptr, A.NB, nullptr, 0, 0);
+        k_wl_fill<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A);
+        k_wl_links<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A);
+        ctx->launches += 5;
+    }
     mark(ctx, pf, KN_LEVELS);
     const size_t sweep_smem = (size_t)ctx->stage_doubles * sizeof(double);
     if (ctx->tune.sweep_warps == 4)
@@ -351,6 +393,12 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
         k_iterate<8><<<std::min(A.W, ctx->sm_count), 256, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles,
                                                                                      ctx->tune.sweep_max_split);
     ctx->launches += 4;
+    for (int wi = 0; wi < nw; wi++) {          // one wide world at a time, on every SM
+        k_wsweep_init<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+        k_wsweep_seed<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+        k_wsweep<<<ctx->sm_count, SWEEP_THREADS, 0, ctx->stream>>>(A, wi);
+        ctx->launches += 3;
+    }
     mark(ctx, pf, KN_SOLVE);
     if (ctx->has_triggers) {
         k_triggers<<<148 * 4, 128, 4 * sizeof(EpaWork), ctx->stream>>>(A);
@@ -360,7 +408,9 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
     k_hash_clear<<<grid_for(ctx->cache_cap, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
     k_cache_copy<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
+    if (nw) { k_wcache_copy<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A); ctx->launches++; }
     k_hash_build<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
+    if (nw) { k_whash_build<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A); ctx->launches++; }
     k_flip<<<1, 1, 0, ctx->stream>>>(A);
     ctx->launches += 5;
     mark(ctx, pf, KN_CACHE);
@@ -373,6 +423,24 @@ void stage_joints(OmiCtx *ctx, Prof *pf, int gated) {
         ctx->launches++;
     }
     mark(ctx, pf, KN_JOINTS);
+}
+
+// integrate positions and / or sleep (k_finalize's modes) for every world:
+// one block per world, and the wide worlds' grid passes
+void stage_finalize(OmiCtx *ctx, int mode) {
+    Arena &A = ctx->A;
+    k_finalize<<<std::min(A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(A, mode, ctx->fin_cap);
+    ctx->launches++;
+    if (A.n_wide) {
+        const int bgrid = wide_grid(ctx, ctx->wide_max_n, 256), cgrid = wide_grid(ctx, A.contact_cap, 256);
+        k_wfinalize<<<dim3(bgrid, A.n_wide), 256, 0, ctx->stream>>>(A, mode, 0);
+        ctx->launches++;
+        if (mode & FIN_SLEEP) {
+            k_wfinalize<<<dim3(cgrid, A.n_wide), 256, 0, ctx->stream>>>(A, mode, 1);
+            for (int ph = 2; ph <= 4; ph++) k_wfinalize<<<dim3(bgrid, A.n_wide), 256, 0, ctx->stream>>>(A, mode, ph);
+            ctx->launches += 4;
+        }
+    }
 }
 
 // one full step (world.py:410-430) for every active world
@@ -388,8 +456,7 @@ void enqueue_step(OmiCtx *ctx, Prof *pf) {
     stage_compact(ctx, pf);
     stage_solve(ctx, pf);
     stage_joints(ctx, pf, 1);
-    k_finalize<<<std::min(A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(A, FIN_POSITIONS | FIN_SLEEP | FIN_COUNT | FIN_GATED, ctx->fin_cap);
-    ctx->launches++;
+    stage_finalize(ctx, FIN_POSITIONS | FIN_SLEEP | FIN_COUNT | FIN_GATED);
     mark(ctx, pf, KN_FINALIZE);
 }
 
@@ -429,6 +496,7 @@ int capture(OmiCtx *ctx) {
     const int64_t before = ctx->launches;
     enqueue_step(ctx, nullptr);
     e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->graph_launches = ctx->launches - before;
     ctx->launches = before;
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(&ctx->graph, g, 0);
@@ -438,13 +506,7 @@ int capture(OmiCtx *ctx) {
 }
 
 int64_t step_launches(OmiCtx *ctx) {
-    // kernels per captured step (same sequence as enqueue_step)
-    int64_t n = 1 + 1 + 1 + 3 + 1 + 2 + 1 + 1 + 3 + 1 + 1 + 1 + 4 + 5 + 1;
-    if (ctx->A.NJ > 0) n += 1;
-    if (ctx->has_triggers) n += 1;
-    if (ctx->has_meshes) n += 2;
-    if (ctx->moving_meshes) n += 1;
-    return n;
+    return ctx->graph_launches;        // kernels of the captured step (counted while capturing)
 }
 
 // errors the status words of completed steps carry: a sweep wait that ran
@@ -539,6 +601,7 @@ int omi_create(int device, OmiCtx **out) {
         {(const void *)k_levels, LEVEL_SMEM_INTS * (int)sizeof(int), "k_levels"},
         {(const void *)k_finalize, 2 * 8192 * (int)sizeof(int), "k_finalize"},
         {(const void *)k_prep, PREP_THREADS * CD * (int)sizeof(double), "k_prep"},
+        {(const void *)k_wsort_tiles, WSORT_TILE * 24, "k_wsort_tiles"},
     };
     for (const auto &f : smem) {
         e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
@@ -918,11 +981,40 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= alloc(ctx, ctx->statics, A.hused_n, 4);
     rc |= alloc(ctx, ctx->statics, A.parity, 1);
     rc |= alloc(ctx, ctx->statics, A.status, ST_WORDS);
+    // wide worlds: colliding worlds above wide_min_bodies run their per-world stages on many blocks
+    {
+        ctx->h_wide.clear();
+        std::vector<uint8_t> flag(W, 0);
+        ctx->wide_max_n = 0;
+        for (int w = 0; w < W; w++) {
+            const int n = s->w_body_off[w + 1] - s->w_body_off[w];
+            if ((s->w_flags[w] & OMI_WF_COLLISION) && n > ctx->wide_min_bodies) {
+                flag[w] = 1;
+                ctx->h_wide.push_back(w);
+                ctx->wide_max_n = std::max(ctx->wide_max_n, n);
+            }
+        }
+        A.n_wide = (int)ctx->h_wide.size();
+        ctx->wide_merge_passes = 0;
+        for (int64_t t = WSORT_TILE; t < ctx->wide_max_n; t *= 2) ctx->wide_merge_passes++;
+        rc |= upload(ctx, const_cast<int *&>(A.wide_w), ctx->h_wide.empty() ? nullptr : ctx->h_wide.data(),
+                     std::max<size_t>(ctx->h_wide.size(), 1));
+        rc |= upload(ctx, const_cast<uint8_t *&>(A.w_wide), flag.data(), W);
+        rc |= alloc(ctx, ctx->statics, A.wide_state, (size_t)std::max(A.n_wide, 1) * WIDE_STATE_INTS);
+        rc |= alloc(ctx, ctx->statics, A.wl_cnt, A.n_wide ? (size_t)NB : 1);
+        rc |= alloc(ctx, ctx->statics, A.wl_bstart, A.n_wide ? (size_t)NB + 1 : 1);
+        rc |= alloc(ctx, ctx->statics, A.k_total, 1);
+    }
     if (rc) return rc;
     ctx->max_world_n = max_n;
     ctx->max_world_j = max_j;
-    ctx->sort_cap = std::min(std::max(max_nc, 1), 8192);
-    ctx->sort_block = max_nc > 2048 ? 1024 : (max_nc > 512 ? 512 : 256);
+    int max_nc_narrow = 0;          // the largest colliding world the one-block-per-world sort takes
+    for (int w = 0; w < W; w++) {
+        const int n = s->w_body_off[w + 1] - s->w_body_off[w];
+        if ((s->w_flags[w] & OMI_WF_COLLISION) && n <= ctx->wide_min_bodies) max_nc_narrow = std::max(max_nc_narrow, n);
+    }
+    ctx->sort_cap = std::min(std::max(max_nc_narrow, 1), 8192);
+    ctx->sort_block = max_nc_narrow > 2048 ? 1024 : (max_nc_narrow > 512 ? 512 : 256);
     // sleep flags and union-find parents of the largest world (two ints per body, <= 64 KB)
     ctx->fin_cap = std::min(std::max(max_n, 1), 8192);
     // body buckets of the largest world: 2 ints per body + 2 per run (~1.5 runs per body)
@@ -1330,6 +1422,12 @@ int omi_set_tuning(OmiCtx *ctx, const OmiTuning *t) {
     return 0;
 }
 
+int omi_set_wide_threshold(OmiCtx *ctx, int32_t bodies) {
+    if (!ctx || bodies < 0) return OMI_E_ARG;
+    ctx->wide_min_bodies = bodies;
+    return 0;
+}
+
 int omi_get_tuning(OmiCtx *ctx, OmiTuning *t) {
     if (!ctx || !t) return OMI_E_ARG;
     *t = ctx->tune;
@@ -1420,7 +1518,7 @@ int omi_solve_joints(OmiCtx *ctx) {
 
 int omi_integrate_positions(OmiCtx *ctx) {
     STAGE_PRELUDE
-    k_finalize<<<std::min(ctx->A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(ctx->A, FIN_POSITIONS, ctx->fin_cap);
+    stage_finalize(ctx, FIN_POSITIONS);
     ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1429,7 +1527,7 @@ int omi_integrate_positions(OmiCtx *ctx) {
 
 int omi_update_sleep(OmiCtx *ctx) {
     STAGE_PRELUDE
-    k_finalize<<<std::min(ctx->A.W, 65535), 256, (size_t)2 * ctx->fin_cap * sizeof(int), ctx->stream>>>(ctx->A, FIN_SLEEP, ctx->fin_cap);
+    stage_finalize(ctx, FIN_SLEEP);
     ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));

@@ -1,0 +1,579 @@
+// Wide worlds: the stages that run one block per world elsewhere (sort,
+// sweep links, wake, contact sweep, warm-start cache store, positions and
+// sleep) spread over many blocks for worlds large enough that one block (one
+// SM) would bound the step. The results are the same bits as the
+// one-block forms: the same arithmetic in the same dependency order.
+//
+// Launches carry the wide world's index in blockIdx.y (or as an argument for
+// the sweep); x runs over the world's bodies, contacts or runs, grid-stride.
+#pragma once
+#include "kernels2.cuh"
+
+namespace omi {
+
+// per wide world, ints of global counters (zeroed before the solve stage)
+constexpr int WIDE_STATE_INTS = 32;
+enum { WS_HEAD = 0, WS_TAIL = 8, WS_CLAIMED = 16, WS_ABORT = 17, WS_HIST = 18, WS_CASCADE = 22 };
+// bodies per sort tile (sorted in shared memory, then merged in global memory)
+constexpr int WSORT_TILE = 4096;
+constexpr int WSORT_THREADS = 512;
+
+__device__ __forceinline__ int wide_tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int wide_stride() { return gridDim.x * blockDim.x; }
+
+// ---------------------------------------------------------------------------
+// sort (np.argsort(min_x, kind='stable'), broadphase.py:261): tiles sorted in
+// shared memory by the merge sort of k_sort, then merged pairwise in global
+// memory (each element placed by its rank in the partner run), then the
+// sorted rows written as k_sort writes them
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(WSORT_THREADS) k_wsort_tiles(Arena A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    const int off = A.w_body_off[w], n = A.w_body_n[w];
+    const int t0 = blockIdx.x * WSORT_TILE;
+    if (t0 >= n) return;
+    const int m = min(WSORT_TILE, n - t0);
+    double *k0 = reinterpret_cast<double *>(smem), *k1 = k0 + WSORT_TILE;
+    int *v0 = reinterpret_cast<int *>(k1 + WSORT_TILE), *v1 = v0 + WSORT_TILE;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        k0[i] = A.aabb_min[(off + t0 + i) * 3] + 0.0;      // -0.0 == 0.0; NaN stays NaN (sorts last)
+        v0[i] = t0 + i;
+    }
+    __syncthreads();
+    for (int width = 1; width < m; width <<= 1) {
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const int seg = (i / (2 * width)) * (2 * width);
+            const int mid = min(seg + width, m), end = min(seg + 2 * width, m);
+            const double key = k0[i];
+            const int val = v0[i];
+            int lo, hi, base;
+            if (i < mid) { lo = mid; hi = end; base = i - seg; }
+            else { lo = seg; hi = mid; base = i - mid; }
+            const int start = lo;
+            while (lo < hi) {
+                const int q = (lo + hi) >> 1;
+                if (key_less(k0[q], v0[q], key, val)) lo = q + 1; else hi = q;
+            }
+            const int pos = seg + base + (lo - start);
+            k1[pos] = key;
+            v1[pos] = val;
+        }
+        __syncthreads();
+        double *tk = k0; k0 = k1; k1 = tk;
+        int *tv = v0; v0 = v1; v1 = tv;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        A.sort_k[0][off + t0 + i] = k0[i];
+        A.sort_v[0][off + t0 + i] = v0[i];
+    }
+}
+
+// one merge pass over runs of `width` elements: buffer src -> 1 - src
+__global__ void k_wsort_merge(Arena A, int width, int src) {
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    const int off = A.w_body_off[w], n = A.w_body_n[w];
+    const double *ks = A.sort_k[src] + off;
+    const int *vs = A.sort_v[src] + off;
+    double *kd = A.sort_k[1 - src] + off;
+    int *vd = A.sort_v[1 - src] + off;
+    for (int i = wide_tid(); i < n; i += wide_stride()) {
+        const int seg = (int)(((int64_t)i / (2 * (int64_t)width)) * 2 * width);
+        const int mid = (int)min((int64_t)seg + width, (int64_t)n), end = (int)min((int64_t)seg + 2 * (int64_t)width, (int64_t)n);
+        const double key = ks[i];
+        const int val = vs[i];
+        int lo, hi, base;
+        if (i < mid) { lo = mid; hi = end; base = i - seg; }
+        else { lo = seg; hi = mid; base = i - mid; }
+        const int start = lo;
+        while (lo < hi) {
+            const int q = (lo + hi) >> 1;
+            if (key_less(ks[q], vs[q], key, val)) lo = q + 1; else hi = q;
+        }
+        const int pos = seg + base + (lo - start);
+        kd[pos] = key;
+        vd[pos] = val;
+    }
+}
+
+// the sorted rows of the step's broadphase, from buffer src (as k_sort<true>)
+__global__ void k_wsort_rows(Arena A, int src) {
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    const int off = A.w_body_off[w], n = A.w_body_n[w];
+    for (int i = wide_tid(); i < n; i += wide_stride()) {
+        const int body = off + A.sort_v[src][off + i];
+        A.order[off + i] = body;
+        A.sorted_x[off + i] = A.sort_k[src][off + i];
+        double4 *row = reinterpret_cast<double4 *>(&A.srt_box[(size_t)(off + i) * 8]);
+        const double *lo = &A.aabb_min[body * 3], *hi = &A.aabb_max[body * 3];
+        row[0] = make_double4(lo[0], hi[0], lo[1], hi[1]);
+        row[1] = make_double4(lo[2], hi[2], 0.0, 0.0);
+        const bool sensor = A.tshape[body] >= 0;
+        A.srt_info[off + i] = A.mtype[body] | (A.shape[body] >= 0 && !sensor ? 4 : 0) |
+                              (A.awake[body] ? 8 : 0) | (sensor ? 16 : 0) | (A.filter_row[body] << 5);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// wake (_wake_sleepers, solver.py:321-337): phase 0 looks for a sleeper moving
+// faster than the wake threshold among the contacts (then the pass must run
+// in contact order: one thread does it); phase 1 wakes, in parallel when no
+// woken body can wake another (as k_wake decides per world)
+// ---------------------------------------------------------------------------
+__global__ void k_wwake(Arena A, int phase) {
+    if (overflowed(A)) return;
+    const int wi = blockIdx.y, w = A.wide_w[wi];
+    if (!world_collides(A, w)) return;
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    int *st = A.wide_state + wi * WIDE_STATE_INTS;
+    const double thr = 0.15 * 0.15;
+    if (phase == 0) {
+        bool cascade = false;
+        for (int k = c0 + wide_tid(); k < c1; k += wide_stride()) {
+            const int e[2] = {A.c_a[k], A.c_b[k]};
+            for (int j = 0; j < 2; j++) {
+                const int x = e[j];
+                cascade |= A.mtype[x] == 2 && !A.awake[x] && speed2(&A.v[x * 3]) > thr;
+            }
+        }
+        if (__syncthreads_or(cascade) && threadIdx.x == 0) atomicOr(&st[WS_CASCADE], 1);
+        return;
+    }
+    if (*(volatile int *)&st[WS_CASCADE]) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            atomicAdd(&A.status[ST_CASCADE], 1);
+            for (int k = c0; k < c1; k++) {
+                const int a = A.c_a[k], b = A.c_b[k];
+                if (!A.awake[b]) {
+                    const int t = A.mtype[a];
+                    if (t == 1 || (t == 2 && A.awake[a] && speed2(&A.v[a * 3]) > thr)) wake_body(A, b);
+                }
+                if (!A.awake[a]) {
+                    const int t = A.mtype[b];
+                    if (t == 1 || (t == 2 && A.awake[b] && speed2(&A.v[b * 3]) > thr)) wake_body(A, a);
+                }
+            }
+        }
+        return;
+    }
+    for (int k = c0 + wide_tid(); k < c1; k += wide_stride()) {
+        const int a = A.c_a[k], b = A.c_b[k];
+        const int ta = A.mtype[a], tb = A.mtype[b];
+        if (!A.awake[b] && (ta == 1 || (ta == 2 && A.awake[a] && speed2(&A.v[a * 3]) > thr))) wake_body(A, b);
+        if (!A.awake[a] && (tb == 1 || (tb == 2 && A.awake[b] && speed2(&A.v[b * 3]) > thr))) wake_body(A, a);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sweep links (k_levels' runs, buckets and predecessor / successor codes) in
+// five grid passes and two scans:
+//   k_wl_flags  per contact: starts a run? (wide worlds only); zero buckets
+//   (scan of the flags over all contacts)
+//   k_wl_runs   per run start: run_k, run_a, run_b; per wide world: w_runs
+//   k_wl_count  per run: run_n, bucket counts of its dynamic bodies
+//   (scan of the counts over all bodies)
+//   k_wl_fill   per run: its index into both bodies' buckets
+//   k_wl_links  per run: predecessor / successor codes, run_kn, run_need
+// ---------------------------------------------------------------------------
+__global__ void k_wl_flags(Arena A) {
+    if (overflowed(A)) return;
+    const int Ktot = A.contact_scan[A.pair_scan[A.NB]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *A.k_total = Ktot;
+    for (int k = wide_tid(); k < Ktot; k += wide_stride()) {
+        const int a = A.c_a[k], b = A.c_b[k];
+        const int w = A.body_world[a];
+        int start = 0;
+        if (world_wide(A, w) && world_collides(A, w)) {
+            int c0, c1;
+            world_contacts(A, w, c0, c1);
+            start = k == c0 || a != A.c_a[k - 1] || b != A.c_b[k - 1];
+            if (!start && (A.kind[a] == 5 || A.kind[b] == 5))
+                start = A.c_n[k * 3] != A.c_n[k * 3 - 3] || A.c_n[k * 3 + 1] != A.c_n[k * 3 - 2] ||
+                        A.c_n[k * 3 + 2] != A.c_n[k * 3 - 1];
+        }
+        A.wl_flag[k] = start;
+    }
+    for (int i = wide_tid(); i < A.NB; i += wide_stride()) A.wl_cnt[i] = 0;
+}
+
+__global__ void k_wl_runs(Arena A) {
+    if (overflowed(A)) return;
+    const int Ktot = A.contact_scan[A.pair_scan[A.NB]];
+    for (int k = wide_tid(); k < Ktot; k += wide_stride()) {
+        if (!A.wl_flag[k]) continue;
+        const int a = A.c_a[k], b = A.c_b[k];
+        const int w = A.body_world[a];
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        const int r = A.wl_scan[k] - A.wl_scan[c0];
+        A.run_k[c0 + r] = k - c0;
+        A.run_a[c0 + r] = A.mtype[a] == 2 ? a : -1;
+        A.run_b[c0 + r] = A.mtype[b] == 2 ? b : -1;
+    }
+    for (int wi = wide_tid(); wi < A.n_wide; wi += wide_stride()) {
+        const int w = A.wide_w[wi];
+        if (!world_collides(A, w)) continue;
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        const int K = c1 - c0;
+        A.w_runs[w] = K ? A.wl_scan[c1] - A.wl_scan[c0] : 0;
+        if (K >= (1 << 24)) {                      // run_kn packs contact offsets in 24 bits
+            A.w_runs[w] = 0;
+            atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+        }
+    }
+}
+
+__global__ void k_wl_count(Arena A) {
+    if (overflowed(A)) return;
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int K = c1 - c0, R = A.w_runs[w];
+    for (int r = wide_tid(); r < R; r += wide_stride()) {
+        const int end = r + 1 < R ? A.run_k[c0 + r + 1] : K;
+        A.run_n[c0 + r] = end - A.run_k[c0 + r];
+        const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+        if (a >= 0) atomicAdd(&A.wl_cnt[a], 1);
+        if (b >= 0) atomicAdd(&A.wl_cnt[b], 1);
+    }
+}
+
+__global__ void k_wl_fill(Arena A) {
+    if (overflowed(A)) return;
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int R = A.w_runs[w];
+    for (int r = wide_tid(); r < R; r += wide_stride()) {
+        const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+        // counts go back down to zero as the slots are taken (bucket order does not matter)
+        if (a >= 0) A.wl_list[A.wl_bstart[a] + atomicSub(&A.wl_cnt[a], 1) - 1] = r;
+        if (b >= 0) A.wl_list[A.wl_bstart[b] + atomicSub(&A.wl_cnt[b], 1) - 1] = r;
+    }
+}
+
+__global__ void k_wl_links(Arena A) {
+    if (overflowed(A)) return;
+    const int w = A.wide_w[blockIdx.y];
+    if (!world_collides(A, w)) return;
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int R = A.w_runs[w];
+    for (int r = wide_tid(); r < R; r += wide_stride()) {
+        const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+        int pa = LEVEL_NONE, pb = LEVEL_NONE, sa = LEVEL_NONE, sb = LEVEL_NONE;
+        if (a >= 0) run_link_codes(A.wl_list, A.wl_bstart[a], A.wl_bstart[a + 1], r, pa, sa);
+        if (b >= 0) run_link_codes(A.wl_list, A.wl_bstart[b], A.wl_bstart[b + 1], r, pb, sb);
+        A.run_pa[c0 + r] = pa;
+        A.run_pb[c0 + r] = pb;
+        A.run_sa[c0 + r] = sa;
+        A.run_sb[c0 + r] = sb;
+        A.run_kn[c0 + r] = A.run_k[c0 + r] | (A.run_n[c0 + r] << 24);
+        // (the test hook's run asks for 3 same-pass arrivals of at most 2: it never becomes ready)
+        A.run_need[c0 + r] = ((pa >= 0) + (pb >= 0)) | (((pa != LEVEL_NONE) + (pb != LEVEL_NONE)) << 2) |
+                             (r == A.stall_run ? 3 : 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the contact sweep of one wide world on many blocks: the dataflow of
+// k_iterate's sweep_world (same entries, same predecessor counts, same
+// per-class rings) with its state in global memory - arrival counts, the
+// ring and the ring counters - and device-scope release / acquire in place of
+// block scope. Velocities, positions and impulses stay in their global
+// arrays. A block claims only published entries, so the blocks need not all
+// be resident at once. Every wait is
+// bounded by Arena::spin_limit; a wait that runs out sets the world's abort
+// flag, which ends every other wait, and ST_SWEEP_TIMEOUT. The roots are
+// published by a launch of their own (k_wsweep_seed), so no block waits on
+// work that only another block could start: with several groups' sweeps on
+// the GPU at once, whichever blocks are resident make progress.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_gpu(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v) {
+    asm volatile("st.release.gpu.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// the ring of a wide world: per class its slot count and first slot
+struct WideRings {
+    int size[SWEEP_CLASSES], base[SWEEP_CLASSES];
+};
+
+__device__ __forceinline__ void wide_push(int *ring, int *st, const WideRings &wr, int e, int n) {
+    const int c = entry_class(e >> PASS_SHIFT, n, true);
+    const int pos = atomicAdd(&st[WS_TAIL + c], 1);
+    if (pos >= wr.size[c]) { atomicExch(&st[WS_ABORT], 1); return; }   // never with a consistent graph
+    st_release_gpu(&ring[wr.base[c] + pos], e + 1);
+}
+
+// arrival counts zeroed, ring cleared, runs counted by length (for the class sizes)
+__global__ void k_wsweep_init(Arena A, int wi) {
+    __shared__ int hist[4];
+    if (overflowed(A)) return;
+    const int w = A.wide_w[wi];
+    if (!world_collides(A, w)) return;
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int R = A.w_runs[w], N = world_passes(A, w) * R;
+    if (threadIdx.x < 4) hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (int r = wide_tid(); r < R; r += wide_stride()) {
+        A.run_done[c0 + r] = 0;
+        atomicAdd(&hist[min(A.run_kn[c0 + r] >> 24, 4) - 1], 1);
+    }
+    int *ring = A.c_order + (size_t)c0 * A.max_passes;
+    for (int e = wide_tid(); e < N; e += wide_stride()) ring[e] = 0;
+    __syncthreads();
+    if (threadIdx.x < 4 && hist[threadIdx.x])
+        atomicAdd(&A.wide_state[wi * WIDE_STATE_INTS + WS_HIST + threadIdx.x], hist[threadIdx.x]);
+}
+
+// per class: slots and first slot of the ring (class = (pass 0 ? 4 : 0) +
+// min(run length, 4) - 1), from the run-length counts of k_wsweep_init
+__device__ __forceinline__ void wide_rings(const int *st, int P, WideRings &wr) {
+    int acc = 0;
+    for (int c = 0; c < SWEEP_CLASSES; c++) {
+        const int cnt = st[WS_HIST + (c & 3)];
+        wr.size[c] = c >= 4 ? cnt : cnt * (P - 1);
+        wr.base[c] = acc;
+        acc += wr.size[c];
+    }
+}
+
+// the entries with no predecessor - pass-0 runs that start both bodies'
+// chains - published before the sweep starts, so that no block of the sweep
+// depends on another block having started
+__global__ void k_wsweep_seed(Arena A, int wi) {
+    __shared__ WideRings wr;
+    if (overflowed(A)) return;
+    const int w = A.wide_w[wi];
+    if (!world_collides(A, w)) return;
+    int *st = A.wide_state + wi * WIDE_STATE_INTS;
+    const int R = A.w_runs[w];
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    if (threadIdx.x == 0) wide_rings(st, world_passes(A, w), wr);
+    __syncthreads();
+    int *ring = A.c_order + (size_t)c0 * A.max_passes;
+    for (int r = wide_tid(); r < R; r += wide_stride())
+        if ((A.run_need[c0 + r] & 3) == 0) wide_push(ring, st, wr, r, A.run_kn[c0 + r] >> 24);
+}
+
+__global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
+    __shared__ WideRings wr;
+    if (overflowed(A)) return;
+    const int w = A.wide_w[wi];
+    if (!world_collides(A, w)) return;
+    int *st = A.wide_state + wi * WIDE_STATE_INTS;
+    const int R = A.w_runs[w];
+    if (R == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = 0;
+        return;
+    }
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int P = world_passes(A, w);
+    const int N = P * R;
+    if (threadIdx.x == 0) wide_rings(st, P, wr);
+    __syncthreads();
+    int *ring = A.c_order + (size_t)c0 * A.max_passes;
+    int *arrived = A.run_done + c0;
+    const int *run_kn = A.run_kn + c0, *run_need = A.run_need + c0;
+    const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
+    const bool warm = (A.w_flags[w] & WF_WARM) != 0;
+    const bool vel = warm || A.w_iters[w] > 0;
+    const double slop = A.w_solver[w * 2 + 1];
+    VelView V;
+    V.s = nullptr;
+    V.b0 = A.w_body_off[w];
+    ImpView I;
+    I.s = nullptr;
+    I.c0 = c0;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int lo = 0, cnt = 0;
+        if (lane == 0) {
+            const int first = ((threadIdx.x >> 5) + blockIdx.x) & (SWEEP_CLASSES - 1);
+            for (int it = 0;; it++) {
+                if (ld_relaxed_gpu(&st[WS_CLAIMED]) >= N || ld_relaxed_gpu(&st[WS_ABORT])) { cnt = -1; break; }
+                bool got = false;
+                for (int j = 0; j < SWEEP_CLASSES && !got; j++) {
+                    const int c = (first + j) & (SWEEP_CLASSES - 1);
+                    const int h = ld_relaxed_gpu(&st[WS_HEAD + c]);
+                    const int t = min(ld_relaxed_gpu(&st[WS_TAIL + c]), wr.size[c]);
+                    if (t > h) {
+                        const int want = min(t - h, 32);
+                        if (atomicCAS(&st[WS_HEAD + c], h, h + want) == h) {
+                            atomicAdd(&st[WS_CLAIMED], want);
+                            lo = wr.base[c] + h;
+                            cnt = want;
+                            got = true;
+                        }
+                    }
+                }
+                if (got) break;
+                if (it >= A.spin_limit) { atomicExch(&st[WS_ABORT], 1); cnt = -1; break; }
+                __nanosleep(64);
+            }
+        }
+        cnt = __shfl_sync(FULL, cnt, 0);
+        lo = __shfl_sync(FULL, lo, 0);
+        if (cnt < 0) break;
+        if (lane < cnt) {
+            int e1 = 0;
+            for (int it = 0; it < A.spin_limit; it++) {   // the pusher is between its two steps
+                e1 = ld_acquire_gpu(&ring[lo + lane]);
+                if (e1 || ld_relaxed_gpu(&st[WS_ABORT])) break;
+            }
+            if (e1 == 0) atomicExch(&st[WS_ABORT], 1);
+            else {
+                const int e = e1 - 1;
+                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
+                const int v = __ldg(run_kn + r);
+                const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+                double row0[CD];
+                load_row(A, k0, row0);
+                const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                // release this entry's writes, then count into the successors
+                fence_acq_rel_gpu();
+                const int sides[2] = {sa, sb};
+#pragma unroll
+                for (int sd = 0; sd < 2; sd++) {
+                    const int sc = sides[sd];
+                    int ps, rs;
+                    if (sc >= 0) { ps = p; rs = sc; }
+                    else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
+                    else continue;
+                    if (atomicAdd(&arrived[rs], 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
+                        fence_acq_rel_gpu();             // acquire the other arrivals' writes
+                        wide_push(ring, st, wr, (ps << PASS_SHIFT) | rs, __ldg(run_kn + rs) >> 24);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && ld_relaxed_gpu(&st[WS_ABORT])) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweep
+}
+
+// ---------------------------------------------------------------------------
+// warm-start cache store of wide worlds (k_cache_copy, k_hash_build per world)
+// ---------------------------------------------------------------------------
+__global__ void k_wcache_copy(Arena A) {
+    if (overflowed(A)) return;
+    cache_copy_world(A, A.wide_w[blockIdx.y], *A.parity, wide_tid(), wide_stride());
+}
+
+__global__ void k_whash_build(Arena A) {
+    if (overflowed(A)) return;
+    hash_runs(A, 1 - *A.parity, A.wide_w[blockIdx.y], wide_tid(), wide_stride());
+}
+
+// ---------------------------------------------------------------------------
+// integrate positions and sleep of wide worlds (k_finalize's passes, each a
+// grid launch; the union-find works on the global parent array of the world,
+// roots the island's smallest index, so labels match k_finalize's):
+//   phase 0: positions; per body slow / ready flags, timer, parent = self
+//   phase 1: per contact: contacted flags and unions of dynamic pairs
+//   phase 2: per body: island label (root)
+//   phase 3: per body: a contacted body not ready marks its island not ready
+//   phase 4: per body: sleep or wake, island -1 without contact, rest at zero
+// ---------------------------------------------------------------------------
+__global__ void k_wfinalize(Arena A, int mode, int phase) {
+    if ((mode & FIN_GATED) && overflowed(A)) return;
+    const int w = A.wide_w[blockIdx.y];
+    if (!A.w_active[w]) return;
+    const double dt = A.w_dt[w];
+    const int b0 = A.w_body_off[w], nb = A.w_body_n[w], b1 = b0 + nb;
+    const bool sleep = (mode & FIN_SLEEP) && (A.w_flags[w] & WF_SLEEP);
+    int *flag = A.b_flag + b0, *parent = A.b_parent + b0;
+    if (phase == 0) {
+        for (int i = b0 + wide_tid(); i < b1; i += wide_stride()) {
+            if (mode & FIN_POSITIONS) {
+                const int t = A.mtype[i];
+                if ((t == 2 || t == 1) && A.awake[i]) {
+                    double *p = &A.pos[i * 3], *q = &A.q[i * 4];
+                    const double *v = &A.v[i * 3], *om = &A.w[i * 3];
+                    for (int c = 0; c < 3; c++) p[c] = p[c] + v[c] * dt;
+                    const double ax = om[0], ay = om[1], az = om[2], aw = 0.0;
+                    const double bx = q[0], by = q[1], bz = q[2], bw = q[3];
+                    double m[4];
+                    m[0] = aw * bx + ax * bw + ay * bz - az * by;
+                    m[1] = aw * by - ax * bz + ay * bw + az * bx;
+                    m[2] = aw * bz + ax * by - ay * bx + az * bw;
+                    m[3] = aw * bw - ax * bx - ay * by - az * bz;
+                    double s[4];
+                    for (int c = 0; c < 4; c++) s[c] = q[c] + (0.5 * m[c]) * dt;
+                    const double n = sqrt(((s[0] * s[0] + s[1] * s[1]) + s[2] * s[2]) + s[3] * s[3]);
+                    const double d = np_max(n, 1e-12);
+                    for (int c = 0; c < 4; c++) q[c] = s[c] / d;
+                }
+            }
+            if (!(mode & FIN_SLEEP)) continue;
+            if (!sleep) { A.b_island[i] = -1; continue; }
+            const double lin2 = 0.08 * 0.08, ang2 = 0.25 * 0.25;
+            const bool dyn_i = A.mtype[i] == 2;
+            const bool slow = dyn_i && speed2(&A.v[i * 3]) < lin2 && speed2(&A.w[i * 3]) < ang2;
+            if (slow) A.timer[i] += dt; else A.timer[i] = 0.0;
+            const bool ready = slow && A.timer[i] > 0.4;
+            flag[i - b0] = (slow ? BF_SLOW : 0) | (ready ? BF_READY : 0);
+            parent[i - b0] = i - b0;
+        }
+        return;
+    }
+    if (!sleep) return;
+    if (phase == 1) {
+        if (!world_collides(A, w)) return;
+        int c0, c1;
+        world_contacts(A, w, c0, c1);
+        for (int k = c0 + wide_tid(); k < c1; k += wide_stride()) {
+            const int a = A.c_a[k], b = A.c_b[k];
+            const bool da = A.mtype[a] == 2, db = A.mtype[b] == 2;
+            if (da) atomicOr(&flag[a - b0], BF_CONTACTED);
+            if (db) atomicOr(&flag[b - b0], BF_CONTACTED);
+            if (da && db) uf_union(parent, a - b0, b - b0);
+        }
+    } else if (phase == 2) {
+        for (int i = wide_tid(); i < nb; i += wide_stride()) A.b_island[b0 + i] = b0 + uf_find(parent, i);
+    } else if (phase == 3) {
+        for (int i = wide_tid(); i < nb; i += wide_stride()) {
+            const int f = ((volatile int *)flag)[i];
+            if ((f & BF_CONTACTED) && !(f & BF_READY)) atomicOr(&flag[A.b_island[b0 + i] - b0], BF_NOTREADY);
+        }
+    } else {
+        for (int i = b0 + wide_tid(); i < b1; i += wide_stride()) {
+            const int f = ((volatile int *)flag)[i - b0];
+            const bool dyn_i = A.mtype[i] == 2;
+            bool to_sleep;
+            if (f & BF_CONTACTED) to_sleep = !(((volatile int *)flag)[A.b_island[i] - b0] & BF_NOTREADY);
+            else to_sleep = dyn_i && (f & BF_READY);
+            if (!(f & BF_CONTACTED)) A.b_island[i] = -1;
+            if (to_sleep) A.awake[i] = 0;
+            if (dyn_i && !(f & BF_SLOW)) A.awake[i] = 1;
+            if (!A.awake[i] && dyn_i) {
+                for (int c = 0; c < 3; c++) { A.v[i * 3 + c] = 0.0; A.w[i * 3 + c] = 0.0; }
+            }
+        }
+    }
+}
+
+}  // namespace omi

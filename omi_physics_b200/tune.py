@@ -150,10 +150,13 @@ def _time_steps(groups, steps: int, warmup: int) -> float:
 
 
 def autotune(worlds: Sequence, dts: Sequence[float] = None, device: int = 0, steps: int = 10,
-             warmup: int = 3, rounds: int = 2, groups: Sequence[int] = None, save: bool = True) -> dict:
+             warmup: int = 3, rounds: int = 2, groups: Sequence[int] = None, save: bool = True,
+             preroll: int = 0) -> dict:
     """Search the launch configuration and the group count for ``worlds`` on
-    ``device`` and cache the result. The worlds' host columns are not
-    touched (their clocks are restored)."""
+    ``device`` and cache the result. Every candidate is timed after
+    ``preroll`` steps from the worlds' state (the regime the workload runs
+    in, e.g. settled piles). The worlds' host columns are not touched (their
+    clocks are restored)."""
     import torch
     from .groups import WorldGroups
     times = [w.time for w in worlds]
@@ -165,7 +168,7 @@ def autotune(worlds: Sequence, dts: Sequence[float] = None, device: int = 0, ste
         grp = WorldGroups(worlds, dts=dts, groups=g0, device=device, tuning=None, own_streams=True)
         seen = []
         try:
-            grp.step(warmup)                    # into contact, buffers grown
+            grp.step(preroll + warmup)          # into the workload's regime, buffers grown
 
             def measure_launch(cfg):
                 grp.set_tuning(cfg)
@@ -181,7 +184,7 @@ def autotune(worlds: Sequence, dts: Sequence[float] = None, device: int = 0, ste
             grp = WorldGroups(worlds, dts=dts, groups=g, device=device, tuning=None, own_streams=True)
             try:
                 grp.set_tuning(launch)
-                grp.step(warmup)
+                grp.step(preroll + warmup)
                 t = _time_steps(grp, steps, warmup)
                 trials += 1
             finally:

@@ -18,6 +18,7 @@ from omi_physics_b200 import build
 
 LIMITS = {            # kernel name fragment -> register ceiling
     'k_iterate': 224,
+    'k_wsweep': 224,
     'k_prep': 128,
     'k_finalize': 64,
     'k_pair_count': 64,
