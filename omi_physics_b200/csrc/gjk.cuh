@@ -38,13 +38,17 @@ struct Proxy {
     int m;
 };
 
-// Vertex indices are below EPA_V, so faces and edges are stored as bytes
-// (about 11 KB per warp).
+// Vertex indices are below EPA_V, so faces and edges are stored as bytes.
+// The lanes' rebuild marks the directed edges of the visible faces in a
+// bit table indexed by (from, to) and writes the new face list into F2.
+constexpr int EPA_EDGE_WORDS = (EPA_V * EPA_V + 31) / 32;
 struct EpaWork {
     double V[EPA_V][9];    // Minkowski point v, witness a, witness b
     unsigned char F[EPA_F][3];
     unsigned char E[EPA_E][2];
     unsigned char Ealive[EPA_E];
+    unsigned char F2[EPA_F][3];
+    unsigned int seen[EPA_EDGE_WORDS];   // zero between rebuilds
 };
 static_assert(EPA_V <= 256, "face and edge vertex indices are stored as bytes");
 
@@ -274,10 +278,10 @@ __device__ inline int closest_face(const EpaWork &W, int nf, double *bn, double 
     return win;
 }
 
-// _rebuild (gjk.py:197-217): visible faces found by all lanes, the ordered
-// horizon-edge dictionary kept by lane 0. Returns the new face count or -1
+// _rebuild (gjk.py:197-217) by lane 0 alone: the ordered horizon-edge
+// dictionary as the reference keeps it. Returns the new face count or -1
 // when the bounded storage (at most `face_cap` <= EPA_F faces) would overflow.
-__device__ inline int rebuild(EpaWork &W, int nf, int ni, int face_cap = EPA_F) {
+__device__ inline int rebuild_serial(EpaWork &W, int nf, int ni, int face_cap = EPA_F) {
     int out = 0;
     if (lane_id() == 0) {
         const double *w = W.V[ni];
@@ -320,6 +324,118 @@ __device__ inline int rebuild(EpaWork &W, int nf, int ni, int face_cap = EPA_F) 
     __syncwarp();
     return __shfl_sync(0xffffffffu, out, 0);
 }
+
+#ifdef OMI_HOST_EMULATION
+__device__ inline int rebuild(EpaWork &W, int nf, int ni, int face_cap = EPA_F) {
+    return rebuild_serial(W, nf, ni, face_cap);
+}
+#else
+__device__ __forceinline__ int edge_key(int u, int v) { return u * EPA_V + v; }
+
+// _rebuild (gjk.py:197-217) with the lanes splitting the faces. The
+// reference walks the faces that see the new point in order, and for each
+// of a face's edges (a, b), (b, c), (c, a) deletes the reverse edge from an
+// insertion-ordered dict if present, else inserts the edge; the surviving
+// edges, in insertion order, each make a new face with the new point, after
+// the faces that do not see it (in order). When no directed edge occurs
+// twice among the visible faces (a closed polytope: every edge borders two
+// faces), an edge survives exactly when its reverse is not among them, and
+// its insertion order is its own place in the walk - both found in parallel
+// from a bit table of the visible edges. A directed edge seen twice (a
+// degenerate polytope) falls back to the dictionary walk of rebuild_serial.
+__device__ inline int rebuild(EpaWork &W, int nf, int ni, int face_cap = EPA_F) {
+    const unsigned lane = lane_id();
+    const unsigned lt = (1u << lane) - 1u;
+    const double *w = W.V[ni];
+    bool dup = false;
+    int nvis = 0;
+    // visibility and the visible edges' bits
+    for (int base = 0; base < nf; base += 32) {
+        const int f = base + (int)lane;
+        bool vis = false;
+        if (f < nf) {
+            const double *a = W.V[W.F[f][0]];
+            double e1[3], e2[3], nr[3], wa[3];
+            sub3(W.V[W.F[f][1]], a, e1); sub3(W.V[W.F[f][2]], a, e2);
+            cross_np(e1, e2, nr);
+            sub3(w, a, wa);
+            vis = dot_blas(nr, wa) > 0;
+        }
+        if (vis) {
+            for (int e = 0; e < 3; e++) {
+                const int k = edge_key(W.F[f][e], W.F[f][(e + 1) % 3]);
+                const unsigned bit = 1u << (k & 31);
+                dup |= (atomicOr(&W.seen[k >> 5], bit) & bit) != 0;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, vis);
+        if (lane == 0) reinterpret_cast<unsigned *>(W.E)[base >> 5] = m;   // visibility words (E as scratch)
+        nvis += __popc(m);
+    }
+    __syncwarp();
+    dup = __any_sync(0xffffffffu, dup);
+    const unsigned *vmask = reinterpret_cast<const unsigned *>(W.E);
+    int out = -1;
+    if (!dup) {
+        // kept faces, in order, then the surviving edges' new faces, in walk order
+        const int K = nf - nvis;
+        int nk = 0, ns = 0;
+        for (int base = 0; base < nf; base += 32) {
+            const int f = base + (int)lane;
+            const unsigned m = vmask[base >> 5];
+            const bool valid = f < nf, vis = valid && ((m >> lane) & 1u);
+            const bool keep = valid && !vis;
+            const unsigned km = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int pos = nk + __popc(km & lt);
+                W.F2[pos][0] = W.F[f][0]; W.F2[pos][1] = W.F[f][1]; W.F2[pos][2] = W.F[f][2];
+            }
+            nk += __popc(km);
+            int cnt = 0;
+            bool surv[3] = {false, false, false};
+            if (vis) {
+                for (int e = 0; e < 3; e++) {
+                    const int u = W.F[f][e], v = W.F[f][(e + 1) % 3];
+                    const int k = edge_key(v, u);
+                    surv[e] = !((W.seen[k >> 5] >> (k & 31)) & 1u);
+                    cnt += surv[e];
+                }
+            }
+            int pre = cnt;                                    // inclusive warp scan of the counts
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                if ((int)lane >= o) pre += y;
+            }
+            int pos = K + ns + pre - cnt;
+            for (int e = 0; e < 3; e++) {
+                if (!surv[e]) continue;
+                if (pos < face_cap) {
+                    W.F2[pos][0] = W.F[f][e]; W.F2[pos][1] = W.F[f][(e + 1) % 3]; W.F2[pos][2] = (unsigned char)ni;
+                }
+                pos++;
+            }
+            ns += __shfl_sync(0xffffffffu, pre, 31);
+        }
+        out = K + ns > face_cap ? -1 : K + ns;
+    }
+    // clear the visible edges' bits for the next rebuild
+    __syncwarp();
+    for (int base = 0; base < nf; base += 32) {
+        const int f = base + (int)lane;
+        if (f < nf && ((vmask[base >> 5] >> lane) & 1u))
+            for (int e = 0; e < 3; e++) {
+                const int k = edge_key(W.F[f][e], W.F[f][(e + 1) % 3]);
+                atomicAnd(&W.seen[k >> 5], ~(1u << (k & 31)));
+            }
+    }
+    __syncwarp();
+    if (dup) return rebuild_serial(W, nf, ni, face_cap);
+    if (out > 0)
+        for (int i = (int)lane; i < out; i += 32) { W.F[i][0] = W.F2[i][0]; W.F[i][1] = W.F2[i][1]; W.F[i][2] = W.F2[i][2]; }
+    __syncwarp();
+    return out;
+}
+#endif
 
 // _contact_from_face + _barycentric (gjk.py:220-246)
 __device__ inline void face_contact(const EpaWork &W, int f, const double *nrm, double dist,
@@ -377,6 +493,7 @@ __device__ inline int epa(const Proxy &A, const Proxy &B, EpaWork &W, const Vt *
         const int init[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 3, 2}};
         for (int f = 0; f < 4; f++) for (int k = 0; k < 3; k++) W.F[f][k] = init[f][k];
     }
+    for (int i = lane_id(); i < EPA_EDGE_WORDS; i += WARP_LANES) W.seen[i] = 0u;
     __syncwarp();
     int nf = 4;
     double bn[3], bd;

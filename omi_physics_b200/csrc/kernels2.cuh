@@ -135,6 +135,9 @@ __global__ void k_hash_rebuild(Arena A, int t) {
 // ---------------------------------------------------------------------------
 enum { J_IA = 0, J_IB = 9, J_RA = 18, J_RB = 21, J_LU = 24, J_PIV = 33, J_BIAS = 36, J_N = 39,
        J_MASS = 42, J_BIASS = 43 };
+// joint iterations the wavefront schedule buffers hold per joint (a world
+// with more iterations sweeps iteration by iteration)
+constexpr int JOINT_WAVE_ITERS = 32;
 
 // joints.py:278-283: (R * invI) @ R.T through BLAS; zero for the world (-1)
 __device__ inline void joint_inv_inertia(const Arena &A, int i, double *W) {
@@ -336,6 +339,61 @@ __device__ inline void joint_solve(const Arena &A, int j, double dt) {
     joint_apply(A, b, &D[J_IB], &D[J_RB], P);
 }
 
+// A motor whose body is not dynamic changes only its own accumulated impulse
+// (it reads that body's constant angular velocity and writes nothing else).
+__device__ __forceinline__ bool motor_alone(const Arena &A, int j) {
+    return A.j_type[j] == 2 && (A.j_a[j] < 0 || A.mtype[A.j_a[j]] != 2);
+}
+
+// Wavefront levels of all joint iterations of one world (one warp): entry
+// e = it * J + jj is joint jj in iteration it; its level is one more than
+// that of the latest earlier entry, in the reference's order (iteration by
+// iteration, joints in registration order), sharing a dynamic body with it.
+// Iteration it + 1 of a joint so starts as soon as its own bodies are done
+// with iteration it: a chain of J joints takes about J + 2 * iters levels
+// instead of iters * J. A lone motor (motor_alone) runs all its iterations in
+// its iteration-0 entry, at level 0. Entries of one level share no dynamic
+// body, so running the levels in order repeats the sequential arithmetic.
+__device__ inline int warp_joint_levels(const Arena &A, int j0, int J, int iters, int *last, int *level,
+                                        int last_base) {
+    const int lane = threadIdx.x & 31;
+    const int n = J * iters;
+    int maxl = -1;
+    for (int base = 0; base < n; base += 32) {
+        const int e = base + lane;
+        const bool valid = e < n;
+        int a = -1, b = -1;
+        if (valid) {
+            const int j = j0 + e % J;
+            a = A.j_a[j];
+            b = A.j_type[j] == 2 ? -1 : A.j_b[j];
+        }
+        const bool da = a >= 0 && A.mtype[a] == 2, db = b >= 0 && A.mtype[b] == 2;
+        int lvl = 0;
+        if (da) lvl = max(lvl, ((volatile int *)last)[a - last_base] + 1);
+        if (db) lvl = max(lvl, ((volatile int *)last)[b - last_base] + 1);
+        unsigned conflict = 0;
+        for (int q = 0; q < 32; q++) {
+            const int aq = __shfl_sync(FULL, a, q), bq = __shfl_sync(FULL, b, q);
+            const bool c = q < lane && ((da && (a == aq || a == bq)) || (db && (b == aq || b == bq)));
+            conflict |= (c ? 1u : 0u) << q;
+        }
+        for (int q = 0; q < 32; q++) {
+            const int lq = __shfl_sync(FULL, lvl, q);
+            if ((conflict >> q) & 1u) lvl = max(lvl, lq + 1);
+        }
+        if (valid) {
+            level[e] = lvl;
+            if (da) atomicMax(&last[a - last_base], lvl);
+            if (db) atomicMax(&last[b - last_base], lvl);
+            maxl = max(maxl, lvl);
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(FULL, maxl, o));
+    return maxl + 1;
+}
+
 __global__ void k_joints(Arena A, int gated) {
     __shared__ int s_D;
     if (gated && overflowed(A)) return;
@@ -355,21 +413,36 @@ __global__ void k_joints(Arena A, int gated) {
         const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
         for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_last[i] = -1;
         __syncthreads();
+        const int iters = A.w_jiters[w];
+        const bool waves = iters <= JOINT_WAVE_ITERS;   // the schedule buffers hold that many iterations
+        const int E = waves ? J * iters : J;
+        int *lvl = A.j_level + (size_t)j0 * JOINT_WAVE_ITERS;
+        int *order = A.j_order + (size_t)j0 * JOINT_WAVE_ITERS;
+        int *ls = A.j_level_start + (size_t)j0 * JOINT_WAVE_ITERS + w;
+        int *cursor = A.j_level_start + ((size_t)A.NJ * JOINT_WAVE_ITERS + A.W + 1) + (size_t)j0 * JOINT_WAVE_ITERS + w;
         if (threadIdx.x < 32) {
-            const int D = warp_levels(J, A.j_a + j0, A.j_b + j0, A.mtype, A.b_last, A.j_level + j0);
+            const int D = waves ? warp_joint_levels(A, j0, J, iters, A.b_last, lvl, 0)
+                                : warp_levels(J, A.j_a + j0, A.j_b + j0, A.mtype, A.b_last, lvl);
             if (threadIdx.x == 0) s_D = D;
         }
         __syncthreads();
         const int D = s_D;
-        int *ls = A.j_level_start + j0 + w;
-        int *cursor = A.j_level_start + (A.NJ + A.W + 1) + j0 + w;
-        int *order = A.j_order + j0;
-        bucket_levels(J, D, A.j_level + j0, ls, cursor, order);
-        const int iters = A.w_jiters[w];
-        for (int it = 0; it < iters; it++) {
+        bucket_levels(E, D, lvl, ls, cursor, order);
+        if (waves) {
             for (int l = 0; l < D; l++) {
-                for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) joint_solve(A, j0 + order[q], dt);
+                for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) {
+                    const int e = order[q], j = j0 + e % J;
+                    if (!motor_alone(A, j)) joint_solve(A, j, dt);
+                    else if (e < J) for (int k = 0; k < iters; k++) joint_solve(A, j, dt);
+                }
                 __syncthreads();
+            }
+        } else {
+            for (int it = 0; it < iters; it++) {
+                for (int l = 0; l < D; l++) {
+                    for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) joint_solve(A, j0 + order[q], dt);
+                    __syncthreads();
+                }
             }
         }
     }

@@ -86,7 +86,8 @@ struct OmiCtx {
     int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
     // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
     int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
-    OmiTuning tune = {8, 4, 256, 16, 128, 4};   // launch configuration (omi_set_tuning)
+    OmiTuning tune = {8, 4, 256, 16, 128, 4, 32, 16};   // launch configuration (omi_set_tuning)
+    int cluster_max = 0;                        // largest thread-block cluster of k_csweep the GPU schedules
     // wide worlds (their stages on many blocks): the worlds, bodies of the largest, sort merge passes
     std::vector<int> h_wide;
     int wide_max_n = 0, wide_merge_passes = 0;
@@ -161,6 +162,9 @@ int grid_for(int n, int block, int cap) {
     int g = (n + block - 1) / block;
     return std::max(1, std::min(g, cap));
 }
+
+// dynamic shared memory of one k_csweep CTA (what a block may hold, less its static part)
+size_t sweep_cluster_smem() { return (size_t)SWEEP_SMEM_DOUBLES * sizeof(double) - 256; }
 
 // blocks of `block` threads for n items of a wide world, at most 8 per SM
 int wide_grid(const OmiCtx *ctx, int n, int block) {
@@ -393,11 +397,27 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
         k_iterate<8><<<std::min(A.W, ctx->sm_count), 256, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles,
                                                                                      ctx->tune.sweep_max_split);
     ctx->launches += 4;
-    for (int wi = 0; wi < nw; wi++) {          // one wide world at a time, on every SM
-        k_wsweep_init<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
-        k_wsweep_seed<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
-        k_wsweep<<<ctx->sm_count, SWEEP_THREADS, 0, ctx->stream>>>(A, wi);
-        ctx->launches += 3;
+    const int csmem_ints = (int)(sweep_cluster_smem() / sizeof(int));
+    if (nw && ctx->tune.wide_cluster == 16) {
+        for (int wi = 0; wi < nw; wi++)
+            k_csweep<16><<<16, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints);
+        ctx->launches += nw;
+    } else if (nw && ctx->tune.wide_cluster == 8) {
+        for (int wi = 0; wi < nw; wi++)
+            k_csweep<8><<<8, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints);
+        ctx->launches += nw;
+    } else if (nw && ctx->tune.wide_sweep_blocks == 1) {
+        // one block per wide world: the per-world sweep with its shared-memory staging
+        k_wsweep_one<<<nw, SWEEP_THREADS, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles);
+        ctx->launches++;
+    } else {
+        const int wb = std::min(ctx->tune.wide_sweep_blocks, ctx->sm_count);
+        for (int wi = 0; wi < nw; wi++) {      // one wide world at a time, on wb SMs
+            k_wsweep_init<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+            k_wsweep_seed<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+            k_wsweep<<<wb, SWEEP_THREADS, 0, ctx->stream>>>(A, wi);
+            ctx->launches += 3;
+        }
     }
     mark(ctx, pf, KN_SOLVE);
     if (ctx->has_triggers) {
@@ -602,6 +622,7 @@ int omi_create(int device, OmiCtx **out) {
         {(const void *)k_finalize, 2 * 8192 * (int)sizeof(int), "k_finalize"},
         {(const void *)k_prep, PREP_THREADS * CD * (int)sizeof(double), "k_prep"},
         {(const void *)k_wsort_tiles, WSORT_TILE * 24, "k_wsort_tiles"},
+        {(const void *)k_wsweep_one, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_wsweep_one"},
     };
     for (const auto &f : smem) {
         e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
@@ -610,6 +631,30 @@ int omi_create(int device, OmiCtx **out) {
             *out = ctx;
             return rc;
         }
+    }
+    // the cluster sweep: 16 CTAs when the GPU schedules such clusters, else 8
+    ctx->cluster_max = 0;
+    {
+        const int bytes = (int)sweep_cluster_smem();
+        if (cudaFuncSetAttribute(k_csweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+            cudaFuncSetAttribute(k_csweep<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+            cudaFuncSetAttribute(k_csweep<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            for (int c : {16, 8}) {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = c; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(c); cfg.blockDim = dim3(SWEEP_THREADS); cfg.dynamicSmemBytes = bytes;
+                cfg.attrs = at; cfg.numAttrs = 1;
+                int n = 0;
+                const cudaError_t q = c == 16 ? cudaOccupancyMaxActiveClusters(&n, (void *)k_csweep<16>, &cfg)
+                                              : cudaOccupancyMaxActiveClusters(&n, (void *)k_csweep<8>, &cfg);
+                if (q == cudaSuccess && n >= 1) { ctx->cluster_max = c; break; }
+                cudaGetLastError();
+            }
+        }
+        cudaGetLastError();
+        ctx->tune.wide_cluster = ctx->cluster_max;
     }
     *out = ctx;
     return 0;
@@ -946,9 +991,9 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     rc |= upload(ctx, A.j_has_local_b, s->j_has_local_b, NJ);
     rc |= upload(ctx, A.j_has_length, s->j_has_length, NJ);
     rc |= alloc(ctx, ctx->statics, A.j_data, (size_t)NJ * JD);
-    rc |= alloc(ctx, ctx->statics, A.j_level, NJ);
-    rc |= alloc(ctx, ctx->statics, A.j_order, NJ);
-    rc |= alloc(ctx, ctx->statics, A.j_level_start, 2 * ((size_t)NJ + W + 1));
+    rc |= alloc(ctx, ctx->statics, A.j_level, (size_t)NJ * JOINT_WAVE_ITERS);
+    rc |= alloc(ctx, ctx->statics, A.j_order, (size_t)NJ * JOINT_WAVE_ITERS);
+    rc |= alloc(ctx, ctx->statics, A.j_level_start, 2 * ((size_t)NJ * JOINT_WAVE_ITERS + W + 1));
     // per-body scratch
     rc |= alloc(ctx, ctx->statics, A.order, NB);
     rc |= alloc(ctx, ctx->statics, A.sorted_x, NB);
@@ -1414,7 +1459,10 @@ int omi_set_tuning(OmiCtx *ctx, const OmiTuning *t) {
                     (t->pair_block == 128 || t->pair_block == 256 || t->pair_block == 512) &&
                     t->pair_blocks_per_sm >= 1 && t->pair_blocks_per_sm <= 32 &&
                     (t->narrow_block == 64 || t->narrow_block == 128 || t->narrow_block == 256) &&
-                    (t->gjk_warps == 2 || t->gjk_warps == 4 || t->gjk_warps == 8);
+                    (t->gjk_warps == 2 || t->gjk_warps == 4 || t->gjk_warps == 8) &&
+                    t->wide_sweep_blocks >= 1 && t->wide_sweep_blocks <= 1024 &&
+                    (t->wide_cluster == 0 || t->wide_cluster == 8 || t->wide_cluster == 16) &&
+                    t->wide_cluster <= ctx->cluster_max;
     if (!ok) return fail(ctx, OMI_E_ARG, "launch configuration out of range");
     cudaStreamSynchronize(ctx->stream);
     drop_graph(ctx);                     // re-captured with the new launches on the next step

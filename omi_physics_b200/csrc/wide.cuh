@@ -7,6 +7,8 @@
 // Launches carry the wide world's index in blockIdx.y (or as an argument for
 // the sweep); x runs over the world's bodies, contacts or runs, grid-stride.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "kernels2.cuh"
 
 namespace omi {
@@ -411,6 +413,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
         int lo = 0, cnt = 0;
         if (lane == 0) {
             const int first = ((threadIdx.x >> 5) + blockIdx.x) & (SWEEP_CLASSES - 1);
+            int idle = 0;
             for (int it = 0;; it++) {
                 if (ld_relaxed_gpu(&st[WS_CLAIMED]) >= N || ld_relaxed_gpu(&st[WS_ABORT])) { cnt = -1; break; }
                 bool got = false;
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
                 }
                 if (got) break;
                 if (it >= A.spin_limit) { atomicExch(&st[WS_ABORT], 1); cnt = -1; break; }
-                __nanosleep(64);
+                __nanosleep(min(32 << min(idle++, 5), 1024));      // back off while nothing is ready
             }
         }
         cnt = __shfl_sync(FULL, cnt, 0);
@@ -473,6 +476,217 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
     }
     if (lane == 0 && ld_relaxed_gpu(&st[WS_ABORT])) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
     if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweep
+}
+
+// the sweep of wide world blockIdx.x by one block: k_iterate's sweep_world on
+// the tables the wide links wrote (the same format as k_levels')
+__global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep_one(Arena A, int smem_doubles) {
+    extern __shared__ __align__(16) double smem_d[];
+    __shared__ SweepShared sh;
+    if (overflowed(A)) return;
+    const int w = A.wide_w[blockIdx.x];
+    if (!world_collides(A, w)) return;
+    sweep_world(A, w, smem_d, smem_doubles, threadIdx.x, SWEEP_THREADS, 0, sh);
+}
+
+// ---------------------------------------------------------------------------
+// The contact sweep of one wide world on one thread-block cluster of C CTAs
+// (co-scheduled by the hardware, so every CTA of it is resident). The runs
+// are split into C contiguous ranges (contacts come in pair order, so a range
+// is a slab of the world); CTA b owns the entries of its range: their arrival
+// counts and work ring live in its shared memory (or, when they do not fit,
+// in the world's global slices of them) and only its warps claim them. An
+// entry whose last predecessor finishes in another CTA is counted and
+// published through distributed shared memory with cluster-scope release /
+// acquire; everything else stays CTA-local. The dataflow - entries, their
+// predecessor counts, the per-class rings - is k_iterate's, so the results
+// are the same bits. Velocities, positions and impulses stay in global
+// memory. Waits are bounded as in k_wsweep.
+// ---------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+
+struct ClusterShared {
+    int head[SWEEP_CLASSES], tail[SWEEP_CLASSES], size[SWEEP_CLASSES], base[SWEEP_CLASSES];
+    int hist[4];
+    int claimed, abort;
+};
+
+__device__ __forceinline__ int ld_acquire_cluster(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cluster.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cluster(int *p, int v) {
+    asm volatile("st.release.cluster.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_cluster() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+
+// the CTA owning run r of R, and the first run of CTA b, for C CTAs
+__device__ __forceinline__ int cl_home(int r, int R, int C) { return (int)(((long long)r * C) / R); }
+__device__ __forceinline__ int cl_first(int b, int R, int C) { return (int)(((long long)b * R + C - 1) / C); }
+
+// where CTA h keeps its arrival counts and ring
+struct ClusterHome {
+    int *arrived;    // indexed by run - first run of h
+    int *ring;
+};
+
+template <int C>
+__device__ __forceinline__ ClusterHome cl_home_arrays(const Arena &A, cg::cluster_group &cluster, int *csm, int h,
+                                                      int R, int P, int c0, int smem_ints, int me) {
+    const int r0 = cl_first(h, R, C), rb = cl_first(h + 1, R, C) - r0;
+    ClusterHome H;
+    if ((long long)(P + 1) * rb <= smem_ints) {
+        int *base = h == me ? csm : cluster.map_shared_rank(csm, h);
+        H.arrived = base;
+        H.ring = base + rb;
+    } else {
+        H.arrived = A.run_done + c0 + r0;
+        H.ring = A.c_order + (size_t)c0 * A.max_passes + (size_t)P * r0;
+    }
+    return H;
+}
+
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csweep(Arena A, int wi, int smem_ints) {
+    extern __shared__ __align__(16) int csm[];
+    __shared__ ClusterShared cs;
+    cg::cluster_group cluster = cg::this_cluster();
+    // every CTA takes the same early exits (they read the same words), so all
+    // or none reach the cluster barriers below
+    if (overflowed(A)) return;
+    const int w = A.wide_w[wi];
+    if (!world_collides(A, w)) return;
+    const int R = A.w_runs[w];
+    if (R == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = 0;
+        return;
+    }
+    const int me = (int)cluster.block_rank();
+    int c0, c1;
+    world_contacts(A, w, c0, c1);
+    const int P = world_passes(A, w);
+    const int r0 = cl_first(me, R, C), Rb = cl_first(me + 1, R, C) - r0;
+    const int Nb = P * Rb;
+    int *gabort = &A.wide_state[wi * WIDE_STATE_INTS + WS_ABORT];
+    const ClusterHome mine = cl_home_arrays<C>(A, cluster, csm, me, R, P, c0, smem_ints, me);
+    if (threadIdx.x < SWEEP_CLASSES) { cs.head[threadIdx.x] = 0; cs.tail[threadIdx.x] = 0; }
+    if (threadIdx.x < 4) cs.hist[threadIdx.x] = 0;
+    if (threadIdx.x == 0) { cs.claimed = 0; cs.abort = 0; }
+    __syncthreads();
+    for (int i = threadIdx.x; i < Rb; i += blockDim.x) {
+        mine.arrived[i] = 0;
+        atomicAdd(&cs.hist[min(A.run_kn[c0 + r0 + i] >> 24, 4) - 1], 1);
+    }
+    for (int e = threadIdx.x; e < Nb; e += blockDim.x) mine.ring[e] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = 0; c < SWEEP_CLASSES; c++) {
+            const int cnt = cs.hist[c & 3];
+            cs.size[c] = c >= 4 ? cnt : cnt * (P - 1);
+            cs.base[c] = acc;
+            acc += cs.size[c];
+        }
+    }
+    __threadfence_block();
+    cluster.sync();               // every CTA's ring and counts ready before any push crosses CTAs
+    const int *run_kn = A.run_kn + c0, *run_need = A.run_need + c0;
+    const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
+    const bool warm = (A.w_flags[w] & WF_WARM) != 0;
+    const bool vel = warm || A.w_iters[w] > 0;
+    const double slop = A.w_solver[w * 2 + 1];
+    VelView V;
+    V.s = nullptr;
+    V.b0 = A.w_body_off[w];
+    ImpView I;
+    I.s = nullptr;
+    I.c0 = c0;
+    // publish entry e (run rs of pass ps) to its home's ring
+    auto push = [&](int e, int rs) {
+        const int h = cl_home(rs, R, C);
+        ClusterShared *hs = h == me ? &cs : cluster.map_shared_rank(&cs, h);
+        const ClusterHome H = h == me ? mine : cl_home_arrays<C>(A, cluster, csm, h, R, P, c0, smem_ints, me);
+        const int c = entry_class(e >> PASS_SHIFT, __ldg(run_kn + rs) >> 24, true);
+        const int pos = atomicAdd(&hs->tail[c], 1);
+        if (pos >= hs->size[c]) { cs.abort = 1; atomicExch(gabort, 1); return; }   // never with a consistent graph
+        st_release_cluster(&H.ring[hs->base[c] + pos], e + 1);
+    };
+    for (int r = r0 + (int)threadIdx.x; r < r0 + Rb; r += blockDim.x)
+        if ((__ldg(run_need + r) & 3) == 0) push(r, r);
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int lo = 0, cnt = 0;
+        if (lane == 0) {
+            const int first = (threadIdx.x >> 5) & (SWEEP_CLASSES - 1);
+            for (int it = 0;; it++) {
+                if (*(volatile int *)&cs.claimed >= Nb || *(volatile int *)&cs.abort) { cnt = -1; break; }
+                bool got = false;
+                for (int j = 0; j < SWEEP_CLASSES && !got; j++) {
+                    const int c = (first + j) & (SWEEP_CLASSES - 1);
+                    const int h = *(volatile int *)&cs.head[c];
+                    const int t = min(*(volatile int *)&cs.tail[c], cs.size[c]);
+                    if (t > h) {
+                        const int want = min(t - h, 32);
+                        if (atomicCAS(&cs.head[c], h, h + want) == h) {
+                            atomicAdd(&cs.claimed, want);
+                            lo = cs.base[c] + h;
+                            cnt = want;
+                            got = true;
+                        }
+                    }
+                }
+                if (got) break;
+                if (it >= A.spin_limit) { cs.abort = 1; atomicExch(gabort, 1); cnt = -1; break; }
+                if ((it & 255) == 255 && ld_relaxed_gpu(gabort)) { cs.abort = 1; cnt = -1; break; }
+                __nanosleep(32);
+            }
+        }
+        cnt = __shfl_sync(FULL, cnt, 0);
+        lo = __shfl_sync(FULL, lo, 0);
+        if (cnt < 0) break;
+        if (lane < cnt) {
+            int e1 = 0;
+            for (int it = 0; it < A.spin_limit; it++) {   // the pusher is between its two steps
+                e1 = ld_acquire_cluster(&mine.ring[lo + lane]);
+                if (e1 || *(volatile int *)&cs.abort) break;
+            }
+            if (e1 == 0) { cs.abort = 1; atomicExch(gabort, 1); }
+            else {
+                const int e = e1 - 1;
+                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
+                const int v = __ldg(run_kn + r);
+                const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+                double row0[CD];
+                load_row(A, k0, row0);
+                const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                fence_acq_rel_cluster();                 // release this entry's writes
+                const int sides[2] = {sa, sb};
+#pragma unroll
+                for (int sd = 0; sd < 2; sd++) {
+                    const int sc = sides[sd];
+                    int ps, rs;
+                    if (sc >= 0) { ps = p; rs = sc; }
+                    else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
+                    else continue;
+                    const int h = cl_home(rs, R, C);
+                    int *arr = h == me ? mine.arrived + (rs - r0)
+                                       : cl_home_arrays<C>(A, cluster, csm, h, R, P, c0, smem_ints, me).arrived +
+                                             (rs - cl_first(h, R, C));
+                    if (atomicAdd(arr, 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
+                        fence_acq_rel_cluster();         // acquire the other arrivals' writes
+                        push((ps << PASS_SHIFT) | rs, rs);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && *(volatile int *)&cs.abort) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
+    if (me == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweeps
+    __syncthreads();
+    cluster.sync();               // no CTA leaves while another may still reach its shared memory
 }
 
 // ---------------------------------------------------------------------------

@@ -25,7 +25,7 @@ import math
 import os
 from typing import Callable, Dict, Optional, Sequence
 
-from ._lib import DEFAULT_TUNING
+from ._lib import OmiError
 
 #: values each launch parameter may take, the default first
 SPACE = {
@@ -35,6 +35,8 @@ SPACE = {
     'pair_blocks_per_sm': (16, 8, 32),
     'narrow_block': (128, 64, 256),
     'gjk_warps': (4, 2, 8),
+    'wide_sweep_blocks': (32, 1, 8, 16, 64, 148),
+    'wide_cluster': (16, 8, 0),
 }
 #: group counts tried for a many-world workload (a single world is one group)
 GROUP_CHOICES = (4, 2, 3, 6)
@@ -171,10 +173,14 @@ def autotune(worlds: Sequence, dts: Sequence[float] = None, device: int = 0, ste
             grp.step(preroll + warmup)          # into the workload's regime, buffers grown
 
             def measure_launch(cfg):
-                grp.set_tuning(cfg)
+                try:
+                    grp.set_tuning(cfg)
+                except OmiError:                # a choice this GPU cannot run (e.g. a 16-CTA cluster)
+                    return float('inf')
                 seen.append(_time_steps(grp, steps, warmup))
                 return seen[-1]
-            launch, ms, n = coordinate_search(measure_launch, SPACE, dict(DEFAULT_TUNING), rounds)
+            start = grp.batches[0].ctx.tuning()  # the library's defaults for this GPU
+            launch, ms, n = coordinate_search(measure_launch, SPACE, start, rounds)
             trials += n
         finally:
             grp.close()
