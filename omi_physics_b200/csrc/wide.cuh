@@ -508,7 +508,7 @@ namespace cg = cooperative_groups;
 struct ClusterShared {
     int head[SWEEP_CLASSES], tail[SWEEP_CLASSES], size[SWEEP_CLASSES], base[SWEEP_CLASSES];
     int hist[4];
-    int claimed, abort;
+    int claimed, abort, n_owned, fit, staged, imp_staged;
 };
 
 __device__ __forceinline__ int ld_acquire_cluster(const int *p) {
@@ -525,7 +525,17 @@ __device__ __forceinline__ void fence_acq_rel_cluster() { asm volatile("fence.ac
 __device__ __forceinline__ int cl_home(int r, int R, int C) { return (int)(((long long)r * C) / R); }
 __device__ __forceinline__ int cl_first(int b, int R, int C) { return (int)(((long long)b * R + C - 1) / C); }
 
-// where CTA h keeps its arrival counts and ring
+// Shared memory of CTA h (ints; rb = its runs): arrival counts (rb), work
+// ring (P * rb), the slots of each run's two bodies (2 * rb), the bodies it
+// owns (2 * rb at most: a body is owned by the CTA of its first run), then,
+// 8-byte aligned, the owned bodies' records - v (3), w (3), pos (3) - and,
+// when room is left, the impulses of its contacts.
+constexpr int CL_REC = 9;
+__device__ __forceinline__ int cl_ints(int rb, int P) { return rb * (1 + P + 2 + 2); }
+__device__ __forceinline__ int cl_rec_off(int rb, int P) { return (cl_ints(rb, P) + 1) & ~1; }   // in ints
+
+// where CTA h keeps its arrival counts and ring (its shared memory when the
+// tables fit, else the world's global slices of them)
 struct ClusterHome {
     int *arrived;    // indexed by run - first run of h
     int *ring;
@@ -536,7 +546,7 @@ __device__ __forceinline__ ClusterHome cl_home_arrays(const Arena &A, cg::cluste
                                                       int R, int P, int c0, int smem_ints, int me) {
     const int r0 = cl_first(h, R, C), rb = cl_first(h + 1, R, C) - r0;
     ClusterHome H;
-    if ((long long)(P + 1) * rb <= smem_ints) {
+    if ((long long)cl_ints(rb, P) <= smem_ints) {
         int *base = h == me ? csm : cluster.map_shared_rank(csm, h);
         H.arrived = base;
         H.ring = base + rb;
@@ -547,6 +557,67 @@ __device__ __forceinline__ ClusterHome cl_home_arrays(const Arena &A, cg::cluste
     return H;
 }
 
+// run_pass on staged bodies: ra / rb are the bodies' records (v, w, pos) in
+// their owners' shared memory, or nullptr for a body that is not dynamic
+// (read from the global arrays, never written)
+__device__ __forceinline__ void run_pass_rec(const Arena &A, double *ra, double *rb, const ImpView &I,
+                                             const double *row0, int k0, int n, bool vel, bool warm_pass,
+                                             bool pos_pass, double slop) {
+    PairRow r;
+    load_pair(row0, r);
+    PairVel s;
+    double pa[3], pb[3];
+    for (int q = 0; q < 3; q++) {
+        s.la[q] = ra ? ra[q] : A.v[r.a * 3 + q];
+        s.aa[q] = ra ? ra[3 + q] : A.w[r.a * 3 + q];
+        s.lb[q] = rb ? rb[q] : A.v[r.b * 3 + q];
+        s.ab[q] = rb ? rb[3 + q] : A.w[r.b * 3 + q];
+    }
+    if (pos_pass)
+        for (int q = 0; q < 3; q++) {
+            pa[q] = ra ? ra[6 + q] : A.pos[r.a * 3 + q];
+            pb[q] = rb ? rb[6 + q] : A.pos[r.b * 3 + q];
+        }
+    double cur[C_PART];
+#pragma unroll
+    for (int q = 0; q < C_PART; q++) cur[q] = row0[q];
+    for (int i = 0; i < n; i++) {
+        ContactRow c;
+        load_contact(cur, c);
+        if (i + 1 < n) {
+            const double2 *g = reinterpret_cast<const double2 *>(&A.c_data[(size_t)(k0 + i + 1) * CD]);
+#pragma unroll
+            for (int q = 0; q < C_PART / 2; q++) {
+                const double2 t = __ldg(g + q);
+                cur[2 * q] = t.x;
+                cur[2 * q + 1] = t.y;
+            }
+        }
+        if (vel) {
+            double *ip = imp_ptr(A, I, k0 + i);
+            double imp[3] = {ip[0], ip[1], ip[2]};
+            if (warm_pass) contact_warm(s, r, c, imp);
+            else {
+                contact_solve(s, r, c, imp);
+                ip[0] = imp[0]; ip[1] = imp[1]; ip[2] = imp[2];
+            }
+        }
+        if (pos_pass) contact_position(pa, pb, r, c, slop);
+    }
+    if (r.da) for (int q = 0; q < 3; q++) { ra[q] = s.la[q]; ra[3 + q] = s.aa[q]; }
+    if (r.db) for (int q = 0; q < 3; q++) { rb[q] = s.lb[q]; rb[3 + q] = s.ab[q]; }
+    if (pos_pass) {
+        if (r.da) for (int q = 0; q < 3; q++) ra[6 + q] = pa[q];
+        if (r.db) for (int q = 0; q < 3; q++) rb[6 + q] = pb[q];
+    }
+}
+
+// The sweep on one cluster. Bodies: when every CTA's share fits (the
+// cluster agrees on it), each dynamic body's record lives in the shared
+// memory of the CTA of its first run and the others reach it through
+// distributed shared memory; otherwise records are the global arrays.
+// A CTA whose successors and written records are all its own releases with
+// a CTA-scope fence, else cluster scope.
 template <int C>
 __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csweep(Arena A, int wi, int smem_ints) {
     extern __shared__ __align__(16) int csm[];
@@ -565,18 +636,41 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
     const int me = (int)cluster.block_rank();
     int c0, c1;
     world_contacts(A, w, c0, c1);
+    const int K = c1 - c0;
     const int P = world_passes(A, w);
     const int r0 = cl_first(me, R, C), Rb = cl_first(me + 1, R, C) - r0;
     const int Nb = P * Rb;
     int *gabort = &A.wide_state[wi * WIDE_STATE_INTS + WS_ABORT];
+    int *slotmap = A.wl_cnt;                      // per body: owner << 20 | slot (free after the links)
+    const int *run_kn = A.run_kn + c0, *run_need = A.run_need + c0;
+    const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
     const ClusterHome mine = cl_home_arrays<C>(A, cluster, csm, me, R, P, c0, smem_ints, me);
+    const bool tables_local = cl_ints(Rb, P) <= smem_ints;
+    int *rslot = csm + Rb * (1 + P);              // (when tables_local) 2 per run
+    int *owned = rslot + 2 * Rb;                  // (when tables_local) owned bodies
+    double *recs = reinterpret_cast<double *>(csm + cl_rec_off(Rb, P));
     if (threadIdx.x < SWEEP_CLASSES) { cs.head[threadIdx.x] = 0; cs.tail[threadIdx.x] = 0; }
     if (threadIdx.x < 4) cs.hist[threadIdx.x] = 0;
-    if (threadIdx.x == 0) { cs.claimed = 0; cs.abort = 0; }
+    if (threadIdx.x == 0) { cs.claimed = 0; cs.abort = 0; cs.n_owned = 0; }
     __syncthreads();
     for (int i = threadIdx.x; i < Rb; i += blockDim.x) {
+        const int r = r0 + i;
         mine.arrived[i] = 0;
-        atomicAdd(&cs.hist[min(A.run_kn[c0 + r0 + i] >> 24, 4) - 1], 1);
+        atomicAdd(&cs.hist[min(run_kn[r] >> 24, 4) - 1], 1);
+        if (!tables_local) continue;
+        // a body belongs to the CTA of its first run (whose predecessor code points to the previous pass)
+        const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
+        const int pa = A.run_pa[c0 + r], pb = A.run_pb[c0 + r];
+        if (a >= 0 && pa < 0 && pa != LEVEL_NONE) {
+            const int sl = atomicAdd(&cs.n_owned, 1);
+            owned[sl] = a;
+            slotmap[a] = (me << 20) | sl;
+        }
+        if (b >= 0 && pb < 0 && pb != LEVEL_NONE) {
+            const int sl = atomicAdd(&cs.n_owned, 1);
+            owned[sl] = b;
+            slotmap[b] = (me << 20) | sl;
+        }
     }
     for (int e = threadIdx.x; e < Nb; e += blockDim.x) mine.ring[e] = 0;
     __syncthreads();
@@ -588,20 +682,60 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
             cs.base[c] = acc;
             acc += cs.size[c];
         }
+        cs.fit = tables_local && (long long)cl_rec_off(Rb, P) + 2LL * CL_REC * cs.n_owned <= smem_ints;
     }
-    __threadfence_block();
-    cluster.sync();               // every CTA's ring and counts ready before any push crosses CTAs
-    const int *run_kn = A.run_kn + c0, *run_need = A.run_need + c0;
-    const int *run_sa = A.run_sa + c0, *run_sb = A.run_sb + c0;
+    __threadfence();
+    cluster.sync();               // rings, counts, ownership and fit flags ready cluster-wide
+    if (threadIdx.x == 0) {
+        int all = 1;
+        for (int h = 0; h < C; h++) all &= cluster.map_shared_rank(&cs, h)->fit;
+        cs.staged = all;
+    }
+    __syncthreads();
+    const bool staged = cs.staged != 0;
+    // impulses of this CTA's contacts (a contiguous range: its runs') in shared memory when room is left
+    const int k_lo = Rb ? (run_kn[r0] & 0xFFFFFF) : 0;
+    const int k_hi = Rb ? (r0 + Rb < R ? (run_kn[r0 + Rb] & 0xFFFFFF) : K) : 0;
+    ImpView I;
+    I.s = nullptr;
+    I.c0 = c0 + k_lo;
+    if (staged) {
+        for (int i = threadIdx.x; i < cs.n_owned; i += blockDim.x) {
+            const int body = owned[i];
+            double *rec = recs + (size_t)i * CL_REC;
+            for (int q = 0; q < 3; q++) {
+                rec[q] = A.v[body * 3 + q];
+                rec[3 + q] = A.w[body * 3 + q];
+                rec[6 + q] = A.pos[body * 3 + q];
+            }
+        }
+        for (int i = threadIdx.x; i < Rb; i += blockDim.x) {
+            const int a = A.run_a[c0 + r0 + i], b = A.run_b[c0 + r0 + i];
+            rslot[2 * i] = a >= 0 ? slotmap[a] : -1;
+            rslot[2 * i + 1] = b >= 0 ? slotmap[b] : -1;
+        }
+        const long long imp_off = ((long long)cl_rec_off(Rb, P) + 2LL * CL_REC * cs.n_owned + 3) & ~3LL;
+        if (imp_off + 2LL * 3 * (k_hi - k_lo) <= smem_ints) {
+            I.s = reinterpret_cast<double *>(csm + imp_off);
+            for (int i = threadIdx.x; i < 3 * (k_hi - k_lo); i += blockDim.x) I.s[i] = A.c_imp[(c0 + k_lo) * 3 + i];
+        }
+    }
+    __syncthreads();
+    cluster.sync();               // every record staged before any CTA reaches another's
     const bool warm = (A.w_flags[w] & WF_WARM) != 0;
     const bool vel = warm || A.w_iters[w] > 0;
     const double slop = A.w_solver[w * 2 + 1];
     VelView V;
     V.s = nullptr;
     V.b0 = A.w_body_off[w];
-    ImpView I;
-    I.s = nullptr;
-    I.c0 = c0;
+    // the record of a staged body in its owner's shared memory
+    auto rec_of = [&](int slot) -> double * {
+        if (slot < 0) return nullptr;
+        const int h = slot >> 20;
+        const int hr = cl_first(h + 1, R, C) - cl_first(h, R, C);
+        double *base = reinterpret_cast<double *>((h == me ? csm : cluster.map_shared_rank(csm, h)) + cl_rec_off(hr, P));
+        return base + (size_t)(slot & 0xFFFFF) * CL_REC;
+    };
     // publish entry e (run rs of pass ps) to its home's ring
     auto push = [&](int e, int rs) {
         const int h = cl_home(rs, R, C);
@@ -610,7 +744,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
         const int c = entry_class(e >> PASS_SHIFT, __ldg(run_kn + rs) >> 24, true);
         const int pos = atomicAdd(&hs->tail[c], 1);
         if (pos >= hs->size[c]) { cs.abort = 1; atomicExch(gabort, 1); return; }   // never with a consistent graph
-        st_release_cluster(&H.ring[hs->base[c] + pos], e + 1);
+        if (h == me) st_release_cta(&H.ring[hs->base[c] + pos], e + 1);
+        else st_release_cluster(&H.ring[hs->base[c] + pos], e + 1);
     };
     for (int r = r0 + (int)threadIdx.x; r < r0 + Rb; r += blockDim.x)
         if ((__ldg(run_need + r) & 3) == 0) push(r, r);
@@ -660,16 +795,40 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                 double row0[CD];
                 load_row(A, k0, row0);
                 const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
-                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
-                fence_acq_rel_cluster();                 // release this entry's writes
+                bool remote;
+                if (staged) {
+                    const int s0 = rslot[2 * (r - r0)], s1 = rslot[2 * (r - r0) + 1];
+                    run_pass_rec(A, rec_of(s0), rec_of(s1), I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                    remote = (s0 >= 0 && (s0 >> 20) != me) || (s1 >= 0 && (s1 >> 20) != me);
+                } else {
+                    run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                    remote = true;                       // global records: other CTAs read them
+                }
+                int ps_[2], rs_[2], m = 0;
                 const int sides[2] = {sa, sb};
 #pragma unroll
                 for (int sd = 0; sd < 2; sd++) {
                     const int sc = sides[sd];
-                    int ps, rs;
-                    if (sc >= 0) { ps = p; rs = sc; }
-                    else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
-                    else continue;
+                    if (sc >= 0) { ps_[m] = p; rs_[m] = sc; m++; }
+                    else if (sc != LEVEL_NONE && p + 1 < P) { ps_[m] = p + 1; rs_[m] = -sc - 1; m++; }
+                }
+                // a successor owned elsewhere, or one whose other predecessor is owned
+                // elsewhere (whose last arrival may then acquire these writes), needs
+                // the cluster-scope release
+                for (int q = 0; q < m && !remote; q++) {
+                    const int rs = rs_[q];
+                    remote |= cl_home(rs, R, C) != me;
+                    const int pc[2] = {__ldg(A.run_pa + c0 + rs), __ldg(A.run_pb + c0 + rs)};
+                    for (int t = 0; t < 2; t++) {
+                        if (pc[t] == LEVEL_NONE) continue;
+                        const int pr = pc[t] >= 0 ? pc[t] : -pc[t] - 1;
+                        remote |= cl_home(pr, R, C) != me;
+                    }
+                }
+                // release this entry's writes: to this CTA alone, or to the cluster
+                if (remote) fence_acq_rel_cluster(); else fence_acq_rel_cta();
+                for (int q = 0; q < m; q++) {
+                    const int rs = rs_[q], ps = ps_[q];
                     const int h = cl_home(rs, R, C);
                     int *arr = h == me ? mine.arrived + (rs - r0)
                                        : cl_home_arrays<C>(A, cluster, csm, h, R, P, c0, smem_ints, me).arrived +
@@ -686,7 +845,20 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
     if (lane == 0 && *(volatile int *)&cs.abort) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
     if (me == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweeps
     __syncthreads();
-    cluster.sync();               // no CTA leaves while another may still reach its shared memory
+    cluster.sync();               // every entry done: records final, no CTA reaches another's memory after this
+    if (staged) {
+        for (int i = threadIdx.x; i < cs.n_owned; i += blockDim.x) {
+            const int body = owned[i];
+            const double *rec = recs + (size_t)i * CL_REC;
+            for (int q = 0; q < 3; q++) {
+                A.v[body * 3 + q] = rec[q];
+                A.w[body * 3 + q] = rec[3 + q];
+                A.pos[body * 3 + q] = rec[6 + q];
+            }
+        }
+        if (I.s)
+            for (int i = threadIdx.x; i < 3 * (k_hi - k_lo); i += blockDim.x) A.c_imp[(c0 + k_lo) * 3 + i] = I.s[i];
+    }
 }
 
 // ---------------------------------------------------------------------------
