@@ -527,11 +527,16 @@ __device__ __forceinline__ int cl_first(int b, int R, int C) { return (int)(((lo
 
 // Shared memory of CTA h (ints; rb = its runs): arrival counts (rb), work
 // ring (P * rb), the slots of each run's two bodies (2 * rb), the bodies it
-// owns (2 * rb at most: a body is owned by the CTA of its first run), then,
-// 8-byte aligned, the owned bodies' records - v (3), w (3), pos (3) - and,
-// when room is left, the impulses of its contacts.
+// owns (2 * rb at most: a body is owned by the CTA of its first run), its
+// runs' tables (CL_TAB * rb: packed first contact and count, need counts,
+// the two successor codes, and whether a predecessor lies in another CTA),
+// then, 8-byte aligned, the owned bodies' records - v (3), w (3), pos (3) -
+// and, when room is left, the impulses of its contacts.
 constexpr int CL_REC = 9;
-__device__ __forceinline__ int cl_ints(int rb, int P) { return rb * (1 + P + 2 + 2); }
+constexpr int CL_TAB = 5;
+enum { CT_KN = 0, CT_NEED = 1, CT_SA = 2, CT_SB = 3, CT_XPRED = 4 };
+__device__ __forceinline__ int cl_tab_off(int rb, int P) { return rb * (1 + P + 2 + 2); }
+__device__ __forceinline__ int cl_ints(int rb, int P) { return rb * (1 + P + 2 + 2 + CL_TAB); }
 __device__ __forceinline__ int cl_rec_off(int rb, int P) { return (cl_ints(rb, P) + 1) & ~1; }   // in ints
 
 // where CTA h keeps its arrival counts and ring (its shared memory when the
@@ -653,11 +658,24 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
     if (threadIdx.x < 4) cs.hist[threadIdx.x] = 0;
     if (threadIdx.x == 0) { cs.claimed = 0; cs.abort = 0; cs.n_owned = 0; }
     __syncthreads();
+    int *rtab = csm + cl_tab_off(Rb, P);         // (when tables_local) CL_TAB per run
     for (int i = threadIdx.x; i < Rb; i += blockDim.x) {
         const int r = r0 + i;
         mine.arrived[i] = 0;
         atomicAdd(&cs.hist[min(run_kn[r] >> 24, 4) - 1], 1);
         if (!tables_local) continue;
+        {
+            int *t = rtab + CL_TAB * i;
+            t[CT_KN] = run_kn[r];
+            t[CT_NEED] = run_need[r];
+            t[CT_SA] = run_sa[r];
+            t[CT_SB] = run_sb[r];
+            int x = 0;
+            const int pc[2] = {A.run_pa[c0 + r], A.run_pb[c0 + r]};
+            for (int q = 0; q < 2; q++)
+                if (pc[q] != LEVEL_NONE) x |= cl_home(pc[q] >= 0 ? pc[q] : -pc[q] - 1, R, C) != me;
+            t[CT_XPRED] = x;
+        }
         // a body belongs to the CTA of its first run (whose predecessor code points to the previous pass)
         const int a = A.run_a[c0 + r], b = A.run_b[c0 + r];
         const int pa = A.run_pa[c0 + r], pb = A.run_pb[c0 + r];
@@ -728,6 +746,15 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
     VelView V;
     V.s = nullptr;
     V.b0 = A.w_body_off[w];
+    // run rs's table row in its home CTA (DSMEM when remote); nullptr when the
+    // home's tables are not in shared memory
+    auto tab_of = [&](int rs) -> const int * {
+        const int h = cl_home(rs, R, C);
+        const int h0 = cl_first(h, R, C), hr = cl_first(h + 1, R, C) - h0;
+        if ((long long)cl_ints(hr, P) > smem_ints) return nullptr;
+        const int *base = (h == me ? csm : cluster.map_shared_rank(csm, h)) + cl_tab_off(hr, P);
+        return base + CL_TAB * (rs - h0);
+    };
     // the record of a staged body in its owner's shared memory
     auto rec_of = [&](int slot) -> double * {
         if (slot < 0) return nullptr;
@@ -736,19 +763,19 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
         double *base = reinterpret_cast<double *>((h == me ? csm : cluster.map_shared_rank(csm, h)) + cl_rec_off(hr, P));
         return base + (size_t)(slot & 0xFFFFF) * CL_REC;
     };
-    // publish entry e (run rs of pass ps) to its home's ring
-    auto push = [&](int e, int rs) {
+    // publish entry e (run rs of pass ps, run length n) to its home's ring
+    auto push = [&](int e, int rs, int n) {
         const int h = cl_home(rs, R, C);
         ClusterShared *hs = h == me ? &cs : cluster.map_shared_rank(&cs, h);
         const ClusterHome H = h == me ? mine : cl_home_arrays<C>(A, cluster, csm, h, R, P, c0, smem_ints, me);
-        const int c = entry_class(e >> PASS_SHIFT, __ldg(run_kn + rs) >> 24, true);
+        const int c = entry_class(e >> PASS_SHIFT, n, true);
         const int pos = atomicAdd(&hs->tail[c], 1);
         if (pos >= hs->size[c]) { cs.abort = 1; atomicExch(gabort, 1); return; }   // never with a consistent graph
         if (h == me) st_release_cta(&H.ring[hs->base[c] + pos], e + 1);
         else st_release_cluster(&H.ring[hs->base[c] + pos], e + 1);
     };
     for (int r = r0 + (int)threadIdx.x; r < r0 + Rb; r += blockDim.x)
-        if ((__ldg(run_need + r) & 3) == 0) push(r, r);
+        if ((__ldg(run_need + r) & 3) == 0) push(r, r, __ldg(run_kn + r) >> 24);
     const int lane = threadIdx.x & 31;
     for (;;) {
         int lo = 0, cnt = 0;
@@ -790,11 +817,12 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
             else {
                 const int e = e1 - 1;
                 const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
-                const int v = __ldg(run_kn + r);
+                const int *tr = tables_local ? rtab + CL_TAB * (r - r0) : nullptr;
+                const int v = tr ? tr[CT_KN] : __ldg(run_kn + r);
                 const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
                 double row0[CD];
                 load_row(A, k0, row0);
-                const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                const int sa = tr ? tr[CT_SA] : __ldg(run_sa + r), sb = tr ? tr[CT_SB] : __ldg(run_sb + r);
                 bool remote;
                 if (staged) {
                     const int s0 = rslot[2 * (r - r0)], s1 = rslot[2 * (r - r0) + 1];
@@ -812,18 +840,18 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                     if (sc >= 0) { ps_[m] = p; rs_[m] = sc; m++; }
                     else if (sc != LEVEL_NONE && p + 1 < P) { ps_[m] = p + 1; rs_[m] = -sc - 1; m++; }
                 }
-                // a successor owned elsewhere, or one whose other predecessor is owned
-                // elsewhere (whose last arrival may then acquire these writes), needs
-                // the cluster-scope release
-                for (int q = 0; q < m && !remote; q++) {
+                // successor tables (their need counts and lengths), and whether any
+                // successor, or any successor's other predecessor, lies in another CTA
+                // (whose last arrival may then acquire these writes): then the release
+                // is cluster scope
+                int needs[2] = {0, 0}, lens[2] = {0, 0};
+                for (int q = 0; q < m; q++) {
                     const int rs = rs_[q];
-                    remote |= cl_home(rs, R, C) != me;
-                    const int pc[2] = {__ldg(A.run_pa + c0 + rs), __ldg(A.run_pb + c0 + rs)};
-                    for (int t = 0; t < 2; t++) {
-                        if (pc[t] == LEVEL_NONE) continue;
-                        const int pr = pc[t] >= 0 ? pc[t] : -pc[t] - 1;
-                        remote |= cl_home(pr, R, C) != me;
-                    }
+                    const int *ts = tab_of(rs);
+                    needs[q] = ts ? ts[CT_NEED] : __ldg(run_need + rs);
+                    lens[q] = (ts ? ts[CT_KN] : __ldg(run_kn + rs)) >> 24;
+                    if (cl_home(rs, R, C) != me) remote = true;
+                    else if (!ts || ts[CT_XPRED]) remote = true;
                 }
                 // release this entry's writes: to this CTA alone, or to the cluster
                 if (remote) fence_acq_rel_cluster(); else fence_acq_rel_cta();
@@ -833,9 +861,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                     int *arr = h == me ? mine.arrived + (rs - r0)
                                        : cl_home_arrays<C>(A, cluster, csm, h, R, P, c0, smem_ints, me).arrived +
                                              (rs - cl_first(h, R, C));
-                    if (atomicAdd(arr, 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
+                    if (atomicAdd(arr, 1) + 1 == need_of(needs[q], ps)) {
                         fence_acq_rel_cluster();         // acquire the other arrivals' writes
-                        push((ps << PASS_SHIFT) | rs, rs);
+                        push((ps << PASS_SHIFT) | rs, rs, lens[q]);
                     }
                 }
             }
