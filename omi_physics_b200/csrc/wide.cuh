@@ -814,8 +814,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                 if (e1 || *(volatile int *)&cs.abort) break;
             }
             if (e1 == 0) { cs.abort = 1; atomicExch(gabort, 1); }
-            else for (int e = e1 - 1; e >= 0;) {
-                // entry e, then (continuation) one successor it made ready in this CTA
+            else {
+                const int e = e1 - 1;
                 const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
                 const int *tr = tables_local ? rtab + CL_TAB * (r - r0) : nullptr;
                 const int v = tr ? tr[CT_KN] : __ldg(run_kn + r);
@@ -855,7 +855,6 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                 }
                 // release this entry's writes: to this CTA alone, or to the cluster
                 if (remote) fence_acq_rel_cluster(); else fence_acq_rel_cta();
-                int next = -1;
                 for (int q = 0; q < m; q++) {
                     const int rs = rs_[q], ps = ps_[q];
                     const int h = cl_home(rs, R, C);
@@ -864,14 +863,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                                              (rs - cl_first(h, R, C));
                     if (atomicAdd(arr, 1) + 1 == need_of(needs[q], ps)) {
                         fence_acq_rel_cluster();         // acquire the other arrivals' writes
-                        const int en = (ps << PASS_SHIFT) | rs;
-                        // the first ready successor of this CTA runs next on this thread (it
-                        // counts as claimed; its ring slot stays unused), the others are published
-                        if (next < 0 && h == me) { next = en; atomicAdd(&cs.claimed, 1); }
-                        else push(en, rs, lens[q]);
+                        push((ps << PASS_SHIFT) | rs, rs, lens[q]);
                     }
                 }
-                e = next;
             }
         }
         __syncwarp();
