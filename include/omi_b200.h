@@ -169,7 +169,7 @@ int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t s
  * (128/256/512) and blocks per SM (1-32) of the pair count and emit passes,
  * narrow_block = block size of the analytic narrowphase and clipping (64,
  * 128, 256), gjk_warps = warps (one pair each) per GJK/EPA block (2, 4, 8).
- * Defaults: 8, 4, 256, 16, 128, 4, 32, and 16 (8 on a GPU without 16-CTA clusters).
+ * Defaults: 8, 4, 256, 16, 128, 4, 32, 16 (8 on a GPU without 16-CTA clusters), 32.
  * A change re-captures the step graph. */
 typedef struct OmiTuning {
     int32_t sweep_warps, sweep_max_split, pair_block, pair_blocks_per_sm, narrow_block, gjk_warps;
@@ -180,6 +180,9 @@ typedef struct OmiTuning {
      * (each owning a slab of the runs, crossing entries through distributed shared
      * memory), in place of wide_sweep_blocks; 0 = off */
     int32_t wide_cluster;
+    /* ready contact-sweep entries a warp claims at once (8, 16 or 32): fewer leave more
+     * warps free to take an entry the moment it becomes ready */
+    int32_t sweep_claim;
 } OmiTuning;
 int omi_set_tuning(OmiCtx *ctx, const OmiTuning *tuning);
 int omi_get_tuning(OmiCtx *ctx, OmiTuning *tuning);

@@ -90,7 +90,7 @@ class OmiTuning(C.Structure):
     """Mirror of ``struct OmiTuning`` (the step's launch configuration)."""
     _fields_ = [(n, C.c_int32) for n in ('sweep_warps', 'sweep_max_split', 'pair_block',
                                           'pair_blocks_per_sm', 'narrow_block', 'gjk_warps',
-                                          'wide_sweep_blocks', 'wide_cluster')]
+                                          'wide_sweep_blocks', 'wide_cluster', 'sweep_claim')]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
@@ -98,7 +98,8 @@ class OmiTuning(C.Structure):
 
 #: the library's default launch configuration
 DEFAULT_TUNING = dict(sweep_warps=8, sweep_max_split=4, pair_block=256, pair_blocks_per_sm=16,
-                      narrow_block=128, gjk_warps=4, wide_sweep_blocks=32, wide_cluster=16)
+                      narrow_block=128, gjk_warps=4, wide_sweep_blocks=32, wide_cluster=16,
+                      sweep_claim=32)
 
 #: every symbol include/omi_b200.h declares, with (restype, argtypes)
 PROTOTYPES = {

@@ -46,6 +46,7 @@ struct Arena {
     int spin_limit;                 // polls before a sweep wait gives up (ST_SWEEP_TIMEOUT)
     int epa_faces;                  // EPA polytope face bound (<= EPA_F; ST_EPA_LIMIT past it)
     int stall_run;                  // test hook: world-local run whose sweep entries never become ready (-1: none)
+    int sweep_claim;                // ready sweep entries a warp claims at once (1-32; launch configuration)
     // wide worlds: large worlds whose stages run on many blocks (wide.cuh) instead of one
     // block per world; the per-world kernels skip them
     int n_wide;

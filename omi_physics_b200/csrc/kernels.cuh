@@ -1874,7 +1874,7 @@ __device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_
                     const int h = *(volatile int *)&sh.head[c];
                     const int t = min(*(volatile int *)&sh.tail[c], sh.size[c]);
                     if (t > h) {
-                        const int want = min(t - h, 32);
+                        const int want = min(t - h, A.sweep_claim);
                         if (atomicCAS(&sh.head[c], h, h + want) == h) {
                             atomicAdd(&sh.claimed, want);
                             lo = sh.base[c] + h;

@@ -86,7 +86,7 @@ struct OmiCtx {
     int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
     // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
     int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
-    OmiTuning tune = {8, 4, 256, 16, 128, 4, 32, 16};   // launch configuration (omi_set_tuning)
+    OmiTuning tune = {8, 4, 256, 16, 128, 4, 32, 16, 32};   // launch configuration (omi_set_tuning)
     int cluster_max = 0;                        // largest thread-block cluster of k_csweep the GPU schedules
     // wide worlds (their stages on many blocks): the worlds, bodies of the largest, sort merge passes
     std::vector<int> h_wide;
@@ -878,6 +878,7 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     A.spin_limit = ctx->spin_limit;
     A.epa_faces = ctx->epa_faces;
     A.stall_run = ctx->stall_run;
+    A.sweep_claim = ctx->tune.sweep_claim;
     int rc = 0;
     // worlds
     rc |= upload(ctx, const_cast<int *&>(A.w_body_off), s->w_body_off, W + 1);
@@ -1462,11 +1463,13 @@ int omi_set_tuning(OmiCtx *ctx, const OmiTuning *t) {
                     (t->gjk_warps == 2 || t->gjk_warps == 4 || t->gjk_warps == 8) &&
                     t->wide_sweep_blocks >= 1 && t->wide_sweep_blocks <= 1024 &&
                     (t->wide_cluster == 0 || t->wide_cluster == 8 || t->wide_cluster == 16) &&
-                    t->wide_cluster <= ctx->cluster_max;
+                    t->wide_cluster <= ctx->cluster_max &&
+                    (t->sweep_claim == 8 || t->sweep_claim == 16 || t->sweep_claim == 32);
     if (!ok) return fail(ctx, OMI_E_ARG, "launch configuration out of range");
     cudaStreamSynchronize(ctx->stream);
     drop_graph(ctx);                     // re-captured with the new launches on the next step
     ctx->tune = *t;
+    ctx->A.sweep_claim = t->sweep_claim;
     return 0;
 }
 

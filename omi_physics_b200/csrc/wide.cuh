@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
                     const int h = ld_relaxed_gpu(&st[WS_HEAD + c]);
                     const int t = min(ld_relaxed_gpu(&st[WS_TAIL + c]), wr.size[c]);
                     if (t > h) {
-                        const int want = min(t - h, 32);
+                        const int want = min(t - h, A.sweep_claim);
                         if (atomicCAS(&st[WS_HEAD + c], h, h + want) == h) {
                             atomicAdd(&st[WS_CLAIMED], want);
                             lo = wr.base[c] + h;
@@ -789,7 +789,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
                     const int h = *(volatile int *)&cs.head[c];
                     const int t = min(*(volatile int *)&cs.tail[c], cs.size[c]);
                     if (t > h) {
-                        const int want = min(t - h, 32);
+                        const int want = min(t - h, A.sweep_claim);
                         if (atomicCAS(&cs.head[c], h, h + want) == h) {
                             atomicAdd(&cs.claimed, want);
                             lo = cs.base[c] + h;

@@ -652,6 +652,9 @@ GOLDEN_SCENES = {
     'conveyor': lambda api=None, backend=None: conveyor(api, backend),
     'degenerate': lambda api=None, backend=None: degenerate(api, backend),
     'rods': lambda api=None, backend=None: rods(api, backend),
+    # a hull pile late in its settling, some of it asleep (the convex configuration's regime)
+    'convex_late': lambda api=None, backend=None: convex_pile(api, backend, n=1200, seed=13, arena=16.0,
+                                                              height=8.0),
 }
 
 

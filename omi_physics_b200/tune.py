@@ -37,6 +37,7 @@ SPACE = {
     'gjk_warps': (4, 2, 8),
     'wide_sweep_blocks': (32, 1, 8, 16, 64, 148),
     'wide_cluster': (16, 8, 0),
+    'sweep_claim': (32, 16, 8),
 }
 #: group counts tried for a many-world workload (a single world is one group)
 GROUP_CHOICES = (4, 2, 3, 6)

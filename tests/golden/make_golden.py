@@ -44,7 +44,8 @@ STEPS = {'pyramid': (50, (0, 3, 12, 30, 44)), 'debris': (240, (0, 90, 150, 239))
          'spheres': (120, (0, 60, 119)), 'capsules': (180, (0, 40, 100, 179)),
          'zones': (150, (0, 40, 90, 149)), 'terrain': (200, (0, 100, 160, 199)),
          'ridge': (150, (0, 70, 149)), 'conveyor': (150, (0, 70, 149)),
-         'degenerate': (300, (0, 1, 30, 118, 125, 250, 299)), 'rods': (240, (0, 1, 60, 150, 239))}
+         'degenerate': (300, (0, 1, 30, 118, 125, 250, 299)), 'rods': (240, (0, 1, 60, 150, 239)),
+         'convex_late': (300, (220, 280, 299))}
 
 
 def _pairs_array(pairs):

@@ -5,7 +5,7 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
 SCENES = ('pyramid', 'debris', 'convex', 'chain', 'spheres', 'capsules', 'zones', 'terrain', 'ridge', 'conveyor',
-          'degenerate', 'rods')
+          'degenerate', 'rods', 'convex_late')
 
 
 def load(name):

@@ -3,10 +3,9 @@
 * debris field, 4096 bodies (1/120 s, 8 iterations): 240 steps, compared bit
   for bit at checkpoints;
 * convex-hull pile, 32768 bodies (50% boxes, 25% spheres, 25% hulls through
-  GJK/EPA, walled arena): 20 steps, compared bit for bit every 5 steps. This
-  world is larger than every shared-memory stage buffer, so it runs the
-  global-memory forms of the sort, the sweep links, the sweep itself and the
-  island pass;
+  GJK/EPA, walled arena): its whole 300-step run, compared bit for bit every
+  50 steps. Both this world and the debris field are wide worlds (their sort,
+  sweep links, wake, sweep, cache store and sleep pass on many blocks);
 * capsule pile, 4096 bodies (30% capsules, 20% cylinders, the rest boxes and
   spheres): 120 steps, compared bit for bit every 40 steps;
 * terrain, 2000 bodies on an 18,432-triangle static mesh: 120 steps, compared
@@ -71,8 +70,12 @@ def test_debris_4096_full_size():
 
 
 def test_convex_pile_32768_full_size():
+    """The whole 300-step run of the configuration (a wide world: its
+    per-world stages on many blocks, the sweep on a thread-block cluster),
+    bit for bit against the oracle every 50 steps, sleep flags and islands
+    included."""
     w, meta = scenes.convex_pile(n=32768, seed=0)
-    b = _run_exact(w, meta['dt'], 20, 5, 'convex32768')
+    b = _run_exact(w, meta['dt'], 300, 50, 'convex32768')
     assert b.counts()[1][0] > 10000
 
 

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 STATE = ('_position', '_orientation', '_linear_velocity', '_angular_velocity', '_awake', '_sleep_timer')
 OTHER = dict(sweep_warps=4, sweep_max_split=1, pair_block=512, pair_blocks_per_sm=8, narrow_block=64,
-             gjk_warps=8, wide_sweep_blocks=1, wide_cluster=0)
+             gjk_warps=8, wide_sweep_blocks=1, wide_cluster=0, sweep_claim=8)
 
 
 def _worlds():
@@ -23,7 +23,8 @@ def _worlds():
 
 @pytest.mark.parametrize('cfg,wide', [(OTHER, None), (dict(sweep_warps=8, sweep_max_split=2, pair_block=128,
                                                           pair_blocks_per_sm=32, narrow_block=256, gjk_warps=2,
-                                                          wide_sweep_blocks=5, wide_cluster=8), None),
+                                                          wide_sweep_blocks=5, wide_cluster=8, sweep_claim=16),
+                                       None),
                                       (OTHER, '0'), (dict(OTHER, wide_sweep_blocks=7), '0'),
                                       (dict(OTHER, wide_cluster=8), '0'), (dict(OTHER, wide_cluster=16), '0')])
 def test_any_launch_configuration_gives_the_same_bits(cfg, wide, monkeypatch):

@@ -31,7 +31,7 @@ def fake_timer(best, noise=None):
 
 def test_coordinate_search_finds_the_separable_optimum():
     best = dict(sweep_warps=4, sweep_max_split=1, pair_block=512, pair_blocks_per_sm=8,
-                narrow_block=64, gjk_warps=8, wide_sweep_blocks=16, wide_cluster=8)
+                narrow_block=64, gjk_warps=8, wide_sweep_blocks=16, wide_cluster=8, sweep_claim=8)
     measure, calls = fake_timer(best)
     cfg, t, trials = tune.coordinate_search(measure, tune.SPACE, dict(DEFAULT_TUNING))
     assert cfg == best
