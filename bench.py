@@ -387,10 +387,11 @@ def run_ours(args, rank, world, local):
         barrier(world)
     if not args.no_extras and rank == 0:
         extras['plain'] = plain_per_world(worlds, reqs, args.plain_sample, local, args.preroll)
+    note = _tuning_note(grp)
     grp.close()
     return dict(value=value, ms=ms_max, N=total_N, P=P, K=K, launches=launches, setup_s=setup_s,
                 ticks=ticks, roofline=roofline, e2e=e2e, clocks=clk.summary(), extras=extras,
-                NB=NB, tuning=_tuning_note(grp))
+                NB=NB, tuning=note)
 
 
 def _tuning_note(grp):

@@ -5,6 +5,8 @@ import os
 import subprocess
 import sys
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -55,3 +57,25 @@ def test_clock_sampler_reads_nvml_and_summarises(monkeypatch):
     assert calls[0] == 'init' and calls[-1] == 'shutdown'
     assert s['samples'] >= 3 and s['sm_max_mhz'] == 1965 and s['sm_mhz'] == 1965
     assert s['reasons'] == ['sw_power_cap']
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('args', [
+    ['--worlds', '24', '--steps', '3', '--warmup', '3', '--preroll', '10', '--no-extras'],
+    ['--workload', 'pyramid', '--config-steps', '6', '--no-extras'],
+])
+def test_bench_runs_end_to_end_and_prints_its_line(args):
+    """bench.py itself, small: it exits 0 and prints one JSON line with the
+    contract's keys (a crash here would cost the measured run)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, os.path.join(root, 'bench.py')] + args, capture_output=True,
+                         text=True, timeout=900, cwd=root)
+    assert res.returncode == 0, res.stderr[-2000:]
+    line = json.loads(res.stdout.strip().splitlines()[-1])
+    for key in ('metric', 'value', 'unit', 'n_gpus', 'steps', 'warmup', 'ms_per_step', 'higher_is_better',
+                'scaling', 'dtype', 'config', 'e2e', 'roofline', 'clocks', 'gpu_launches', 'tuning'):
+        assert key in line, key
+    assert line['value'] > 0 and line['gpu_launches'] > 0
