@@ -78,7 +78,26 @@ def parse():
                          'strong = one mix split across the ranks by body-count bin-packing')
     ap.add_argument('--config-steps', type=int, default=None,
                     help='steps of a configuration run (default: the configuration\'s own count)')
+    ap.add_argument('--just-step', type=int, default=0,
+                    help='only build the workload (--workload, --worlds, --seed) as one batch, step it '
+                         'this many times and exit: the program a profiler captures')
     return ap.parse_args()
+
+
+def just_step(args):
+    """Build the workload as one WorldBatch on cuda:0 and step it; no timing."""
+    import torch
+    from omi_physics_b200 import WorldBatch, scenes
+    if args.workload == 'serving-mix':
+        _, worlds = build_mix(args.worlds, args.seed)
+        dts = [w.fixed_dt for w in worlds]
+    else:
+        worlds, dts = scenes.CONFIGS[args.workload][0]()
+    b = WorldBatch(worlds, dts=dts)
+    b.step(args.just_step)
+    torch.cuda.synchronize()
+    print(json.dumps({'workload': args.workload, 'worlds': len(worlds), 'steps': args.just_step,
+                      'contacts': int(b.counts()[1].sum())}))
 
 
 # ---------------------------------------------------------------------------
@@ -911,6 +930,8 @@ def main_config(args, rank, world_size, local):
 
 def main():
     args = parse()
+    if args.just_step:
+        return just_step(args)
     rank, world, local = dist_init(args.gpus)
     if args.workload != 'serving-mix':
         main_config(args, rank, world, local)

@@ -169,7 +169,7 @@ int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t s
  * (128/256/512) and blocks per SM (1-32) of the pair count and emit passes,
  * narrow_block = block size of the analytic narrowphase and clipping (64,
  * 128, 256), gjk_warps = warps (one pair each) per GJK/EPA block (2, 4, 8).
- * Defaults: 8, 4, 256, 16, 128, 4, 32, 16 (8 on a GPU without 16-CTA clusters), 32.
+ * Defaults: 8, 4, 256, 16, 128, 4, 16, 16 (8 on a GPU without 16-CTA clusters), 32.
  * A change re-captures the step graph. */
 typedef struct OmiTuning {
     int32_t sweep_warps, sweep_max_split, pair_block, pair_blocks_per_sm, narrow_block, gjk_warps;
@@ -178,7 +178,8 @@ typedef struct OmiTuning {
     int32_t wide_sweep_blocks;
     /* 8 or 16: a wide world's contact sweep on one thread-block cluster of that many CTAs
      * (each owning a slab of the runs, crossing entries through distributed shared
-     * memory), in place of wide_sweep_blocks; 0 = off */
+     * memory) while every CTA's body records fit its shared memory, else on
+     * wide_sweep_blocks blocks (the cluster sweeps every world when that is 1); 0 = off */
     int32_t wide_cluster;
     /* ready contact-sweep entries a warp claims at once (8, 16 or 32): fewer leave more
      * warps free to take an entry the moment it becomes ready */
@@ -192,6 +193,13 @@ int omi_get_tuning(OmiCtx *ctx, OmiTuning *tuning);
  * for bit). Default 3072; 0 makes every colliding world wide. Applies from
  * the next omi_load / omi_reserve_slots. (No counterpart in the reference.) */
 int omi_set_wide_threshold(OmiCtx *ctx, int32_t bodies);
+/* Shared-memory ints each CTA of the wide contact sweep's thread-block
+ * cluster may use (0, the default: all it has). The cluster sweeps a wide
+ * world whose body records fit its CTAs' shared memory and hands any other
+ * to the many-block sweep (unless wide_sweep_blocks is 1); a smaller budget
+ * makes it hand off smaller worlds - the same results, bit for bit. (No
+ * counterpart in the reference.) */
+int omi_set_cluster_budget(OmiCtx *ctx, int32_t ints);
 /* Check a scene the way omi_load does, on the host only (no device, no
  * context): every index a kernel would follow is range-checked. Returns 0 or
  * the status omi_load would return, with the message in err (err_cap bytes,
@@ -384,8 +392,10 @@ int omi_sweep_pairs_noalloc(const double *aabb_min, const double *aabb_max,
 /* Critical path of each world's last contact sweep (n_worlds ints;
  * diagnostics): the longest chain of runs that must follow one another,
  * weighted by their contact counts - the sequential sweep's length in contact
- * solves, after independent runs are overlapped. No counterpart in the
- * reference (whose sweep is the full sequence). */
+ * solves, after independent runs are overlapped. A wide world's sweep does
+ * not track it: -1 when a thread-block cluster swept it, -2 when the
+ * many-block sweep did. No counterpart in the reference (whose sweep is the
+ * full sequence). */
 int omi_world_levels(OmiCtx *ctx, int32_t *levels);
 
 /* per-kernel device time (ms) of the last profiled step, see omi_profile_step */

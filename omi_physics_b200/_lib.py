@@ -98,7 +98,7 @@ class OmiTuning(C.Structure):
 
 #: the library's default launch configuration
 DEFAULT_TUNING = dict(sweep_warps=8, sweep_max_split=4, pair_block=256, pair_blocks_per_sm=16,
-                      narrow_block=128, gjk_warps=4, wide_sweep_blocks=32, wide_cluster=16,
+                      narrow_block=128, gjk_warps=4, wide_sweep_blocks=16, wide_cluster=16,
                       sweep_claim=32)
 
 #: every symbol include/omi_b200.h declares, with (restype, argtypes)
@@ -114,6 +114,7 @@ PROTOTYPES = {
     'omi_set_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
     'omi_get_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
     'omi_set_wide_threshold': (C.c_int, [C.c_void_p, C.c_int32]),
+    'omi_set_cluster_budget': (C.c_int, [C.c_void_p, C.c_int32]),
     'omi_load': (C.c_int, [C.c_void_p, C.POINTER(OmiScene)]),
     'omi_set_active': (C.c_int, [C.c_void_p, U8]),
     'omi_set_world_params': (C.c_int, [C.c_void_p, D, I, I, I]),
@@ -263,6 +264,11 @@ class Context:
         cur.update(cfg)
         t = OmiTuning(**{k: int(cur[k]) for k in DEFAULT_TUNING})
         self.call('set_tuning', C.byref(t))
+
+    def set_cluster_budget(self, ints: int = 0) -> None:
+        """Shared-memory ints per CTA of the wide sweep's cluster (0: all);
+        smaller budgets hand smaller wide worlds to the many-block sweep."""
+        self.call('set_cluster_budget', int(ints))
 
     def tuning(self) -> dict:
         t = OmiTuning()

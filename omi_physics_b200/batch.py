@@ -206,7 +206,9 @@ class WorldBatch:
         return np.where(lab >= 0, lab - self.offsets[i], -1)
 
     def levels(self) -> np.ndarray:
-        """Critical path of each world's last contact sweep, in contact solves."""
+        """Critical path of each world's last contact sweep, in contact solves
+        (a wide world: -1 when a thread-block cluster swept it, -2 when the
+        many-block sweep did; neither tracks it)."""
         out = np.zeros(len(self.worlds), np.int32)
         self.ctx.call('world_levels', ptr(out, I))
         return out

@@ -165,8 +165,8 @@ __device__ inline void skew(const double *r, double *S) {
     S[6] = -r[1]; S[7] = r[0]; S[8] = 0.0;
 }
 
-__device__ inline void joint_prepare(const Arena &A, int j) {
-    double *D = &A.j_data[(size_t)j * JD];
+// prepares joint j's row into D (JD doubles: shared memory or j_data)
+__device__ inline void joint_prepare(const Arena &A, int j, double *D) {
     const int t = A.j_type[j];
     if (t == 2) {                                    // AngularMotor.prepare
         const int body = A.j_a[j];
@@ -226,14 +226,21 @@ __device__ inline void joint_prepare(const Arena &A, int j) {
             D[J_BIAS + k] = 0.2 * (pb - pa);
         }
         // LU with partial pivoting of K, kept for every iteration's solve
+#pragma unroll
         for (int jj = 0; jj < 3; jj++) {
             int p = jj;
             double best = fabs(K[jj * 3 + jj]);
+#pragma unroll
             for (int i = jj + 1; i < 3; i++)
                 if (fabs(K[i * 3 + jj]) > best) { best = fabs(K[i * 3 + jj]); p = i; }
             D[J_PIV + jj] = (double)p;
-            if (p != jj)
-                for (int k = 0; k < 3; k++) { const double tt = K[jj * 3 + k]; K[jj * 3 + k] = K[p * 3 + k]; K[p * 3 + k] = tt; }
+            // row swap with static indices (a dynamic one would put K in local memory)
+#pragma unroll
+            for (int i = jj + 1; i < 3; i++)
+                if (p == i)
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { const double tt = K[jj * 3 + k]; K[jj * 3 + k] = K[i * 3 + k]; K[i * 3 + k] = tt; }
+#pragma unroll
             for (int i = jj + 1; i < 3; i++) {
                 const double l = K[i * 3 + jj] / K[jj * 3 + jj];
                 K[i * 3 + jj] = l;
@@ -279,23 +286,35 @@ __device__ inline void joint_prepare(const Arena &A, int j) {
     D[J_BIASS] = 0.2 * (dist - A.j_length[j]);
 }
 
-__device__ inline void joint_apply(const Arena &A, int i, const double *invI, const double *r,
+// where the joint solve reads and writes body velocities: a world's range
+// [lo, lo + n) of bodies staged in shared memory (v then w, 6 per body), or
+// the global arrays (s == nullptr)
+struct JointVel {
+    double *s;
+    int lo;
+    __device__ __forceinline__ double *v(const Arena &A, int i) const { return s ? s + (i - lo) * 6 : &A.v[i * 3]; }
+    __device__ __forceinline__ double *w(const Arena &A, int i) const { return s ? s + (i - lo) * 6 + 3 : &A.w[i * 3]; }
+};
+
+__device__ inline void joint_apply(const Arena &A, const JointVel &V, int i, const double *invI, const double *r,
                                    const double *P) {
     if (i < 0 || A.mtype[i] != 2) return;
-    for (int q = 0; q < 3; q++) A.v[i * 3 + q] = A.v[i * 3 + q] + A.inv_mass[i] * P[q];
+    double *v = V.v(A, i), *w = V.w(A, i);
+    for (int q = 0; q < 3; q++) v[q] = v[q] + A.inv_mass[i] * P[q];
     double c[3];
     cross_np(r, P, c);
-    for (int q = 0; q < 3; q++) A.w[i * 3 + q] = A.w[i * 3 + q] + gemv_row(&invI[q * 3], c);
+    for (int q = 0; q < 3; q++) w[q] = w[q] + gemv_row(&invI[q * 3], c);
 }
 
-__device__ inline void joint_solve(const Arena &A, int j, double dt) {
-    const double *D = &A.j_data[(size_t)j * JD];
+// one solve of joint j (prepared row D) on the velocities V
+__device__ inline void joint_solve(const Arena &A, int j, const double *D, const JointVel &V, double dt) {
     const int t = A.j_type[j];
     if (t == 2) {                                    // AngularMotor.solve
         const int body = A.j_a[j];
         if (body < 0) return;
         const double *ax = &A.j_axis[j * 3];
-        const double wv = dot_blas(&A.w[body * 3], ax);
+        double *wb = V.w(A, body);
+        const double wv = dot_blas(wb, ax);
         double impulse = D[J_MASS] * (A.j_target[j] - wv);
         const double limit = A.j_max_force[j] * dt;
         double nw = A.j_accum[j] + impulse;
@@ -305,19 +324,22 @@ __device__ inline void joint_solve(const Arena &A, int j, double dt) {
         A.j_accum[j] = nw;
         if (A.mtype[body] != 2) return;
         const double P[3] = {ax[0] * impulse, ax[1] * impulse, ax[2] * impulse};
-        for (int q = 0; q < 3; q++) A.w[body * 3 + q] = A.w[body * 3 + q] + gemv_row(&D[J_IA + q * 3], P);
+        for (int q = 0; q < 3; q++) wb[q] = wb[q] + gemv_row(&D[J_IA + q * 3], P);
         return;
     }
     const int a = A.j_a[j], b = A.j_b[j];
     double va[3] = {0.0, 0.0, 0.0}, vb[3] = {0.0, 0.0, 0.0}, P[3], nP[3], c[3];
-    if (b >= 0) { cross_np(&A.w[b * 3], &D[J_RB], c); for (int q = 0; q < 3; q++) vb[q] = A.v[b * 3 + q] + c[q]; }
-    if (a >= 0) { cross_np(&A.w[a * 3], &D[J_RA], c); for (int q = 0; q < 3; q++) va[q] = A.v[a * 3 + q] + c[q]; }
+    if (b >= 0) { cross_np(V.w(A, b), &D[J_RB], c); const double *v = V.v(A, b); for (int q = 0; q < 3; q++) vb[q] = v[q] + c[q]; }
+    if (a >= 0) { cross_np(V.w(A, a), &D[J_RA], c); const double *v = V.v(A, a); for (int q = 0; q < 3; q++) va[q] = v[q] + c[q]; }
     if (t == 0) {                                    // PointConstraint.solve
         double x[3];
         for (int q = 0; q < 3; q++) x[q] = -((vb[q] - va[q]) + D[J_BIAS + q] / dt);
+#pragma unroll
         for (int jj = 0; jj < 3; jj++) {
             const int p = (int)D[J_PIV + jj];
-            if (p != jj) { const double tt = x[jj]; x[jj] = x[p]; x[p] = tt; }
+#pragma unroll
+            for (int i = jj + 1; i < 3; i++)           // static indices: x stays in registers
+                if (p == i) { const double tt = x[jj]; x[jj] = x[i]; x[i] = tt; }
         }
         const double *L = &D[J_LU];
         for (int i = 0; i < 3; i++)
@@ -335,8 +357,8 @@ __device__ inline void joint_solve(const Arena &A, int j, double dt) {
         for (int q = 0; q < 3; q++) P[q] = impulse * D[J_N + q];
     }
     neg3(P, nP);
-    joint_apply(A, a, &D[J_IA], &D[J_RA], nP);
-    joint_apply(A, b, &D[J_IB], &D[J_RB], P);
+    joint_apply(A, V, a, &D[J_IA], &D[J_RA], nP);
+    joint_apply(A, V, b, &D[J_IB], &D[J_RB], P);
 }
 
 // A motor whose body is not dynamic changes only its own accumulated impulse
@@ -394,57 +416,149 @@ __device__ inline int warp_joint_levels(const Arena &A, int j0, int J, int iters
     return maxl + 1;
 }
 
-__global__ void k_joints(Arena A, int gated) {
-    __shared__ int s_D;
+// shared memory of one k_joints block (one world at a time), in doubles: a
+// 128-link chain at 12 iterations needs about 2.5K (velocities 0.8K,
+// schedule 1.8K); seven blocks fit on an SM
+constexpr int JOINT_SMEM_DOUBLES = 4096;
+
+// inclusive prefix sums of a[0..n) by one warp (each lane sums a chunk)
+__device__ inline void warp_scan_inclusive(int *a, int n) {
+    const int lane = threadIdx.x & 31;
+    const int per = (n + 31) >> 5;
+    const int s0 = min(lane * per, n), s1 = min(s0 + per, n);
+    int sum = 0;
+    for (int i = s0; i < s1; i++) sum += a[i];
+    int x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    int run = x - sum;
+    for (int i = s0; i < s1; i++) {
+        run += a[i];
+        a[i] = run;
+    }
+    __syncwarp();
+}
+
+// _solve_joints (world.py:599-611): wake, prepare, then every joint
+// iteration in the reference's order, as wavefront levels. One warp per world
+// (one block of 32 threads): a chain's levels hold a few entries each (about
+// one per iteration in flight), so a warp fills them and steps from level to
+// level with __syncwarp alone. The joints' body velocities and the schedule
+// (levels, order, level starts) live in the block's shared memory as far as
+// `smem_doubles` goes, else in the global arrays; the velocities go back to
+// the global arrays at the end.
+__global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_doubles) {
+    extern __shared__ __align__(16) double jsm[];
     if (gated && overflowed(A)) return;
+    const int lane = threadIdx.x & 31;
     for (int w = blockIdx.x; w < A.W; w += gridDim.x) {
         if (!A.w_active[w]) continue;
         const int j0 = A.w_joint_off[w], J = A.w_joint_n[w], j1 = j0 + J;
         if (J == 0) continue;
         const double dt = A.w_dt[w];
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const int iters = A.w_jiters[w];
+        const bool waves = iters <= JOINT_WAVE_ITERS;   // the schedule buffers hold that many iterations
+        const int E = waves ? J * iters : J;
+        // the joints' bodies span [lo, hi]
+        int lo = 0x7FFFFFFF, hi = -1;
+        for (int j = j0 + lane; j < j1; j += 32) {
+            const int a = A.j_a[j], b = A.j_b[j];
+            if (a >= 0) { lo = min(lo, a); hi = max(hi, a); }
+            if (b >= 0) { lo = min(lo, b); hi = max(hi, b); }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(FULL, lo, o));
+            hi = max(hi, __shfl_xor_sync(FULL, hi, o));
+        }
+        const int nbr = hi >= lo ? hi - lo + 1 : 0;
+        // shared memory: the velocities, then the levels and the order, then
+        // (once the level count is known) the level starts; the prepared rows
+        // stay in j_data (read-only once prepared, they are served by L1)
+        long long used = 0;
+        JointVel V;
+        V.s = nullptr;
+        V.lo = lo;
+        if (nbr > 0 && 6LL * nbr <= smem_doubles) { V.s = jsm; used = 6LL * nbr; }
+        int *ip = reinterpret_cast<int *>(jsm + used);
+        const long long ints_free = 2LL * (smem_doubles - used);
+        int *last, *lvl, *order;
+        int last_base;
+        long long iused = 0;
+        if ((long long)nbr + 2LL * E <= ints_free) {
+            last = ip;
+            last_base = lo;
+            lvl = last + nbr;
+            order = lvl + E;
+            iused = (long long)nbr + 2LL * E;
+        } else {
+            last = A.b_last;
+            last_base = 0;
+            lvl = A.j_level + (size_t)j0 * JOINT_WAVE_ITERS;
+            order = A.j_order + (size_t)j0 * JOINT_WAVE_ITERS;
+        }
+        for (int j = j0 + lane; j < j1; j += 32) {
             if (A.j_type[j] == 2) { if (A.j_a[j] >= 0) wake_body(A, A.j_a[j]); }
             else {
                 if (A.j_a[j] >= 0) wake_body(A, A.j_a[j]);
                 if (A.j_b[j] >= 0) wake_body(A, A.j_b[j]);
             }
-            joint_prepare(A, j);
+            joint_prepare(A, j, &A.j_data[(size_t)j * JD]);
         }
-        const int b0 = A.w_body_off[w], b1 = b0 + A.w_body_n[w];
-        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) A.b_last[i] = -1;
-        __syncthreads();
-        const int iters = A.w_jiters[w];
-        const bool waves = iters <= JOINT_WAVE_ITERS;   // the schedule buffers hold that many iterations
-        const int E = waves ? J * iters : J;
-        int *lvl = A.j_level + (size_t)j0 * JOINT_WAVE_ITERS;
-        int *order = A.j_order + (size_t)j0 * JOINT_WAVE_ITERS;
-        int *ls = A.j_level_start + (size_t)j0 * JOINT_WAVE_ITERS + w;
-        int *cursor = A.j_level_start + ((size_t)A.NJ * JOINT_WAVE_ITERS + A.W + 1) + (size_t)j0 * JOINT_WAVE_ITERS + w;
-        if (threadIdx.x < 32) {
-            const int D = waves ? warp_joint_levels(A, j0, J, iters, A.b_last, lvl, 0)
-                                : warp_levels(J, A.j_a + j0, A.j_b + j0, A.mtype, A.b_last, lvl);
-            if (threadIdx.x == 0) s_D = D;
-        }
-        __syncthreads();
-        const int D = s_D;
-        bucket_levels(E, D, lvl, ls, cursor, order);
-        if (waves) {
-            for (int l = 0; l < D; l++) {
-                for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) {
-                    const int e = order[q], j = j0 + e % J;
-                    if (!motor_alone(A, j)) joint_solve(A, j, dt);
-                    else if (e < J) for (int k = 0; k < iters; k++) joint_solve(A, j, dt);
-                }
-                __syncthreads();
-            }
+        for (int i = lane; i < nbr; i += 32) last[lo + i - last_base] = -1;
+        __syncwarp();
+        const int D = waves ? warp_joint_levels(A, j0, J, iters, last, lvl, last_base)
+                            : warp_levels(J, A.j_a + j0, A.j_b + j0, A.mtype, last, lvl, last_base);
+        int *ls, *cur;
+        if (iused > 0 && iused + 2LL * (D + 1) <= ints_free) {
+            ls = ip + iused;
+            cur = ls + D + 1;
         } else {
-            for (int it = 0; it < iters; it++) {
-                for (int l = 0; l < D; l++) {
-                    for (int q = ls[l] + threadIdx.x; q < ls[l + 1]; q += blockDim.x) joint_solve(A, j0 + order[q], dt);
-                    __syncthreads();
-                }
-            }
+            ls = A.j_level_start + (size_t)j0 * JOINT_WAVE_ITERS + w;
+            cur = A.j_level_start + ((size_t)A.NJ * JOINT_WAVE_ITERS + A.W + 1) + (size_t)j0 * JOINT_WAVE_ITERS + w;
         }
+        // bucket the entries by level: ls[l] = first slot of level l
+        for (int l = lane; l <= D; l += 32) ls[l] = 0;
+        __syncwarp();
+        for (int k = lane; k < E; k += 32)
+            if (lvl[k] + 1 <= D) atomicAdd(&ls[lvl[k] + 1], 1);
+        __syncwarp();
+        warp_scan_inclusive(ls, D + 1);
+        for (int l = lane; l <= D; l += 32) cur[l] = ls[l];
+        __syncwarp();
+        for (int k = lane; k < E; k += 32) {
+            // a lone motor's entries carry bit 31: its iteration-0 entry runs all its iterations
+            const bool alone = waves && motor_alone(A, j0 + k % J);
+            order[atomicAdd(&cur[lvl[k]], 1)] = k | (alone ? (int)0x80000000u : 0);
+        }
+        if (V.s)
+            for (int i = lane; i < nbr; i += 32)
+                for (int q = 0; q < 3; q++) {
+                    V.s[i * 6 + q] = A.v[(size_t)(lo + i) * 3 + q];
+                    V.s[i * 6 + 3 + q] = A.w[(size_t)(lo + i) * 3 + q];
+                }
+        __syncwarp();
+        const int rounds = waves ? 1 : iters;
+        for (int it = 0; it < rounds; it++)
+            for (int l = 0; l < D; l++) {
+                const int qa = ls[l], qb = ls[l + 1];
+                for (int q = qa + lane; q < qb; q += 32) {
+                    const int v = order[q], e = v & 0x7FFFFFFF, jj = e % J, j = j0 + jj;
+                    const double *Dr = &A.j_data[(size_t)j * JD];
+                    if (v >= 0) joint_solve(A, j, Dr, V, dt);
+                    else if (e < J) for (int k = 0; k < iters; k++) joint_solve(A, j, Dr, V, dt);
+                }
+                __syncwarp();
+            }
+        if (V.s)
+            for (int i = lane; i < nbr; i += 32)
+                if (A.mtype[lo + i] == 2)
+                    for (int q = 0; q < 3; q++) {
+                        A.v[(size_t)(lo + i) * 3 + q] = V.s[i * 6 + q];
+                        A.w[(size_t)(lo + i) * 3 + q] = V.s[i * 6 + 3 + q];
+                    }
+        __syncwarp();
     }
 }
 

@@ -86,8 +86,9 @@ struct OmiCtx {
     int cap_blocks = 0;            // resident k_capsule_triangles blocks per SM
     // bounds a test may lower (omi_set_limits): sweep wait polls, EPA faces, stalled run
     int spin_limit = SPIN_LIMIT_DEFAULT, epa_faces = EPA_F, stall_run = -1;
-    OmiTuning tune = {8, 4, 256, 16, 128, 4, 32, 16, 32};   // launch configuration (omi_set_tuning)
+    OmiTuning tune = {8, 4, 256, 16, 128, 4, 16, 16, 32};   // launch configuration (omi_set_tuning)
     int cluster_max = 0;                        // largest thread-block cluster of k_csweep the GPU schedules
+    int cluster_ints = 0;                       // shared-memory ints a k_csweep CTA may use (0: all it has)
     // wide worlds (their stages on many blocks): the worlds, bodies of the largest, sort merge passes
     std::vector<int> h_wide;
     int wide_max_n = 0, wide_merge_passes = 0;
@@ -397,21 +398,33 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
         k_iterate<8><<<std::min(A.W, ctx->sm_count), 256, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles,
                                                                                      ctx->tune.sweep_max_split);
     ctx->launches += 4;
-    const int csmem_ints = (int)(sweep_cluster_smem() / sizeof(int));
-    if (nw && ctx->tune.wide_cluster == 16) {
-        for (int wi = 0; wi < nw; wi++)
-            k_csweep<16><<<16, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints);
-        ctx->launches += nw;
-    } else if (nw && ctx->tune.wide_cluster == 8) {
-        for (int wi = 0; wi < nw; wi++)
-            k_csweep<8><<<8, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints);
-        ctx->launches += nw;
+    const int csmem_full = (int)(sweep_cluster_smem() / sizeof(int));
+    const int csmem_ints = ctx->cluster_ints > 0 ? std::min(ctx->cluster_ints, csmem_full) : csmem_full;
+    const int wb = std::min(ctx->tune.wide_sweep_blocks, ctx->sm_count);
+    if (nw && (ctx->tune.wide_cluster == 16 || ctx->tune.wide_cluster == 8)) {
+        // the cluster sweeps a world whose records fit its shared memory; the
+        // many-block sweep after it takes the world otherwise (it returns at
+        // once when the cluster swept); with one wide block chosen the
+        // cluster sweeps every world itself
+        const int handoff = wb > 1;
+        for (int wi = 0; wi < nw; wi++) {
+            if (ctx->tune.wide_cluster == 16)
+                k_csweep<16><<<16, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints, handoff);
+            else
+                k_csweep<8><<<8, SWEEP_THREADS, sweep_cluster_smem(), ctx->stream>>>(A, wi, csmem_ints, handoff);
+            ctx->launches++;
+            if (handoff) {
+                k_wsweep_init<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+                k_wsweep_seed<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
+                k_wsweep<<<wb, SWEEP_THREADS, 0, ctx->stream>>>(A, wi);
+                ctx->launches += 3;
+            }
+        }
     } else if (nw && ctx->tune.wide_sweep_blocks == 1) {
         // one block per wide world: the per-world sweep with its shared-memory staging
         k_wsweep_one<<<nw, SWEEP_THREADS, sweep_smem, ctx->stream>>>(A, ctx->stage_doubles);
         ctx->launches++;
     } else {
-        const int wb = std::min(ctx->tune.wide_sweep_blocks, ctx->sm_count);
         for (int wi = 0; wi < nw; wi++) {      // one wide world at a time, on wb SMs
             k_wsweep_init<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
             k_wsweep_seed<<<cgrid, 256, 0, ctx->stream>>>(A, wi);
@@ -439,7 +452,8 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
 void stage_joints(OmiCtx *ctx, Prof *pf, int gated) {
     Arena &A = ctx->A;
     if (A.NJ > 0) {
-        k_joints<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A, gated);
+        k_joints<<<std::min(A.W, 65535), 32, JOINT_SMEM_DOUBLES * sizeof(double), ctx->stream>>>(A, gated,
+                                                                                          JOINT_SMEM_DOUBLES);
         ctx->launches++;
     }
     mark(ctx, pf, KN_JOINTS);
@@ -623,6 +637,7 @@ int omi_create(int device, OmiCtx **out) {
         {(const void *)k_prep, PREP_THREADS * CD * (int)sizeof(double), "k_prep"},
         {(const void *)k_wsort_tiles, WSORT_TILE * 24, "k_wsort_tiles"},
         {(const void *)k_wsweep_one, SWEEP_SMEM_DOUBLES * (int)sizeof(double), "k_wsweep_one"},
+        {(const void *)k_joints, JOINT_SMEM_DOUBLES * (int)sizeof(double), "k_joints"},
     };
     for (const auto &f : smem) {
         e = cudaFuncSetAttribute(f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, f.bytes);
@@ -1476,6 +1491,14 @@ int omi_set_tuning(OmiCtx *ctx, const OmiTuning *t) {
 int omi_set_wide_threshold(OmiCtx *ctx, int32_t bodies) {
     if (!ctx || bodies < 0) return OMI_E_ARG;
     ctx->wide_min_bodies = bodies;
+    return 0;
+}
+
+int omi_set_cluster_budget(OmiCtx *ctx, int32_t ints) {
+    if (!ctx || ints < 0) return OMI_E_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);                     // the budget is a launch argument of the captured sweep
+    ctx->cluster_ints = ints;
     return 0;
 }
 

@@ -15,7 +15,12 @@ namespace omi {
 
 // per wide world, ints of global counters (zeroed before the solve stage)
 constexpr int WIDE_STATE_INTS = 32;
-enum { WS_HEAD = 0, WS_TAIL = 8, WS_CLAIMED = 16, WS_ABORT = 17, WS_HIST = 18, WS_CASCADE = 22 };
+enum { WS_HEAD = 0, WS_TAIL = 8, WS_CLAIMED = 16, WS_ABORT = 17, WS_HIST = 18, WS_CASCADE = 22, WS_SWEPT = 23 };
+// set by the cluster sweep when it swept the world this step: the many-block
+// sweep launched after it then has nothing to do
+__device__ __forceinline__ bool wide_swept(const Arena &A, int wi) {
+    return A.wide_state[wi * WIDE_STATE_INTS + WS_SWEPT] != 0;
+}
 // bodies per sort tile (sorted in shared memory, then merged in global memory)
 constexpr int WSORT_TILE = 4096;
 constexpr int WSORT_THREADS = 512;
@@ -328,7 +333,7 @@ __device__ __forceinline__ void wide_push(int *ring, int *st, const WideRings &w
 // arrival counts zeroed, ring cleared, runs counted by length (for the class sizes)
 __global__ void k_wsweep_init(Arena A, int wi) {
     __shared__ int hist[4];
-    if (overflowed(A)) return;
+    if (overflowed(A) || wide_swept(A, wi)) return;
     const int w = A.wide_w[wi];
     if (!world_collides(A, w)) return;
     int c0, c1;
@@ -364,7 +369,7 @@ __device__ __forceinline__ void wide_rings(const int *st, int P, WideRings &wr) 
 // depends on another block having started
 __global__ void k_wsweep_seed(Arena A, int wi) {
     __shared__ WideRings wr;
-    if (overflowed(A)) return;
+    if (overflowed(A) || wide_swept(A, wi)) return;
     const int w = A.wide_w[wi];
     if (!world_collides(A, w)) return;
     int *st = A.wide_state + wi * WIDE_STATE_INTS;
@@ -380,7 +385,7 @@ __global__ void k_wsweep_seed(Arena A, int wi) {
 
 __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
     __shared__ WideRings wr;
-    if (overflowed(A)) return;
+    if (overflowed(A) || wide_swept(A, wi)) return;
     const int w = A.wide_w[wi];
     if (!world_collides(A, w)) return;
     int *st = A.wide_state + wi * WIDE_STATE_INTS;
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
         __syncwarp();
     }
     if (lane == 0 && ld_relaxed_gpu(&st[WS_ABORT])) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweep
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.w_levels[w] = -2;     // not tracked on the many-block sweep
 }
 
 // the sweep of wide world blockIdx.x by one block: k_iterate's sweep_world on
@@ -623,8 +628,14 @@ __device__ __forceinline__ void run_pass_rec(const Arena &A, double *ra, double 
 // distributed shared memory; otherwise records are the global arrays.
 // A CTA whose successors and written records are all its own releases with
 // a CTA-scope fence, else cluster scope.
+// With `handoff`, a world whose records do not fit is left to the many-block
+// sweep launched after this kernel (on 16 SMs with every record and table in
+// global memory the cluster is slower than that sweep on 32: a hull pile of
+// 32768 bodies at 72K runs takes 13.4 ms here against 8.3 ms there); a world
+// the cluster sweeps is marked WS_SWEPT, which ends the many-block launches.
 template <int C>
-__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csweep(Arena A, int wi, int smem_ints) {
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csweep(Arena A, int wi, int smem_ints,
+                                                                                   int handoff) {
     extern __shared__ __align__(16) int csm[];
     __shared__ ClusterShared cs;
     cg::cluster_group cluster = cg::this_cluster();
@@ -711,6 +722,16 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
     }
     __syncthreads();
     const bool staged = cs.staged != 0;
+    if (handoff) {
+        // every CTA reads the same flags, so all leave here or none; the
+        // barrier keeps each CTA's shared memory alive until every other has
+        // read its fit flag
+        if (!staged) {
+            cluster.sync();
+            return;
+        }
+        if (me == 0 && threadIdx.x == 0) A.wide_state[wi * WIDE_STATE_INTS + WS_SWEPT] = 1;
+    }
     // impulses of this CTA's contacts (a contiguous range: its runs') in shared memory when room is left
     const int k_lo = Rb ? (run_kn[r0] & 0xFFFFFF) : 0;
     const int k_hi = Rb ? (r0 + Rb < R ? (run_kn[r0 + Rb] & 0xFFFFFF) : K) : 0;
@@ -871,7 +892,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
         __syncwarp();
     }
     if (lane == 0 && *(volatile int *)&cs.abort) atomicOr(&A.status[ST_SWEEP_TIMEOUT], 1);
-    if (me == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the wide sweeps
+    if (me == 0 && threadIdx.x == 0) A.w_levels[w] = -1;     // not tracked on the cluster sweep
     __syncthreads();
     cluster.sync();               // every entry done: records final, no CTA reaches another's memory after this
     if (staged) {

@@ -35,7 +35,7 @@ SPACE = {
     'pair_blocks_per_sm': (16, 8, 32),
     'narrow_block': (128, 64, 256),
     'gjk_warps': (4, 2, 8),
-    'wide_sweep_blocks': (32, 1, 8, 16, 64, 148),
+    'wide_sweep_blocks': (16, 1, 8, 24, 32, 64, 148),
     'wide_cluster': (16, 8, 0),
     'sweep_claim': (32, 16, 8),
 }

@@ -84,4 +84,34 @@ def test_wide_and_per_world_worlds_in_one_arena(monkeypatch):
             for col in ('position', 'orientation', 'linear_velocity', 'angular_velocity', 'sleep_timer'):
                 assert np.array_equal(getattr(w, '_' + col)[:n], st[col]), tag + ' ' + col
             assert np.array_equal(w._awake[:n], st['awake']), tag
-    assert (b.levels()[[1, 3]] == -1).all() and (b.levels()[[0, 2, 4]] >= 0).all()
+    assert (b.levels()[[1, 3]] < 0).all() and (b.levels()[[0, 2, 4]] >= 0).all()
+
+
+@pytest.mark.parametrize('budget', [64, 1400, 0])
+def test_cluster_hands_off_worlds_that_do_not_fit(budget):
+    """The cluster sweep takes a wide world only while every CTA's body
+    records and run tables fit its shared memory; otherwise the many-block
+    sweep launched after it does. A budget of 64 ints per CTA fits no world
+    (every step hands off), 1400 lies near the debris world's needs as its
+    contacts grow (the form may change between steps), 0 is the whole of
+    shared memory (the cluster sweeps every step). Every step matches the
+    oracle bit for bit, whichever form swept it."""
+    w, meta = scenes.debris(n=512, seed=1, extent=8.0, height=12.0, ground=30.0)
+    dt = meta['dt']
+    o = pyoracle.OracleWorld.from_world(w)
+    b = WorldBatch([w], dts=[dt])
+    if b.ctx.tuning()['wide_cluster'] == 0:
+        pytest.skip('this GPU schedules no sweep cluster')
+    b.ctx.set_cluster_budget(budget)
+    forms = set()
+    for s in range(150):
+        b.step(1)
+        b.sync_to_host()
+        o.step(dt)
+        P._compare_step(b, w, o, 'budget %d step %d' % (budget, s))
+        forms.add(int(b.levels()[0]))
+    if budget == 64:
+        assert forms <= {-2, 0}
+    if budget == 0:
+        assert -1 in forms and -2 not in forms
+    b.ctx.set_cluster_budget(0)

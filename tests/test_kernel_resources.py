@@ -27,6 +27,7 @@ LIMITS = {            # kernel name fragment -> register ceiling
     'k_refit': 96,
     'k_integrate_forces': 64,
     'k_capsule_triangles': 128,
+    'k_joints': 128,
 }
 
 
