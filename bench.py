@@ -94,7 +94,11 @@ def just_step(args):
     else:
         worlds, dts = scenes.CONFIGS[args.workload][0]()
     b = WorldBatch(worlds, dts=dts)
-    b.step(args.just_step)
+    # one step per call: a step that overflows its buffers is re-run at once,
+    # so the k-th launch of a kernel belongs to step k (plus one per overflow)
+    # and not to a batch of steps made no-ops behind an overflow
+    for _ in range(args.just_step):
+        b.step(1)
     torch.cuda.synchronize()
     print(json.dumps({'workload': args.workload, 'worlds': len(worlds), 'steps': args.just_step,
                       'contacts': int(b.counts()[1].sum())}))

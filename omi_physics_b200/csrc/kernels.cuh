@@ -8,6 +8,8 @@
 // overflow is known before any body state is modified and the step can be
 // re-run after the buffers grow.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "arena.cuh"
 #include "geometry.cuh"
 #include "gjk.cuh"
@@ -17,6 +19,17 @@ namespace omi {
 
 constexpr int WF_SLEEP = 1, WF_WARM = 2, WF_COLLISION = 4;
 constexpr unsigned FULL = 0xffffffffu;
+
+// a slot of a work list whose order does not matter: the lanes that reach
+// this call together take consecutive slots with one increment of the list's
+// counter (one increment per lane serialises every list entry of a launch on
+// one address)
+__device__ __forceinline__ int list_slot(int *counter) {
+    cooperative_groups::coalesced_group g = cooperative_groups::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+    return g.shfl(base, 0) + (int)g.thread_rank();
+}
 
 __device__ __forceinline__ bool pairs_over(const Arena &A) {
     return A.pair_scan[A.NB] > A.pair_cap;
@@ -510,7 +523,7 @@ __global__ void k_narrow(Arena A) {
         int cnt = 0;
         const int kindp = A.pair_solid[p];
         if (kindp == 2) {
-            A.trig_list[atomicAdd(A.trig_n, 1)] = p;     // overlap tested after the solve
+            A.trig_list[list_slot(A.trig_n)] = p;     // overlap tested after the solve
         } else if (kindp == 1) {
             const int a = A.pair_a[p], b = A.pair_b[p];
             const int ka = A.kind[a], kb = A.kind[b];
@@ -519,9 +532,9 @@ __global__ void k_narrow(Arena A) {
                 // the mesh route (collide.py:272-306): counted by k_mesh_count,
                 // written straight into the contact arrays by k_mesh_emit
                 A.pair_solid[p] = 3;
-                A.mesh_list[atomicAdd(A.mesh_n, 1)] = p;
+                A.mesh_list[list_slot(A.mesh_n)] = p;
             } else if (ka >= 3 || kb >= 3) {
-                const int idx = atomicAdd(A.gjk_n, 1);
+                const int idx = list_slot(A.gjk_n);
                 A.gjk_list[idx] = p;
             } else {
                 double nrm[3], pts[12], dep[4];
@@ -536,7 +549,7 @@ __global__ void k_narrow(Arena A) {
                     double depth;
                     if (box_box_sat(pa, Ra, ha, pb, Rb, hb, nrm, depth)) {
                         s[0] = nrm[0]; s[1] = nrm[1]; s[2] = nrm[2]; s[3] = depth;
-                        A.clip_list[atomicAdd(A.clip_n, 1)] = p;
+                        A.clip_list[list_slot(A.clip_n)] = p;
                     }
                 } else if (ka == 1 && kb == 1) {
                     cnt = sphere_sphere(pa, ha[0], pb, hb[0], nrm, pts, dep);

@@ -98,17 +98,18 @@ __device__ inline void hash_runs(const Arena &A, int t, int w, int first, int st
         int len = 1;
         while (e + len < off + n && ca[e + len] == ca[e] && cb[e + len] == cb[e]) len++;
         const unsigned long long key = pair_key(ca[e], cb[e]);
-        int s = hash_slot(key, A.hash_mask);
+        int s = hash_slot(key, A.hash_mask), fresh = -1;
         for (int probe = 0; probe <= A.hash_mask; probe++) {
             const unsigned long long prev = atomicCAS(&A.hkey[t][s], ~0ull, key);
             if (prev == ~0ull || prev == key) {
                 A.hval[t][s * 2] = e;
                 A.hval[t][s * 2 + 1] = len;
-                if (prev == ~0ull) A.hused[t][atomicAdd(&A.hused_n[t], 1)] = s;
+                if (prev == ~0ull) fresh = s;
                 break;
             }
             s = (s + 1) & A.hash_mask;
         }
+        if (fresh >= 0) A.hused[t][list_slot(&A.hused_n[t])] = fresh;   // the slots the next clear empties
     }
 }
 
@@ -130,8 +131,9 @@ __global__ void k_hash_rebuild(Arena A, int t) {
 }
 
 // ---------------------------------------------------------------------------
-// joints (world.py:599-611, joints.py:60-212), one CTA per world; prepare in
-// parallel, then joint_iterations sweeps in registration order by levels
+// joints (world.py:599-611, joints.py:60-212), one warp per world; prepare in
+// parallel, then every joint iteration in registration order, as wavefront
+// levels
 // ---------------------------------------------------------------------------
 enum { J_IA = 0, J_IB = 9, J_RA = 18, J_RB = 21, J_LU = 24, J_PIV = 33, J_BIAS = 36, J_N = 39,
        J_MASS = 42, J_BIASS = 43 };
@@ -416,10 +418,11 @@ __device__ inline int warp_joint_levels(const Arena &A, int j0, int J, int iters
     return maxl + 1;
 }
 
-// shared memory of one k_joints block (one world at a time), in doubles: a
-// 128-link chain at 12 iterations needs about 2.5K (velocities 0.8K,
-// schedule 1.8K); seven blocks fit on an SM
-constexpr int JOINT_SMEM_DOUBLES = 4096;
+// shared memory of one k_joints block (one world at a time), in doubles, at
+// most: the launch sizes it to the scene's largest need (joint_smem_need);
+// a 128-link chain at 12 iterations needs about 8.7K (rows 6.1K, velocities
+// 0.8K, schedule 1.8K), so three blocks fit on an SM
+constexpr int JOINT_SMEM_DOUBLES = 13312;
 
 // inclusive prefix sums of a[0..n) by one warp (each lane sums a chunk)
 __device__ inline void warp_scan_inclusive(int *a, int n) {
@@ -445,10 +448,11 @@ __device__ inline void warp_scan_inclusive(int *a, int n) {
 // iteration in the reference's order, as wavefront levels. One warp per world
 // (one block of 32 threads): a chain's levels hold a few entries each (about
 // one per iteration in flight), so a warp fills them and steps from level to
-// level with __syncwarp alone. The joints' body velocities and the schedule
-// (levels, order, level starts) live in the block's shared memory as far as
-// `smem_doubles` goes, else in the global arrays; the velocities go back to
-// the global arrays at the end.
+// level with __syncwarp alone. The prepared rows, the joints' body
+// velocities and the schedule (levels, order, level starts) live in the
+// block's shared memory as far as `smem_doubles` goes, else in the global
+// arrays (rows in L1 lose to shared memory: the solve stalls on them); the
+// velocities go back to the global arrays at the end.
 __global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_doubles) {
     extern __shared__ __align__(16) double jsm[];
     if (gated && overflowed(A)) return;
@@ -473,14 +477,16 @@ __global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_d
             hi = max(hi, __shfl_xor_sync(FULL, hi, o));
         }
         const int nbr = hi >= lo ? hi - lo + 1 : 0;
-        // shared memory: the velocities, then the levels and the order, then
-        // (once the level count is known) the level starts; the prepared rows
-        // stay in j_data (read-only once prepared, they are served by L1)
+        // shared memory: the prepared rows, the velocities, the levels and the
+        // order, then (once the level count is known) the level starts; each
+        // in the global arrays when it does not fit
         long long used = 0;
+        double *rows = nullptr;
+        if ((long long)J * JD <= smem_doubles) { rows = jsm; used = (long long)J * JD; }
         JointVel V;
         V.s = nullptr;
         V.lo = lo;
-        if (nbr > 0 && 6LL * nbr <= smem_doubles) { V.s = jsm; used = 6LL * nbr; }
+        if (nbr > 0 && used + 6LL * nbr <= smem_doubles) { V.s = jsm + used; used += 6LL * nbr; }
         int *ip = reinterpret_cast<int *>(jsm + used);
         const long long ints_free = 2LL * (smem_doubles - used);
         int *last, *lvl, *order;
@@ -504,7 +510,7 @@ __global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_d
                 if (A.j_a[j] >= 0) wake_body(A, A.j_a[j]);
                 if (A.j_b[j] >= 0) wake_body(A, A.j_b[j]);
             }
-            joint_prepare(A, j, &A.j_data[(size_t)j * JD]);
+            joint_prepare(A, j, rows ? rows + (size_t)(j - j0) * JD : &A.j_data[(size_t)j * JD]);
         }
         for (int i = lane; i < nbr; i += 32) last[lo + i - last_base] = -1;
         __syncwarp();
@@ -545,7 +551,7 @@ __global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_d
                 const int qa = ls[l], qb = ls[l + 1];
                 for (int q = qa + lane; q < qb; q += 32) {
                     const int v = order[q], e = v & 0x7FFFFFFF, jj = e % J, j = j0 + jj;
-                    const double *Dr = &A.j_data[(size_t)j * JD];
+                    const double *Dr = rows ? rows + (size_t)jj * JD : &A.j_data[(size_t)j * JD];
                     if (v >= 0) joint_solve(A, j, Dr, V, dt);
                     else if (e < J) for (int k = 0; k < iters; k++) joint_solve(A, j, Dr, V, dt);
                 }

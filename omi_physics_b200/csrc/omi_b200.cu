@@ -89,6 +89,7 @@ struct OmiCtx {
     OmiTuning tune = {8, 4, 256, 16, 128, 4, 16, 16, 32};   // launch configuration (omi_set_tuning)
     int cluster_max = 0;                        // largest thread-block cluster of k_csweep the GPU schedules
     int cluster_ints = 0;                       // shared-memory ints a k_csweep CTA may use (0: all it has)
+    int joint_smem = 0;                         // doubles of shared memory a k_joints block takes
     // wide worlds (their stages on many blocks): the worlds, bodies of the largest, sort merge passes
     std::vector<int> h_wide;
     int wide_max_n = 0, wide_merge_passes = 0;
@@ -162,6 +163,23 @@ int passes_of(int flags, int iters) {
 int grid_for(int n, int block, int cap) {
     int g = (n + block - 1) / block;
     return std::max(1, std::min(g, cap));
+}
+
+// shared memory (doubles) k_joints wants for one world's joints: prepared
+// rows, the velocities of the joints' body range and the schedule (levels
+// and order of every entry, and level starts for a chain's J + 2 iters
+// levels with room to spare), capped at JOINT_SMEM_DOUBLES
+int joint_smem_need(const int *ja, const int *jb, int nj, int iters) {
+    if (nj <= 0) return 0;
+    int lo = INT32_MAX, hi = -1;
+    for (int j = 0; j < nj; j++)
+        for (int b : {ja[j], jb[j]})
+            if (b >= 0) { lo = std::min(lo, b); hi = std::max(hi, b); }
+    const int64_t nbr = hi >= lo ? hi - lo + 1 : 0;
+    const int64_t E = iters <= JOINT_WAVE_ITERS ? (int64_t)nj * std::max(iters, 0) : nj;
+    const int64_t ints = nbr + 2 * E + 2 * ((int64_t)nj + 2 * std::max(iters, 0) + 66);
+    const int64_t need = (int64_t)nj * JD + 6 * nbr + (ints + 1) / 2;
+    return (int)std::min<int64_t>(need, JOINT_SMEM_DOUBLES);
 }
 
 // dynamic shared memory of one k_csweep CTA (what a block may hold, less its static part)
@@ -452,8 +470,8 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
 void stage_joints(OmiCtx *ctx, Prof *pf, int gated) {
     Arena &A = ctx->A;
     if (A.NJ > 0) {
-        k_joints<<<std::min(A.W, 65535), 32, JOINT_SMEM_DOUBLES * sizeof(double), ctx->stream>>>(A, gated,
-                                                                                          JOINT_SMEM_DOUBLES);
+        const int jsd = std::max(ctx->joint_smem, 256);
+        k_joints<<<std::min(A.W, 65535), 32, (size_t)jsd * sizeof(double), ctx->stream>>>(A, gated, jsd);
         ctx->launches++;
     }
     mark(ctx, pf, KN_JOINTS);
@@ -1087,6 +1105,13 @@ static int load_impl(OmiCtx *ctx, const OmiScene *s, const int *body_n, const in
     // ring (~1.5 runs per body x passes)
     ctx->stage_doubles = (int)std::min<int64_t>(SWEEP_SMEM_DOUBLES,
                                                 (int64_t)std::max(max_nc, 1) * (16 + A.max_passes) + 64);
+    ctx->joint_smem = 0;
+    for (int w = 0; w < W; w++) {
+        const int j0 = s->w_joint_off[w], nj = s->w_joint_off[w + 1] - j0;
+        if (nj > 0)
+            ctx->joint_smem = std::max(ctx->joint_smem,
+                                       joint_smem_need(s->j_a + j0, s->j_b + j0, nj, s->w_joint_iters[w]));
+    }
     const int pair_cap = std::max(4096, 4 * NB);
     rc = alloc_dynamic(ctx, pair_cap, 2 * pair_cap);
     if (rc) return rc;
@@ -1242,6 +1267,14 @@ int omi_load_world(OmiCtx *ctx, int32_t slot, const OmiScene *o) {
         if (o->j_type[j] == OMI_JOINT_MOTOR && o->j_a[j] < 0) return fail(ctx, OMI_E_ARG, "motor body");
         ja[j] = o->j_a[j] < 0 ? -1 : o->j_a[j] + b0;
         jb[j] = o->j_b[j] < 0 ? -1 : o->j_b[j] + b0;
+    }
+    {   // a world whose joints want more of k_joints' shared memory re-captures the step
+        const int need = joint_smem_need(o->j_a, o->j_b, nj, o->w_joint_iters[0]);
+        if (need > ctx->joint_smem) {
+            cudaStreamSynchronize(ctx->stream);
+            drop_graph(ctx);
+            ctx->joint_smem = need;
+        }
     }
     int rc = 0;
     rc |= put(ctx, A.pos + (size_t)b0 * 3, o->pos, (size_t)n * 3);

@@ -301,7 +301,12 @@ __global__ void k_wl_links(Arena A) {
 // flag, which ends every other wait, and ST_SWEEP_TIMEOUT. The roots are
 // published by a launch of their own (k_wsweep_seed), so no block waits on
 // work that only another block could start: with several groups' sweeps on
-// the GPU at once, whichever blocks are resident make progress.
+// the GPU at once, whichever blocks are resident make progress. A thread
+// whose arrival makes a successor ready runs that successor next itself
+// (counted as claimed) and publishes only a second one: a chain of entries
+// then skips the ring's publish, poll, claim and slot read between its
+// links, four to five device-memory round trips each (the hull pile's late
+// sweep: 7.8 -> 6.3 ms at 72K runs).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int ld_acquire_gpu(const int *p) {
     int v;
@@ -452,28 +457,39 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
             }
             if (e1 == 0) atomicExch(&st[WS_ABORT], 1);
             else {
-                const int e = e1 - 1;
-                const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
-                const int v = __ldg(run_kn + r);
-                const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
-                double row0[CD];
-                load_row(A, k0, row0);
-                const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
-                run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
-                // release this entry's writes, then count into the successors
-                fence_acq_rel_gpu();
-                const int sides[2] = {sa, sb};
+                int e = e1 - 1;
+                for (int hop = 0; e >= 0; hop++) {
+                    const int r = e & PASS_MASK, p = e >> PASS_SHIFT;
+                    const int v = __ldg(run_kn + r);
+                    const int k0 = c0 + (v & 0xFFFFFF), n = v >> 24;
+                    double row0[CD];
+                    load_row(A, k0, row0);
+                    const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+                    run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
+                    // release this entry's writes, then count into the successors
+                    fence_acq_rel_gpu();
+                    const int sides[2] = {sa, sb};
+                    int next = -1;
 #pragma unroll
-                for (int sd = 0; sd < 2; sd++) {
-                    const int sc = sides[sd];
-                    int ps, rs;
-                    if (sc >= 0) { ps = p; rs = sc; }
-                    else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
-                    else continue;
-                    if (atomicAdd(&arrived[rs], 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
-                        fence_acq_rel_gpu();             // acquire the other arrivals' writes
-                        wide_push(ring, st, wr, (ps << PASS_SHIFT) | rs, __ldg(run_kn + rs) >> 24);
+                    for (int sd = 0; sd < 2; sd++) {
+                        const int sc = sides[sd];
+                        int ps, rs;
+                        if (sc >= 0) { ps = p; rs = sc; }
+                        else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
+                        else continue;
+                        if (atomicAdd(&arrived[rs], 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
+                            fence_acq_rel_gpu();             // acquire the other arrivals' writes
+                            if (next < 0) { next = (ps << PASS_SHIFT) | rs; continue; }
+                            wide_push(ring, st, wr, (ps << PASS_SHIFT) | rs, __ldg(run_kn + rs) >> 24);
+                        }
                     }
+                    // a successor this entry made ready runs next on this thread,
+                    // counted as claimed, instead of going through the ring
+                    if (next >= 0) {
+                        atomicAdd(&st[WS_CLAIMED], 1);
+                        if ((hop & 15) == 15 && ld_relaxed_gpu(&st[WS_ABORT])) break;
+                    }
+                    e = next;
                 }
             }
         }
