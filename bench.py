@@ -2,8 +2,9 @@
 
 Default workload (N=1): the batched serving mix — 1024 independent debris
 worlds, body counts log-uniform in [16, 2048], all resident in HBM and
-advanced as 4 concurrently stepped groups (one context, stream and CUDA graph
-per group; one "step" = every world advances one dt). Reported beside it:
+advanced as concurrently stepped groups (the autotuner's cached group count
+for this GPU and workload, else 4; one context, stream and CUDA graph per
+group; one "step" = every world advances one dt). Reported beside it:
   * e2e: the same steps through the C ABI with every world's mutable state
     uploaded from pinned host memory and downloaded back every step (each
     group round-trips independently, so copies overlap other groups' kernels);
@@ -19,9 +20,12 @@ per group; one "step" = every world advances one dt). Reported beside it:
 
 ``--impl reference`` times the reference CPU implementation on the same
 workload and prints its JSON line (rank 0 only under torchrun).
-Multi-GPU (torchrun): each rank steps its own seeded copy of the mix — worlds
-are independent, so there is no collective on the data path (weak scaling);
-the barrier and the max-over-ranks time use torch.distributed.
+Multi-GPU (torchrun): each rank steps its own seeded copy of the mix (weak
+scaling, the default) or its bin-packed share of one mix (``--scaling
+strong``) — worlds are independent, so there is no collective on the data
+path; the barrier and the max-over-ranks time use torch.distributed.
+``--workload`` times one of the other benchmark configurations over its whole
+run instead.
 """
 import argparse
 import json
@@ -370,9 +374,18 @@ def run_ours(args, rank, world, local):
         tr = json.load(open(tpath)).get(dominant)
         if tr is not None:
             traffic = tr.get('bytes_per_body', 0.0) * NB + tr.get('bytes_per_contact', 0.0) * K
+    n_groups = len(grp.batches)
     roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': round(achieved, 3), 'peak': peak,
                 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': traffic,
                 'algorithmic_bytes': alg, 'kernel_ms': dom_ms,
+                'basis': ('the stage\'s CUDA-event time summed over the %d groups, each group\'s steps '
+                          'launched eagerly one group after another (in the timed step the groups run '
+                          'concurrently, so kernel_ms may exceed ms_per_step); bytes and time both sum '
+                          'over the groups' % n_groups),
+                'launches_per_step': n_groups,
+                'kernel_ms_per_launch': dom_ms / max(n_groups, 1),
+                'step_frac': (sum(algorithmic_bytes(g, NB, P, K) for g in STAGE_GROUPS)
+                              / (ms / args.steps / 1e3) / 1e9 / peak),
                 'peak_source': 'measured' if 'hbm_gbs' in peaks else 'fallback',
                 'stage_ms': {k: round(v, 4) for k, v in groups.items()},
                 'kernel_group_ms': {k: round(v, 4) for k, v in prof.items()}}
