@@ -49,54 +49,70 @@ __global__ void k_hash_clear(Arena A) {
         A.hkey[nxt][A.hused[nxt][i]] = ~0ull;
 }
 
-// world w's entries first, first + stride, ... of the next cache buffer: a
-// CTA per world (threadIdx.x, blockDim.x), or a whole grid for a wide world
-__device__ __forceinline__ void cache_copy_world(const Arena &A, int w, int cur, int first, int stride) {
+// entry e of world w in the next cache buffer: this step's contact c0 + e
+// when the world refreshes its cache, else the entry kept from the current one
+__device__ __forceinline__ void cache_copy_entry(const Arena &A, int w, int cur, int e) {
     const int nxt = 1 - cur;
-    const int dst = A.w_cache_off[nxt][w], n = A.w_cache_n[nxt][w];
+    const int d = A.w_cache_off[nxt][w] + e;
     if (A.w_cache_new[w]) {
         int c0, c1;
         world_contacts(A, w, c0, c1);
-        for (int e = first; e < n; e += stride) {
-            const int k = c0 + e, d = dst + e;
-            A.cache_a[nxt][d] = A.c_a[k];
-            A.cache_b[nxt][d] = A.c_b[k];
-            for (int c = 0; c < 3; c++) {
-                A.cache_pt[nxt][d * 3 + c] = A.c_pt[k * 3 + c];
-                A.cache_imp[nxt][d * 3 + c] = A.c_imp[k * 3 + c];
-            }
+        const int k = c0 + e;
+        A.cache_a[nxt][d] = A.c_a[k];
+        A.cache_b[nxt][d] = A.c_b[k];
+        for (int c = 0; c < 3; c++) {
+            A.cache_pt[nxt][d * 3 + c] = A.c_pt[k * 3 + c];
+            A.cache_imp[nxt][d * 3 + c] = A.c_imp[k * 3 + c];
         }
     } else {
-        const int src = A.w_cache_off[cur][w];
-        for (int e = first; e < n; e += stride) {
-            const int s = src + e, d = dst + e;
-            A.cache_a[nxt][d] = A.cache_a[cur][s];
-            A.cache_b[nxt][d] = A.cache_b[cur][s];
-            for (int c = 0; c < 3; c++) {
-                A.cache_pt[nxt][d * 3 + c] = A.cache_pt[cur][s * 3 + c];
-                A.cache_imp[nxt][d * 3 + c] = A.cache_imp[cur][s * 3 + c];
-            }
+        const int s = A.w_cache_off[cur][w] + e;
+        A.cache_a[nxt][d] = A.cache_a[cur][s];
+        A.cache_b[nxt][d] = A.cache_b[cur][s];
+        for (int c = 0; c < 3; c++) {
+            A.cache_pt[nxt][d * 3 + c] = A.cache_pt[cur][s * 3 + c];
+            A.cache_imp[nxt][d * 3 + c] = A.cache_imp[cur][s * 3 + c];
         }
     }
 }
 
-__global__ void k_cache_copy(Arena A) {   // CTA per world
-    if (overflowed(A)) return;
-    const int cur = *A.parity;
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x)
-        if (!world_wide(A, w)) cache_copy_world(A, w, cur, threadIdx.x, blockDim.x);
+// entries of buffer t in use: the worlds' entries are packed in world order
+__device__ __forceinline__ int cache_total(const Arena &A, int t) {
+    return A.W > 0 ? A.w_cache_off[t][A.W - 1] + A.w_cache_n[t][A.W - 1] : 0;
 }
 
-// insert one key per run of equal (a, b) entries into table t; entries
-// first, first + stride, ... of the world's range (a CTA per world, or a
-// whole grid for a wide world)
-__device__ inline void hash_runs(const Arena &A, int t, int w, int first, int stride) {
-    const int off = A.w_cache_off[t][w], n = A.w_cache_n[t][w];
+// the world that entry d of buffer t belongs to: the last world whose first
+// entry is at or before d (an empty world shares its offset with the next
+// world, which is the one that holds d)
+__device__ __forceinline__ int cache_world(const Arena &A, int t, int d) {
+    int lo = 0, hi = A.W;
+    while (lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if (A.w_cache_off[t][m] <= d) lo = m + 1; else hi = m;
+    }
+    return lo - 1;
+}
+
+// Every world's entries of the next buffer, one thread per entry over the
+// whole grid (a world's entries no longer wait for one CTA to stride through
+// them; the largest world set the time of the CTA-per-world form).
+__global__ void k_cache_copy(Arena A) {
+    if (overflowed(A)) return;
+    const int cur = *A.parity, nxt = 1 - cur;
+    const int total = cache_total(A, nxt);
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < total; d += gridDim.x * blockDim.x) {
+        const int w = cache_world(A, nxt, d);
+        cache_copy_entry(A, w, cur, d - A.w_cache_off[nxt][w]);
+    }
+}
+
+// insert one key per run of equal (a, b) entries of buffer t's range
+// [lo, hi) into table t, looking at entries lo + first, lo + first + stride, ...
+__device__ inline void hash_range(const Arena &A, int t, int lo, int hi, int first, int stride) {
     const int *ca = A.cache_a[t], *cb = A.cache_b[t];
-    for (int e = off + first; e < off + n; e += stride) {
-        if (e > off && ca[e] == ca[e - 1] && cb[e] == cb[e - 1]) continue;
+    for (int e = lo + first; e < hi; e += stride) {
+        if (e > lo && ca[e] == ca[e - 1] && cb[e] == cb[e - 1]) continue;
         int len = 1;
-        while (e + len < off + n && ca[e + len] == ca[e] && cb[e + len] == cb[e]) len++;
+        while (e + len < hi && ca[e + len] == ca[e] && cb[e + len] == cb[e]) len++;
         const unsigned long long key = pair_key(ca[e], cb[e]);
         int s = hash_slot(key, A.hash_mask), fresh = -1;
         for (int probe = 0; probe <= A.hash_mask; probe++) {
@@ -113,11 +129,20 @@ __device__ inline void hash_runs(const Arena &A, int t, int w, int first, int st
     }
 }
 
-__global__ void k_hash_build(Arena A) {   // CTA per world, table = next buffer
+// world w's runs (a CTA per world)
+__device__ inline void hash_runs(const Arena &A, int t, int w, int first, int stride) {
+    const int off = A.w_cache_off[t][w];
+    hash_range(A, t, off, off + A.w_cache_n[t][w], first, stride);
+}
+
+// Every world's runs at once, over the whole grid, table = next buffer. Body
+// indices are global and no two worlds share a body, so a run (one body
+// pair) never reaches into the next world: scanning the packed buffer as
+// one range finds exactly the runs the per-world scan finds.
+__global__ void k_hash_build(Arena A) {
     if (overflowed(A)) return;
     const int nxt = 1 - *A.parity;
-    for (int w = blockIdx.x; w < A.W; w += gridDim.x)
-        if (!world_wide(A, w)) hash_runs(A, nxt, w, threadIdx.x, blockDim.x);
+    hash_range(A, nxt, 0, cache_total(A, nxt), blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 __global__ void k_flip(Arena A) {

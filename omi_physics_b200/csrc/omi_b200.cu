@@ -458,10 +458,10 @@ void stage_solve(OmiCtx *ctx, Prof *pf) {
     mark(ctx, pf, KN_TRIGGERS);
     k_cache_plan<<<1, 1024, 0, ctx->stream>>>(A);
     k_hash_clear<<<grid_for(ctx->cache_cap, 256, SM_CAP), 256, 0, ctx->stream>>>(A);
-    k_cache_copy<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
-    if (nw) { k_wcache_copy<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A); ctx->launches++; }
-    k_hash_build<<<std::min(A.W, 65535), 128, 0, ctx->stream>>>(A);
-    if (nw) { k_whash_build<<<dim3(cgrid, nw), 256, 0, ctx->stream>>>(A); ctx->launches++; }
+    // every world's entries (wide ones included) over the whole grid
+    const int kgrid_cache = grid_for(ctx->cache_cap, 256, SM_CAP);
+    k_cache_copy<<<kgrid_cache, 256, 0, ctx->stream>>>(A);
+    k_hash_build<<<kgrid_cache, 256, 0, ctx->stream>>>(A);
     k_flip<<<1, 1, 0, ctx->stream>>>(A);
     ctx->launches += 5;
     mark(ctx, pf, KN_CACHE);

@@ -927,19 +927,6 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(SWEEP_THREADS) k_csw
 }
 
 // ---------------------------------------------------------------------------
-// warm-start cache store of wide worlds (k_cache_copy, k_hash_build per world)
-// ---------------------------------------------------------------------------
-__global__ void k_wcache_copy(Arena A) {
-    if (overflowed(A)) return;
-    cache_copy_world(A, A.wide_w[blockIdx.y], *A.parity, wide_tid(), wide_stride());
-}
-
-__global__ void k_whash_build(Arena A) {
-    if (overflowed(A)) return;
-    hash_runs(A, 1 - *A.parity, A.wide_w[blockIdx.y], wide_tid(), wide_stride());
-}
-
-// ---------------------------------------------------------------------------
 // integrate positions and sleep of wide worlds (k_finalize's passes, each a
 // grid launch; the union-find works on the global parent array of the world,
 // roots the island's smallest index, so labels match k_finalize's):
