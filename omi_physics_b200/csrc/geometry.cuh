@@ -184,9 +184,12 @@ __device__ inline int clip_faces(const double *ca, const double *Ra, const doubl
     for (int r = 0; r < 3; r++) neg[r] = -ref_n[r];
     double isign = 0.0, rsign = 0.0;
     int iaxis = face_axis(iR, neg, &isign);
-    double poly[16 * 3], buf[16 * 3];
+    // two polygon buffers used in turn (each clip reads one and writes the
+    // other); the contact points then go into the one not holding the polygon
+    double bufs[2][16 * 3];
+    int cur_b = 0;
     int np_ = 4;
-    face_vertices(ic, iR, ih, iaxis, isign, poly);
+    face_vertices(ic, iR, ih, iaxis, isign, bufs[0]);
     int raxis = face_axis(rR, ref_n, &rsign);
     double refv[12];
     face_vertices(rc, rR, rh, raxis, rsign, refv);
@@ -197,6 +200,8 @@ __device__ inline int clip_faces(const double *ca, const double *Ra, const doubl
             double s = si == 0 ? 1.0 : -1.0;
             double pn0 = rR[other] * s, pn1 = rR[3 + other] * s, pn2 = rR[6 + other] * s;
             double offset = (rc[0] * pn0 + rc[1] * pn1 + rc[2] * pn2) + rh[other];
+            const double *poly = bufs[cur_b];
+            double *buf = bufs[cur_b ^ 1];
             int nb = 0;
             for (int i = 0; i < np_; i++) {
                 const double *cur = &poly[i * 3];
@@ -214,11 +219,12 @@ __device__ inline int clip_faces(const double *ca, const double *Ra, const doubl
                 }
             }
             np_ = nb;
-            for (int i = 0; i < nb * 3; i++) poly[i] = buf[i];
+            cur_b ^= 1;
             if (np_ == 0) break;
         }
     }
-    double allp[16 * 3], alld[16];
+    const double *poly = bufs[cur_b];
+    double *allp = bufs[cur_b ^ 1], alld[16];
     int nc = 0;
     for (int i = 0; i < np_; i++) {
         const double *p = &poly[i * 3];
@@ -239,15 +245,22 @@ __device__ inline int clip_faces(const double *ca, const double *Ra, const doubl
 
 // the separating-axis part of box_box: false when separated, else the
 // contact normal (A -> B) and the minimum overlap
-__device__ inline bool box_box_sat(const double *ca, const double *Ra, const double *ha,
-                                   const double *cb, const double *Rb, const double *hb,
-                                   double *normal, double &depth) {
+// the best axis so far of the separating-axis test: the smallest overlap and
+// its axis, signed to point from A to B
+struct SatBest {
+    double depth, x, y, z;
+};
+__device__ __forceinline__ void sat_begin(SatBest &b) { b.depth = 1e300; b.x = 0.0; b.y = 0.0; b.z = 0.0; }
+
+// Axes k_lo .. k_hi - 1 of the 15 in the reference's order: A's columns, B's
+// columns, then the normalised edge crosses A_i x B_j, skipped when
+// |c|^2 <= EPS^2. False at the first separating axis; else b keeps the
+// first axis of smallest overlap (strict <). Running 0..6 and then 6..15
+// with the same b is the 15-axis loop.
+__device__ inline bool sat_axes(int k_lo, int k_hi, const double *ca, const double *Ra, const double *ha,
+                                const double *cb, const double *Rb, const double *hb, SatBest &b) {
     const double d0 = cb[0] - ca[0], d1 = cb[1] - ca[1], d2 = cb[2] - ca[2];
-    double best_depth = 1e300, bx = 0.0, by = 0.0, bz = 0.0;
-    normal[0] = normal[1] = normal[2] = 0.0;
-    // axes in the reference's order: A's columns, B's columns, then the
-    // normalised edge crosses A_i x B_j skipped when |c|^2 <= EPS^2
-    for (int k = 0; k < 15; k++) {
+    for (int k = k_lo; k < k_hi; k++) {
         double a0, a1, a2;
         if (k < 3) { a0 = Ra[k]; a1 = Ra[3 + k]; a2 = Ra[6 + k]; }
         else if (k < 6) { a0 = Rb[k - 3]; a1 = Rb[k]; a2 = Rb[k + 3]; }
@@ -270,14 +283,24 @@ __device__ inline bool box_box_sat(const double *ca, const double *Ra, const dou
         double proj = a0 * d0 + a1 * d1 + a2 * d2;
         double overlap = ra + rb - fabs(proj);
         if (overlap < 0.0) return false;
-        if (overlap < best_depth) {
-            best_depth = overlap;
-            if (proj >= 0.0) { bx = a0; by = a1; bz = a2; }
-            else { bx = -a0; by = -a1; bz = -a2; }
+        if (overlap < b.depth) {
+            b.depth = overlap;
+            if (proj >= 0.0) { b.x = a0; b.y = a1; b.z = a2; }
+            else { b.x = -a0; b.y = -a1; b.z = -a2; }
         }
     }
-    normal[0] = bx; normal[1] = by; normal[2] = bz;
-    depth = best_depth;
+    return true;
+}
+
+__device__ inline bool box_box_sat(const double *ca, const double *Ra, const double *ha,
+                                   const double *cb, const double *Rb, const double *hb,
+                                   double *normal, double &depth) {
+    SatBest b;
+    sat_begin(b);
+    normal[0] = normal[1] = normal[2] = 0.0;
+    if (!sat_axes(0, 15, ca, Ra, ha, cb, Rb, hb, b)) return false;
+    normal[0] = b.x; normal[1] = b.y; normal[2] = b.z;
+    depth = b.depth;
     return true;
 }
 

@@ -544,11 +544,14 @@ __global__ void k_narrow(Arena A) {
                 quat_to_matrix(&A.q[a * 4], Ra);
                 quat_to_matrix(&A.q[b * 4], Rb);
                 if (ka == 2 && kb == 2) {
-                    // separating axes here; the touching pairs (about a third)
-                    // clip their faces in k_clip, away from the separated ones
-                    double depth;
-                    if (box_box_sat(pa, Ra, ha, pb, Rb, hb, nrm, depth)) {
-                        s[0] = nrm[0]; s[1] = nrm[1]; s[2] = nrm[2]; s[3] = depth;
+                    // the six face axes here (they separate most candidate
+                    // pairs); the pairs they leave carry their best axis so
+                    // far to k_edge_clip, which runs the nine edge axes and
+                    // clips the touching ones, in warps of survivors only
+                    SatBest best;
+                    sat_begin(best);
+                    if (sat_axes(0, 6, pa, Ra, ha, pb, Rb, hb, best)) {
+                        s[0] = best.x; s[1] = best.y; s[2] = best.z; s[3] = best.depth;
                         A.clip_list[list_slot(A.clip_n)] = p;
                     }
                 } else if (ka == 1 && kb == 1) {
@@ -572,20 +575,26 @@ __global__ void k_narrow(Arena A) {
     }
 }
 
-// face clipping of the touching box-box pairs k_narrow found
-// (_collide_native.pyx:79-263), one thread per pair, into the pair's slot
-__global__ void k_clip(Arena A) {
+// the box-box pairs no face axis separated (k_narrow), one thread per pair:
+// the nine edge axes from the best face axis k_narrow left in the slot, then
+// face clipping of the touching ones (_collide_native.pyx:20-263) into the
+// pair's slot
+__global__ void k_edge_clip(Arena A) {
     if (pairs_over(A)) return;
     const int n = *A.clip_n;
     for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n; it += gridDim.x * blockDim.x) {
         const int p = A.clip_list[it];
         const int a = A.pair_a[p], b = A.pair_b[p];
         double *s = &A.slot[(size_t)p * SLOT];
-        double nrm[3] = {s[0], s[1], s[2]};
-        const double depth = s[3];
         double Ra[9], Rb[9], pts[12], dep[4];
         quat_to_matrix(&A.q[a * 4], Ra);
         quat_to_matrix(&A.q[b * 4], Rb);
+        SatBest best;
+        best.x = s[0]; best.y = s[1]; best.z = s[2]; best.depth = s[3];
+        if (!sat_axes(6, 15, &A.pos[a * 3], Ra, &A.half[a * 3], &A.pos[b * 3], Rb, &A.half[b * 3], best))
+            continue;                                   // separated: k_narrow left the count at 0
+        double nrm[3] = {best.x, best.y, best.z};
+        const double depth = best.depth;
         const int cnt = clip_faces(&A.pos[a * 3], Ra, &A.half[a * 3], &A.pos[b * 3], Rb, &A.half[b * 3], nrm, depth,
                                    pts, dep);
         if (cnt) {

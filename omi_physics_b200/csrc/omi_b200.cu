@@ -354,7 +354,7 @@ void stage_narrow(OmiCtx *ctx, Prof *pf) {
     }
     const int nb = ctx->tune.narrow_block, gw = ctx->tune.gjk_warps;
     k_narrow<<<grid_for(A.pair_cap, nb, SM_CAP), nb, 0, ctx->stream>>>(A);
-    k_clip<<<grid_for(A.pair_cap, nb, SM_CAP), nb, 0, ctx->stream>>>(A);
+    k_edge_clip<<<grid_for(A.pair_cap, nb, SM_CAP), nb, 0, ctx->stream>>>(A);
     ctx->launches += 2;
     mark(ctx, pf, KN_NARROW);
     k_gjk<<<ctx->sm_count * (16 / gw), 32 * gw, gw * sizeof(EpaWork), ctx->stream>>>(A);

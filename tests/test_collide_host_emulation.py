@@ -3,7 +3,7 @@ oracle and the reference's compiled primitives.
 
 ``tests/emulation/collide_host.cpp`` includes
 ``omi_physics_b200/csrc/geometry.cuh`` (the functions ``k_narrow`` and
-``k_clip`` run per pair) and answers seeded box-box, sphere-sphere and
+``k_edge_clip`` run per pair) and answers seeded box-box, sphere-sphere and
 sphere-box pairs and quaternions: random poses plus the degenerate families
 the step meets (aligned faces, coincident centres, exact zero-depth face
 contact, quarter turns, near-parallel edges whose cross products the
