@@ -3,7 +3,7 @@ oracle and the reference's compiled primitives.
 
 ``tests/emulation/collide_host.cpp`` includes
 ``omi_physics_b200/csrc/geometry.cuh`` (the functions ``k_narrow`` and
-``k_edge_clip`` run per pair) and answers seeded box-box, sphere-sphere and
+``k_edge_clip`` run per pair, and the face-axes-then-edge-axes split those two kernels make of the box-box test) and answers seeded box-box, sphere-sphere and
 sphere-box pairs and quaternions: random poses plus the degenerate families
 the step meets (aligned faces, coincident centres, exact zero-depth face
 contact, quarter turns, near-parallel edges whose cross products the
@@ -45,6 +45,8 @@ def emu(tmp_path_factory):
     lib = C.CDLL(out)
     lib.emu_box_box.argtypes = [D] * 9
     lib.emu_box_box.restype = C.c_int
+    lib.emu_box_box_split.argtypes = [D] * 9
+    lib.emu_box_box_split.restype = C.c_int
     lib.emu_sphere_sphere.argtypes = [D, C.c_double, D, C.c_double, D, D, D]
     lib.emu_sphere_sphere.restype = C.c_int
     lib.emu_sphere_box.argtypes = [D, C.c_double, D, D, D, D, D, D]
@@ -139,12 +141,13 @@ def test_box_box(emu):
         Rb = _mat(ol.or_quat_to_matrix, qb)
         cb = ca + d
         g = _box_pair(emu.emu_box_box, ca, Ra, ha, cb, Rb, hb)
+        s = _box_pair(emu.emu_box_box_split, ca, Ra, ha, cb, Rb, hb)   # the step's two-kernel form
         o = _box_pair(ol.or_box_box, ca, Ra, ha, cb, Rb, hb)
-        assert g[0] == o[0], (ca, qa, ha, cb, qb, hb)
+        assert g[0] == o[0] and s[0] == o[0], (ca, qa, ha, cb, qb, hb)
         if o[0]:
             hits += 1
-            for x, y in zip(g[1:], o[1:]):
-                assert np.array_equal(x, y), (ca, qa, ha, cb, qb, hb)
+            for x, y, z in zip(g[1:], s[1:], o[1:]):
+                assert np.array_equal(x, z) and np.array_equal(y, z), (ca, qa, ha, cb, qb, hb)
         if native is not None:
             n, nrm, pts, dep = native.box_box(ca, Ra.reshape(3, 3), ha, cb, Rb.reshape(3, 3), hb)
             assert n == o[0], (ca, qa, ha, cb, qb, hb)
