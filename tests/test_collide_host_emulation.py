@@ -3,8 +3,9 @@ oracle and the reference's compiled primitives.
 
 ``tests/emulation/collide_host.cpp`` includes
 ``omi_physics_b200/csrc/geometry.cuh`` (the functions ``k_narrow`` and
-``k_edge_clip`` run per pair, and the face-axes-then-edge-axes split those two kernels make of the box-box test) and answers seeded box-box, sphere-sphere and
-sphere-box pairs and quaternions: random poses plus the degenerate families
+``k_edge_clip`` run per pair, and the split of the box-box test between
+those two kernels: face axes, then edge axes) and answers seeded box-box,
+sphere-sphere and sphere-box pairs and quaternions: random poses plus the degenerate families
 the step meets (aligned faces, coincident centres, exact zero-depth face
 contact, quarter turns, near-parallel edges whose cross products the
 separating-axis test skips, a sphere centre inside a box). Every answer
