@@ -31,6 +31,8 @@ extern "C" {
 #define OMI_E_LIMIT (-7)        /* the step completed, but some convex pairs outgrew the bounded EPA
                                    polytope and their contacts were dropped (the reference's EPA,
                                    gjk.py:120-217, keeps an unbounded face list) */
+#define OMI_E_BOUNDS (-8)       /* bounds-checked build only: a device index check failed; the access
+                                   was skipped and the step's results are not valid */
 
 /* Shape types, combine modes, joint types: same meaning as the reference's
  * model.Shape.type, model.combine modes (model.py:231-243) and joints.py. */
@@ -161,6 +163,23 @@ int64_t omi_device_bytes(OmiCtx *ctx);
  * every world (-1 = none), so a test can make a wait run out. 0 restores a
  * default. Applies to the next step (the step graph is re-captured). */
 int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t stall_run);
+/* 1 in the bounds-checked debug build of this library (_omi_b200_checked.so,
+ * compiled with -DOMI_BOUNDS_CHECK), else 0. No counterpart in the reference
+ * (its Cython accelerators are compiled with boundscheck=False). The checked
+ * build tests the indices the step's kernels take from data (pair and contact
+ * bodies, shapes and hull point ranges, filter rows, solver-row bodies,
+ * sweep successors, joint bodies) before using them; a failed check skips
+ * the access, is counted on the device, and omi_step / omi_sync return
+ * OMI_E_BOUNDS naming the first one. Nothing traps. The shipped build
+ * compiles the checks out. */
+int omi_bounds_checked(void);
+/* Test hook of the bounds-checked build: from the next step on, the
+ * narrowphase checks candidate pair `pair` (its index in omi_get_pairs'
+ * list) as if its first body index were past the arena, so the check fails
+ * and the step returns OMI_E_BOUNDS; -1 turns it off. One setting per
+ * device, shared by every context on it. The shipped build returns
+ * OMI_E_UNSUPPORTED. No counterpart in the reference. */
+int omi_bounds_probe(OmiCtx *ctx, int32_t pair);
 /* Launch configuration of the step's kernels (no counterpart in the
  * reference): results do not depend on it, only speed, so an autotuner may
  * pick it per GPU and workload. sweep_warps = warps per contact-sweep block

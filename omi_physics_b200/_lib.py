@@ -9,15 +9,20 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, '_omi_b200.so')
+#: the shipped library, and its bounds-checked debug build (device index
+#: checks that report OMI_E_BOUNDS instead of reading out of range), which
+#: ``OMI_B200_CHECKED=1`` in the environment selects for the whole process
+LIB_PATH_SHIPPED = os.path.join(HERE, '_omi_b200.so')
+LIB_PATH_CHECKED = os.path.join(HERE, '_omi_b200_checked.so')
+LIB_PATH = LIB_PATH_CHECKED if os.environ.get('OMI_B200_CHECKED', '') not in ('', '0') else LIB_PATH_SHIPPED
 
 D = C.POINTER(C.c_double)
 I = C.POINTER(C.c_int32)
 I64 = C.POINTER(C.c_int64)
 U8 = C.POINTER(C.c_uint8)
 
-OMI_E_CUDA, OMI_E_ARG, OMI_E_UNSUPPORTED, OMI_E_STATE, OMI_E_TIMEOUT, OMI_E_OOM, OMI_E_LIMIT = (
-    -1, -2, -3, -4, -5, -6, -7)
+OMI_E_CUDA, OMI_E_ARG, OMI_E_UNSUPPORTED, OMI_E_STATE, OMI_E_TIMEOUT, OMI_E_OOM, OMI_E_LIMIT, OMI_E_BOUNDS = (
+    -1, -2, -3, -4, -5, -6, -7, -8)
 WF_SLEEP, WF_WARM, WF_COLLISION, WF_ACTIVE = 1, 2, 4, 8
 
 
@@ -45,6 +50,11 @@ class SweepTimeout(OmiError):
 class EpaLimit(OmiError):
     """The step completed, but some convex pairs outgrew the bounded EPA
     polytope and their contacts were dropped (the reference's EPA is unbounded)."""
+
+
+class BoundsError(OmiError):
+    """Bounds-checked build only: a device index check failed (the access was
+    skipped, the step's results are not valid); the message names the first."""
 
 
 class OmiScene(C.Structure):
@@ -110,6 +120,8 @@ PROTOTYPES = {
     'omi_set_budget': (C.c_int, [C.c_void_p, C.c_int64]),
     'omi_device_bytes': (C.c_int64, [C.c_void_p]),
     'omi_set_limits': (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    'omi_bounds_checked': (C.c_int, []),
+    'omi_bounds_probe': (C.c_int, [C.c_void_p, C.c_int32]),
     'omi_validate_scene': (C.c_int, [C.POINTER(OmiScene), C.c_char_p, C.c_int32]),
     'omi_set_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
     'omi_get_tuning': (C.c_int, [C.c_void_p, C.POINTER(OmiTuning)]),
@@ -170,8 +182,8 @@ def load_library():
     global _LIB
     if _LIB is None:
         if not os.path.exists(LIB_PATH):
-            raise OmiError(OMI_E_STATE, 'CUDA library %s is not built; run '
-                           '`python -m omi_physics_b200.build`' % LIB_PATH)
+            raise OmiError(OMI_E_STATE, 'CUDA library %s is not built; run `python -m omi_physics_b200.build%s`'
+                           % (LIB_PATH, ' --checked' if LIB_PATH == LIB_PATH_CHECKED else ''))
         lib = C.CDLL(LIB_PATH)
         for name, (res, args) in PROTOTYPES.items():
             fn = getattr(lib, name)
@@ -227,7 +239,7 @@ class Context:
         if rc < 0:
             msg = self.lib.omi_last_error(self.h).decode() or what
             cls = {OMI_E_UNSUPPORTED: UnsupportedFeature, OMI_E_OOM: OutOfBudget, OMI_E_TIMEOUT: SweepTimeout,
-                   OMI_E_LIMIT: EpaLimit}.get(rc, OmiError)
+                   OMI_E_LIMIT: EpaLimit, OMI_E_BOUNDS: BoundsError}.get(rc, OmiError)
             raise cls(rc, '%s: %s' % (what, msg) if what else msg)
         return rc
 

@@ -32,8 +32,48 @@ enum {
     ST_GJK_ITEMS = 5,    // convex pairs routed to GJK/EPA in the last step
     ST_CONTACTS_NEEDED = 6,
     ST_SWEEP_TIMEOUT = 7, // a sweep wait ran out (never expected; the step is reported failed)
-    ST_WORDS = 8
+    ST_BOUNDS = 8,       // bounds-checked build: failed index checks (the accesses were skipped)
+    ST_BOUNDS_SITE = 9,  // the first failed check: its site (BoundsSite)
+    ST_BOUNDS_INDEX = 10, // ... and the index it refused
+    ST_WORDS = 11
 };
+
+// Sites of the bounds-checked build's index checks (-DOMI_BOUNDS_CHECK,
+// `_omi_b200_checked.so`): indices a kernel takes from data rather than from
+// its own loop bounds, before the access they guard.
+enum BoundsSite {
+    BS_PAIR_BODY = 1,     // a candidate pair's body (narrowphase)
+    BS_SHAPE = 2,         // a body's shape, and a hull's point range (GJK/EPA proxies)
+    BS_CONTACT_BODY = 3,  // a contact's body (solver prep)
+    BS_SWEEP_BODY = 4,    // a solver row's body, outside its world's staged rows (contact sweep)
+    BS_SWEEP_RUN = 5,     // a successor run of a sweep entry (contact sweep)
+    BS_JOINT_BODY = 6,    // a joint's body (joints)
+    BS_ISLAND_BODY = 7,   // a contact body outside its world (islands and sleep)
+    BS_FILTER_ROW = 8,    // a filter-matrix row (broadphase windows)
+};
+
+// In the bounds-checked build, OMI_BOUNDS(A, i, n, site, on_fail) checks
+// 0 <= i < n; a failed check counts itself in ST_BOUNDS (the first one also
+// records its site and index) and runs on_fail - a `continue`, `return` or
+// assignment that skips the guarded access. It never traps: the host reports
+// the step as failed (OMI_E_BOUNDS). In the shipped build the macro expands to
+// nothing, so its device code is exactly the unchecked code.
+#ifdef OMI_BOUNDS_CHECK
+#define OMI_BOUNDS(A, i, n, site, on_fail) \
+    if (!::omi::bounds_ok((A).status, (long long)(i), (long long)(n), (site))) { on_fail; }
+#else
+#define OMI_BOUNDS(A, i, n, site, on_fail)
+#endif
+#ifdef __CUDACC__
+__device__ __forceinline__ bool bounds_ok(int *status, long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    if (atomicAdd(&status[ST_BOUNDS], 1) == 0) {
+        status[ST_BOUNDS_SITE] = site;
+        status[ST_BOUNDS_INDEX] = (int)i;
+    }
+    return false;
+}
+#endif
 
 // default bounds of the device's waits and of the EPA polytope; a context may
 // lower them (omi_set_limits) so that a test can make them run out

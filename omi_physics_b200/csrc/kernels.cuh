@@ -271,6 +271,8 @@ __device__ __forceinline__ bool row_keep(const Arena &A, int w, const double4 &a
     keep &= ((ia & 3) == 2) | ((ib & 3) == 2);
     if (keep) {
         const int rows = A.w_filter_rows[w];
+        OMI_BOUNDS(A, ia >> 5, rows, BS_FILTER_ROW, return false)
+        OMI_BOUNDS(A, ib >> 5, rows, BS_FILTER_ROW, return false)
         keep = A.filter_matrix[A.w_filter_off[w] + (ia >> 5) * rows + (ib >> 5)] != 0;
     }
     return keep;
@@ -511,6 +513,17 @@ __global__ void k_integrate_forces(Arena A, int gated) {
     }
 }
 
+#ifdef OMI_BOUNDS_CHECK
+// Test hook of the bounds-checked build (omi_bounds_probe): the narrowphase
+// checks candidate pair g_bounds_probe as if its first body index were past
+// the arena, so a test can make a check fail without corrupting anything.
+// -1 (the default) is off. One variable per device, for every context there.
+__device__ int g_bounds_probe = -1;
+__device__ __forceinline__ int bounds_probe(int p, int a, int nb) {
+    return p == *(volatile int *)&g_bounds_probe ? nb : a;
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // narrowphase (narrowphase.py:78-100): one thread per solid pair for the
 // analytic routes; convex pairs are queued for the GJK/EPA kernel. Results go
@@ -526,6 +539,8 @@ __global__ void k_narrow(Arena A) {
             A.trig_list[list_slot(A.trig_n)] = p;     // overlap tested after the solve
         } else if (kindp == 1) {
             const int a = A.pair_a[p], b = A.pair_b[p];
+            OMI_BOUNDS(A, bounds_probe(p, a, A.NB), A.NB, BS_PAIR_BODY, A.slot_cnt[p] = 0; continue)
+            OMI_BOUNDS(A, b, A.NB, BS_PAIR_BODY, A.slot_cnt[p] = 0; continue)
             const int ka = A.kind[a], kb = A.kind[b];
             double *s = &A.slot[(size_t)p * SLOT];
             if (ka == 5 || kb == 5) {
@@ -610,6 +625,20 @@ __global__ void k_edge_clip(Arena A) {
 
 // make_proxy (body.py:214-237) of shape s at body i's pose
 __device__ inline void make_proxy_shape(const Arena &A, int s, int i, Proxy &P) {
+#ifdef OMI_BOUNDS_CHECK
+    // a shape or hull point range outside the tables: a point proxy at the
+    // body's centre (no table read; the step is reported as failed)
+    if (!bounds_ok(A.status, s, A.NS, BS_SHAPE) ||
+        (A.pt_cnt[s] > 0 && !bounds_ok(A.status, (long long)A.pt_off[s] + A.pt_cnt[s] - 1, A.NPTS, BS_SHAPE))) {
+        P.kind = 1;
+        quat_to_matrix(&A.q[i * 4], P.R);
+        for (int c = 0; c < 3; c++) { P.c[c] = A.pos[i * 3 + c]; P.h[c] = 0.0; }
+        P.r = 0.0;
+        P.local = A.points;
+        P.m = 0;
+        return;
+    }
+#endif
     P.kind = A.shape_type[s];
     quat_to_matrix(&A.q[i * 4], P.R);
     for (int c = 0; c < 3; c++) P.c[c] = A.pos[i * 3 + c];
@@ -1330,7 +1359,11 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prep(Arena A) {
     for (int base = blockIdx.x * PREP_THREADS; base < Ktot; base += gridDim.x * PREP_THREADS) {
         const int k = base + threadIdx.x;
         bool ok = false;
-        if (k < Ktot) {
+        if (k < Ktot
+#ifdef OMI_BOUNDS_CHECK
+            && (bounds_ok(A.status, A.c_a[k], A.NB, BS_CONTACT_BODY) & bounds_ok(A.status, A.c_b[k], A.NB, BS_CONTACT_BODY))
+#endif
+        ) {
             const int w = A.body_world[A.c_a[k]];
             if (world_collides(A, w)) {
                 prep_contact(A, w, k, (A.w_flags[w] & WF_WARM) != 0, cur, rows + threadIdx.x * CD);
@@ -1665,6 +1698,15 @@ __device__ __forceinline__ void load_row(const Arena &A, int k, double *row) {
     }
 }
 
+#ifdef OMI_BOUNDS_CHECK
+// both bodies of a solver row inside the world's rows [b0, b0 + nb) (the
+// sweep stages and indexes velocities by body - b0)
+__device__ __forceinline__ bool sweep_rows_ok(const Arena &A, const double *row, int b0, int nb) {
+    const int2 ab = *reinterpret_cast<const int2 *>(&row[R_AB]);
+    return bounds_ok(A.status, ab.x - b0, nb, BS_SWEEP_BODY) & bounds_ok(A.status, ab.y - b0, nb, BS_SWEEP_BODY);
+}
+#endif
+
 // One pass over one run (all its contacts, in order) by one thread; row0 is
 // the first contact's row, the next contact's part is loaded while the
 // current one is solved.
@@ -1930,6 +1972,9 @@ __device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_
                 // codes for the finish slot and the successors, loaded during the solve
                 const int ca = __ldg(run_pa + r), cb = __ldg(run_pb + r);
                 const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+#ifdef OMI_BOUNDS_CHECK
+                if (sweep_rows_ok(A, row0, b0, nb))
+#endif
                 run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
                 // finish slot (critical-path diagnostics), off the solve's path
                 int t0 = 0;
@@ -1947,6 +1992,7 @@ __device__ __forceinline__ void sweep_world(const Arena &A, int w, double *smem_
                     if (sc >= 0) { ps = p; rs = sc; }
                     else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
                     else continue;
+                    OMI_BOUNDS(A, rs, R, BS_SWEEP_RUN, continue)
                     if (atomicAdd(&arrived[rs], 1) + 1 == need_of(needpk[rs], ps)) {
                         fence_acq_rel_cta();             // acquire the other arrivals' writes
                         sweep_push(ring, sh, (ps << PASS_SHIFT) | rs, kn[rs] >> 24, abort);

@@ -486,6 +486,17 @@ __global__ void __launch_bounds__(32, 1) k_joints(Arena A, int gated, int smem_d
         if (!A.w_active[w]) continue;
         const int j0 = A.w_joint_off[w], J = A.w_joint_n[w], j1 = j0 + J;
         if (J == 0) continue;
+#ifdef OMI_BOUNDS_CHECK
+        {   // every joint body inside the world's rows, else the world's joints are skipped
+            const int b0 = A.w_body_off[w], nb = A.w_body_n[w];
+            bool bad = false;
+            for (int j = j0 + lane; j < j1; j += 32) {
+                if (A.j_a[j] >= 0 && !bounds_ok(A.status, A.j_a[j] - b0, nb, BS_JOINT_BODY)) bad = true;
+                if (A.j_b[j] >= 0 && !bounds_ok(A.status, A.j_b[j] - b0, nb, BS_JOINT_BODY)) bad = true;
+            }
+            if (__any_sync(FULL, bad)) continue;
+        }
+#endif
         const double dt = A.w_dt[w];
         const int iters = A.w_jiters[w];
         const bool waves = iters <= JOINT_WAVE_ITERS;   // the schedule buffers hold that many iterations
@@ -680,6 +691,8 @@ __global__ void k_finalize(Arena A, int mode, int cap) {
             world_contacts(A, w, c0, c1);
             for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
                 const int a = A.c_a[k], b = A.c_b[k];
+                OMI_BOUNDS(A, a - b0, nb, BS_ISLAND_BODY, continue)
+                OMI_BOUNDS(A, b - b0, nb, BS_ISLAND_BODY, continue)
                 const bool da = A.mtype[a] == 2, db = A.mtype[b] == 2;
                 if (da) atomicOr(&flag[a - b0], BF_CONTACTED);
                 if (db) atomicOr(&flag[b - b0], BF_CONTACTED);

@@ -567,6 +567,17 @@ int64_t step_launches(OmiCtx *ctx) {
 // reference's unbounded EPA would have made one)
 int status_errors(OmiCtx *ctx) {
     const int *st = ctx->h_status;
+    if (st[ST_BOUNDS]) {
+        static const char *sites[] = {"?", "narrowphase pair body", "shape or hull point range",
+                                      "contact body", "solver row body outside its world",
+                                      "sweep successor run", "joint body outside its world",
+                                      "contact body outside its world (islands)", "filter-matrix row"};
+        const int site = st[ST_BOUNDS_SITE];
+        return fail(ctx, OMI_E_BOUNDS, std::to_string(st[ST_BOUNDS]) + " device index check(s) failed, the first at " +
+                                           sites[site >= 1 && site <= 8 ? site : 0] + " (index " +
+                                           std::to_string(st[ST_BOUNDS_INDEX]) +
+                                           "); the accesses were skipped and the step's results are not valid");
+    }
     if (st[ST_SWEEP_TIMEOUT])
         return fail(ctx, OMI_E_TIMEOUT, "contact sweep wait timed out (the step did not complete; "
                                         "restore the worlds' state before stepping on)");
@@ -595,7 +606,7 @@ int run_steps(OmiCtx *ctx, int n, bool sync) {
         if (!sync) return 0;
         int rc = read_status(ctx);
         if (rc) return rc;
-        if (ctx->h_status[ST_SWEEP_TIMEOUT]) return status_errors(ctx);
+        if (ctx->h_status[ST_SWEEP_TIMEOUT] || ctx->h_status[ST_BOUNDS]) return status_errors(ctx);
         const int done = ctx->h_status[ST_STEPS_DONE];
         remaining -= done;
         if (remaining > 0) {
@@ -1478,10 +1489,32 @@ int omi_sync(OmiCtx *ctx) {
     if (!ctx) return OMI_E_ARG;
     int rc = read_status(ctx);
     if (rc) return rc;
-    if (ctx->h_status[ST_SWEEP_TIMEOUT]) return status_errors(ctx);
+    if (ctx->h_status[ST_SWEEP_TIMEOUT] || ctx->h_status[ST_BOUNDS]) return status_errors(ctx);
     if (ctx->h_status[ST_OVERFLOW])
         return fail(ctx, OMI_E_STATE, "an asynchronous step overflowed its buffers; re-run with omi_step");
     return status_errors(ctx);
+}
+
+int omi_bounds_checked(void) {
+#ifdef OMI_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int omi_bounds_probe(OmiCtx *ctx, int32_t pair) {
+    if (!ctx) return OMI_E_ARG;
+#ifdef OMI_BOUNDS_CHECK
+    if (pair < -1) return fail(ctx, OMI_E_ARG, "omi_bounds_probe: pair must be >= -1");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));     // no step of this context reads it meanwhile
+    CK(cudaMemcpyToSymbol(g_bounds_probe, &pair, sizeof(int)));
+    return 0;
+#else
+    (void)pair;
+    return fail(ctx, OMI_E_UNSUPPORTED, "omi_bounds_probe: this is not the bounds-checked build");
+#endif
 }
 
 int omi_set_limits(OmiCtx *ctx, int32_t spin_limit, int32_t epa_faces, int32_t stall_run) {

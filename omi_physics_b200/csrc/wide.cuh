@@ -465,6 +465,9 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
                     double row0[CD];
                     load_row(A, k0, row0);
                     const int sa = __ldg(run_sa + r), sb = __ldg(run_sb + r);
+#ifdef OMI_BOUNDS_CHECK
+                    if (sweep_rows_ok(A, row0, V.b0, A.w_body_n[w]))
+#endif
                     run_pass(A, V, I, row0, k0, n, vel, warm && p == 0, p == 0, slop);
                     // release this entry's writes, then count into the successors
                     fence_acq_rel_gpu();
@@ -477,6 +480,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) k_wsweep(Arena A, int wi) {
                         if (sc >= 0) { ps = p; rs = sc; }
                         else if (sc != LEVEL_NONE && p + 1 < P) { ps = p + 1; rs = -sc - 1; }
                         else continue;
+                        OMI_BOUNDS(A, rs, R, BS_SWEEP_RUN, continue)
                         if (atomicAdd(&arrived[rs], 1) + 1 == need_of(__ldg(run_need + rs), ps)) {
                             fence_acq_rel_gpu();             // acquire the other arrivals' writes
                             if (next < 0) { next = (ps << PASS_SHIFT) | rs; continue; }
