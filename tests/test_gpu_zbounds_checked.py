@@ -75,6 +75,8 @@ print('probe ok:', msg)
 
 
 def test_checked_build_is_clean_on_real_worlds_and_reports_a_failed_check():
+    from omi_physics_b200 import build
+    build.build(checked=True)                 # a no-op when it is up to date
     env = dict(os.environ, OMI_B200_CHECKED='1', PYTHONPATH=ROOT)
     env.pop('OMI_WIDE_THRESHOLD', None)
     res = subprocess.run([sys.executable, '-c', 'ROOT = %r\n' % ROOT + CHILD], env=env, cwd=ROOT,
